@@ -1,0 +1,519 @@
+"""Plain-array descriptions of one FDTD run (the "plan"), shared by the CUDA engine and the CPU oracle.
+
+A plan holds only NumPy arrays and Python scalars, so it can be built from lightsmith's own engine inputs
+(duck-typed: ``PMLSpec``, ``DispersiveGroup``, ``DFTMonitor`` and the source objects of
+``lightsmith/backends/_fdtd``), from this module's dataclasses of the same names, or loaded from an ``.npz``
+fixture, with no lightsmith installation.
+
+Layouts follow lightsmith's engine (``backends/_fdtd/engine.py:16-18``): fields stacked as F[3, N0, N1, N2]
+(C order, N2 fastest), flat index ``((c * N0 + i) * N1 + j) * N2 + k`` (``engine.py:103-105``). E_c sits at
+node + e_c/2 and H_c at node + (1 - e_c)/2 in cell units.
+"""
+
+from __future__ import annotations
+
+import io
+import json
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# --- material / boundary / monitor descriptions (same fields as lightsmith's engine dataclasses) ---------
+
+
+@dataclass(frozen=True)
+class Pole:
+    """One ADE pole P'' + gamma P' + omega0^2 P = sigma E (``media.py:25-29``)."""
+
+    sigma: float
+    omega0: float
+    gamma: float
+
+
+@dataclass(frozen=True)
+class Medium:
+    """eps_inf plus poles (``media.py:32-40``)."""
+
+    eps_inf: float
+    poles: tuple = ()
+    label: str = ""
+
+    @property
+    def dispersive(self) -> bool:
+        return bool(self.poles)
+
+
+@dataclass
+class PMLSpec:
+    """CPML thickness per axis and its grading (``engine.py:184-191``)."""
+
+    cells: tuple
+    m: float = 3.0
+    kappa_max: float = 1.0
+    alpha_max: float = 0.0
+    eps_ref: float = 1.0
+    eps_ref_high: float | None = None
+
+
+@dataclass
+class DispersiveGroup:
+    """E nodes integrated in D-form (``engine.py:129-137``): flat E indices, media, fractions (S, n) and the
+    harmonic-path weight w (None for pure cells)."""
+
+    idx: np.ndarray
+    media: list
+    frac: np.ndarray
+    w: np.ndarray | None
+
+
+@dataclass
+class DFTMonitor:
+    """Running DFT of E at e_idx and of the mean of H at h_idx1/h_idx2 (``engine.py:194-210``).
+
+    ``source`` selects whose arrays are sampled: None for the grid, else a source object (its own E/H, e.g.
+    the 1D feed line or the Bloch column) or a source's incident-reference view."""
+
+    omega: np.ndarray
+    e_idx: np.ndarray
+    h_idx1: np.ndarray | None = None
+    h_idx2: np.ndarray | None = None
+    energy: int = 0
+    source: object | None = None
+    acc_e: object = field(default=None, repr=False)
+    acc_h: object = field(default=None, repr=False)
+
+    def results(self):
+        def host(a):
+            if a is None:
+                return None
+            if hasattr(a, "detach"):
+                a = a.detach().cpu().numpy()
+            return np.asarray(a).astype(complex)
+        return host(self.acc_e), host(self.acc_h)
+
+
+# --- region helpers ----------------------------------------------------------------------------------
+
+
+def e_range(c: int, a: int, n: int, periodic: bool) -> tuple[int, int]:
+    """Stepped index range [lo, hi) of E_c along axis a (``engine.py:47-60``, no mirror planes): tangential E
+    stays 0 on the outer (PEC) planes; periodic axes step the real cells 1..n-2 between two ghost planes."""
+    if periodic or a != c:
+        return 1, n - 1
+    return 0, n - 1
+
+
+def h_range(c: int, a: int, n: int, periodic: bool) -> tuple[int, int]:
+    """Stepped index range of H_c along axis a (``engine.py:63-66``, no mirror planes)."""
+    if periodic:
+        return 1, n - 1
+    return (0, n) if a == c else (0, n - 1)
+
+
+def flat_index(c, i, j, k, shape):
+    n0, n1, n2 = shape
+    return ((np.asarray(c) * n0 + np.asarray(i)) * n1 + np.asarray(j)) * n2 + np.asarray(k)
+
+
+def pole_coefficients(pole, dt: float) -> tuple[float, float, float]:
+    """Central-difference ADE coefficients (c1, c2, c3) of P^{n+1} = c1 P^n + c2 P^{n-1} + c3 E^n
+    (``engine.py:108-111``)."""
+    half = pole.gamma * dt / 2
+    den = 1 + half
+    return (2 - pole.omega0 ** 2 * dt ** 2) / den, -(1 - half) / den, pole.sigma * dt ** 2 / den
+
+
+# --- CPML terms --------------------------------------------------------------------------------------
+
+
+def cpml_profiles(pml, shape, spacing, dt):
+    """Per axis d with a CPML: (lo_n, hi_n, {"E": (b, c, kappa), "H": (b, c, kappa)}) with 1D profiles over the
+    axis' node positions u (E) and half-integer positions u + 1/2 (H), as graded in ``engine.py:355-371``:
+    sigma = sigma_max rho^m, sigma_max = 0.8 (m + 1) / (sqrt(eps_ref) dx) (the high side may use its own eps),
+    kappa = 1 + (kappa_max - 1) rho^m, alpha = alpha_max (1 - rho) inside the layer, b = exp(-(sigma/kappa +
+    alpha) dt), c = sigma (b - 1) / (sigma kappa + kappa^2 alpha)."""
+    out = {}
+    for d in range(3):
+        lo_n, hi_n = (int(v) for v in pml.cells[d])
+        if not (lo_n or hi_n):
+            continue
+        N = shape[d]
+        dx = spacing[d]
+        s_lo = 0.8 * (pml.m + 1) / (np.sqrt(pml.eps_ref) * dx)
+        s_hi = 0.8 * (pml.m + 1) / (np.sqrt(pml.eps_ref_high or pml.eps_ref) * dx)
+        prof = {}
+        for kind, half in (("E", 0.0), ("H", 0.5)):
+            u = np.arange(N, dtype=float) + half
+            r_lo = np.clip((lo_n - u) / lo_n, 0, 1) if lo_n else np.zeros_like(u)
+            r_hi = np.clip((u - (N - 1 - hi_n)) / hi_n, 0, 1) if hi_n else np.zeros_like(u)
+            rho = np.maximum(r_lo, r_hi)
+            sig = np.where(r_lo >= r_hi, s_lo, s_hi) * rho ** pml.m
+            kap = 1 + (pml.kappa_max - 1) * rho ** pml.m
+            alp = pml.alpha_max * (1 - rho) * (rho > 0)
+            b = np.exp(-(sig / kap + alp) * dt)
+            den = sig * kap + kap ** 2 * alp
+            c = np.where(sig > 0, sig * (b - 1) / np.where(den > 0, den, 1), 0.0)
+            prof[kind] = (b, c, kap)
+        out[d] = (lo_n, hi_n, prof)
+    return out
+
+
+def cpml_terms(pml, shape, periodic):
+    """The CPML correction terms in lightsmith's order (``engine.py:373-418``): per axis d, per field (E then
+    H), per component c != d, per side (low, high) a slab of c's stepped region restricted along d.
+
+    Returns dicts {field, c, d, src, sgn, lo, hi, region}: ``src`` is the differentiated component, ``sgn`` the
+    curl sign of the term, ``region`` the slab as three (start, stop) pairs."""
+    terms = []
+    for d in range(3):
+        lo_n, hi_n = (int(v) for v in pml.cells[d])
+        if not (lo_n or hi_n):
+            continue
+        if periodic[d]:
+            raise ValueError("a periodic axis cannot have a PML")
+        N = shape[d]
+        for fld in ("E", "H"):
+            for c in range(3):
+                if c == d:
+                    continue
+                d1, d2 = (c + 1) % 3, (c + 2) % 3
+                src, sgn = (d2, 1.0) if d == d1 else (d1, -1.0)
+                if fld == "H":
+                    sgn = -sgn
+                rng = e_range if fld == "E" else h_range
+                R = [rng(c, a, shape[a], periodic[a]) for a in range(3)]
+                start, stop = R[d]
+                sides = []
+                if lo_n:
+                    sides.append((start, min(stop, lo_n + 1)))
+                if hi_n:
+                    sides.append((max(start, N - 2 - hi_n), stop))
+                for a, b in sides:
+                    if b <= a:
+                        continue
+                    reg = list(R)
+                    reg[d] = (a, b)
+                    terms.append({"field": fld, "c": c, "d": d, "src": src, "sgn": sgn, "region": tuple(reg)})
+    return terms
+
+
+# --- sources -----------------------------------------------------------------------------------------
+
+
+@dataclass
+class TablePoints:
+    """Correction points of a table-fed TF/SF box for one kind ("E": E nodes fed by H_inc, "H": the
+    reverse), in application order: target flat node, first table index of its quintic stencil, integer
+    and fractional fine time at n = 0, and the coefficient."""
+
+    node: np.ndarray
+    base: np.ndarray
+    i0: np.ndarray
+    u0: np.ndarray
+    coef: np.ndarray
+
+
+@dataclass
+class TableSource:
+    """TF/SF plane wave fed from time tables of the exact discrete background (``layered.py:254-482``)."""
+
+    tables: np.ndarray  # flat (rows * L,)
+    inc_table: np.ndarray  # flat (3 * L,)
+    m: int
+    cmax: int
+    E: TablePoints | None
+    H: TablePoints | None
+    inc: tuple  # (base[3], i0[3], u0[3]) of the incident-reference view
+    view: object = None  # the object DFTMonitor(source=...) names for the incident view
+
+
+@dataclass
+class DipoleSource:
+    """Point current spread over the E nodes around it (``emission.py:97-142``): E[idx] -= coef * wave[n]."""
+
+    idx: np.ndarray
+    coef: np.ndarray
+    wave: np.ndarray
+
+
+@dataclass
+class LinePoints:
+    """1D-feed corrections of one kind: target flat node, 1D index i0, interpolation weight w (0 when the
+    slab has none), coefficient; in application order (``tfsf.py:184-193``)."""
+
+    node: np.ndarray
+    i0: np.ndarray
+    w: np.ndarray
+    coef: np.ndarray
+
+
+@dataclass
+class LineSource:
+    """TF/SF fed by a 1D auxiliary Yee line with graded absorbers (``tfsf.py:108-211``)."""
+
+    M: int
+    m_src: int
+    ca: np.ndarray
+    cb: np.ndarray
+    da: np.ndarray
+    db: np.ndarray
+    wave: np.ndarray
+    E: LinePoints | None
+    H: LinePoints | None
+    owner: object = None  # the object DFTMonitor(source=...) names for the line's own arrays
+
+
+@dataclass
+class ColumnSource:
+    """One-sided TF/SF plane of a Bloch-periodic cell fed by a 3 x 3 x nz column engine with the same Bloch
+    phases (``tfsf.py:214-296``)."""
+
+    column: dict  # the column's own plan
+    k_src: int
+    k_launch: int
+    phase: np.ndarray  # (nx, ny) complex
+    amp: tuple  # two complex sheet amplitudes (E_x, E_y)
+    wave: np.ndarray
+    cE: float
+    cH: float
+    owner: object = None
+
+
+@dataclass
+class ModeSource:
+    """Rank-r mode source on a port plane (``ports.py:294-378``): H[h] += mH @ tE[n], E[e] += mE @ tH[n]."""
+
+    h_idx: np.ndarray
+    mH: np.ndarray
+    tab_E: np.ndarray
+    e_idx: np.ndarray
+    mE: np.ndarray
+    tab_H: np.ndarray
+
+
+def _points_by_slab(slabs, shape, kind, make):
+    n_cells = int(np.prod(shape))
+    grid = np.arange(n_cells).reshape(shape)
+    rows = []
+    for s in slabs:
+        if s[0] != kind:
+            continue
+        rows.append(make(s, grid, n_cells))
+    if not rows:
+        return None
+    return rows
+
+
+def table_source_from(src, shape) -> TableSource:
+    """TableSource from a constructed ``ObliqueLayeredPlaneWave`` (before ``bind``, which drops its tables).
+
+    Its ``slabs`` are (kind, c, region, base, i0, u0, coef array, slab shape) (``layered.py:397-402``)."""
+    out = {}
+    for kind in ("E", "H"):
+        def make(s, grid, n_cells):
+            _, c, region, base, i0, u0, arr, shape_ = s
+            nodes = c * n_cells + grid[region].reshape(-1)
+            n = nodes.size
+            return (nodes, np.broadcast_to(np.asarray(base), (n,)), np.broadcast_to(np.asarray(i0), (n,)),
+                    np.broadcast_to(np.asarray(u0, dtype=float), (n,)),
+                    np.broadcast_to(np.asarray(arr, dtype=float), shape_).reshape(-1))
+        rows = _points_by_slab(src.slabs, shape, kind, make)
+        out[kind] = None if rows is None else TablePoints(*(np.concatenate([r[j] for r in rows]) for j in range(5)))
+    base, i0, u0 = src.inc
+    return TableSource(tables=np.asarray(src.tables, dtype=float).reshape(-1),
+                       inc_table=np.asarray(src.inc_table, dtype=float).reshape(-1), m=int(src.m),
+                       cmax=int(src.cmax), E=out["E"], H=out["H"],
+                       inc=(np.asarray(base, np.int64), np.asarray(i0, np.int64), np.asarray(u0, float)),
+                       view=getattr(src, "view", None))
+
+
+def line_source_from(src, shape) -> LineSource:
+    """LineSource from a constructed ``TFSFPlaneWave``: slabs (kind, c, region, coef, i0, w, shape)
+    (``tfsf.py:141-147``)."""
+    out = {}
+    for kind in ("E", "H"):
+        def make(s, grid, n_cells):
+            _, c, region, coef, i0, w, shape_ = s
+            nodes = c * n_cells + grid[region].reshape(-1)
+            n = nodes.size
+            return (nodes, np.asarray(i0, np.int64).reshape(-1),
+                    np.zeros(n) if w is None else np.asarray(w, float).reshape(-1), np.full(n, float(coef)))
+        rows = _points_by_slab(src.slabs, shape, kind, make)
+        out[kind] = None if rows is None else LinePoints(*(np.concatenate([r[j] for r in rows]) for j in range(4)))
+    return LineSource(M=int(src.M), m_src=int(src.m_src), ca=np.asarray(src.ca, float), cb=np.asarray(src.cb, float),
+                      da=np.asarray(src.da, float), db=np.asarray(src.db, float), wave=np.asarray(src.wave, float),
+                      E=out["E"], H=out["H"], owner=src)
+
+
+def column_source_from(src, single: bool) -> ColumnSource:
+    """ColumnSource from a constructed ``BlochPlaneSource`` (``tfsf.py:227-246,256-269``)."""
+    nz = src.shape[2]
+    col = make_plan(shape=(3, 3, nz), dx=src.spacing, dt=src.dt, single=single,
+                    inv_eps=np.full((3, 3, 3, nz), 1 / src.eps_b), groups=[], pml=src.pml, sources=[], monitors=[],
+                    dft_stride=1, periodic=(True, True, False), bloch=(*src.kpar, 0.0))
+    return ColumnSource(column=col, k_src=int(src.k_src), k_launch=int(src.k_launch),
+                        phase=np.asarray(src.phase, complex).reshape(src.shape[0] - 2, src.shape[1] - 2),
+                        amp=(complex(src.amp[0]), complex(src.amp[1])), wave=np.asarray(src.wave, float),
+                        cE=src.dt / (src.eps_b * src.spacing[2]), cH=src.dt / src.spacing[2], owner=src)
+
+
+def source_plan(src, shape, single: bool):
+    """Plain description of one source object; raises for kinds without a CUDA implementation."""
+    if isinstance(src, (TableSource, DipoleSource, LineSource, ColumnSource, ModeSource)):
+        return src
+    kind = type(src).__name__
+    if kind == "ObliqueLayeredPlaneWave":
+        return table_source_from(src, shape)
+    if kind == "PointDipole":
+        return DipoleSource(np.asarray(src.idx, np.int64), np.asarray(src.coef, float), np.asarray(src.wave, float))
+    if kind == "TFSFPlaneWave":
+        return line_source_from(src, shape)
+    if kind == "BlochPlaneSource":
+        return column_source_from(src, single)
+    if kind == "ModeSource":
+        return ModeSource(np.asarray(src.h_idx, np.int64), np.asarray(src.mH, float), np.asarray(src.tab_E, float),
+                          np.asarray(src.e_idx, np.int64), np.asarray(src.mE, float), np.asarray(src.tab_H, float))
+    raise NotImplementedError(f"lightsmith-b200 has no CUDA path for the source {kind}")
+
+
+# --- the plan ----------------------------------------------------------------------------------------
+
+
+def _media_plan(media):
+    return [{"eps_inf": float(m.eps_inf), "poles": [(float(p.sigma), float(p.omega0), float(p.gamma)) for p in m.poles]}
+            for m in media]
+
+
+def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors, dft_stride,
+              periodic=(False, False, False), bloch=(0.0, 0.0, 0.0), offdiag=None, time_monitors=(),
+              mirror=(0, 0, 0), widths=None) -> dict:
+    """The plan of lightsmith's ``Engine(...)`` keyword arguments (``engine.py:231-241``).
+
+    Graded grids, mirror planes and the conformal off-diagonal / vertex-tensor terms have no CUDA path here and
+    are rejected."""
+    shape = tuple(int(n) for n in shape)
+    spacing = tuple(float(v) for v in np.broadcast_to(np.asarray(dx, dtype=float), (3,)))
+    if widths is not None and any(w is not None for w in widths):
+        raise NotImplementedError("graded grids have no CUDA path in lightsmith-b200")
+    if any(int(np.sign(m)) for m in mirror):
+        raise NotImplementedError("mirror planes have no CUDA path in lightsmith-b200")
+    if offdiag is not None and len(getattr(offdiag, "comp", ())):
+        raise NotImplementedError("conformal off-diagonal terms have no CUDA path in lightsmith-b200")
+    if time_monitors:
+        raise NotImplementedError("time monitors have no CUDA path in lightsmith-b200")
+    periodic = tuple(bool(p) for p in periodic)
+    bloch = tuple(float(k) for k in bloch)
+    if any(k and not p for k, p in zip(bloch, periodic)):
+        raise ValueError("a Bloch wavevector needs a periodic axis")
+    grp = []
+    for g in groups:
+        if type(g).__name__ == "TensorMesh":
+            raise NotImplementedError("vertex-tensor (conformal metal) groups have no CUDA path in lightsmith-b200")
+        grp.append({"idx": np.asarray(g.idx, np.int64), "media": _media_plan(g.media),
+                    "frac": np.asarray(g.frac, float), "w": None if g.w is None else np.asarray(g.w, float)})
+    plan = {
+        "shape": shape, "spacing": spacing, "dt": float(dt), "single": bool(single), "periodic": periodic,
+        "bloch": bloch, "complex": any(bloch), "stride": int(dft_stride),
+        "inv_eps": np.asarray(inv_eps, dtype=float).reshape((3,) + shape),
+        "pml": {"cells": tuple(tuple(int(v) for v in c) for c in pml.cells), "m": float(pml.m),
+                "kappa_max": float(pml.kappa_max), "alpha_max": float(pml.alpha_max), "eps_ref": float(pml.eps_ref),
+                "eps_ref_high": None if pml.eps_ref_high is None else float(pml.eps_ref_high)},
+        "groups": grp,
+        "sources": [source_plan(s, shape, single) for s in sources],
+    }
+    mons = []
+    for m in monitors:
+        space = _monitor_space(m.source, sources, plan["sources"])
+        mons.append({"omega": np.asarray(m.omega, float), "e_idx": np.asarray(m.e_idx, np.int64),
+                     "h_idx1": None if m.h_idx1 is None else np.asarray(m.h_idx1, np.int64),
+                     "h_idx2": None if m.h_idx2 is None else np.asarray(m.h_idx2, np.int64),
+                     "energy": int(m.energy), "space": space})
+    plan["monitors"] = mons
+    return plan
+
+
+def _monitor_space(obj, sources, plans):
+    """("grid",) or (kind, source number): which arrays a monitor samples."""
+    if obj is None:
+        return ("grid", -1)
+    for i, (s, p) in enumerate(zip(sources, plans)):
+        if isinstance(p, TableSource) and (obj is p.view or obj is getattr(s, "view", None)):
+            return ("view", i)
+        if isinstance(p, (LineSource, ColumnSource)) and (obj is s or obj is p.owner):
+            return ("line" if isinstance(p, LineSource) else "column", i)
+    raise NotImplementedError(f"a monitor samples {type(obj).__name__}, which has no CUDA path")
+
+
+# --- (de)serialisation -------------------------------------------------------------------------------
+
+
+def _flatten(obj, prefix, arrays):
+    """JSON skeleton of obj with its arrays moved into `arrays` under path-like keys."""
+    if isinstance(obj, np.ndarray):
+        key = prefix or "root"
+        arrays[key] = obj
+        return {"__array__": key}
+    if isinstance(obj, dict):
+        return {k: _flatten(v, f"{prefix}/{k}", arrays) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return {"__seq__": type(obj).__name__, "items": [_flatten(v, f"{prefix}/{i}", arrays) for i, v in enumerate(obj)]}
+    if isinstance(obj, complex):
+        return {"__complex__": [obj.real, obj.imag]}
+    for cls in (TableSource, TablePoints, DipoleSource, LineSource, LinePoints, ColumnSource, ModeSource):
+        if isinstance(obj, cls):
+            d = {k: v for k, v in obj.__dict__.items() if k not in ("view", "owner")}
+            return {"__class__": cls.__name__, "fields": _flatten(d, prefix, arrays)}
+    if isinstance(obj, (np.integer,)):
+        return int(obj)
+    if isinstance(obj, (np.floating,)):
+        return float(obj)
+    if isinstance(obj, np.bool_):
+        return bool(obj)
+    return obj
+
+
+_CLASSES = {c.__name__: c for c in (TableSource, TablePoints, DipoleSource, LineSource, LinePoints, ColumnSource,
+                                     ModeSource)}
+
+
+def _unflatten(obj, arrays):
+    if isinstance(obj, dict):
+        if "__array__" in obj:
+            return np.asarray(arrays[obj["__array__"]])
+        if "__seq__" in obj:
+            items = [_unflatten(v, arrays) for v in obj["items"]]
+            return tuple(items) if obj["__seq__"] == "tuple" else items
+        if "__complex__" in obj:
+            return complex(*obj["__complex__"])
+        if "__class__" in obj:
+            return _CLASSES[obj["__class__"]](**_unflatten(obj["fields"], arrays))
+        return {k: _unflatten(v, arrays) for k, v in obj.items()}
+    return obj
+
+
+def dumps(tree) -> dict:
+    """A dict of arrays (for ``np.savez_compressed``) holding `tree` (plans, results, nested dicts)."""
+    arrays = {}
+    skel = _flatten(tree, "", arrays)
+    arrays["__skeleton__"] = np.frombuffer(json.dumps(skel).encode(), dtype=np.uint8)
+    return arrays
+
+
+def loads(arrays) -> dict:
+    skel = json.loads(bytes(np.asarray(arrays["__skeleton__"])).decode())
+    return _unflatten(skel, arrays)
+
+
+def save(path, tree) -> None:
+    np.savez_compressed(path, **dumps(tree))
+
+
+def load(path) -> dict:
+    with np.load(path, allow_pickle=False) as z:
+        return loads({k: z[k] for k in z.files})
+
+
+def to_bytes(tree) -> bytes:
+    buf = io.BytesIO()
+    np.savez_compressed(buf, **dumps(tree))
+    return buf.getvalue()

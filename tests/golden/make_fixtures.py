@@ -1,0 +1,345 @@
+"""Generate the golden fixtures in this directory by running lightsmith's own FDTD (v0.3.0, CPU, float64).
+
+Run here (where the lightsmith sources are available), not on the GPU host:
+
+    python tests/golden/make_fixtures.py [/path/to/lightsmith/src]
+
+Each ``engine_*.npz`` holds the plan of one small seeded ``Engine`` run (built from the same objects the
+reference engine was given, before it bound them) and the reference's fields, DFT accumulators and monitor
+energy after a number of chunks. ``solve_*.npz`` holds one ``ls.solve(sim, "fdtd", "cpu")`` run: the plan
+the reference's scattering driver built, its post-processing inputs and its cross sections.
+
+``array_api_compat`` is not installed here; ``shim/`` supplies the few names the reference uses.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+sys.path[:0] = [os.path.join(HERE, "shim"), REF_SRC, REPO]
+
+import lightsmith as ls  # noqa: E402
+from lightsmith.backends._fdtd import engine as ref_engine  # noqa: E402
+from lightsmith.backends._fdtd import scattering as ref_scattering  # noqa: E402
+from lightsmith.backends._fdtd.emission import PointDipole  # noqa: E402
+from lightsmith.backends._fdtd.layered import ObliqueLayeredPlaneWave  # noqa: E402
+from lightsmith.backends._fdtd.media import Medium, Pole  # noqa: E402
+from lightsmith.backends._fdtd.ports import ModeSource  # noqa: E402
+from lightsmith.backends._fdtd.setup import flux_points, voxelise  # noqa: E402
+from lightsmith.backends._fdtd.tfsf import BlochPlaneSource, TFSFPlaneWave  # noqa: E402
+from lightsmith.device import Device  # noqa: E402
+
+from lightsmith_b200 import plan as P  # noqa: E402
+
+CPU = Device("numpy", "cpu")
+HBARC = 197.3269804
+# the dispersive metal of the 128^3 sphere workload: eps_inf 5.9, Drude 9.0 eV / 0.07 eV, Lorentz poles
+# (1.3 @ 2.6 eV, 0.6 eV) and (1.5 @ 3.7 eV, 1.0 eV)
+METAL = Medium(5.9, (Pole((9.0 / HBARC) ** 2, 0.0, 0.07 / HBARC),
+                     Pole(1.3 * (2.6 / HBARC) ** 2, 2.6 / HBARC, 0.6 / HBARC),
+                     Pole(1.5 * (3.7 / HBARC) ** 2, 3.7 / HBARC, 1.0 / HBARC)), "metal")
+
+
+def advance_pulse(src, n_steps: int, lead: int = 12):
+    """Start a source's pulse `lead` steps before its waveform first reaches 1e-3 of its peak, so that a short
+    fixture run sees the whole pulse: the same waveform, advanced in time (tables: all start times moved
+    together, which keeps the incident field consistent)."""
+    if hasattr(src, "tables"):
+        env = np.abs(src.tables).reshape(-1, src.tables.shape[-1]).max(axis=0)
+        first = int(np.nonzero(env > 1e-3 * env.max())[0][0]) * src.m
+        i0_min = min(int(np.min(s[4])) for s in src.slabs)
+        shift = max(0, first - i0_min - lead)
+        src.slabs = [(k, c, r, b, i0 + shift, u0, a, sh) for k, c, r, b, i0, u0, a, sh in src.slabs]
+        src.inc = (src.inc[0], src.inc[1] + shift, src.inc[2])
+        return
+    w = np.asarray(src.wave)
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    shift = max(0, first - lead)
+    src.wave = np.concatenate([w[shift:], np.zeros(shift)])[:n_steps + 8]
+
+
+def run_engine_case(name: str, kw: dict, n_chunks: int, snap: int = 1):
+    for src in kw["sources"]:
+        if not isinstance(src, ModeSource):
+            advance_pulse(src, n_chunks * kw["dft_stride"])
+    plan = P.make_plan(**kw)  # before Engine() binds the sources (the table source drops its tables then)
+    eng = ref_engine.Engine(CPU, **kw)
+    snaps = {}
+    for i in range(n_chunks):
+        eng.chunk()
+        if i + 1 == snap:
+            snaps["E_snap"], snaps["H_snap"] = eng.E.copy(), eng.H.copy()
+    out = {"E": np.asarray(eng.E), "H": np.asarray(eng.H), "n": int(eng.n[0]), "energy": np.asarray(eng.energy),
+           "n_chunks": n_chunks, "snap": snap, **snaps,
+           "acc_e": [np.asarray(m.acc_e) for m in kw["monitors"]],
+           "acc_h": [np.zeros(0) if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]}
+    for src in kw["sources"]:
+        if hasattr(src, "col"):
+            out["col_E"], out["col_H"] = np.asarray(src.col.E), np.asarray(src.col.H)
+        if isinstance(src, TFSFPlaneWave):
+            out["line_E"], out["line_H"] = np.asarray(src.E_flat), np.asarray(src.H_flat)
+    P.save(os.path.join(HERE, f"engine_{name}.npz"), {"plan": plan, "out": out})
+    print(name, plan["shape"], "steps", out["n"], "max|E|", float(np.abs(out["E"]).max()))
+
+
+def plane_monitor(shape, k, omega, energy):
+    """E_x, E_y on node plane k with the H pair straddling it (the periodic driver's plane layout)."""
+    i, j = np.meshgrid(np.arange(1, shape[0] - 1), np.arange(1, shape[1] - 1), indexing="ij")
+    i, j = i.ravel(), j.ravel()
+    e = np.concatenate([P.flat_index(0, i, j, k, shape), P.flat_index(1, i, j, k, shape)])
+    h1 = np.concatenate([P.flat_index(1, i, j, k - 1, shape), P.flat_index(0, i, j, k - 1, shape)])
+    h2 = np.concatenate([P.flat_index(1, i, j, k, shape), P.flat_index(0, i, j, k, shape)])
+    return ref_engine.DFTMonitor(omega, e, h1, h2, energy=energy)
+
+
+def case_yee_cpml_dipole():
+    rng = np.random.default_rng(1)
+    shape, dx = (18, 16, 20), 5.0
+    dt = 0.99 * dx / np.sqrt(3)
+    ie = 1.0 / rng.uniform(1.0, 12.25, size=(3,) + shape)
+    pml = ref_engine.PMLSpec(cells=((4, 3), (3, 4), (4, 4)), alpha_max=0.02, eps_ref=1.7)
+    om = 2 * np.pi / np.array([300.0, 400.0, 550.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(41.3, 38.2, 52.7), pdir=(0.3, 0.5, 0.8),
+                      inv_eps=ie, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    mons = [plane_monitor(shape, 10, om, 1), plane_monitor(shape, 6, om, 2)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[dip],
+              monitors=mons, dft_stride=3)
+    run_engine_case("yee_cpml_dipole", kw, 12, snap=1)
+
+
+def case_kappa_noncubic():
+    rng = np.random.default_rng(2)
+    shape, sp = (14, 17, 15), (4.0, 5.0, 6.0)
+    dt = 0.95 / np.sqrt(sum(1 / d ** 2 for d in sp))
+    ie = np.broadcast_to(1.0 / rng.uniform(1.0, 6.0, size=shape), (3,) + shape).copy()
+    pml = ref_engine.PMLSpec(cells=((3, 4), (4, 3), (3, 3)), kappa_max=3.0, alpha_max=0.03, eps_ref=1.2,
+                             eps_ref_high=2.25)
+    om = 2 * np.pi / np.array([350.0, 500.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=4.0, dt=dt, pos=(28.0, 30.0, 31.0), pdir=(0.0, 0.0, 1.0),
+                      inv_eps=ie, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    dip_idx = dip.idx  # the dipole is spread on a 4 nm lattice: only its node list and weights matter here
+    mons = [plane_monitor(shape, 7, om, 1)]
+    kw = dict(shape=shape, dx=sp, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[dip],
+              monitors=mons, dft_stride=4)
+    assert len(dip_idx)
+    run_engine_case("kappa_noncubic", kw, 8, snap=2)
+
+
+def sphere_slot_fn(center, radius, slot=1):
+    c = np.asarray(center, float)
+
+    def fn(pts):
+        return np.where(np.sum((pts - c) ** 2, axis=-1) <= radius ** 2, slot, 0).astype(int)
+    return fn
+
+
+def case_ade_groups():
+    shape, dx = (22, 22, 22), 2.0
+    host = Medium(1.33 ** 2, (), "medium")
+    media = [host, METAL]
+    ctr = np.array([21.0, 21.3, 20.7])
+    inv_eps, groups, stats, od = voxelise(sphere_slot_fn(ctr, 9.0), media, shape, np.zeros(3), dx,
+                                          np.array([2, 2, 2]), np.array([20, 20, 20]), mode="subpixel")
+    assert od is None and any(g.w is not None for g in groups) and any(g.w is None for g in groups)
+    dt = 0.99 * dx / np.sqrt(3)
+    pml = ref_engine.PMLSpec(cells=((4, 4),) * 3, alpha_max=0.01, eps_ref=host.eps_inf)
+    om = 2 * np.pi / np.array([450.0, 550.0, 700.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(21.0, 30.5, 22.0), pdir=(1.0, 0.0, 0.0),
+                      inv_eps=inv_eps, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    lo, hi = np.array([5, 5, 5]), np.array([16, 16, 16])
+    sca = flux_points(lo, hi, shape, dx)
+    mons = [ref_engine.DFTMonitor(om, sca[0], sca[1], sca[2], energy=1), plane_monitor(shape, 11, om, 2)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=inv_eps, groups=groups, pml=pml, sources=[dip],
+              monitors=mons, dft_stride=5)
+    run_engine_case("ade_groups", kw, 16, snap=2)
+
+
+def case_tfsf_table():
+    shape, dx = (27, 25, 29), 3.0
+    host = Medium(1.33 ** 2, (), "medium")
+    glass = Medium(2.25, (), "glass")
+    media = [host, METAL, glass]
+    ctr = np.array([13, 12, 14]) * dx
+
+    def slot(pts):
+        r1 = np.sum((pts - ctr - np.array([-4.0, 0.0, 0.0])) ** 2, axis=-1) <= 7.0 ** 2
+        r2 = np.sum((pts - ctr - np.array([6.0, 1.0, 2.0])) ** 2, axis=-1) <= 5.0 ** 2
+        return np.where(r1, 1, np.where(r2, 2, 0)).astype(int)
+    inv_eps, groups, stats, od = voxelise(slot, media, shape, np.zeros(3), dx, np.array([5, 5, 5]),
+                                          np.array([22, 20, 24]), mode="staircase")
+    dt = 0.99 * dx / np.sqrt(3)
+    wl = np.linspace(420.0, 780.0, 5)
+    om = 2 * np.pi / wl
+    omega_c, omega_half = 0.5 * (om.min() + om.max()), max(0.5 * np.ptp(om), 0.15 * om.mean())
+    lo, hi = np.array([6, 6, 6]), np.array([20, 18, 22])
+    khat = np.array([0.3, -0.4, 1.0])
+    khat /= np.linalg.norm(khat)
+    ehat = np.cross(khat, [0.0, 1.0, 0.0])
+    ehat /= np.linalg.norm(ehat)
+    src = ObliqueLayeredPlaneWave(shape=shape, origin=np.zeros(3), spacing=dx, dt=dt, lo=lo, hi=hi, khat=khat,
+                                  ehat=ehat, inv_eps=inv_eps, host=host, omega_c=omega_c, omega_half=omega_half,
+                                  max_steps=400, omega_min=om.min())
+    pml = ref_engine.PMLSpec(cells=((4, 4),) * 3, alpha_max=0.02, eps_ref=host.eps_inf)
+    sca = flux_points(lo - 2, hi + 2, shape, dx)
+    tot = flux_points(lo + 2, hi - 2, shape, dx)
+    mons = [ref_engine.DFTMonitor(om, sca[0], sca[1], sca[2], energy=True),
+            ref_engine.DFTMonitor(om, tot[0], tot[1], tot[2], energy=2),
+            ref_engine.DFTMonitor(om, np.arange(3), source=src.view)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=inv_eps, groups=groups, pml=pml, sources=[src],
+              monitors=mons, dft_stride=7)
+    run_engine_case("tfsf_table", kw, 20, snap=3)
+
+
+def case_line_periodic():
+    shape, dx = (8, 7, 40), 10.0
+    sp = (12.0, 11.0, 10.0)
+    rng = np.random.default_rng(4)
+    ie = np.full((3,) + shape, 1.0)
+    ie[:, :, :, 20:26] = 1.0 / rng.uniform(2.0, 6.0, size=(3, shape[0], shape[1], 6))
+    dt = 0.95 / np.sqrt(sum(1 / d ** 2 for d in sp))
+    om = 2 * np.pi / np.array([500.0, 650.0, 800.0])
+    big = 10 ** 9
+    src = TFSFPlaneWave(shape=shape, origin=np.array([-12.0, -11.0, -100.0]), dx=sp, dt=dt,
+                        r0=np.array([0.0, 0.0, 50.0]), lo=np.array([-big, -big, 14]), hi=np.array([big, big, big]),
+                        khat=np.array([0.0, 0.0, 1.0]), ehat=np.array([0.6, 0.8, 0.0]), eps_b=1.0,
+                        omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000, periodic=(True, True, False))
+    pml = ref_engine.PMLSpec(cells=((0, 0), (0, 0), (8, 8)), alpha_max=0.01, eps_ref=1.0, eps_ref_high=2.0)
+    e, h1, h2 = src.probe()
+    mons = [plane_monitor(shape, 12, om, 1), plane_monitor(shape, 29, om, 1),
+            ref_engine.DFTMonitor(om, e, h1, h2, source=src)]
+    kw = dict(shape=shape, dx=sp, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[src],
+              monitors=mons, dft_stride=4, periodic=(True, True, False))
+    run_engine_case("line_periodic", kw, 20, snap=2)
+
+
+def case_bloch_column():
+    shape = (9, 8, 44)
+    sp = (30.0, 32.0, 10.0)
+    rng = np.random.default_rng(5)
+    ie = np.full((3,) + shape, 1.0)
+    xx = np.arange(shape[0])[:, None]
+    yy = np.arange(shape[1])[None, :]
+    pillar = ((xx - 4) ** 2 + (yy - 4) ** 2 <= 4)
+    for z in range(22, 30):
+        ie[:, :, :, z] = np.where(pillar, 1 / 5.76, 1.0)
+    ie[:, :, :, 30:] = 1 / 2.1025
+    ie *= rng.uniform(0.98, 1.0, size=ie.shape)
+    dt = 0.95 / np.sqrt(sum(1 / d ** 2 for d in sp))
+    lam = 600.0
+    omega = 2 * np.pi / lam
+    kpar = (omega * np.sin(0.5) * np.cos(0.3), omega * np.sin(0.5) * np.sin(0.3))
+    pml = ref_engine.PMLSpec(cells=((0, 0), (0, 0), (8, 8)), alpha_max=0.01, eps_ref=1.0, eps_ref_high=2.1)
+    from dataclasses import replace
+    src = BlochPlaneSource(shape=shape, spacing=sp, dt=dt, k_src=14, k_launch=13, kpar=kpar, pol="p", eps_b=1.0,
+                           pml=replace(pml, eps_ref_high=None), omega_c=omega, omega_half=0.1 * omega, max_steps=20000)
+    om = np.array([omega])
+    e, h1, h2 = src.probe(16)
+    mons = [plane_monitor(shape, 11, om, 1), plane_monitor(shape, 34, om, 1),
+            ref_engine.DFTMonitor(om, e, h1, h2, source=src)]
+    kw = dict(shape=shape, dx=sp, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[src],
+              monitors=mons, dft_stride=3, periodic=(True, True, False), bloch=(kpar[0], kpar[1], 0.0))
+    run_engine_case("bloch_column", kw, 25, snap=2)
+
+
+def case_mode_source():
+    rng = np.random.default_rng(6)
+    shape, dx = (16, 14, 18), 20.0
+    ie = 1.0 / rng.uniform(2.0, 12.0, size=(3,) + shape)
+    dt = 0.95 * dx / np.sqrt(3)
+    pml = ref_engine.PMLSpec(cells=((3, 3),) * 3, alpha_max=0.01, eps_ref=2.07)
+    # a port plane at x = 5: H targets on the half plane outside it, E targets on the plane (ports.py:346-360)
+    jj, kk = np.meshgrid(np.arange(3, 11), np.arange(4, 14), indexing="ij")
+    jj, kk = jj.ravel(), kk.ravel()
+    nw = jj.size
+    src = ModeSource.__new__(ModeSource)
+    src.h_idx = np.concatenate([P.flat_index(2, 4, jj, kk, shape), P.flat_index(1, 4, jj, kk, shape)])
+    src.e_idx = np.concatenate([P.flat_index(1, 5, jj, kk, shape), P.flat_index(2, 5, jj, kk, shape)])
+    r_e, r_h, L = 3, 2, 200
+    src.mH = rng.normal(size=(2 * nw, r_e)) * 0.05
+    src.mE = rng.normal(size=(2 * nw, r_h)) * 0.05
+    t = np.arange(L) * dt
+    env = np.exp(-((t - 60 * dt) / (18 * dt)) ** 2)
+    src.tab_E = env[:, None] * np.sin(0.2 * np.arange(L)[:, None] + rng.uniform(0, 3, r_e)[None, :])
+    src.tab_H = env[:, None] * np.cos(0.2 * np.arange(L)[:, None] + rng.uniform(0, 3, r_h)[None, :])
+    om = np.array([2 * np.pi / 1550.0, 2 * np.pi / 1300.0])
+    i, k = np.meshgrid(np.arange(1, 15), np.arange(1, 17), indexing="ij")
+    e = P.flat_index(1, i.ravel(), 11, k.ravel(), shape)
+    h1 = P.flat_index(2, i.ravel(), 10, k.ravel(), shape)
+    h2 = P.flat_index(2, i.ravel(), 11, k.ravel(), shape)
+    mons = [ref_engine.DFTMonitor(om, e, h1, h2, energy=1)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[src],
+              monitors=mons, dft_stride=2)
+    run_engine_case("mode_source", kw, 30, snap=5)
+
+
+# --- a whole ls.solve of the dispersive-sphere scattering problem ---------------------------------------
+
+
+def solve_case(name: str, sim):
+    rec = {}
+    Base = ref_scattering.Engine
+    fp_orig = ref_scattering.flux_points
+
+    class Recording(Base):
+        def __init__(self, device, **kw):
+            rec["plan"] = P.make_plan(**kw)
+            rec["kw"] = kw
+            super().__init__(device, **kw)
+            rec["eng"] = self
+
+    boxes = []
+
+    def flux_points_rec(*a, **k):
+        out = fp_orig(*a, **k)
+        boxes.append(out)
+        return out
+    ref_scattering.Engine = Recording
+    ref_scattering.flux_points = flux_points_rec
+    try:
+        res = ls.solve(sim, "fdtd", "cpu")
+    finally:
+        ref_scattering.Engine = Base
+        ref_scattering.flux_points = fp_orig
+    kw, eng = rec["kw"], rec["eng"]
+    src = kw["sources"][0]
+    omega = 2 * np.pi / sim.wavelength_array()
+    sca, tot = boxes
+    post = {"omega": omega, "n_sym": 1.0, "n_inc": float(src.n_inc), "sca_coeff": sca[3], "tot_coeff": tot[3],
+            "unit": src.incident_reference(omega), "bg_e": src.background(omega, tot[0], "E"),
+            "bg_h": 0.5 * (src.background(omega, tot[1], "H") + src.background(omega, tot[2], "H")),
+            "steps": int(res.provenance["steps"])}
+    out = {"c_ext": np.asarray(res.c_ext_nm2), "c_sca": np.asarray(res.c_sca_nm2), "c_abs": np.asarray(res.c_abs_nm2),
+           "acc_e": [np.asarray(m.acc_e) for m in kw["monitors"]],
+           "acc_h": [np.zeros(0) if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]],
+           "energy": np.asarray(eng.energy), "n": int(eng.n[0])}
+    P.save(os.path.join(HERE, f"solve_{name}.npz"), {"plan": rec["plan"], "post": post, "out": out})
+    print(name, rec["plan"]["shape"], "steps", post["steps"], "C_ext", out["c_ext"])
+
+
+def sphere_problem(mesh: str):
+    mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
+                          poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
+                                 {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
+    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=mat)], medium_index=1.33,
+                         wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
+                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry="off", mesh_refinement=mesh,
+                                               padding_nm=8.0, pml_gap_nm=8.0, dft_stride=10,
+                                               run_time_fs=399.5 * 2.2863 / 299.792458)})
+
+
+CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_noncubic,
+         "ade_groups": case_ade_groups, "tfsf_table": case_tfsf_table, "line_periodic": case_line_periodic,
+         "bloch_column": case_bloch_column, "mode_source": case_mode_source,
+         "solve_sphere_staircase": lambda: solve_case("sphere_staircase", sphere_problem("staircase")),
+         "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel"))}
+
+if __name__ == "__main__":
+    which = sys.argv[2:] or list(CASES)
+    for c in which:
+        CASES[c]()
