@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Throughput of the plain 3D FDTD loop on B200: Gcell-updates/s and the HBM roofline fraction.
+
+Workload (lightsmith's plain-FDTD throughput case): a 640^3 FP32 grid, 16-cell CPML on every face,
+i.i.d. permittivity uniform in [1, 12.25] drawn from a seed, a Gaussian point-current pulse at the centre,
+a 16-frequency running DFT on the centre z plane. One bench step is one chunk: dft_stride FDTD time steps
+plus one DFT sample (lightsmith's unit of work, ``Engine.chunk``), replayed as a CUDA graph.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference] [--n 640]
+
+``--impl reference`` times the reference algorithm on the host CPU (the NumPy oracle, float64 as lightsmith
+runs on CPUs, all host threads) on a 128^3 sample of the same workload. Under torchrun each rank runs an
+independent replica (the plain solver does not shard) and rank 0 prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "FDTD Gcell-updates/s"
+UNIT = "Gcell-updates/s"
+CPU_SAMPLE_N = 128
+# algorithmic bytes of one FP32 cell update with isotropic eps: E and H read once and written once (6 + 6
+# values) and one coefficient read; each CPML (cell, axis) pair adds 4 psi values read and written
+BYTES_PER_CELL = (12 + 1) * 4
+BYTES_PER_CPML_PAIR = 4 * 2 * 4
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=640)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _peak():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def _ncu_traffic_per_cell():
+    """DRAM bytes per cell update of the bulk kernels from the committed ncu summary, if any."""
+    path = os.path.join(HERE, "profiles", "yee_bulk_throughput.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_cell_update:\s*([0-9.]+)", text)
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi samples (every 200 ms) of one GPU while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.proc = None
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(self.NAMES, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _gpu_uuid(torch, dev):
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:  # noqa: BLE001 (older torch)
+        return None
+
+
+def cpu_sample(n: int, chunks: int, warmup: int, threads: int):
+    """The oracle (float64, as lightsmith runs on CPUs) on an n^3 sample of the workload; Gcell-updates/s."""
+    from lightsmith_b200.workloads import throughput_plan
+    from oracle.engine import OracleEngine
+
+    plan = throughput_plan(n, max_steps=400 * (chunks + warmup + 2), single=False, seed=1)
+    eng = OracleEngine(plan, threads=threads)
+    for _ in range(warmup):
+        eng.chunk()
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        eng.chunk()
+    dt = time.perf_counter() - t0
+    eng.close()
+    cells = n ** 3
+    return cells * plan["stride"] * chunks / dt / 1e9, dt, plan["stride"]
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    threads = _threads()
+    # each bench step is one chunk of the 128^3 sample
+    value, secs, stride = cpu_sample(CPU_SAMPLE_N, args.steps, args.warmup, threads)
+    sample = (f"{CPU_SAMPLE_N}^3 grid of the same workload (CPML 16, random eps, centre dipole, 16-frequency DFT "
+              f"plane), {args.steps} chunks of {stride} steps after {args.warmup}, NumPy float64 oracle, "
+              f"{threads} threads")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(args.steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"plain FDTD throughput, {CPU_SAMPLE_N}^3 CPU sample of the 640^3 case",
+                      "grid": [CPU_SAMPLE_N] * 3, "dft_stride": stride},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import cells_in_cpml, throughput_band, throughput_plan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    n = args.n
+    shape = (n, n, n)
+    K, W = args.steps, args.warmup
+    R = max(1, min(K, 6))  # chunks of the kernel-timing pass
+    _, _, _, _, stride = throughput_band()
+    total_chunks = W + 2 * K + R + 2
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234)
+    inv = 1.0 / (torch.rand(shape, generator=gen, device=dev, dtype=torch.float32) * 11.25 + 1.0)
+    plan = throughput_plan(n, inv_eps=inv, max_steps=stride * total_chunks + 8, single=True)
+    eng = Engine.from_plan(plan, device=dev)
+    inv_host = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    inv_host.copy_(inv)
+    del inv, plan["inv_eps"]
+    torch.cuda.empty_cache()
+    cells = n ** 3
+
+    eng.chunk(W, use_graph=True)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = Clocks(_gpu_uuid(torch, dev)) if rank == 0 else None
+    time.sleep(0.3 if clocks else 0.0)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    start.record(eng.stream)
+    eng.chunk(K, use_graph=True)
+    end.record(eng.stream)
+    torch.cuda.synchronize(dev)
+    ms = start.elapsed_time(end)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * cells * stride * K / (ms_max / 1e3) / 1e9
+
+    # the bulk Yee kernels alone: CUDA events around each launch on the engine's stream
+    bulk_ms, bulk_launches = eng.chunk_timed(R)
+    steps_timed = R * stride
+    step_ms = bulk_ms / steps_timed
+    alg_bytes = cells * BYTES_PER_CELL + cells_in_cpml(eng.plan) * BYTES_PER_CPML_PAIR
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    peak, peak_kind = _peak()
+    tpc = _ncu_traffic_per_cell()
+
+    # end to end through the C ABI with host buffers: permittivity from pinned host memory, K chunks, the DFT
+    # accumulators and the energy back to pinned host memory
+    acc = [m["acc_e"] for m in eng.monitors] + [m["acc_h"] for m in eng.monitors if m["acc_h"] is not None]
+    acc_host = [torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for a in acc]
+    energy_host = torch.empty(2, dtype=torch.float64, pin_memory=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(eng.stream):
+        e0.record(eng.stream)
+        eng.load_inv_eps(inv_host)
+        eng.chunk(K, use_graph=True)
+        for h, d in zip(acc_host, acc):
+            h.copy_(d, non_blocking=True)
+        energy_host.copy_(eng.energy, non_blocking=True)
+        e1.record(eng.stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    te = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * cells * stride * K / (float(te.item()) / 1e3) / 1e9
+    h2d = inv_host.numel() * 4
+    d2h = sum(a.numel() * a.element_size() for a in acc) + 16
+    finite = bool(np.isfinite(energy_host.numpy()).all())
+    launches = eng.launches_per_chunk() * K
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = _threads()
+        v, secs, st = cpu_sample(CPU_SAMPLE_N, 6, 1, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{CPU_SAMPLE_N}^3 grid of the same workload, 6 chunks of {st} steps, NumPy float64 "
+                         f"oracle on {threads} threads ({secs:.1f} s)"}
+    eng.close()
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+               "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32", "data": "synthetic",
+               "config": {"workload": f"plain FDTD throughput: {n}^3 FP32 grid, 16-cell CPML on all faces, i.i.d. "
+                                      "eps in [1, 12.25], centre dipole pulse, 16-frequency DFT on one plane",
+                          "grid": list(shape), "cpml_cells": 16, "dft_freqs": 16, "dft_stride": stride,
+                          "step": f"one chunk = {stride} FDTD steps + one DFT sample, CUDA graph replay",
+                          "l2": "inputs larger than L2 (about 8 GB of state per replica)",
+                          "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_source": peak_kind,
+                            "traffic": None if tpc is None else tpc * cells,
+                            "kernel": "bulk Yee H + E updates with fused CPML, per FDTD step",
+                            "alg_bytes_per_step": alg_bytes, "kernel_ms_per_step": step_ms,
+                            "bulk_launches_timed": bulk_launches},
+               "cpu_baseline": cpu,
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                       "fields_finite": finite},
+               "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

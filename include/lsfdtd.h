@@ -1,0 +1,243 @@
+/*
+ * lsfdtd: B200 (sm_100a) kernels for lightsmith's 3D FDTD time-stepping loop, behind a C ABI.
+ *
+ * The ABI replaces the device-side engine of lightsmith v0.3.0 (src/lightsmith/backends/_fdtd/engine.py):
+ * an engine handle is built from plain device pointers and sizes (all device memory is owned by the caller,
+ * e.g. PyTorch tensors; the library allocates none), then stepped in chunks of `dft_stride` steps followed by
+ * one DFT sample, on a caller stream, optionally replayed as a CUDA graph. Handles are not thread-safe; one
+ * handle per run. Every function returns LSFDTD_OK (0) or an error code; lsfdtd_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * Field arrays are stacked F[3][N0][N1][N2] (N2 fastest), exactly lightsmith's E/H layout, so the flat
+ * indices lightsmith's set-up code produces (monitors, sources, dispersive nodes) are used unchanged.
+ * Complex fields (a Bloch wavevector) are interleaved (re, im) pairs of the field precision.
+ */
+#ifndef LSFDTD_H
+#define LSFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSFDTD_ABI_VERSION 1
+
+enum { LSFDTD_F32 = 0, LSFDTD_F64 = 1 };
+enum {
+  LSFDTD_OK = 0,
+  LSFDTD_EINVAL = 1,      /* bad argument or inconsistent description */
+  LSFDTD_ECUDA = 2,       /* a CUDA call failed (the message names it) */
+  LSFDTD_EUNSUPPORTED = 3,
+  LSFDTD_ERANGE = 4       /* the run would read a source waveform past its end */
+};
+#define LSFDTD_MAX_MEDIA 4
+#define LSFDTD_MAX_POLES 6
+
+typedef struct lsfdtd_engine lsfdtd_engine;
+
+/* Grid, bulk coefficients and run state. Replaces Engine.__init__'s field arrays and curl coefficients
+ * (engine.py:231-315): cbE[c] = (dt/dx or dt) * (1/eps)_c over the whole grid (the three may alias one
+ * array when eps is isotropic). step: completed-step counter (Engine.n, engine.py:271). energy: the two
+ * decay-energy proxies (Engine.energy, engine.py:315). */
+typedef struct {
+  int32_t shape[3];
+  int32_t precision;   /* LSFDTD_F32 or LSFDTD_F64 */
+  int32_t is_complex;  /* nonzero under a Bloch wavevector */
+  int32_t periodic[3];
+  double spacing[3];   /* nm; all equal for cubic cells */
+  double dt;           /* nm/c */
+  double bloch[3];     /* rad/nm per periodic axis */
+  int32_t dft_stride;
+  void* E;             /* device, zeroed */
+  void* H;             /* device, zeroed */
+  const void* cbE[3];  /* device, field precision (real) */
+  int64_t* step;       /* device, one int64 */
+  double* energy;      /* device, two doubles */
+} lsfdtd_grid_desc;
+
+/* One CPML axis (Engine._build_pml, engine.py:344-418). Profiles have one entry per node position along the
+ * axis: [0] at the E positions u, [1] at the H positions u + 1/2; b = exp(-(sigma/kappa + alpha) dt),
+ * c = sigma (b - 1) / (sigma kappa + kappa^2 alpha), k = 1/kappa - 1 (NULL when kappa is 1 everywhere).
+ * psi[field][component][side]: zeroed device slabs sized by lsfdtd_cpml_slab() (NULL where that is empty). */
+typedef struct {
+  int32_t axis;
+  int32_t cells_lo, cells_hi;
+  const void* b[2];
+  const void* c[2];
+  const void* k[2];
+  void* psi[2][3][2];
+} lsfdtd_pml_desc;
+
+/* D-form ADE nodes (the _Group of engine.py:722-793). Pure group: one dispersive medium. Mixed group
+ * (subpixel interface cells): harmonic path weight w, h0 = sum of f_s/eps_inf_s over non-dispersive media,
+ * inv_a = 1/sum_s f_s eps_inf_s, frac = [n_media][n] fractions of the dispersive media. Coefficients per
+ * dispersive medium and pole: P^{n+1} = c1 P^n + c2 P^{n-1} + c3 E (engine.py:108-111). state: zeroed
+ * device buffer of lsfdtd_group_state_len() * n field scalars. */
+typedef struct {
+  int64_t n;
+  const int64_t* idx;
+  int32_t mixed, has_h, has_a;
+  int32_t n_media;
+  int32_t n_poles[LSFDTD_MAX_MEDIA];
+  double c1[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  double c2[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  double c3[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  double inv_eps_inf[LSFDTD_MAX_MEDIA];
+  const void* h0;
+  const void* inv_a;
+  const void* w;
+  const void* frac;
+  void* state;
+} lsfdtd_group_desc;
+
+/* Correction points of one kind as a CSR list per target node: entries offsets[t] .. offsets[t+1] of node t
+ * are applied in order (a node on two box faces gets both). */
+typedef struct {
+  int64_t n_nodes;
+  const int64_t* nodes;    /* flat E (kind E) or H (kind H) indices */
+  const int64_t* offsets;  /* n_nodes + 1 */
+  int64_t n_entries;
+} lsfdtd_csr;
+
+/* Table-fed TF/SF box (ObliqueLayeredPlaneWave, layered.py:254-482): target += coef * quintic interpolation
+ * of the table at fine time (n + i0 + u0) / m; view[3] receives the incident-reference E every step. */
+typedef struct {
+  const void* table;
+  int64_t table_len;
+  const void* inc_table;
+  int64_t inc_len;
+  int32_t m;
+  int64_t cmax;
+  lsfdtd_csr pts[2];   /* [0]: E targets, [1]: H targets */
+  const int64_t* base[2];
+  const int64_t* i0[2];
+  const void* u0[2];
+  const void* coef[2];
+  const int64_t* inc_base; /* 3 */
+  const int64_t* inc_i0;   /* 3 */
+  const void* inc_u0;      /* 3 */
+  void* view;              /* device, 3 field-precision scalars */
+} lsfdtd_table_source_desc;
+
+/* Point current (PointDipole, emission.py:97-150): E[idx] -= coef * wave[n]. */
+typedef struct {
+  int32_t n;
+  const int64_t* idx;
+  const void* coef;
+  const void* wave;
+  int64_t wave_len;
+} lsfdtd_dipole_desc;
+
+/* 1D-fed TF/SF (TFSFPlaneWave, tfsf.py:108-211): line arrays E_line/H_line of M nodes with their update
+ * coefficients (full length M), soft source wave at m_src, and the corrections of each kind. */
+typedef struct {
+  int32_t M, m_src;
+  const void* ca;
+  const void* cb;
+  const void* da;
+  const void* db;
+  const void* wave;
+  int64_t wave_len;
+  void* E_line;
+  void* H_line;
+  lsfdtd_csr pts[2];
+  const int64_t* i0[2];
+  const void* w[2];
+  const void* coef[2];
+} lsfdtd_line_source_desc;
+
+/* Bloch column source (BlochPlaneSource, tfsf.py:214-296): `column` is a 3 x 3 x nz engine with the same
+ * precision, complex fields and Bloch phases; phase[nx][ny] (complex) maps its field onto the plane. */
+typedef struct {
+  lsfdtd_engine* column;
+  int32_t k_src, k_launch;
+  const void* phase;
+  double amp[2][2];  /* (re, im) of the E_x and E_y sheet amplitudes */
+  const void* wave;
+  int64_t wave_len;
+  double cE, cH;
+} lsfdtd_column_source_desc;
+
+/* Port mode source (ModeSource, ports.py:294-378): H[h_idx] += mH @ tab_E[n], E[e_idx] += mE @ tab_H[n]. */
+typedef struct {
+  int32_t n_h, r_e;
+  const int64_t* h_idx;
+  const void* mH;     /* [n_h][r_e] */
+  const void* tab_E;  /* [len_E][r_e] */
+  int64_t len_E;
+  int32_t n_e, r_h;
+  const int64_t* e_idx;
+  const void* mE;     /* [n_e][r_h] */
+  const void* tab_H;  /* [len_H][r_h] */
+  int64_t len_H;
+} lsfdtd_mode_source_desc;
+
+/* Running-DFT monitor (DFTMonitor, engine.py:194-210): acc_e [n_freq][n_e] and acc_h [n_freq][n_h] are
+ * complex128 (interleaved doubles). The sampled arrays are the grid's (space 0), a 1D line's or the
+ * incident view's (space 1: real field-precision arrays), or a Bloch column's (space 2). energy: 0, or
+ * group 1 / 2 of the decay-energy proxy (monitors without H contribute none, as in the reference). */
+typedef struct {
+  int32_t n_freq;
+  const double* omega;
+  int64_t n_e;
+  const int64_t* e_idx;
+  int64_t n_h;
+  const int64_t* h_idx1;
+  const int64_t* h_idx2;
+  void* acc_e;
+  void* acc_h;
+  int32_t energy;
+  int32_t space;
+  const void* E_src;
+  const void* H_src;
+} lsfdtd_monitor_desc;
+
+int32_t lsfdtd_abi_version(void);
+const char* lsfdtd_last_error(void);
+
+/* Stepped range [start, start + len) along `axis` of the CPML slab of `field` (0 E, 1 H), `component`,
+ * `side` (0 low, 1 high): the slab's psi array holds the grid with that axis cut to len. */
+int32_t lsfdtd_cpml_slab(const int32_t shape[3], const int32_t periodic[3], int32_t axis, int32_t cells_lo,
+                         int32_t cells_hi, int32_t field, int32_t component, int32_t side, int32_t* start,
+                         int32_t* len);
+/* field scalars of state per node of a dispersive group */
+int64_t lsfdtd_group_state_len(int32_t mixed, int32_t n_media, const int32_t* n_poles);
+
+int32_t lsfdtd_engine_create(const lsfdtd_grid_desc* grid, lsfdtd_engine** out);
+int32_t lsfdtd_engine_destroy(lsfdtd_engine* eng);
+int32_t lsfdtd_engine_set_pml(lsfdtd_engine* eng, const lsfdtd_pml_desc* pml);
+int32_t lsfdtd_engine_add_group(lsfdtd_engine* eng, const lsfdtd_group_desc* g);
+/* sources act in the order they are added (Engine.step, engine.py:665-678) */
+int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s);
+int32_t lsfdtd_engine_add_dipole(lsfdtd_engine* eng, const lsfdtd_dipole_desc* s);
+int32_t lsfdtd_engine_add_line_source(lsfdtd_engine* eng, const lsfdtd_line_source_desc* s);
+int32_t lsfdtd_engine_add_column_source(lsfdtd_engine* eng, const lsfdtd_column_source_desc* s);
+int32_t lsfdtd_engine_add_mode_source(lsfdtd_engine* eng, const lsfdtd_mode_source_desc* s);
+int32_t lsfdtd_engine_add_monitor(lsfdtd_engine* eng, const lsfdtd_monitor_desc* m);
+/* bytes of device scratch the monitors' energy reduction needs; set it before the first sample */
+int32_t lsfdtd_engine_scratch_bytes(lsfdtd_engine* eng, size_t* bytes);
+int32_t lsfdtd_engine_set_scratch(lsfdtd_engine* eng, void* scratch, size_t bytes);
+
+/* n_steps time steps (Engine.step, engine.py:665-678), no sample */
+int32_t lsfdtd_engine_step(lsfdtd_engine* eng, int32_t n_steps, void* stream);
+/* one DFT sample of every monitor (Engine._sample, engine.py:568-592) */
+int32_t lsfdtd_engine_sample(lsfdtd_engine* eng, void* stream);
+/* n_chunks x (dft_stride steps + one sample) (Engine.chunk, engine.py:680-683). With use_graph, the first
+ * call captures one chunk as a CUDA graph on `stream` (which must not be the legacy default stream) and every
+ * chunk replays it (Engine.make_runner, engine.py:685-709). */
+int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_graph, void* stream);
+/* Diagnostic: n_chunks eager chunks with CUDA events around every bulk Yee-update kernel; synchronises
+ * `stream`, then returns the summed kernel time (ms) and the number of such launches. */
+int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* stream, double* bulk_ms,
+                                  int64_t* bulk_launches);
+/* steps completed so far, as the host has launched them */
+int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng);
+/* kernel launches one chunk issues (for launch accounting) */
+int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,132 @@
+"""ctypes binding of the C ABI in ``include/lsfdtd.h`` (``liblsfdtd.so``, built in-tree by ``build.py``).
+
+The structures mirror the header field by field. Loading fails loudly when the library is missing: there is
+no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblsfdtd.so")
+
+F32, F64 = 0, 1
+OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE = 0, 1, 2, 3, 4
+MAX_MEDIA, MAX_POLES = 4, 6
+
+vp = C.c_void_p
+i32 = C.c_int32
+i64 = C.c_int64
+f64 = C.c_double
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("shape", i32 * 3), ("precision", i32), ("is_complex", i32), ("periodic", i32 * 3),
+                ("spacing", f64 * 3), ("dt", f64), ("bloch", f64 * 3), ("dft_stride", i32),
+                ("E", vp), ("H", vp), ("cbE", vp * 3), ("step", vp), ("energy", vp)]
+
+
+class PmlDesc(C.Structure):
+    _fields_ = [("axis", i32), ("cells_lo", i32), ("cells_hi", i32), ("b", vp * 2), ("c", vp * 2), ("k", vp * 2),
+                ("psi", ((vp * 2) * 3) * 2)]
+
+
+class GroupDesc(C.Structure):
+    _fields_ = [("n", i64), ("idx", vp), ("mixed", i32), ("has_h", i32), ("has_a", i32), ("n_media", i32),
+                ("n_poles", i32 * MAX_MEDIA), ("c1", (f64 * MAX_POLES) * MAX_MEDIA),
+                ("c2", (f64 * MAX_POLES) * MAX_MEDIA), ("c3", (f64 * MAX_POLES) * MAX_MEDIA),
+                ("inv_eps_inf", f64 * MAX_MEDIA), ("h0", vp), ("inv_a", vp), ("w", vp), ("frac", vp), ("state", vp)]
+
+
+class Csr(C.Structure):
+    _fields_ = [("n_nodes", i64), ("nodes", vp), ("offsets", vp), ("n_entries", i64)]
+
+
+class TableSourceDesc(C.Structure):
+    _fields_ = [("table", vp), ("table_len", i64), ("inc_table", vp), ("inc_len", i64), ("m", i32), ("cmax", i64),
+                ("pts", Csr * 2), ("base", vp * 2), ("i0", vp * 2), ("u0", vp * 2), ("coef", vp * 2),
+                ("inc_base", vp), ("inc_i0", vp), ("inc_u0", vp), ("view", vp)]
+
+
+class DipoleDesc(C.Structure):
+    _fields_ = [("n", i32), ("idx", vp), ("coef", vp), ("wave", vp), ("wave_len", i64)]
+
+
+class LineSourceDesc(C.Structure):
+    _fields_ = [("M", i32), ("m_src", i32), ("ca", vp), ("cb", vp), ("da", vp), ("db", vp), ("wave", vp),
+                ("wave_len", i64), ("E_line", vp), ("H_line", vp), ("pts", Csr * 2), ("i0", vp * 2), ("w", vp * 2),
+                ("coef", vp * 2)]
+
+
+class ColumnSourceDesc(C.Structure):
+    _fields_ = [("column", vp), ("k_src", i32), ("k_launch", i32), ("phase", vp), ("amp", (f64 * 2) * 2),
+                ("wave", vp), ("wave_len", i64), ("cE", f64), ("cH", f64)]
+
+
+class ModeSourceDesc(C.Structure):
+    _fields_ = [("n_h", i32), ("r_e", i32), ("h_idx", vp), ("mH", vp), ("tab_E", vp), ("len_E", i64),
+                ("n_e", i32), ("r_h", i32), ("e_idx", vp), ("mE", vp), ("tab_H", vp), ("len_H", i64)]
+
+
+class MonitorDesc(C.Structure):
+    _fields_ = [("n_freq", i32), ("omega", vp), ("n_e", i64), ("e_idx", vp), ("n_h", i64), ("h_idx1", vp),
+                ("h_idx2", vp), ("acc_e", vp), ("acc_h", vp), ("energy", i32), ("space", i32), ("E_src", vp),
+                ("H_src", vp)]
+
+
+# every exported symbol of include/lsfdtd.h with its ctypes signature
+SIGNATURES = {
+    "lsfdtd_abi_version": (i32, []),
+    "lsfdtd_last_error": (C.c_char_p, []),
+    "lsfdtd_cpml_slab": (i32, [C.POINTER(i32), C.POINTER(i32), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
+                               C.POINTER(i32)]),
+    "lsfdtd_group_state_len": (i64, [i32, i32, C.POINTER(i32)]),
+    "lsfdtd_engine_create": (i32, [C.POINTER(GridDesc), C.POINTER(vp)]),
+    "lsfdtd_engine_destroy": (i32, [vp]),
+    "lsfdtd_engine_set_pml": (i32, [vp, C.POINTER(PmlDesc)]),
+    "lsfdtd_engine_add_group": (i32, [vp, C.POINTER(GroupDesc)]),
+    "lsfdtd_engine_add_table_source": (i32, [vp, C.POINTER(TableSourceDesc)]),
+    "lsfdtd_engine_add_dipole": (i32, [vp, C.POINTER(DipoleDesc)]),
+    "lsfdtd_engine_add_line_source": (i32, [vp, C.POINTER(LineSourceDesc)]),
+    "lsfdtd_engine_add_column_source": (i32, [vp, C.POINTER(ColumnSourceDesc)]),
+    "lsfdtd_engine_add_mode_source": (i32, [vp, C.POINTER(ModeSourceDesc)]),
+    "lsfdtd_engine_add_monitor": (i32, [vp, C.POINTER(MonitorDesc)]),
+    "lsfdtd_engine_scratch_bytes": (i32, [vp, C.POINTER(C.c_size_t)]),
+    "lsfdtd_engine_set_scratch": (i32, [vp, vp, C.c_size_t]),
+    "lsfdtd_engine_step": (i32, [vp, i32, vp]),
+    "lsfdtd_engine_sample": (i32, [vp, vp]),
+    "lsfdtd_engine_chunk": (i32, [vp, i32, i32, vp]),
+    "lsfdtd_engine_chunk_timed": (i32, [vp, i32, vp, C.POINTER(f64), C.POINTER(i64)]),
+    "lsfdtd_engine_steps": (i64, [vp]),
+    "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
+}
+
+_lib = None
+
+
+class LsfdtdError(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded library (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"lightsmith-b200: {LIB_PATH} is missing; build it with "
+                              "`python -c 'import lightsmith_b200.build as b; b.build()'` (needs nvcc)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int, what: str) -> None:
+    if code != OK:
+        msg = lib().lsfdtd_last_error().decode(errors="replace")
+        raise LsfdtdError(f"{what} failed (code {code}): {msg}")

@@ -1,0 +1,820 @@
+// lsfdtd: the FDTD engine behind the C ABI of include/lsfdtd.h.
+//
+// An engine is a host-side list of kernel launches over caller-owned device memory: the step order of
+// lightsmith's Engine.step (backends/_fdtd/engine.py:665-678) with the Yee/CPML updates fused per field, then
+// the sources' hooks, the dispersive groups and the step counter. Nothing here allocates device memory or
+// synchronises the host, so a chunk can be captured once as a CUDA graph and replayed.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "lsfdtd.h"
+
+#include "ade.cuh"
+#include "common.cuh"
+#include "monitors.cuh"
+#include "sources.cuh"
+#include "yee.cuh"
+
+using namespace lsfdtd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define LS_CUDA(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) return fail(LSFDTD_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LS_LAUNCHED()                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = cudaGetLastError();                                                    \
+    if (e_ != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LS_TRY(x)                 \
+  do {                            \
+    int r_ = (x);                 \
+    if (r_ != LSFDTD_OK) return r_; \
+  } while (0)
+
+// stepped range of a field component along an axis (engine.py:47-66, no mirror planes)
+void region(int field, int c, int a, const int32_t* shape, const int32_t* periodic, int* lo, int* hi) {
+  const int n = shape[a];
+  if (field == 0) {
+    *lo = (periodic[a] || a != c) ? 1 : 0;
+    *hi = n - 1;
+  } else {
+    *lo = periodic[a] ? 1 : 0;
+    *hi = periodic[a] ? n - 1 : (a == c ? n : n - 1);
+  }
+}
+
+int slab(const int32_t* shape, const int32_t* periodic, int d, int lo_n, int hi_n, int field, int c, int side,
+         int* start, int* len) {
+  *start = 0;
+  *len = 0;
+  if (c == d || (side == 0 && !lo_n) || (side == 1 && !hi_n)) return LSFDTD_OK;
+  int st, sp;
+  region(field, c, d, shape, periodic, &st, &sp);
+  int a, b;
+  if (side == 0) {
+    a = st;
+    b = std::min(sp, lo_n + 1);
+  } else {
+    a = std::max(st, shape[d] - 2 - hi_n);
+    b = sp;
+  }
+  if (b > a) {
+    *start = a;
+    *len = b - a;
+  }
+  return LSFDTD_OK;
+}
+
+}  // namespace
+
+struct lsfdtd_engine {
+  lsfdtd_grid_desc desc{};
+  int64_t n_host = 0;
+  int64_t step_limit = std::numeric_limits<int64_t>::max();
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
+  virtual ~lsfdtd_engine() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  virtual int set_pml(const lsfdtd_pml_desc* p) = 0;
+  virtual int add_group(const lsfdtd_group_desc* g) = 0;
+  virtual int add_table(const lsfdtd_table_source_desc* s) = 0;
+  virtual int add_dipole(const lsfdtd_dipole_desc* s) = 0;
+  virtual int add_line(const lsfdtd_line_source_desc* s) = 0;
+  virtual int add_column(const lsfdtd_column_source_desc* s) = 0;
+  virtual int add_mode(const lsfdtd_mode_source_desc* s) = 0;
+  virtual int add_monitor(const lsfdtd_monitor_desc* m) = 0;
+  virtual size_t need_scratch() const = 0;
+  virtual int step(cudaStream_t s) = 0;
+  virtual int sample(cudaStream_t s) = 0;
+  virtual int update_h(cudaStream_t s) = 0;
+  virtual int update_e(cudaStream_t s) = 0;
+  virtual int64_t launches_per_chunk() const = 0;
+};
+
+namespace {
+
+enum SrcKind { kTable, kDipole, kLine, kColumn, kMode };
+
+template <typename F>
+struct Engine final : lsfdtd_engine {
+  using R = typename real_of<F>::type;
+  static constexpr bool kComplex = is_cplx<F>::value;
+
+  YeeArgs<F> y{};
+  double bloch_re[3][2]{}, bloch_im[3][2]{};  // [axis][low/high ghost]
+  std::vector<AdeArgs<F>> groups;
+  struct Table {
+    TableArgs<R> corr[2];
+    bool has[2];
+    const R* Tinc;
+    const long long *inc_base, *inc_i0;
+    const R* inc_u0;
+    R* view;
+  };
+  struct Dipole {
+    const long long* idx;
+    const R* coef;
+    const R* wave;
+    int n;
+  };
+  struct Line {
+    LineArgs<R> corr[2];
+    bool has[2];
+    R *E, *H;
+    const R *ca, *cb, *da, *db, *wave;
+    int M, m_src;
+  };
+  struct Column {
+    lsfdtd_engine* col;
+    int k_src, k_launch;
+    const F* phase;
+    F amp0, amp1;
+    const R* wave;
+    R cE, cH;
+  };
+  struct Mode {
+    lsfdtd_mode_source_desc d;
+  };
+  struct Monitor {
+    int space;
+    MonArgs<F> af;
+    MonArgs<R> ar;
+    long long blocks;
+    int energy;
+  };
+  std::vector<std::pair<SrcKind, size_t>> order;
+  std::vector<Table> tables;
+  std::vector<Dipole> dipoles;
+  std::vector<Line> lines;
+  std::vector<Column> columns;
+  std::vector<Mode> modes;
+  std::vector<Monitor> monitors;
+  long long e_first[2] = {0, 0}, e_count[2] = {0, 0};
+
+  explicit Engine(const lsfdtd_grid_desc& g) {
+    desc = g;
+    const long long cells = (long long)g.shape[0] * g.shape[1] * g.shape[2];
+    for (int a = 0; a < 3; ++a) {
+      y.n[a] = g.shape[a];
+      y.periodic[a] = g.periodic[a];
+      y.inv_d[a] = R(1.0 / g.spacing[a]);
+      y.E[a] = static_cast<F*>(g.E) + a * cells;
+      y.H[a] = static_cast<F*>(g.H) + a * cells;
+      y.cbE[a] = static_cast<const R*>(g.cbE[a]);
+      y.pml[a].on = 0;
+      // Bloch ghost phases e^{-+i k L}, L = (n - 2) d (engine.py:606-609)
+      const double kl = g.bloch[a] * (g.shape[a] - 2) * g.spacing[a];
+      bloch_re[a][0] = std::cos(-kl);
+      bloch_im[a][0] = std::sin(-kl);
+      bloch_re[a][1] = std::cos(kl);
+      bloch_im[a][1] = std::sin(kl);
+    }
+    y.uniform = (g.spacing[0] == g.spacing[1] && g.spacing[1] == g.spacing[2]) ? 1 : 0;
+    y.cH = R(y.uniform ? g.dt / g.spacing[0] : g.dt);
+  }
+
+  F* Eflat() const { return static_cast<F*>(desc.E); }
+  F* Hflat() const { return static_cast<F*>(desc.H); }
+
+  int set_pml(const lsfdtd_pml_desc* p) override {
+    const int d = p->axis;
+    if (d < 0 || d > 2) return fail(LSFDTD_EINVAL, "pml axis out of range");
+    if (desc.periodic[d]) return fail(LSFDTD_EINVAL, "a periodic axis cannot have a PML");
+    PmlAxis<F>& q = y.pml[d];
+    q.on = 1;
+    q.div = y.uniform ? R(1) : R(desc.spacing[d]);
+    for (int f = 0; f < 2; ++f) {
+      q.b[f] = static_cast<const R*>(p->b[f]);
+      q.c[f] = static_cast<const R*>(p->c[f]);
+      q.k[f] = static_cast<const R*>(p->k[f]);
+      if (!q.b[f] || !q.c[f]) return fail(LSFDTD_EINVAL, "pml profiles missing");
+      for (int c = 0; c < 3; ++c)
+        for (int s = 0; s < 2; ++s) {
+          int st, ln;
+          slab(desc.shape, desc.periodic, d, p->cells_lo, p->cells_hi, f, c, s, &st, &ln);
+          q.start[f][c][s] = st;
+          q.len[f][c][s] = ln;
+          q.psi[f][c][s] = static_cast<F*>(p->psi[f][c][s]);
+          if (ln > 0 && !q.psi[f][c][s]) return fail(LSFDTD_EINVAL, "pml psi slab missing");
+        }
+    }
+    return LSFDTD_OK;
+  }
+
+  int add_group(const lsfdtd_group_desc* g) override {
+    if (g->n_media < 1 || g->n_media > kMaxMedia) return fail(LSFDTD_EINVAL, "group media count out of range");
+    AdeArgs<F> a{};
+    a.n = g->n;
+    a.idx = reinterpret_cast<const long long*>(g->idx);
+    a.E = Eflat();
+    a.n_media = g->n_media;
+    a.mixed = g->mixed;
+    a.has_h = g->has_h;
+    a.has_a = g->has_a;
+    for (int s = 0; s < g->n_media; ++s) {
+      if (g->n_poles[s] < 0 || g->n_poles[s] > kMaxPoles) return fail(LSFDTD_EINVAL, "pole count out of range");
+      a.n_poles[s] = g->n_poles[s];
+      a.inv_inf[s] = R(g->inv_eps_inf[s]);
+      for (int k = 0; k < g->n_poles[s]; ++k) {
+        a.c1[s][k] = R(g->c1[s][k]);
+        a.c2[s][k] = R(g->c2[s][k]);
+        a.c3[s][k] = R(g->c3[s][k]);
+      }
+    }
+    a.h0 = static_cast<const R*>(g->h0);
+    a.inv_a = static_cast<const R*>(g->inv_a);
+    a.w = static_cast<const R*>(g->w);
+    a.frac = static_cast<const R*>(g->frac);
+    a.state = static_cast<F*>(g->state);
+    if (g->mixed && (!a.w || !a.frac || (g->has_h && !a.h0) || (g->has_a && !a.inv_a)))
+      return fail(LSFDTD_EINVAL, "mixed group arrays missing");
+    if (a.n > 0 && (!a.idx || !a.state)) return fail(LSFDTD_EINVAL, "group arrays missing");
+    groups.push_back(a);
+    return LSFDTD_OK;
+  }
+
+  int add_table(const lsfdtd_table_source_desc* s) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "table-fed sources need real fields");
+    if (s->m < 1) return fail(LSFDTD_EINVAL, "table stride m < 1");
+    Table t{};
+    for (int k = 0; k < 2; ++k) {
+      TableArgs<R>& a = t.corr[k];
+      t.has[k] = s->pts[k].n_nodes > 0;
+      a.T = static_cast<const R*>(s->table);
+      a.m = s->m;
+      a.cmax = s->cmax;
+      a.n_nodes = s->pts[k].n_nodes;
+      a.nodes = reinterpret_cast<const long long*>(s->pts[k].nodes);
+      a.offsets = reinterpret_cast<const long long*>(s->pts[k].offsets);
+      a.base = reinterpret_cast<const long long*>(s->base[k]);
+      a.i0 = reinterpret_cast<const long long*>(s->i0[k]);
+      a.u0 = static_cast<const R*>(s->u0[k]);
+      a.coef = static_cast<const R*>(s->coef[k]);
+      a.target = reinterpret_cast<R*>(k == 0 ? desc.E : desc.H);
+      a.nstep = reinterpret_cast<const long long*>(desc.step);
+    }
+    t.Tinc = static_cast<const R*>(s->inc_table);
+    t.inc_base = reinterpret_cast<const long long*>(s->inc_base);
+    t.inc_i0 = reinterpret_cast<const long long*>(s->inc_i0);
+    t.inc_u0 = static_cast<const R*>(s->inc_u0);
+    t.view = static_cast<R*>(s->view);
+    order.push_back({kTable, tables.size()});
+    tables.push_back(t);
+    return LSFDTD_OK;
+  }
+
+  int add_dipole(const lsfdtd_dipole_desc* s) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "a point dipole needs real fields");
+    Dipole d{reinterpret_cast<const long long*>(s->idx), static_cast<const R*>(s->coef),
+             static_cast<const R*>(s->wave), s->n};
+    step_limit = std::min<int64_t>(step_limit, s->wave_len);
+    order.push_back({kDipole, dipoles.size()});
+    dipoles.push_back(d);
+    return LSFDTD_OK;
+  }
+
+  int add_line(const lsfdtd_line_source_desc* s) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "a 1D-fed source needs real fields");
+    Line l{};
+    l.E = static_cast<R*>(s->E_line);
+    l.H = static_cast<R*>(s->H_line);
+    l.ca = static_cast<const R*>(s->ca);
+    l.cb = static_cast<const R*>(s->cb);
+    l.da = static_cast<const R*>(s->da);
+    l.db = static_cast<const R*>(s->db);
+    l.wave = static_cast<const R*>(s->wave);
+    l.M = s->M;
+    l.m_src = s->m_src;
+    if (l.m_src < 1 || l.m_src >= l.M - 1) return fail(LSFDTD_EINVAL, "line source node out of range");
+    for (int k = 0; k < 2; ++k) {
+      LineArgs<R>& a = l.corr[k];
+      l.has[k] = s->pts[k].n_nodes > 0;
+      a.n_nodes = s->pts[k].n_nodes;
+      a.nodes = reinterpret_cast<const long long*>(s->pts[k].nodes);
+      a.offsets = reinterpret_cast<const long long*>(s->pts[k].offsets);
+      a.i0 = reinterpret_cast<const long long*>(s->i0[k]);
+      a.w = static_cast<const R*>(s->w[k]);
+      a.coef = static_cast<const R*>(s->coef[k]);
+      a.src = k == 0 ? l.H : l.E;  // E corrections read the line's H, H corrections its E
+      a.target = reinterpret_cast<R*>(k == 0 ? desc.E : desc.H);
+    }
+    step_limit = std::min<int64_t>(step_limit, s->wave_len);
+    order.push_back({kLine, lines.size()});
+    lines.push_back(l);
+    return LSFDTD_OK;
+  }
+
+  int add_column(const lsfdtd_column_source_desc* s) override {
+    if (!kComplex) return fail(LSFDTD_EUNSUPPORTED, "a Bloch column source needs complex fields");
+    auto* col = dynamic_cast<Engine<F>*>(s->column);
+    if (!col) return fail(LSFDTD_EINVAL, "column engine of another precision");
+    if (col->desc.shape[0] != 3 || col->desc.shape[1] != 3) return fail(LSFDTD_EINVAL, "column must be 3 x 3 x nz");
+    if (s->k_src < 1 || s->k_src >= desc.shape[2] || s->k_src >= col->desc.shape[2] || s->k_launch < 0 ||
+        s->k_launch >= col->desc.shape[2])
+      return fail(LSFDTD_EINVAL, "column planes out of range");
+    Column c{};
+    c.col = col;
+    c.k_src = s->k_src;
+    c.k_launch = s->k_launch;
+    c.phase = static_cast<const F*>(s->phase);
+    if constexpr (kComplex) {
+      c.amp0 = F{R(s->amp[0][0]), R(s->amp[0][1])};
+      c.amp1 = F{R(s->amp[1][0]), R(s->amp[1][1])};
+    }
+    c.wave = static_cast<const R*>(s->wave);
+    c.cE = R(s->cE);
+    c.cH = R(s->cH);
+    step_limit = std::min<int64_t>(step_limit, s->wave_len);
+    order.push_back({kColumn, columns.size()});
+    columns.push_back(c);
+    return LSFDTD_OK;
+  }
+
+  int add_mode(const lsfdtd_mode_source_desc* s) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "a mode source needs real fields");
+    if (s->r_e < 1 || s->r_h < 1) return fail(LSFDTD_EINVAL, "mode source rank < 1");
+    step_limit = std::min<int64_t>(step_limit, std::min(s->len_E, s->len_H));
+    order.push_back({kMode, modes.size()});
+    modes.push_back(Mode{*s});
+    return LSFDTD_OK;
+  }
+
+  int add_monitor(const lsfdtd_monitor_desc* m) override {
+    Monitor q{};
+    q.space = m->space;
+    q.energy = (m->energy && m->n_h > 0) ? m->energy : 0;
+    if (q.energy < 0 || q.energy > 2) return fail(LSFDTD_EINVAL, "monitor energy group must be 0, 1 or 2");
+    if (m->space < 0 || m->space > 2) return fail(LSFDTD_EINVAL, "monitor space out of range");
+    if (m->space == 2 && !kComplex) return fail(LSFDTD_EINVAL, "a column space needs complex fields");
+    auto fill = [&](auto& a, auto* src_e, auto* src_h) {
+      a.nf = m->n_freq;
+      a.omega = m->omega;
+      a.ne = m->n_e;
+      a.nh = m->n_h;
+      a.e_idx = reinterpret_cast<const long long*>(m->e_idx);
+      a.h1 = reinterpret_cast<const long long*>(m->h_idx1);
+      a.h2 = reinterpret_cast<const long long*>(m->h_idx2);
+      a.acc_e = static_cast<cplx<double>*>(m->acc_e);
+      a.acc_h = static_cast<cplx<double>*>(m->acc_h);
+      a.Esrc = src_e;
+      a.Hsrc = src_h;
+      a.dt = desc.dt;
+      a.nstep = reinterpret_cast<const long long*>(desc.step);
+      a.want_energy = q.energy ? 1 : 0;
+      a.partial = nullptr;
+      a.blocks_e = cdiv(m->n_e, kMonBlock);
+    };
+    if (m->space == 1)
+      fill(q.ar, static_cast<const R*>(m->E_src), static_cast<const R*>(m->H_src));
+    else
+      fill(q.af, static_cast<const F*>(m->E_src), static_cast<const F*>(m->H_src));
+    q.blocks = (long long)cdiv(m->n_e, kMonBlock) + (m->n_h > 0 ? cdiv(m->n_h, kMonBlock) : 0);
+    if (m->n_e <= 0 || m->n_freq <= 0) return fail(LSFDTD_EINVAL, "empty monitor");
+    monitors.push_back(q);
+    layout_energy();
+    return LSFDTD_OK;
+  }
+
+  // energy partials: group 1's monitors first, then group 2's, each block one double
+  void layout_energy() {
+    long long off = 0;
+    for (int g = 1; g <= 2; ++g) {
+      e_first[g - 1] = off;
+      long long cnt = 0;
+      for (auto& q : monitors)
+        if (q.energy == g) cnt += q.blocks;
+      e_count[g - 1] = cnt;
+      off += cnt;
+    }
+  }
+
+  size_t need_scratch() const override { return (size_t)(e_count[0] + e_count[1]) * sizeof(double); }
+
+  int ghosts(F* f, bool low, cudaStream_t s) {
+    for (int a = 0; a < 3; ++a) {
+      if (!desc.periodic[a]) continue;
+      const int n = desc.shape[a];
+      const int dst = low ? 0 : n - 1, src = low ? n - 2 : 1;
+      const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
+      const int na = a == 0 ? desc.shape[1] : desc.shape[0], nb = a == 2 ? desc.shape[1] : desc.shape[2];
+      const long long tot = 3LL * na * nb;
+      k_ghost<F><<<cdiv(tot, 256), 256, 0, s>>>(f, f + cells, f + 2 * cells, desc.shape[0], desc.shape[1],
+                                                 desc.shape[2], a, dst, src, bloch_re[a][low ? 0 : 1],
+                                                 bloch_im[a][low ? 0 : 1]);
+      LS_LAUNCHED();
+    }
+    return LSFDTD_OK;
+  }
+
+  dim3 bulk_grid() const { return dim3(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], 8), desc.shape[0]); }
+
+  int mark(cudaStream_t s, bool begin) {
+    if (!timing) return LSFDTD_OK;
+    cudaEvent_t ev;
+    LS_CUDA(cudaEventCreate(&ev));
+    if (begin) {
+      timing->push_back({ev, nullptr});
+    } else {
+      timing->back().second = ev;
+    }
+    LS_CUDA(cudaEventRecord(ev, s));
+    return LSFDTD_OK;
+  }
+
+  int update_h(cudaStream_t s) override {
+    LS_TRY(ghosts(Eflat(), false, s));
+    LS_TRY(mark(s, true));
+    k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(y);
+    LS_LAUNCHED();
+    LS_TRY(mark(s, false));
+    return LSFDTD_OK;
+  }
+
+  int update_e(cudaStream_t s) override {
+    LS_TRY(ghosts(Hflat(), true, s));
+    LS_TRY(mark(s, true));
+    k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(y);
+    LS_LAUNCHED();
+    LS_TRY(mark(s, false));
+    return LSFDTD_OK;
+  }
+
+  const long long* nstep() const { return reinterpret_cast<const long long*>(desc.step); }
+
+  int hook(int which, cudaStream_t s) {  // 0 correct_H, 1 advance_H, 2 correct_E, 3 advance_E
+    for (auto& o : order) {
+      switch (o.first) {
+        case kTable: {
+          Table& t = tables[o.second];
+          const int k = which == 0 ? 1 : 0;
+          if ((which == 0 || which == 2) && t.has[k]) {
+            k_table_correct<R><<<cdiv(t.corr[k].n_nodes, 128), 128, 0, s>>>(t.corr[k]);
+            LS_LAUNCHED();
+          }
+          if (which == 3 && t.view) {
+            k_table_view<R><<<1, 32, 0, s>>>(t.Tinc, t.corr[0].m, t.corr[0].cmax, t.inc_base, t.inc_i0, t.inc_u0,
+                                             t.view, nstep());
+            LS_LAUNCHED();
+          }
+          break;
+        }
+        case kDipole: {
+          Dipole& d = dipoles[o.second];
+          if (which == 2 && d.n > 0) {
+            k_dipole<R><<<cdiv(d.n, 64), 64, 0, s>>>(reinterpret_cast<R*>(desc.E), d.idx, d.coef, d.n, d.wave,
+                                                      nstep());
+            LS_LAUNCHED();
+          }
+          break;
+        }
+        case kLine: {
+          Line& l = lines[o.second];
+          const int k = which == 0 ? 1 : 0;
+          if ((which == 0 || which == 2) && l.has[k]) {
+            k_line_correct<R><<<cdiv(l.corr[k].n_nodes, 128), 128, 0, s>>>(l.corr[k]);
+            LS_LAUNCHED();
+          }
+          if (which == 1) {
+            k_line_h<R><<<cdiv(l.M, 128), 128, 0, s>>>(l.E, l.H, l.da, l.db, l.M);
+            LS_LAUNCHED();
+          }
+          if (which == 3) {
+            k_line_e<R><<<cdiv(l.M, 128), 128, 0, s>>>(l.E, l.H, l.ca, l.cb, l.M, l.m_src, l.wave, nstep());
+            LS_LAUNCHED();
+          }
+          break;
+        }
+        case kColumn: {
+          Column& c = columns[o.second];
+          auto* col = static_cast<Engine<F>*>(c.col);
+          const int nx = desc.shape[0] - 2, ny = desc.shape[1] - 2, ncz = col->desc.shape[2];
+          const long long ccells = 9LL * ncz;
+          if (which == 0 || which == 2) {
+            F* t0 = which == 0 ? y.H[0] : y.E[0];
+            F* t1 = which == 0 ? y.H[1] : y.E[1];
+            const F* src = which == 0 ? col->Eflat() : col->Hflat();
+            k_column_plane<F><<<cdiv((long long)nx * ny, 128), 128, 0, s>>>(
+                t0, t1, src, src + ccells, c.phase, nx, ny, desc.shape[1], desc.shape[2], c.k_src, ncz,
+                which == 0 ? c.cH : c.cE, which == 0 ? 0 : 1);
+            LS_LAUNCHED();
+          }
+          if (which == 1) LS_TRY(col->update_h(s));
+          if (which == 3) {
+            LS_TRY(col->update_e(s));
+            F* e = col->Eflat();
+            k_column_sheet<F><<<1, 32, 0, s>>>(e, e + ccells, ncz, c.k_launch, c.amp0, c.amp1, c.wave, nstep());
+            LS_LAUNCHED();
+          }
+          break;
+        }
+        case kMode: {
+          const lsfdtd_mode_source_desc& d = modes[o.second].d;
+          if (which == 0 && d.n_h > 0) {
+            k_mode<R><<<cdiv(d.n_h, 128), 128, 0, s>>>(reinterpret_cast<R*>(desc.H),
+                                                       reinterpret_cast<const long long*>(d.h_idx),
+                                                       static_cast<const R*>(d.mH), static_cast<const R*>(d.tab_E),
+                                                       d.n_h, d.r_e, nstep());
+            LS_LAUNCHED();
+          }
+          if (which == 2 && d.n_e > 0) {
+            k_mode<R><<<cdiv(d.n_e, 128), 128, 0, s>>>(reinterpret_cast<R*>(desc.E),
+                                                       reinterpret_cast<const long long*>(d.e_idx),
+                                                       static_cast<const R*>(d.mE), static_cast<const R*>(d.tab_H),
+                                                       d.n_e, d.r_h, nstep());
+            LS_LAUNCHED();
+          }
+          break;
+        }
+      }
+    }
+    return LSFDTD_OK;
+  }
+
+  int step(cudaStream_t s) override {
+    LS_TRY(update_h(s));
+    LS_TRY(hook(0, s));
+    LS_TRY(hook(1, s));
+    LS_TRY(update_e(s));
+    LS_TRY(hook(2, s));
+    for (auto& g : groups) {
+      if (g.n <= 0) continue;
+      k_ade<F><<<cdiv(g.n, 128), 128, 0, s>>>(g);
+      LS_LAUNCHED();
+    }
+    LS_TRY(hook(3, s));
+    k_bump<<<1, 32, 0, s>>>(reinterpret_cast<long long*>(desc.step));
+    LS_LAUNCHED();
+    return LSFDTD_OK;
+  }
+
+  int sample(cudaStream_t s) override {
+    if (!monitors.empty() && need_scratch() > 0 && scratch_bytes < need_scratch())
+      return fail(LSFDTD_EINVAL, "monitor scratch not set or too small");
+    double* part = static_cast<double*>(scratch);
+    long long off[2] = {e_first[0], e_first[1]};
+    for (auto& q : monitors) {
+      double* p = nullptr;
+      if (q.energy) {
+        p = part + off[q.energy - 1];
+        off[q.energy - 1] += q.blocks;
+      }
+      if (q.space == 1) {
+        MonArgs<R> a = q.ar;
+        a.partial = p;
+        k_monitor<R><<<(unsigned)q.blocks, kMonBlock, 0, s>>>(a);
+      } else {
+        MonArgs<F> a = q.af;
+        a.partial = p;
+        k_monitor<F><<<(unsigned)q.blocks, kMonBlock, 0, s>>>(a);
+      }
+      LS_LAUNCHED();
+    }
+    if (e_count[0] + e_count[1] > 0) {
+      k_energy<<<1, 32, 0, s>>>(part, e_first[0], e_count[0], e_first[1], e_count[1], desc.energy);
+      LS_LAUNCHED();
+    }
+    return LSFDTD_OK;
+  }
+
+  int64_t launches_per_chunk() const override {
+    int64_t per_step = 2 + 1;  // H, E, counter
+    int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
+    per_step += 2 * nper;
+    for (auto& g : groups) per_step += g.n > 0;
+    for (auto& o : order) {
+      switch (o.first) {
+        case kTable: per_step += tables[o.second].has[0] + tables[o.second].has[1] + (tables[o.second].view ? 1 : 0); break;
+        case kDipole: per_step += 1; break;
+        case kLine: per_step += lines[o.second].has[0] + lines[o.second].has[1] + 2; break;
+        case kColumn: per_step += 2 + 1 + 2 + 2 * 2; break;  // planes, sheet, column H/E, column ghosts
+        case kMode: per_step += 2; break;
+      }
+    }
+    int64_t per_sample = (int64_t)monitors.size() + (e_count[0] + e_count[1] > 0 ? 1 : 0);
+    return per_step * desc.dft_stride + per_sample;
+  }
+};
+
+lsfdtd_engine* make_engine(const lsfdtd_grid_desc& g) {
+  if (g.precision == LSFDTD_F32) {
+    if (g.is_complex) return new Engine<cplx<float>>(g);
+    return new Engine<float>(g);
+  }
+  if (g.is_complex) return new Engine<cplx<double>>(g);
+  return new Engine<double>(g);
+}
+
+int run_chunk(lsfdtd_engine* e, cudaStream_t s) {
+  for (int i = 0; i < e->desc.dft_stride; ++i) LS_TRY(e->step(s));
+  return e->sample(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t lsfdtd_abi_version(void) { return LSFDTD_ABI_VERSION; }
+
+const char* lsfdtd_last_error(void) { return g_err.c_str(); }
+
+int32_t lsfdtd_cpml_slab(const int32_t shape[3], const int32_t periodic[3], int32_t axis, int32_t cells_lo,
+                         int32_t cells_hi, int32_t field, int32_t component, int32_t side, int32_t* start,
+                         int32_t* len) {
+  if (!shape || !periodic || !start || !len || axis < 0 || axis > 2 || field < 0 || field > 1 || component < 0 ||
+      component > 2 || side < 0 || side > 1)
+    return fail(LSFDTD_EINVAL, "lsfdtd_cpml_slab: argument out of range");
+  int st, ln;
+  slab(shape, periodic, axis, cells_lo, cells_hi, field, component, side, &st, &ln);
+  *start = st;
+  *len = ln;
+  return LSFDTD_OK;
+}
+
+int64_t lsfdtd_group_state_len(int32_t mixed, int32_t n_media, const int32_t* n_poles) {
+  return ade_state_len(mixed, n_media, n_poles);
+}
+
+int32_t lsfdtd_engine_create(const lsfdtd_grid_desc* grid, lsfdtd_engine** out) {
+  if (!grid || !out) return fail(LSFDTD_EINVAL, "null argument");
+  *out = nullptr;
+  for (int a = 0; a < 3; ++a) {
+    if (grid->shape[a] < 3) return fail(LSFDTD_EINVAL, "every axis needs at least 3 nodes");
+    if (!(grid->spacing[a] > 0)) return fail(LSFDTD_EINVAL, "spacing must be positive");
+    if (grid->bloch[a] != 0 && !grid->periodic[a]) return fail(LSFDTD_EINVAL, "a Bloch wavevector needs a periodic axis");
+  }
+  const bool any_bloch = grid->bloch[0] != 0 || grid->bloch[1] != 0 || grid->bloch[2] != 0;
+  if (any_bloch && !grid->is_complex) return fail(LSFDTD_EINVAL, "a Bloch wavevector needs complex fields");
+  if (grid->precision != LSFDTD_F32 && grid->precision != LSFDTD_F64) return fail(LSFDTD_EINVAL, "unknown precision");
+  if (grid->dft_stride < 1) return fail(LSFDTD_EINVAL, "dft_stride < 1");
+  if (!grid->E || !grid->H || !grid->cbE[0] || !grid->cbE[1] || !grid->cbE[2] || !grid->step || !grid->energy)
+    return fail(LSFDTD_EINVAL, "grid arrays missing");
+  const double cells = (double)grid->shape[0] * grid->shape[1] * grid->shape[2];
+  if (cells * 3 > 9.0e18) return fail(LSFDTD_EINVAL, "grid too large");
+  *out = make_engine(*grid);
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_destroy(lsfdtd_engine* eng) {
+  delete eng;
+  return LSFDTD_OK;
+}
+
+#define LS_NEED(p)                                            \
+  do {                                                        \
+    if (!(p)) return fail(LSFDTD_EINVAL, "null argument"); \
+  } while (0)
+
+int32_t lsfdtd_engine_set_pml(lsfdtd_engine* eng, const lsfdtd_pml_desc* p) {
+  LS_NEED(eng && p);
+  return eng->set_pml(p);
+}
+int32_t lsfdtd_engine_add_group(lsfdtd_engine* eng, const lsfdtd_group_desc* g) {
+  LS_NEED(eng && g);
+  return eng->add_group(g);
+}
+int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s) {
+  LS_NEED(eng && s);
+  return eng->add_table(s);
+}
+int32_t lsfdtd_engine_add_dipole(lsfdtd_engine* eng, const lsfdtd_dipole_desc* s) {
+  LS_NEED(eng && s);
+  return eng->add_dipole(s);
+}
+int32_t lsfdtd_engine_add_line_source(lsfdtd_engine* eng, const lsfdtd_line_source_desc* s) {
+  LS_NEED(eng && s);
+  return eng->add_line(s);
+}
+int32_t lsfdtd_engine_add_column_source(lsfdtd_engine* eng, const lsfdtd_column_source_desc* s) {
+  LS_NEED(eng && s && s->column);
+  return eng->add_column(s);
+}
+int32_t lsfdtd_engine_add_mode_source(lsfdtd_engine* eng, const lsfdtd_mode_source_desc* s) {
+  LS_NEED(eng && s);
+  return eng->add_mode(s);
+}
+int32_t lsfdtd_engine_add_monitor(lsfdtd_engine* eng, const lsfdtd_monitor_desc* m) {
+  LS_NEED(eng && m);
+  return eng->add_monitor(m);
+}
+int32_t lsfdtd_engine_scratch_bytes(lsfdtd_engine* eng, size_t* bytes) {
+  LS_NEED(eng && bytes);
+  *bytes = eng->need_scratch();
+  return LSFDTD_OK;
+}
+int32_t lsfdtd_engine_set_scratch(lsfdtd_engine* eng, void* scratch, size_t bytes) {
+  LS_NEED(eng);
+  eng->scratch = scratch;
+  eng->scratch_bytes = bytes;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_step(lsfdtd_engine* eng, int32_t n_steps, void* stream) {
+  LS_NEED(eng);
+  if (n_steps < 0) return fail(LSFDTD_EINVAL, "n_steps < 0");
+  if (eng->n_host + n_steps > eng->step_limit)
+    return fail(LSFDTD_ERANGE, "the run would read a source waveform past its end");
+  auto s = static_cast<cudaStream_t>(stream);
+  for (int i = 0; i < n_steps; ++i) {
+    LS_TRY(eng->step(s));
+    eng->n_host += 1;
+  }
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_sample(lsfdtd_engine* eng, void* stream) {
+  LS_NEED(eng);
+  return eng->sample(static_cast<cudaStream_t>(stream));
+}
+
+int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_graph, void* stream) {
+  LS_NEED(eng);
+  if (n_chunks < 0) return fail(LSFDTD_EINVAL, "n_chunks < 0");
+  if (eng->n_host + (int64_t)n_chunks * eng->desc.dft_stride > eng->step_limit)
+    return fail(LSFDTD_ERANGE, "the run would read a source waveform past its end");
+  auto s = static_cast<cudaStream_t>(stream);
+  if (!use_graph) {
+    for (int c = 0; c < n_chunks; ++c) {
+      LS_TRY(run_chunk(eng, s));
+      eng->n_host += eng->desc.dft_stride;
+    }
+    return LSFDTD_OK;
+  }
+  if (n_chunks > 0 && !eng->exec) {
+    if (s == nullptr || s == cudaStreamLegacy) return fail(LSFDTD_EINVAL, "graph capture needs a created stream");
+    LS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int r = run_chunk(eng, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (r != LSFDTD_OK) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    eng->graph = g;
+    LS_CUDA(cudaGraphInstantiate(&eng->exec, g, 0));
+  }
+  for (int c = 0; c < n_chunks; ++c) {
+    LS_CUDA(cudaGraphLaunch(eng->exec, s));
+    eng->n_host += eng->desc.dft_stride;
+  }
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* stream, double* bulk_ms,
+                                  int64_t* bulk_launches) {
+  LS_NEED(eng && bulk_ms && bulk_launches);
+  if (n_chunks < 0) return fail(LSFDTD_EINVAL, "n_chunks < 0");
+  if (eng->n_host + (int64_t)n_chunks * eng->desc.dft_stride > eng->step_limit)
+    return fail(LSFDTD_ERANGE, "the run would read a source waveform past its end");
+  auto s = static_cast<cudaStream_t>(stream);
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  eng->timing = &ev;
+  int r = LSFDTD_OK;
+  for (int c = 0; c < n_chunks && r == LSFDTD_OK; ++c) {
+    r = run_chunk(eng, s);
+    if (r == LSFDTD_OK) eng->n_host += eng->desc.dft_stride;
+  }
+  eng->timing = nullptr;
+  cudaError_t e = cudaStreamSynchronize(s);
+  double tot = 0.0;
+  for (auto& p : ev) {
+    float ms = 0.f;
+    if (r == LSFDTD_OK && e == cudaSuccess && p.second && cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess)
+      tot += ms;
+    cudaEventDestroy(p.first);
+    if (p.second) cudaEventDestroy(p.second);
+  }
+  if (r != LSFDTD_OK) return r;
+  if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
+  *bulk_ms = tot;
+  *bulk_launches = (int64_t)ev.size();
+  return LSFDTD_OK;
+}
+
+int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng) { return eng ? eng->n_host : -1; }
+
+int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng) { return eng ? eng->launches_per_chunk() : -1; }
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+// Yee E/H curl updates with the CPML psi terms fused in, and the periodic (Bloch) ghost-plane refresh.
+//
+// Step semantics follow lightsmith's engine (backends/_fdtd/engine.py): H_c -= cH (dE_{d2}/dd1 - dE_{d1}/dd2)
+// with forward differences over H_c's stepped region (engine.py:630-635), E_c += cbE_c (dH_{d2}/dd1 -
+// dH_{d1}/dd2) with backward differences over E_c's region (engine.py:645-652), then the CPML terms of each
+// axis d != c: psi = b psi + c' der; F += k' der (kappa > 1 only); F += psi (engine.py:636-643, 656-663).
+// The derivative of a CPML term along d1 is the curl's own difference a, along d2 its b, so the psi update
+// reads no field value the curl did not already load.
+#pragma once
+
+#include "common.cuh"
+
+namespace lsfdtd {
+
+// One CPML axis: graded 1D profiles over the axis' node (E) and half-integer (H) positions, and the psi slabs.
+template <typename F>
+struct PmlAxis {
+  using R = typename real_of<F>::type;
+  int on;
+  const R* b[2];   // [E, H] profiles, length n_d
+  const R* c[2];
+  const R* k[2];   // (1/kappa - 1), null where kappa == 1 everywhere
+  R div;           // non-cubic cells: c' and k' carry 1/dx_d (1 for cubic cells)
+  // psi slab per [field E/H][component][side lo/hi]: start index along d, length, storage
+  int start[2][3][2];
+  int len[2][3][2];
+  F* psi[2][3][2];
+};
+
+template <typename F>
+struct YeeArgs {
+  using R = typename real_of<F>::type;
+  int n[3];
+  int periodic[3];
+  int uniform;     // cubic cells: coefficients carry dt/dx and differences are not rescaled
+  R inv_d[3];
+  R cH;
+  F* E[3];
+  F* H[3];
+  const R* cbE[3];  // per component, full grid (the three may alias one array)
+  PmlAxis<F> pml[3];
+};
+
+__device__ __forceinline__ bool in_e_region(int c, const int* x, const int* n, const int* per) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int lo = (per[a] || a != c) ? 1 : 0;
+    if (x[a] < lo || x[a] >= n[a] - 1) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool in_h_region(int c, const int* x, const int* n, const int* per) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int lo = per[a] ? 1 : 0;
+    int hi = per[a] ? n[a] - 1 : (a == c ? n[a] : n[a] - 1);
+    if (x[a] < lo || x[a] >= hi) return false;
+  }
+  return true;
+}
+
+// index of a psi slab entry: the cell's coordinates with axis d replaced by the offset into the slab
+__device__ __forceinline__ long long psi_index(const int* x, const int* n, int d, int off, int len) {
+  int i0 = d == 0 ? off : x[0];
+  int i1 = d == 1 ? off : x[1];
+  int i2 = d == 2 ? off : x[2];
+  int n1 = d == 1 ? len : n[1];
+  int n2 = d == 2 ? len : n[2];
+  return ((long long)i0 * n1 + i1) * n2 + i2;
+}
+
+// F += CPML terms of component c along every axis d != c. der1 / der2 are the raw differences along
+// d1 / d2; scale is the curl coefficient of this node (cH, or cbE of the node), FLD 0 = E, 1 = H.
+template <int FLD, typename F>
+__device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, const int* x, F der1, F der2,
+                                           typename real_of<F>::type scale) {
+  using R = typename real_of<F>::type;
+  const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (d == c) continue;
+    const PmlAxis<F>& p = g.pml[d];
+    if (!p.on) continue;
+    const F der = d == d1 ? der1 : der2;
+    // curl sign of the term: E_c gets +dH_{d2}/dd1 - dH_{d1}/dd2, H_c the opposite
+    R sgn = (d == d1) ? R(1) : R(-1);
+    if (FLD == 1) sgn = -sgn;
+    const int u = x[d];
+    R s = g.uniform ? scale : scale / p.div;
+    s = sgn * s;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int st = p.start[FLD][c][side], ln = p.len[FLD][c][side];
+      if (u < st || u >= st + ln) continue;
+      F* ps = p.psi[FLD][c][side] + psi_index(x, g.n, d, u - st, ln);
+      F psi = *ps * p.b[FLD][u];
+      if (p.k[FLD]) v += (s * p.k[FLD][u]) * der;
+      psi += der * (s * p.c[FLD][u]);
+      *ps = psi;
+      v += psi;
+    }
+  }
+}
+
+// H update: one thread per node (i, j, k), all three components.
+template <typename F>
+__global__ void __launch_bounds__(256) k_update_h(YeeArgs<F> g) {
+  using R = typename real_of<F>::type;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= g.n[2] || j >= g.n[1]) return;
+  const int x[3] = {i, j, k};
+  const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+  const long long p = i * s0 + j * s1 + k;
+  const long long step[3] = {s0, s1, 1};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!in_h_region(c, x, g.n, g.periodic)) continue;
+    const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const F a = g.E[d2][p + step[d1]] - g.E[d2][p];
+    const F b = g.E[d1][p + step[d2]] - g.E[d1][p];
+    F curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+    F h = g.H[c][p];
+    h = h - curl * g.cH;
+    apply_cpml<1>(h, g, c, x, a, b, g.cH);
+    g.H[c][p] = h;
+  }
+}
+
+// E update: one thread per node, all three components.
+template <typename F>
+__global__ void __launch_bounds__(256) k_update_e(YeeArgs<F> g) {
+  using R = typename real_of<F>::type;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= g.n[2] || j >= g.n[1]) return;
+  const int x[3] = {i, j, k};
+  const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+  const long long p = i * s0 + j * s1 + k;
+  const long long step[3] = {s0, s1, 1};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!in_e_region(c, x, g.n, g.periodic)) continue;
+    const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    const F a = g.H[d2][p] - g.H[d2][p - step[d1]];
+    const F b = g.H[d1][p] - g.H[d1][p - step[d2]];
+    F curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+    const R cb = g.cbE[c][p];
+    F e = g.E[c][p];
+    e = e + curl * cb;
+    apply_cpml<0>(e, g, c, x, a, b, cb);
+    g.E[c][p] = e;
+  }
+}
+
+// Periodic ghost planes of one axis: dst plane <- src plane times a Bloch phase (engine.py:595-611).
+template <typename F>
+__global__ void k_ghost(F* f0, F* f1, F* f2, int n0, int n1, int n2, int axis, int dst, int src, double ph_re,
+                        double ph_im) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  // the plane normal to `axis`: enumerate its two other coordinates
+  int na = axis == 0 ? n1 : n0, nb = axis == 2 ? n1 : n2;
+  if (t >= 3 * na * nb) return;
+  const int comp = t / (na * nb);
+  const int r = t % (na * nb);
+  const int u = r / nb, v = r % nb;
+  int xd[3], xs[3];
+  if (axis == 0) { xd[0] = dst; xs[0] = src; xd[1] = xs[1] = u; xd[2] = xs[2] = v; }
+  else if (axis == 1) { xd[1] = dst; xs[1] = src; xd[0] = xs[0] = u; xd[2] = xs[2] = v; }
+  else { xd[2] = dst; xs[2] = src; xd[0] = xs[0] = u; xd[1] = xs[1] = v; }
+  F* f = comp == 0 ? f0 : (comp == 1 ? f1 : f2);
+  const long long pd = ((long long)xd[0] * n1 + xd[1]) * n2 + xd[2];
+  const long long ps = ((long long)xs[0] * n1 + xs[1]) * n2 + xs[2];
+  f[pd] = apply_phase<F>(f[ps], ph_re, ph_im);
+}
+
+}  // namespace lsfdtd

@@ -384,6 +384,13 @@ def _media_plan(media):
             for m in media]
 
 
+def _inv_eps(inv_eps, shape):
+    a = np.asarray(inv_eps)
+    if a.shape == tuple(shape):
+        return a
+    return np.asarray(a, dtype=float).reshape((3,) + tuple(shape))
+
+
 def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors, dft_stride,
               periodic=(False, False, False), bloch=(0.0, 0.0, 0.0), offdiag=None, time_monitors=(),
               mirror=(0, 0, 0), widths=None) -> dict:
@@ -414,7 +421,8 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
     plan = {
         "shape": shape, "spacing": spacing, "dt": float(dt), "single": bool(single), "periodic": periodic,
         "bloch": bloch, "complex": any(bloch), "stride": int(dft_stride),
-        "inv_eps": np.asarray(inv_eps, dtype=float).reshape((3,) + shape),
+        # (3, N0, N1, N2) per component, or (N0, N1, N2) when eps is isotropic everywhere
+        "inv_eps": _inv_eps(inv_eps, shape),
         "pml": {"cells": tuple(tuple(int(v) for v in c) for c in pml.cells), "m": float(pml.m),
                 "kappa_max": float(pml.kappa_max), "alpha_max": float(pml.alpha_max), "eps_ref": float(pml.eps_ref),
                 "eps_ref_high": None if pml.eps_ref_high is None else float(pml.eps_ref_high)},

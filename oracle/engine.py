@@ -58,6 +58,8 @@ class OracleEngine:
         # the coefficients carry dt alone (engine.py:274-276, 622-627)
         cdx = self.dt / self.spacing[0] if self.uniform else self.dt
         inv_eps = plan["inv_eps"]
+        if inv_eps.ndim == 3:  # isotropic: one array for every component
+            inv_eps = np.broadcast_to(inv_eps, (3,) + inv_eps.shape)
         self.cbE = [np.asarray(cdx * inv_eps[c][tuple(_sl(r) for r in self.RE[c])], self.rdt) for c in range(3)]
         self.cH = cdx
         self.inv_d = tuple(1.0 / d for d in self.spacing)

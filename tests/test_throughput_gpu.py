@@ -1,0 +1,68 @@
+"""The throughput workload (random eps, CPML 16, centre dipole, 16-frequency DFT plane) on the GPU: against
+the oracle at 128^3, and through size-independent properties at the full 640^3 size."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def test_throughput_case_matches_oracle_at_128():
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+    from oracle.engine import OracleEngine
+
+    plan = throughput_plan(128, max_steps=4000, seed=3, single=False)
+    ref = OracleEngine(plan, threads=8)
+    gpu64 = Engine.from_plan(plan, precision="double")
+    gpu32 = Engine.from_plan(plan, precision="single")
+    for _ in range(3):
+        ref.chunk()
+        gpu64.chunk(1, use_graph=True)
+        gpu32.chunk(1, use_graph=True)
+    ref.close()
+    assert np.abs(ref.E).max() > 0
+    assert _rel(gpu64.E.cpu().numpy(), ref.E) < 1e-9
+    assert _rel(gpu64.results(0)[0], ref.monitors[0]["acc_e"]) < 1e-9
+    # float32 fields against the float64 oracle
+    assert _rel(gpu32.E.cpu().numpy(), ref.E) < 3e-4
+    assert _rel(gpu32.results(0)[1], ref.monitors[0]["acc_h"]) < 3e-4
+    np.testing.assert_allclose(gpu32.energy.cpu().numpy()[0], ref.energy[0], rtol=1e-3)
+
+
+@pytest.mark.slow
+def test_full_size_run_is_linear_in_the_source_bit_for_bit():
+    """Every update is linear in the fields, and scaling by 2 is exact in binary floating point: doubling the
+    source current must double every field value exactly, at the full 640^3 size."""
+    import torch
+
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+
+    n = 640
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    inv = 1.0 / (torch.rand((n, n, n), generator=gen, device="cuda", dtype=torch.float32) * 11.25 + 1.0)
+    plan = throughput_plan(n, inv_eps=inv, max_steps=3000)
+    # start the pulse early so that a short run carries a sizeable field
+    w = plan["sources"][0].wave
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    plan["sources"][0].wave = np.concatenate([w[first:], np.zeros(first)])
+    a = Engine.from_plan(plan)
+    a.chunk(2, use_graph=True)
+    e1 = a.E[:, ::7, ::5, ::3].clone()
+    h1 = a.H[:, ::5, ::7, ::3].clone()
+    acc1 = a.monitors[0]["acc_e"].clone()
+    a.close()
+    del a
+    plan["sources"][0].coef = 2 * plan["sources"][0].coef
+    b = Engine.from_plan(plan)
+    b.chunk(2, use_graph=True)
+    assert float(e1.abs().max()) > 0
+    assert torch.equal(b.E[:, ::7, ::5, ::3], 2 * e1)
+    assert torch.equal(b.H[:, ::5, ::7, ::3], 2 * h1)
+    assert torch.equal(b.monitors[0]["acc_e"], 2 * acc1)
+    b.close()
