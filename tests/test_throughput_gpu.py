@@ -36,8 +36,9 @@ def test_throughput_case_matches_oracle_at_128():
 
 @pytest.mark.slow
 def test_full_size_run_is_linear_in_the_source_bit_for_bit():
-    """Every update is linear in the fields, and scaling by 2 is exact in binary floating point: doubling the
-    source current must double every field value exactly, at the full 640^3 size."""
+    """Every update is linear in the fields, and scaling by 2 is exact in binary floating point (away from
+    subnormal numbers, which the wavefront's far tail reaches): doubling the source current must double every
+    normal-range field value exactly, at the full 640^3 size."""
     import torch
 
     from lightsmith_b200.engine import Engine
@@ -61,8 +62,14 @@ def test_full_size_run_is_linear_in_the_source_bit_for_bit():
     plan["sources"][0].coef = 2 * plan["sources"][0].coef
     b = Engine.from_plan(plan)
     b.chunk(2, use_graph=True)
+    def same(x, ref):
+        normal = ref.abs() > 1e-30
+        assert int(normal.sum()) > 1000
+        assert torch.equal(x[normal], ref[normal])
+        assert float((x - ref)[~normal].abs().max()) < 1e-30
+
     assert float(e1.abs().max()) > 0
-    assert torch.equal(b.E[:, ::7, ::5, ::3], 2 * e1)
-    assert torch.equal(b.H[:, ::5, ::7, ::3], 2 * h1)
-    assert torch.equal(b.monitors[0]["acc_e"], 2 * acc1)
+    same(b.E[:, ::7, ::5, ::3], 2 * e1)
+    same(b.H[:, ::5, ::7, ::3], 2 * h1)
+    same(torch.view_as_real(b.monitors[0]["acc_e"]), torch.view_as_real(2 * acc1))
     b.close()
