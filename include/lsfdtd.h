@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LSFDTD_ABI_VERSION 1
+#define LSFDTD_ABI_VERSION 2
 
 enum { LSFDTD_F32 = 0, LSFDTD_F64 = 1 };
 enum {
@@ -55,6 +55,11 @@ typedef struct {
   const void* cbE[3];  /* device, field precision (real) */
   int64_t* step;       /* device, one int64 */
   double* energy;      /* device, two doubles */
+  /* optional second E/H buffers (zeroed, same layout): with them a run without periodic axes whose sources
+   * only correct E advances each step in one fused pass, alternating between the two buffers
+   * (lsfdtd_engine_buffer tells which holds the current fields); NULL: in-place kernels */
+  void* E_alt;
+  void* H_alt;
 } lsfdtd_grid_desc;
 
 /* One CPML axis (Engine._build_pml, engine.py:344-418). Profiles have one entry per node position along the
@@ -68,6 +73,7 @@ typedef struct {
   const void* c[2];
   const void* k[2];
   void* psi[2][3][2];
+  void* psi_alt[3][2]; /* second H psi slabs, used with the grid's second buffers (else NULL) */
 } lsfdtd_pml_desc;
 
 /* D-form ADE nodes (the _Group of engine.py:722-793). Pure group: one dispersive medium. Mixed group
@@ -232,6 +238,13 @@ int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_gr
  * `stream`, then returns the summed kernel time (ms) and the number of such launches. */
 int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* stream, double* bulk_ms,
                                   int64_t* bulk_launches);
+/* which buffer holds the current E/H: 0 the grid's E/H, 1 its E_alt/H_alt */
+int32_t lsfdtd_engine_buffer(const lsfdtd_engine* eng);
+/* whether steps run as the fused single pass (1) or the in-place H and E kernels (0); valid once the
+ * engine is fully described (it is decided at the first step) */
+int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
+/* launch shape of the fused pass: tile_y nodes along y per CTA (8 or 16) and x planes per CTA (>= 1) */
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes);
 /* steps completed so far, as the host has launched them */
 int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng);
 /* kernel launches one chunk issues (for launch accounting) */

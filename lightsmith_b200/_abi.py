@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "liblsfdtd.so")
 F32, F64 = 0, 1
 OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE = 0, 1, 2, 3, 4
 MAX_MEDIA, MAX_POLES = 4, 6
+ABI_VERSION = 2
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -25,12 +26,12 @@ f64 = C.c_double
 class GridDesc(C.Structure):
     _fields_ = [("shape", i32 * 3), ("precision", i32), ("is_complex", i32), ("periodic", i32 * 3),
                 ("spacing", f64 * 3), ("dt", f64), ("bloch", f64 * 3), ("dft_stride", i32),
-                ("E", vp), ("H", vp), ("cbE", vp * 3), ("step", vp), ("energy", vp)]
+                ("E", vp), ("H", vp), ("cbE", vp * 3), ("step", vp), ("energy", vp), ("E_alt", vp), ("H_alt", vp)]
 
 
 class PmlDesc(C.Structure):
     _fields_ = [("axis", i32), ("cells_lo", i32), ("cells_hi", i32), ("b", vp * 2), ("c", vp * 2), ("k", vp * 2),
-                ("psi", ((vp * 2) * 3) * 2)]
+                ("psi", ((vp * 2) * 3) * 2), ("psi_alt", (vp * 2) * 3)]
 
 
 class GroupDesc(C.Structure):
@@ -99,6 +100,9 @@ SIGNATURES = {
     "lsfdtd_engine_sample": (i32, [vp, vp]),
     "lsfdtd_engine_chunk": (i32, [vp, i32, i32, vp]),
     "lsfdtd_engine_chunk_timed": (i32, [vp, i32, vp, C.POINTER(f64), C.POINTER(i64)]),
+    "lsfdtd_engine_buffer": (i32, [vp]),
+    "lsfdtd_engine_fused": (i32, [vp]),
+    "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32]),
     "lsfdtd_engine_steps": (i64, [vp]),
     "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
 }
@@ -122,6 +126,9 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        if L.lsfdtd_abi_version() != ABI_VERSION:
+            raise ImportError(f"{LIB_PATH} has ABI {L.lsfdtd_abi_version()}, this binding expects {ABI_VERSION}; "
+                              "rebuild it")
         _lib = L
     return _lib
 

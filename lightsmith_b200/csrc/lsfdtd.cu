@@ -14,6 +14,7 @@
 
 #include "ade.cuh"
 #include "common.cuh"
+#include "fused.cuh"
 #include "monitors.cuh"
 #include "sources.cuh"
 #include "yee.cuh"
@@ -89,13 +90,18 @@ struct lsfdtd_engine {
   int64_t step_limit = std::numeric_limits<int64_t>::max();
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
-  cudaGraphExec_t exec = nullptr;
-  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};  // one captured chunk per starting buffer
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  int cur = 0;          // buffer holding the current fields
+  int fused = -1;       // -1 undecided, 0 in-place kernels, 1 fused single pass
+  int tile_y = 8, planes = 128;
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    for (int b = 0; b < 2; ++b) {
+      if (exec[b]) cudaGraphExecDestroy(exec[b]);
+      if (graph[b]) cudaGraphDestroy(graph[b]);
+    }
   }
   virtual int set_pml(const lsfdtd_pml_desc* p) = 0;
   virtual int add_group(const lsfdtd_group_desc* g) = 0;
@@ -111,6 +117,7 @@ struct lsfdtd_engine {
   virtual int update_h(cudaStream_t s) = 0;
   virtual int update_e(cudaStream_t s) = 0;
   virtual int64_t launches_per_chunk() const = 0;
+  virtual int decide() = 0;
 };
 
 namespace {
@@ -191,12 +198,71 @@ struct Engine final : lsfdtd_engine {
       bloch_re[a][1] = std::cos(kl);
       bloch_im[a][1] = std::sin(kl);
     }
+    Ebuf[0] = static_cast<F*>(g.E);
+    Hbuf[0] = static_cast<F*>(g.H);
+    Ebuf[1] = static_cast<F*>(g.E_alt);
+    Hbuf[1] = static_cast<F*>(g.H_alt);
     y.uniform = (g.spacing[0] == g.spacing[1] && g.spacing[1] == g.spacing[2]) ? 1 : 0;
     y.cH = R(y.uniform ? g.dt / g.spacing[0] : g.dt);
   }
 
-  F* Eflat() const { return static_cast<F*>(desc.E); }
-  F* Hflat() const { return static_cast<F*>(desc.H); }
+  F* Ebuf[2] = {nullptr, nullptr};
+  F* Hbuf[2] = {nullptr, nullptr};
+  F* psiH[2][3][3][2] = {};  // H psi slabs per [buffer][axis][component][side]
+
+  F* Eflat() const { return Ebuf[cur]; }
+  F* Hflat() const { return Hbuf[cur]; }
+
+  // the fused single pass needs the second buffers, no periodic axis and sources that only correct E
+  int decide() override {
+    if (fused >= 0) return fused;
+    fused = 0;
+    if (kComplex || !Ebuf[1] || !Hbuf[1]) return 0;  // Bloch fields come with periodic axes
+    for (int a = 0; a < 3; ++a)
+      if (desc.periodic[a]) return 0;
+    for (auto& o : order)
+      if (o.first != kDipole) return 0;
+    for (int d = 0; d < 3; ++d) {
+      if (!y.pml[d].on) continue;
+      for (int c = 0; c < 3; ++c)
+        for (int sd = 0; sd < 2; ++sd)
+          if (y.pml[d].len[1][c][sd] > 0 && !psiH[1][d][c][sd]) return 0;
+    }
+    fused = 1;
+    return 1;
+  }
+
+  int fused_step(cudaStream_t s) {
+    const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
+    FusedArgs<F> fa;
+    fa.y = y;
+    const int o = cur ^ 1;
+    for (int a = 0; a < 3; ++a) {
+      fa.y.E[a] = Ebuf[cur] + a * cells;
+      fa.y.H[a] = Hbuf[cur] + a * cells;
+      fa.Eo[a] = Ebuf[o] + a * cells;
+      fa.Ho[a] = Hbuf[o] + a * cells;
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int c = 0; c < 3; ++c)
+        for (int sd = 0; sd < 2; ++sd) {
+          fa.y.pml[d].psi[1][c][sd] = psiH[cur][d][c][sd];
+          fa.psiHo[d][c][sd] = psiH[o][d][c][sd];
+        }
+    fa.seg = planes;
+    const dim3 grid(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], tile_y), cdiv(desc.shape[0], planes));
+    LS_TRY(mark(s, true));
+    if constexpr (!kComplex) {
+      if (tile_y == 16)
+        k_fused_step<F, 16><<<grid, dim3(32, 16), 0, s>>>(fa);
+      else
+        k_fused_step<F, 8><<<grid, dim3(32, 8), 0, s>>>(fa);
+    }
+    LS_LAUNCHED();
+    LS_TRY(mark(s, false));
+    cur = o;
+    return LSFDTD_OK;
+  }
 
   int set_pml(const lsfdtd_pml_desc* p) override {
     const int d = p->axis;
@@ -218,6 +284,10 @@ struct Engine final : lsfdtd_engine {
           q.len[f][c][s] = ln;
           q.psi[f][c][s] = static_cast<F*>(p->psi[f][c][s]);
           if (ln > 0 && !q.psi[f][c][s]) return fail(LSFDTD_EINVAL, "pml psi slab missing");
+          if (f == 1) {
+            psiH[0][d][c][s] = q.psi[f][c][s];
+            psiH[1][d][c][s] = static_cast<F*>(p->psi_alt[c][s]);
+          }
         }
     }
     return LSFDTD_OK;
@@ -228,7 +298,7 @@ struct Engine final : lsfdtd_engine {
     AdeArgs<F> a{};
     a.n = g->n;
     a.idx = reinterpret_cast<const long long*>(g->idx);
-    a.E = Eflat();
+    a.E = nullptr;  // the current buffer, set at launch
     a.n_media = g->n_media;
     a.mixed = g->mixed;
     a.has_h = g->has_h;
@@ -272,7 +342,7 @@ struct Engine final : lsfdtd_engine {
       a.i0 = reinterpret_cast<const long long*>(s->i0[k]);
       a.u0 = static_cast<const R*>(s->u0[k]);
       a.coef = static_cast<const R*>(s->coef[k]);
-      a.target = reinterpret_cast<R*>(k == 0 ? desc.E : desc.H);
+      a.target = nullptr;  // the current E (k = 0) or H buffer, set at launch
       a.nstep = reinterpret_cast<const long long*>(desc.step);
     }
     t.Tinc = static_cast<const R*>(s->inc_table);
@@ -318,7 +388,7 @@ struct Engine final : lsfdtd_engine {
       a.w = static_cast<const R*>(s->w[k]);
       a.coef = static_cast<const R*>(s->coef[k]);
       a.src = k == 0 ? l.H : l.E;  // E corrections read the line's H, H corrections its E
-      a.target = reinterpret_cast<R*>(k == 0 ? desc.E : desc.H);
+      a.target = nullptr;
     }
     step_limit = std::min<int64_t>(step_limit, s->wave_len);
     order.push_back({kLine, lines.size()});
@@ -470,7 +540,9 @@ struct Engine final : lsfdtd_engine {
           Table& t = tables[o.second];
           const int k = which == 0 ? 1 : 0;
           if ((which == 0 || which == 2) && t.has[k]) {
-            k_table_correct<R><<<cdiv(t.corr[k].n_nodes, 128), 128, 0, s>>>(t.corr[k]);
+            TableArgs<R> ta = t.corr[k];
+            ta.target = reinterpret_cast<R*>(k == 0 ? Eflat() : Hflat());
+            k_table_correct<R><<<cdiv(ta.n_nodes, 128), 128, 0, s>>>(ta);
             LS_LAUNCHED();
           }
           if (which == 3 && t.view) {
@@ -483,7 +555,7 @@ struct Engine final : lsfdtd_engine {
         case kDipole: {
           Dipole& d = dipoles[o.second];
           if (which == 2 && d.n > 0) {
-            k_dipole<R><<<cdiv(d.n, 64), 64, 0, s>>>(reinterpret_cast<R*>(desc.E), d.idx, d.coef, d.n, d.wave,
+            k_dipole<R><<<cdiv(d.n, 64), 64, 0, s>>>(reinterpret_cast<R*>(Eflat()), d.idx, d.coef, d.n, d.wave,
                                                       nstep());
             LS_LAUNCHED();
           }
@@ -493,7 +565,9 @@ struct Engine final : lsfdtd_engine {
           Line& l = lines[o.second];
           const int k = which == 0 ? 1 : 0;
           if ((which == 0 || which == 2) && l.has[k]) {
-            k_line_correct<R><<<cdiv(l.corr[k].n_nodes, 128), 128, 0, s>>>(l.corr[k]);
+            LineArgs<R> la = l.corr[k];
+            la.target = reinterpret_cast<R*>(k == 0 ? Eflat() : Hflat());
+            k_line_correct<R><<<cdiv(la.n_nodes, 128), 128, 0, s>>>(la);
             LS_LAUNCHED();
           }
           if (which == 1) {
@@ -532,14 +606,14 @@ struct Engine final : lsfdtd_engine {
         case kMode: {
           const lsfdtd_mode_source_desc& d = modes[o.second].d;
           if (which == 0 && d.n_h > 0) {
-            k_mode<R><<<cdiv(d.n_h, 128), 128, 0, s>>>(reinterpret_cast<R*>(desc.H),
+            k_mode<R><<<cdiv(d.n_h, 128), 128, 0, s>>>(reinterpret_cast<R*>(Hflat()),
                                                        reinterpret_cast<const long long*>(d.h_idx),
                                                        static_cast<const R*>(d.mH), static_cast<const R*>(d.tab_E),
                                                        d.n_h, d.r_e, nstep());
             LS_LAUNCHED();
           }
           if (which == 2 && d.n_e > 0) {
-            k_mode<R><<<cdiv(d.n_e, 128), 128, 0, s>>>(reinterpret_cast<R*>(desc.E),
+            k_mode<R><<<cdiv(d.n_e, 128), 128, 0, s>>>(reinterpret_cast<R*>(Eflat()),
                                                        reinterpret_cast<const long long*>(d.e_idx),
                                                        static_cast<const R*>(d.mE), static_cast<const R*>(d.tab_H),
                                                        d.n_e, d.r_h, nstep());
@@ -553,14 +627,20 @@ struct Engine final : lsfdtd_engine {
   }
 
   int step(cudaStream_t s) override {
-    LS_TRY(update_h(s));
-    LS_TRY(hook(0, s));
-    LS_TRY(hook(1, s));
-    LS_TRY(update_e(s));
+    if (decide()) {
+      LS_TRY(fused_step(s));
+    } else {
+      LS_TRY(update_h(s));
+      LS_TRY(hook(0, s));
+      LS_TRY(hook(1, s));
+      LS_TRY(update_e(s));
+    }
     LS_TRY(hook(2, s));
     for (auto& g : groups) {
       if (g.n <= 0) continue;
-      k_ade<F><<<cdiv(g.n, 128), 128, 0, s>>>(g);
+      AdeArgs<F> ga = g;
+      ga.E = Eflat();
+      k_ade<F><<<cdiv(ga.n, 128), 128, 0, s>>>(ga);
       LS_LAUNCHED();
     }
     LS_TRY(hook(3, s));
@@ -587,6 +667,10 @@ struct Engine final : lsfdtd_engine {
       } else {
         MonArgs<F> a = q.af;
         a.partial = p;
+        if (q.space == 0) {
+          a.Esrc = Eflat();
+          a.Hsrc = Hflat();
+        }
         k_monitor<F><<<(unsigned)q.blocks, kMonBlock, 0, s>>>(a);
       }
       LS_LAUNCHED();
@@ -599,7 +683,7 @@ struct Engine final : lsfdtd_engine {
   }
 
   int64_t launches_per_chunk() const override {
-    int64_t per_step = 2 + 1;  // H, E, counter
+    int64_t per_step = (fused == 1 ? 1 : 2) + 1;  // fused pass or H and E, counter
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
     for (auto& g : groups) per_step += g.n > 0;
@@ -761,23 +845,27 @@ int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_gr
     }
     return LSFDTD_OK;
   }
-  if (n_chunks > 0 && !eng->exec) {
-    if (s == nullptr || s == cudaStreamLegacy) return fail(LSFDTD_EINVAL, "graph capture needs a created stream");
-    LS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int r = run_chunk(eng, s);
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(s, &g);
-    if (r != LSFDTD_OK) {
-      if (g) cudaGraphDestroy(g);
-      return r;
-    }
-    if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
-    eng->graph = g;
-    LS_CUDA(cudaGraphInstantiate(&eng->exec, g, 0));
-  }
+  eng->decide();
   for (int c = 0; c < n_chunks; ++c) {
-    LS_CUDA(cudaGraphLaunch(eng->exec, s));
+    const int b = eng->cur;
+    if (!eng->exec[b]) {
+      if (s == nullptr || s == cudaStreamLegacy) return fail(LSFDTD_EINVAL, "graph capture needs a created stream");
+      LS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int r = run_chunk(eng, s);  // recorded, not run: it also advances the host's buffer index
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(s, &g);
+      eng->cur = b;
+      if (r != LSFDTD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+      eng->graph[b] = g;
+      LS_CUDA(cudaGraphInstantiate(&eng->exec[b], g, 0));
+    }
+    LS_CUDA(cudaGraphLaunch(eng->exec[b], s));
     eng->n_host += eng->desc.dft_stride;
+    if (eng->fused == 1 && (eng->desc.dft_stride & 1)) eng->cur ^= 1;
   }
   return LSFDTD_OK;
 }
@@ -810,6 +898,19 @@ int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* st
   if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
   *bulk_ms = tot;
   *bulk_launches = (int64_t)ev.size();
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_buffer(const lsfdtd_engine* eng) { return eng ? eng->cur : -1; }
+
+int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? eng->decide() : -1; }
+
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes) {
+  LS_NEED(eng);
+  if ((tile_y != 8 && tile_y != 16) || planes < 1) return fail(LSFDTD_EINVAL, "tuning: tile_y 8 or 16, planes >= 1");
+  if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "tuning must be set before the first graph capture");
+  eng->tile_y = tile_y;
+  eng->planes = planes;
   return LSFDTD_OK;
 }
 

@@ -55,16 +55,18 @@ class Engine:
         self._build(plan, _device_name(device), monitor_objs=list(monitors))
 
     @classmethod
-    def from_plan(cls, plan: dict, device="cuda:0", precision: str | None = None, monitor_objs=None) -> "Engine":
-        """An engine for a plain plan; ``precision`` ("single"/"double") overrides the plan's."""
+    def from_plan(cls, plan: dict, device="cuda:0", precision: str | None = None, monitor_objs=None,
+                  fused: bool | None = None) -> "Engine":
+        """An engine for a plain plan; ``precision`` ("single"/"double") overrides the plan's; ``fused=False``
+        keeps the in-place H and E kernels where the single pass would apply."""
         self = cls.__new__(cls)
         if precision is not None:
             plan = {**plan, "single": precision == "single"}
-        self._build(plan, _device_name(device), monitor_objs=monitor_objs)
+        self._build(plan, _device_name(device), monitor_objs=monitor_objs, fused=fused)
         return self
 
     # --- construction ---------------------------------------------------------------------------------------
-    def _build(self, plan: dict, device: str, monitor_objs=None):
+    def _build(self, plan: dict, device: str, monitor_objs=None, fused: bool | None = None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("lightsmith-b200 runs on a CUDA GPU (B200, sm_100a); no CUDA device is visible")
@@ -90,9 +92,15 @@ class Engine:
 
         with torch.cuda.device(self.dev):
             self.stream = torch.cuda.Stream(device=self.dev)
-            self.E = torch.zeros((3,) + self.shape, dtype=self.fdt, device=self.dev)
-            self.H = torch.zeros((3,) + self.shape, dtype=self.fdt, device=self.dev)
-            self.E_flat, self.H_flat = self.E.view(-1), self.H.view(-1)
+            self._E = [torch.zeros((3,) + self.shape, dtype=self.fdt, device=self.dev)]
+            self._H = [torch.zeros((3,) + self.shape, dtype=self.fdt, device=self.dev)]
+            # the fused single-pass step alternates between two field buffers; it serves runs without periodic
+            # axes whose sources only correct E (point dipoles)
+            self.double_buffered = (fused is not False and not any(self.periodic) and not self.complex and
+                                    all(isinstance(s, DipoleSource) for s in plan["sources"]))
+            if self.double_buffered:
+                self._E.append(torch.zeros_like(self._E[0]))
+                self._H.append(torch.zeros_like(self._H[0]))
             self.n = torch.zeros(1, dtype=torch.int64, device=self.dev)
             self.energy = torch.zeros(2, dtype=torch.float64, device=self.dev)
             inv_eps = plan["inv_eps"]
@@ -121,7 +129,9 @@ class Engine:
             g.dt = self.dt
             g.bloch[:] = list(plan["bloch"])
             g.dft_stride = self.stride
-            g.E, g.H = _ptr(self.E), _ptr(self.H)
+            g.E, g.H = _ptr(self._E[0]), _ptr(self._H[0])
+            if self.double_buffered:
+                g.E_alt, g.H_alt = _ptr(self._E[1]), _ptr(self._H[1])
             g.cbE[:] = [_ptr(t) for t in cb]
             g.step, g.energy = _ptr(self.n), _ptr(self.energy)
             h = C.c_void_p()
@@ -179,6 +189,8 @@ class Engine:
                             t = self._zeros(dims, self.fdt)
                             self.psi[(kind, comp, d, side)] = t
                             p.psi[f][comp][side] = _ptr(t)
+                            if kind == "H" and self.double_buffered:
+                                p.psi_alt[comp][side] = _ptr(self._zeros(dims, self.fdt))
             _abi.check(L.lsfdtd_engine_set_pml(self._h, C.byref(p)), "lsfdtd_engine_set_pml")
 
     def _build_group(self, gr, L):
@@ -341,7 +353,7 @@ class Engine:
         torch = _torch()
         kind, i = m["space"]
         if kind == "grid":
-            space, E_src, H_src = 0, self.E, self.H
+            space, E_src, H_src = 0, self._E[0], self._H[0]
         elif kind == "view":
             v = self._src_state[i]["view"]
             space, E_src, H_src = 1, v, v
@@ -439,6 +451,32 @@ class Engine:
     def release(self):
         """Nothing to drop between chunks; the captured graph lives until the engine is closed."""
         _torch().cuda.synchronize(self.dev)
+
+    @property
+    def E(self):
+        """The current E (3, N0, N1, N2): one of two buffers on the fused path."""
+        return self._E[int(_abi.lib().lsfdtd_engine_buffer(self._h))]
+
+    @property
+    def H(self):
+        return self._H[int(_abi.lib().lsfdtd_engine_buffer(self._h))]
+
+    @property
+    def E_flat(self):
+        return self.E.view(-1)
+
+    @property
+    def H_flat(self):
+        return self.H.view(-1)
+
+    @property
+    def fused(self) -> bool:
+        """Whether a step is the fused single pass (decided once the engine is described)."""
+        return bool(_abi.lib().lsfdtd_engine_fused(self._h))
+
+    def set_tuning(self, tile_y: int, planes: int) -> None:
+        """Launch shape of the fused pass (before the first graph capture)."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(tile_y), int(planes)), "lsfdtd_engine_set_tuning")
 
     @property
     def n_host(self) -> int:

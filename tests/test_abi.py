@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol(lib):
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) == set(_abi.SIGNATURES), "ctypes signatures out of step with the header"
-    assert lib.lsfdtd_abi_version() == 1
+    assert lib.lsfdtd_abi_version() == _abi.ABI_VERSION
 
 
 def test_cpml_slabs_match_plan_terms(lib):

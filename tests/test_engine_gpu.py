@@ -74,3 +74,43 @@ def test_source_waveform_end_raises(golden):
     with pytest.raises(LsfdtdError, match="waveform"):
         eng.step(n_wave + 1)
     eng.close()
+
+
+# cases the fused single pass serves (no periodic axis, point-dipole sources)
+FUSED_CASES = ["yee_cpml_dipole", "kappa_noncubic", "ade_groups"]
+
+
+@pytest.mark.parametrize("tile_y,planes", [(8, 3), (16, 5), (16, 128)])
+@pytest.mark.parametrize("case", FUSED_CASES)
+def test_fused_pass_any_launch_shape(case, tile_y, planes, golden):
+    """The fused pass under launch shapes that split x into several segments (each CTA then recomputes the
+    H plane before its segment) still matches lightsmith's engine."""
+    d = golden("engine_" + case)
+    plan, out = d["plan"], d["out"]
+    eng = _engine(plan, "double")
+    eng.set_tuning(tile_y, planes)
+    assert eng.fused
+    for _ in range(out["n_chunks"]):
+        eng.chunk(1, use_graph=True)
+    assert _rel(eng.E.cpu().numpy(), out["E"]) < TOL["double"]
+    assert _rel(eng.H.cpu().numpy(), out["H"]) < TOL["double"]
+    assert _rel(eng.results(0)[1], out["acc_h"][0]) < TOL["double"]
+    eng.close()
+
+
+@pytest.mark.parametrize("case", FUSED_CASES)
+def test_fused_pass_equals_in_place_kernels(case, golden):
+    from lightsmith_b200.engine import Engine
+
+    plan = golden("engine_" + case)["plan"]
+    a = Engine.from_plan(plan, precision="single")
+    b = Engine.from_plan(plan, precision="single", fused=False)
+    assert a.fused and not b.fused
+    a.set_tuning(8, 4)
+    for _ in range(5):
+        a.chunk(1, use_graph=True)
+        b.chunk(1, use_graph=True)
+    assert _rel(a.E.cpu().numpy(), b.E.cpu().numpy()) < 1e-6
+    assert _rel(a.H.cpu().numpy(), b.H.cpu().numpy()) < 1e-6
+    a.close()
+    b.close()

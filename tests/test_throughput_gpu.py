@@ -20,6 +20,8 @@ def test_throughput_case_matches_oracle_at_128():
     ref = OracleEngine(plan, threads=8)
     gpu64 = Engine.from_plan(plan, precision="double")
     gpu32 = Engine.from_plan(plan, precision="single")
+    gpu64.set_tuning(8, 40)  # several x segments per tile column
+    assert gpu64.fused and gpu32.fused
     for _ in range(3):
         ref.chunk()
         gpu64.chunk(1, use_graph=True)
