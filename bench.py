@@ -44,6 +44,9 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-y", type=int, default=8, help="fused pass: nodes along y per CTA (8 or 16)")
+    ap.add_argument("--planes", type=int, default=32, help="fused pass: x planes per CTA")
+    ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring (4, 6, 8)")
     return ap.parse_args()
 
 
@@ -195,6 +198,7 @@ def run_b200(args):
     inv = 1.0 / (torch.rand(shape, generator=gen, device=dev, dtype=torch.float32) * 11.25 + 1.0)
     plan = throughput_plan(n, inv_eps=inv, max_steps=stride * total_chunks + 8, single=True)
     eng = Engine.from_plan(plan, device=dev)
+    eng.set_tuning(args.tile_y, args.planes, args.stages)
     inv_host = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     inv_host.copy_(inv)
     del inv, plan["inv_eps"]
@@ -257,6 +261,8 @@ def run_b200(args):
     d2h = sum(a.numel() * a.element_size() for a in acc) + 16
     finite = bool(np.isfinite(energy_host.numpy()).all())
     launches = eng.launches_per_chunk() * K
+    eng_fused = eng.fused
+    eng_tma = eng.uses_tma
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -275,7 +281,10 @@ def run_b200(args):
                           "grid": list(shape), "cpml_cells": 16, "dft_freqs": 16, "dft_stride": stride,
                           "step": f"one chunk = {stride} FDTD steps + one DFT sample, CUDA graph replay",
                           "l2": "inputs larger than L2 (about 8 GB of state per replica)",
-                          "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+                          "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
+                          "kernel_path": "fused single pass" if eng_fused else "in-place H and E kernels",
+                          "tile": [32, args.tile_y], "planes_per_cta": args.planes, "ring_stages": args.stages,
+                          "copy_engine": "TMA" if eng_tma else "cp.async"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_source": peak_kind,
                             "traffic": None if tpc is None else tpc * cells,

@@ -30,7 +30,8 @@ enum {
   LSFDTD_EINVAL = 1,      /* bad argument or inconsistent description */
   LSFDTD_ECUDA = 2,       /* a CUDA call failed (the message names it) */
   LSFDTD_EUNSUPPORTED = 3,
-  LSFDTD_ERANGE = 4       /* the run would read a source waveform past its end */
+  LSFDTD_ERANGE = 4,      /* the run would read a source waveform past its end */
+  LSFDTD_ETIMEOUT = 5     /* a kernel gave up waiting for its own copies (bounded wait, status word set) */
 };
 #define LSFDTD_MAX_MEDIA 4
 #define LSFDTD_MAX_POLES 6
@@ -222,7 +223,8 @@ int32_t lsfdtd_engine_add_line_source(lsfdtd_engine* eng, const lsfdtd_line_sour
 int32_t lsfdtd_engine_add_column_source(lsfdtd_engine* eng, const lsfdtd_column_source_desc* s);
 int32_t lsfdtd_engine_add_mode_source(lsfdtd_engine* eng, const lsfdtd_mode_source_desc* s);
 int32_t lsfdtd_engine_add_monitor(lsfdtd_engine* eng, const lsfdtd_monitor_desc* m);
-/* bytes of device scratch the monitors' energy reduction needs; set it before the first sample */
+/* bytes of zeroed device scratch the engine needs (a status word, then the monitors' energy partials); set it
+ * before the first step */
 int32_t lsfdtd_engine_scratch_bytes(lsfdtd_engine* eng, size_t* bytes);
 int32_t lsfdtd_engine_set_scratch(lsfdtd_engine* eng, void* scratch, size_t bytes);
 
@@ -243,8 +245,17 @@ int32_t lsfdtd_engine_buffer(const lsfdtd_engine* eng);
 /* whether steps run as the fused single pass (1) or the in-place H and E kernels (0); valid once the
  * engine is fully described (it is decided at the first step) */
 int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
-/* launch shape of the fused pass: tile_y nodes along y per CTA (8 or 16) and x planes per CTA (>= 1) */
-int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes);
+/* launch shape of the fused pass: tile_y nodes along y per CTA (8 or 16), x planes per CTA (>= 1) and the
+ * depth of its copy ring in x planes (4, 6 or 8; the TMA ring) */
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes, int32_t stages);
+/* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting
+ * for its copies, else LSFDTD_OK */
+int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status);
+/* whether the fused pass may copy planes with the Tensor Memory Accelerator (default 1); before the first
+ * step. With 0, or where the layout rules it out (rows not a multiple of 16 bytes), it uses cp.async. */
+int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma);
+/* 1 when steps run the fused pass with TMA copies */
+int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng);
 /* steps completed so far, as the host has launched them */
 int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng);
 /* kernel launches one chunk issues (for launch accounting) */

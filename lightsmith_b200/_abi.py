@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblsfdtd.so")
 
 F32, F64 = 0, 1
-OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE = 0, 1, 2, 3, 4
+OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE, ETIMEOUT = 0, 1, 2, 3, 4, 5
 MAX_MEDIA, MAX_POLES = 4, 6
 ABI_VERSION = 2
 
@@ -101,8 +101,11 @@ SIGNATURES = {
     "lsfdtd_engine_chunk": (i32, [vp, i32, i32, vp]),
     "lsfdtd_engine_chunk_timed": (i32, [vp, i32, vp, C.POINTER(f64), C.POINTER(i64)]),
     "lsfdtd_engine_buffer": (i32, [vp]),
+    "lsfdtd_engine_status": (i32, [vp, vp, C.POINTER(i32)]),
+    "lsfdtd_engine_set_copy_engine": (i32, [vp, i32]),
+    "lsfdtd_engine_uses_tma": (i32, [vp]),
     "lsfdtd_engine_fused": (i32, [vp]),
-    "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32]),
+    "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32, i32]),
     "lsfdtd_engine_steps": (i64, [vp]),
     "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
 }

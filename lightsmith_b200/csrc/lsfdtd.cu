@@ -15,6 +15,9 @@
 #include "ade.cuh"
 #include "common.cuh"
 #include "fused.cuh"
+#include "fused_tma.cuh"
+
+#include <cudaTypedefs.h>
 #include "monitors.cuh"
 #include "sources.cuh"
 #include "yee.cuh"
@@ -94,7 +97,8 @@ struct lsfdtd_engine {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   int cur = 0;          // buffer holding the current fields
   int fused = -1;       // -1 undecided, 0 in-place kernels, 1 fused single pass
-  int tile_y = 8, planes = 128;
+  int tile_y = 8, planes = 128, stages = 4;
+  int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
@@ -118,9 +122,12 @@ struct lsfdtd_engine {
   virtual int update_e(cudaStream_t s) = 0;
   virtual int64_t launches_per_chunk() const = 0;
   virtual int decide() = 0;
+  virtual bool uses_tma() const = 0;
 };
 
 namespace {
+
+constexpr size_t kStatusBytes = 256;
 
 enum SrcKind { kTable, kDipole, kLine, kColumn, kMode };
 
@@ -209,6 +216,11 @@ struct Engine final : lsfdtd_engine {
   F* Ebuf[2] = {nullptr, nullptr};
   F* Hbuf[2] = {nullptr, nullptr};
   F* psiH[2][3][3][2] = {};  // H psi slabs per [buffer][axis][component][side]
+  int pml_cells[3][2] = {};
+  bool attr_set[2] = {false, false};
+  bool tma_ok = false;
+  CUtensorMap mapE[2][3], mapH[2][3], mapC;  // per buffer and component; the coefficient of component 0
+  static constexpr int kStages = 4;  // x planes in the fused pass's copy ring
 
   F* Eflat() const { return Ebuf[cur]; }
   F* Hflat() const { return Hbuf[cur]; }
@@ -229,7 +241,59 @@ struct Engine final : lsfdtd_engine {
           if (y.pml[d].len[1][c][sd] > 0 && !psiH[1][d][c][sd]) return 0;
     }
     fused = 1;
+    tma_ok = use_tma && make_maps() == LSFDTD_OK;
     return 1;
+  }
+
+  // 3D tensor maps (z fastest) of the field buffers and the coefficient, boxes as k_fused_tma copies them
+  bool uses_tma() const override { return tma_ok; }
+
+  template <int TY, int S>
+  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+    if constexpr (!kComplex) {
+      constexpr size_t sm = fused_tma_smem_bytes<F, TY, S>();
+      static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
+      if (!attr) {
+        LS_CUDA(cudaFuncSetAttribute(k_fused_tma<F, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+      }
+      k_fused_tma<F, TY, S><<<grid, dim3(32, TY), sm, s>>>(ta);
+    }
+    return LSFDTD_OK;
+  }
+
+  int make_maps() {
+    const size_t es = sizeof(F);
+    if ((desc.shape[2] * es) % 16 != 0) return LSFDTD_EUNSUPPORTED;
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+      cudaDriverEntryPointQueryResult q;
+      void* fn = nullptr;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !fn)
+        return LSFDTD_EUNSUPPORTED;
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const CUtensorMapDataType dt = sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
+    auto make = [&](CUtensorMap* m, const void* base, unsigned bz, unsigned by) -> bool {
+      if (reinterpret_cast<uintptr_t>(base) % 16) return false;
+      cuuint64_t dims[3] = {(cuuint64_t)desc.shape[2], (cuuint64_t)desc.shape[1], (cuuint64_t)desc.shape[0]};
+      cuuint64_t strides[2] = {(cuuint64_t)desc.shape[2] * es, (cuuint64_t)desc.shape[1] * desc.shape[2] * es};
+      cuuint32_t box[3] = {bz, by, 1};
+      cuuint32_t estr[3] = {1, 1, 1};
+      return encode(m, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const unsigned ty = (unsigned)tile_y;
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 3; ++c) {
+        if (!make(&mapE[b][c], Ebuf[b] + c * cells, 40, ty + 2)) return LSFDTD_EUNSUPPORTED;
+        if (!make(&mapH[b][c], Hbuf[b] + c * cells, 40, ty + 1)) return LSFDTD_EUNSUPPORTED;
+      }
+    if (!make(&mapC, y.cbE[0], 32, ty)) return LSFDTD_EUNSUPPORTED;
+    return LSFDTD_OK;
   }
 
   int fused_step(cudaStream_t s) {
@@ -250,13 +314,61 @@ struct Engine final : lsfdtd_engine {
           fa.psiHo[d][c][sd] = psiH[o][d][c][sd];
         }
     fa.seg = planes;
+    // nodes stepped for every component and outside every CPML slab, per axis
+    for (int ax = 0; ax < 3; ++ax) {
+      int lo = 1, hi = desc.shape[ax] - 1;
+      if (y.pml[ax].on) {
+        lo = std::max(lo, pml_cells[ax][0] ? pml_cells[ax][0] + 1 : 1);
+        hi = std::min(hi, pml_cells[ax][1] ? desc.shape[ax] - 2 - pml_cells[ax][1] : hi);
+      }
+      fa.inner_lo[ax] = lo;
+      fa.inner_hi[ax] = std::max(lo, hi);
+    }
     const dim3 grid(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], tile_y), cdiv(desc.shape[0], planes));
     LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
-      if (tile_y == 16)
-        k_fused_step<F, 16><<<grid, dim3(32, 16), 0, s>>>(fa);
-      else
-        k_fused_step<F, 8><<<grid, dim3(32, 8), 0, s>>>(fa);
+      if (tma_ok) {
+        TmaArgs<F> ta;
+        ta.f = fa;
+        for (int c = 0; c < 3; ++c) {
+          ta.mE[c] = mapE[cur][c];
+          ta.mH[c] = mapH[cur][c];
+        }
+        ta.mC = mapC;
+        ta.status = static_cast<int*>(scratch);
+        // the deepest ring, up to the requested depth, that fits the device's shared memory per CTA
+        int smax = 0, dev = 0;
+        LS_CUDA(cudaGetDevice(&dev));
+        LS_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        auto fits = [&](size_t b) { return b <= (size_t)smax; };
+        int r = LSFDTD_OK;
+        if (tile_y == 16) {
+          if (stages >= 8 && fits(fused_tma_smem_bytes<F, 16, 8>())) r = launch_tma<16, 8>(grid, ta, s);
+          else if (stages >= 6 && fits(fused_tma_smem_bytes<F, 16, 6>())) r = launch_tma<16, 6>(grid, ta, s);
+          else r = launch_tma<16, 4>(grid, ta, s);
+        } else {
+          if (stages >= 8 && fits(fused_tma_smem_bytes<F, 8, 8>())) r = launch_tma<8, 8>(grid, ta, s);
+          else if (stages >= 6 && fits(fused_tma_smem_bytes<F, 8, 6>())) r = launch_tma<8, 6>(grid, ta, s);
+          else r = launch_tma<8, 4>(grid, ta, s);
+        }
+        if (r != LSFDTD_OK) return r;
+      } else if (tile_y == 16) {
+        constexpr size_t sm = fused_smem_bytes<F, 16, kStages>();
+        if (!attr_set[1]) {
+          LS_CUDA(cudaFuncSetAttribute(k_fused_step<F, 16, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+          attr_set[1] = true;
+        }
+        k_fused_step<F, 16, kStages><<<grid, dim3(32, 16), sm, s>>>(fa);
+      } else {
+        constexpr size_t sm = fused_smem_bytes<F, 8, kStages>();
+        if (!attr_set[0]) {
+          LS_CUDA(cudaFuncSetAttribute(k_fused_step<F, 8, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+          attr_set[0] = true;
+        }
+        k_fused_step<F, 8, kStages><<<grid, dim3(32, 8), sm, s>>>(fa);
+      }
     }
     LS_LAUNCHED();
     LS_TRY(mark(s, false));
@@ -270,6 +382,8 @@ struct Engine final : lsfdtd_engine {
     if (desc.periodic[d]) return fail(LSFDTD_EINVAL, "a periodic axis cannot have a PML");
     PmlAxis<F>& q = y.pml[d];
     q.on = 1;
+    pml_cells[d][0] = p->cells_lo;
+    pml_cells[d][1] = p->cells_hi;
     q.div = y.uniform ? R(1) : R(desc.spacing[d]);
     for (int f = 0; f < 2; ++f) {
       q.b[f] = static_cast<const R*>(p->b[f]);
@@ -480,7 +594,8 @@ struct Engine final : lsfdtd_engine {
     }
   }
 
-  size_t need_scratch() const override { return (size_t)(e_count[0] + e_count[1]) * sizeof(double); }
+  // scratch: a status word (256 bytes reserved), then the energy partials
+  size_t need_scratch() const override { return kStatusBytes + (size_t)(e_count[0] + e_count[1]) * sizeof(double); }
 
   int ghosts(F* f, bool low, cudaStream_t s) {
     for (int a = 0; a < 3; ++a) {
@@ -627,6 +742,7 @@ struct Engine final : lsfdtd_engine {
   }
 
   int step(cudaStream_t s) override {
+    if (scratch_bytes < need_scratch()) return fail(LSFDTD_EINVAL, "scratch not set or too small");
     if (decide()) {
       LS_TRY(fused_step(s));
     } else {
@@ -650,9 +766,8 @@ struct Engine final : lsfdtd_engine {
   }
 
   int sample(cudaStream_t s) override {
-    if (!monitors.empty() && need_scratch() > 0 && scratch_bytes < need_scratch())
-      return fail(LSFDTD_EINVAL, "monitor scratch not set or too small");
-    double* part = static_cast<double*>(scratch);
+    if (scratch_bytes < need_scratch()) return fail(LSFDTD_EINVAL, "scratch not set or too small");
+    double* part = reinterpret_cast<double*>(static_cast<char*>(scratch) + kStatusBytes);
     long long off[2] = {e_first[0], e_first[1]};
     for (auto& q : monitors) {
       double* p = nullptr;
@@ -903,14 +1018,40 @@ int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* st
 
 int32_t lsfdtd_engine_buffer(const lsfdtd_engine* eng) { return eng ? eng->cur : -1; }
 
+int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status) {
+  LS_NEED(eng && status);
+  *status = 0;
+  if (!eng->scratch || eng->scratch_bytes < sizeof(int32_t)) return LSFDTD_OK;
+  int32_t v = 0;
+  auto s = static_cast<cudaStream_t>(stream);
+  LS_CUDA(cudaMemcpyAsync(&v, eng->scratch, sizeof(v), cudaMemcpyDeviceToHost, s));
+  LS_CUDA(cudaStreamSynchronize(s));
+  *status = v;
+  if (v) return fail(LSFDTD_ETIMEOUT, "a kernel gave up waiting for its copies (status word set)");
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma) {
+  LS_NEED(eng);
+  if (eng->fused >= 0) return fail(LSFDTD_EINVAL, "the copy engine must be chosen before the first step");
+  eng->use_tma = use_tma ? 1 : 0;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng) { return eng ? (eng->decide() && eng->uses_tma()) : -1; }
+
 int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? eng->decide() : -1; }
 
-int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes) {
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes, int32_t stages) {
   LS_NEED(eng);
-  if ((tile_y != 8 && tile_y != 16) || planes < 1) return fail(LSFDTD_EINVAL, "tuning: tile_y 8 or 16, planes >= 1");
+  if ((tile_y != 8 && tile_y != 16) || planes < 1 || (stages != 4 && stages != 6 && stages != 8))
+    return fail(LSFDTD_EINVAL, "tuning: tile_y 8 or 16, planes >= 1, stages 4, 6 or 8");
   if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "tuning must be set before the first graph capture");
+  if (eng->fused >= 0 && eng->tile_y != tile_y)
+    return fail(LSFDTD_EINVAL, "tile rows must be set before the first step");
   eng->tile_y = tile_y;
   eng->planes = planes;
+  eng->stages = stages;
   return LSFDTD_OK;
 }
 

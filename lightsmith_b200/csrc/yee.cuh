@@ -105,7 +105,7 @@ __device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, con
 
 // H update: one thread per node (i, j, k), all three components.
 template <typename F>
-__global__ void __launch_bounds__(256) k_update_h(YeeArgs<F> g) {
+__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArgs<F> g) {
   using R = typename real_of<F>::type;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) k_update_h(YeeArgs<F> g) {
 
 // E update: one thread per node, all three components.
 template <typename F>
-__global__ void __launch_bounds__(256) k_update_e(YeeArgs<F> g) {
+__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArgs<F> g) {
   using R = typename real_of<F>::type;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;

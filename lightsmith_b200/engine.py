@@ -446,6 +446,7 @@ class Engine:
         a CUDA graph and replayed."""
         def run():
             self.chunk(1, use_graph=use_graphs)
+            self.check_status()  # the driver synchronises once per chunk anyway to read the energy
         return run, bool(use_graphs)
 
     def release(self):
@@ -474,9 +475,27 @@ class Engine:
         """Whether a step is the fused single pass (decided once the engine is described)."""
         return bool(_abi.lib().lsfdtd_engine_fused(self._h))
 
-    def set_tuning(self, tile_y: int, planes: int) -> None:
-        """Launch shape of the fused pass (before the first graph capture)."""
-        _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(tile_y), int(planes)), "lsfdtd_engine_set_tuning")
+    @property
+    def uses_tma(self) -> bool:
+        """Whether the fused pass copies its planes with the Tensor Memory Accelerator."""
+        return bool(_abi.lib().lsfdtd_engine_uses_tma(self._h))
+
+    def set_copy_engine(self, use_tma: bool) -> None:
+        """TMA (default) or cp.async copies for the fused pass; before the first step."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_copy_engine(self._h, int(bool(use_tma))),
+                   "lsfdtd_engine_set_copy_engine")
+
+    def check_status(self) -> None:
+        """Raise if a kernel gave up waiting for its own copies (synchronises the engine's stream)."""
+        st = C.c_int32()
+        _abi.check(_abi.lib().lsfdtd_engine_status(self._h, self.stream.cuda_stream, C.byref(st)),
+                   "lsfdtd_engine_status")
+
+    def set_tuning(self, tile_y: int, planes: int, stages: int = 4) -> None:
+        """Launch shape of the fused pass (before the first graph capture): CTA tile rows, x planes per CTA
+        and depth of the copy ring."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(tile_y), int(planes), int(stages)),
+                   "lsfdtd_engine_set_tuning")
 
     @property
     def n_host(self) -> int:
