@@ -44,9 +44,11 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile-y", type=int, default=8, help="fused pass: nodes along y per CTA (8 or 16)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="0 in-place (vector) kernels, 1 fused pass; -1: pick the faster on this GPU (tuner)")
+    ap.add_argument("--tile-y", type=int, default=8, help="fused pass: tile rows along y")
     ap.add_argument("--planes", type=int, default=32, help="fused pass: x planes per CTA")
-    ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring (4, 6, 8)")
+    ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring")
     return ap.parse_args()
 
 
@@ -192,13 +194,20 @@ def run_b200(args):
     K, W = args.steps, args.warmup
     R = max(1, min(K, 6))  # chunks of the kernel-timing pass
     _, _, _, _, stride = throughput_band()
-    total_chunks = W + 2 * K + R + 2
+    total_chunks = W + 2 * K + R + 2 + 30  # the tuner's eager chunks too
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234)
     inv = 1.0 / (torch.rand(shape, generator=gen, device=dev, dtype=torch.float32) * 11.25 + 1.0)
     plan = throughput_plan(n, inv_eps=inv, max_steps=stride * total_chunks + 8, single=True)
     eng = Engine.from_plan(plan, device=dev)
-    eng.set_tuning(args.tile_y, args.planes, args.stages)
+    if args.variant < 0:
+        from lightsmith_b200.tune import tune_engine
+
+        tuned, _ = tune_engine(eng)
+        variant = tuned[0]
+    else:
+        variant = args.variant
+        eng.set_tuning(args.variant, args.tile_y, args.planes, args.stages)
     inv_host = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     inv_host.copy_(inv)
     del inv, plan["inv_eps"]
@@ -282,13 +291,13 @@ def run_b200(args):
                           "step": f"one chunk = {stride} FDTD steps + one DFT sample, CUDA graph replay",
                           "l2": "inputs larger than L2 (about 8 GB of state per replica)",
                           "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
-                          "kernel_path": "fused single pass" if eng_fused else "in-place H and E kernels",
-                          "tile": [32, args.tile_y], "planes_per_cta": args.planes, "ring_stages": args.stages,
-                          "copy_engine": "TMA" if eng_tma else "cp.async"},
+                          "variant": {0: "in-place H and E kernels", 1: "fused single pass",
+                                      2: "in-place four-node H and E kernels"}[variant],
+                          "copy_engine": ("TMA" if eng_tma else "cp.async") if variant == 1 else None},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_source": peak_kind,
                             "traffic": None if tpc is None else tpc * cells,
-                            "kernel": "bulk Yee H + E updates with fused CPML, per FDTD step",
+                            "kernel": "bulk Yee update (H and E with their CPML terms), per FDTD step",
                             "alg_bytes_per_step": alg_bytes, "kernel_ms_per_step": step_ms,
                             "bulk_launches_timed": bulk_launches},
                "cpu_baseline": cpu,

@@ -243,11 +243,15 @@ int32_t lsfdtd_engine_chunk_timed(lsfdtd_engine* eng, int32_t n_chunks, void* st
 /* which buffer holds the current E/H: 0 the grid's E/H, 1 its E_alt/H_alt */
 int32_t lsfdtd_engine_buffer(const lsfdtd_engine* eng);
 /* whether steps run as the fused single pass (1) or the in-place H and E kernels (0); valid once the
- * engine is fully described (it is decided at the first step) */
+ * engine is fully described (eligibility is decided at the first step) */
 int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
-/* launch shape of the fused pass: tile_y nodes along y per CTA (8 or 16), x planes per CTA (>= 1) and the
- * depth of its copy ring in x planes (4, 6 or 8; the TMA ring) */
-int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes, int32_t stages);
+/* kernel choice and launch shape. variant 0: in-place H and E kernels, one node per thread; variant 2: the
+ * same with four-node vector kernels for FP32 rows of a multiple of four nodes (the other arguments are
+ * ignored for both). variant 1: the fused single pass where the
+ * run allows it (second buffers given, no periodic axis, sources that only correct E): CTA tiles of 32 x
+ * tile_y nodes (8 or 16), x planes per tile (>= 1), copy ring of `stages` x planes (4, 6 or 8). */
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
+                                 int32_t stages);
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting
  * for its copies, else LSFDTD_OK */
 int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status);

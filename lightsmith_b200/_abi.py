@@ -105,7 +105,7 @@ SIGNATURES = {
     "lsfdtd_engine_set_copy_engine": (i32, [vp, i32]),
     "lsfdtd_engine_uses_tma": (i32, [vp]),
     "lsfdtd_engine_fused": (i32, [vp]),
-    "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32, i32]),
+    "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32, i32, i32]),
     "lsfdtd_engine_steps": (i64, [vp]),
     "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
 }

@@ -31,6 +31,8 @@ struct FusedArgs {
   int seg;             // x planes per CTA
   int inner_lo[3];     // nodes [inner_lo, inner_hi) along each axis are stepped for every component and lie
   int inner_hi[3];     // outside every CPML slab
+  int pml_lo[3];       // CPML cells per axis and side (0: none)
+  int pml_hi[3];
 };
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {

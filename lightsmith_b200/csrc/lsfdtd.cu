@@ -6,6 +6,7 @@
 // synchronises the host, so a chunk can be captured once as a CUDA graph and replayed.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <limits>
 #include <string>
 #include <vector>
@@ -16,6 +17,7 @@
 #include "common.cuh"
 #include "fused.cuh"
 #include "fused_tma.cuh"
+#include "yee_vec.cuh"
 
 #include <cudaTypedefs.h>
 #include "monitors.cuh"
@@ -97,7 +99,8 @@ struct lsfdtd_engine {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   int cur = 0;          // buffer holding the current fields
   int fused = -1;       // -1 undecided, 0 in-place kernels, 1 fused single pass
-  int tile_y = 8, planes = 128, stages = 4;
+  int variant = 0;  // 0: in-place H and E kernels; 1: the fused single pass; 2: in-place four-node kernels
+  int tile_y = 8, planes = 32, stages = 4;
   int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
@@ -219,6 +222,7 @@ struct Engine final : lsfdtd_engine {
   int pml_cells[3][2] = {};
   bool attr_set[2] = {false, false};
   bool tma_ok = false;
+  int maps_tile_y = 0;  // tile rows the tensor-map boxes were made for
   CUtensorMap mapE[2][3], mapH[2][3], mapC;  // per buffer and component; the coefficient of component 0
   static constexpr int kStages = 4;  // x planes in the fused pass's copy ring
 
@@ -287,6 +291,7 @@ struct Engine final : lsfdtd_engine {
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     };
     const unsigned ty = (unsigned)tile_y;
+    maps_tile_y = tile_y;
     for (int b = 0; b < 2; ++b)
       for (int c = 0; c < 3; ++c) {
         if (!make(&mapE[b][c], Ebuf[b] + c * cells, 40, ty + 2)) return LSFDTD_EUNSUPPORTED;
@@ -323,10 +328,14 @@ struct Engine final : lsfdtd_engine {
       }
       fa.inner_lo[ax] = lo;
       fa.inner_hi[ax] = std::max(lo, hi);
+      fa.pml_lo[ax] = y.pml[ax].on ? pml_cells[ax][0] : 0;
+      fa.pml_hi[ax] = y.pml[ax].on ? pml_cells[ax][1] : 0;
     }
-    const dim3 grid(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], tile_y), cdiv(desc.shape[0], planes));
+    // CTA-tile kernels have 8 or 16 rows (warp tiles size their own grid below)
+    const dim3 grid(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], tile_y == 16 ? 16 : 8), cdiv(desc.shape[0], planes));
     LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
+      if (tma_ok && maps_tile_y != tile_y) tma_ok = make_maps() == LSFDTD_OK;
       if (tma_ok) {
         TmaArgs<F> ta;
         ta.f = fa;
@@ -353,7 +362,7 @@ struct Engine final : lsfdtd_engine {
         }
         if (r != LSFDTD_OK) return r;
       } else if (tile_y == 16) {
-        constexpr size_t sm = fused_smem_bytes<F, 16, kStages>();
+        constexpr size_t sm = fused_smem_bytes<F, 16, kStages>();  // cp.async ring
         if (!attr_set[1]) {
           LS_CUDA(cudaFuncSetAttribute(k_fused_step<F, 16, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm));
@@ -628,10 +637,56 @@ struct Engine final : lsfdtd_engine {
     return LSFDTD_OK;
   }
 
+  // the in-place kernels' arguments on the current buffers
+  YeeArgs<F> current_args() const {
+    YeeArgs<F> a = y;
+    const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
+    for (int c = 0; c < 3; ++c) {
+      a.E[c] = Ebuf[cur] + c * cells;
+      a.H[c] = Hbuf[cur] + c * cells;
+    }
+    for (int d = 0; d < 3; ++d)
+      for (int c = 0; c < 3; ++c)
+        for (int sd = 0; sd < 2; ++sd) a.pml[d].psi[1][c][sd] = psiH[cur][d][c][sd];
+    return a;
+  }
+
+  VecBounds interior() const {
+    VecBounds b;
+    for (int ax = 0; ax < 3; ++ax) {
+      int lo = 1, hi = desc.shape[ax] - 1;
+      if (y.pml[ax].on) {
+        lo = std::max(lo, pml_cells[ax][0] ? pml_cells[ax][0] + 1 : 1);
+        hi = std::min(hi, pml_cells[ax][1] ? desc.shape[ax] - 2 - pml_cells[ax][1] : hi);
+      }
+      b.lo[ax] = lo;
+      b.hi[ax] = std::max(lo, hi);
+      b.pml_lo[ax] = y.pml[ax].on ? pml_cells[ax][0] : 0;
+      b.pml_hi[ax] = y.pml[ax].on ? pml_cells[ax][1] : 0;
+    }
+    return b;
+  }
+
+  // variant 2: FP32 rows of a multiple of four nodes take the four-node vector kernels
+  bool vec_ok() const {
+    if constexpr (std::is_same<F, float>::value) return variant == 2 && desc.shape[2] % 4 == 0;
+    return false;
+  }
+
   int update_h(cudaStream_t s) override {
     LS_TRY(ghosts(Eflat(), false, s));
+    const YeeArgs<F> a = current_args();
     LS_TRY(mark(s, true));
-    k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(y);
+    if constexpr (std::is_same<F, float>::value) {
+      if (vec_ok()) {
+        const dim3 grid(cdiv(desc.shape[2], 128), cdiv(desc.shape[1], 8), desc.shape[0]);
+        k_update_h_v4<<<grid, dim3(32, 8), 0, s>>>(a, interior());
+      } else {
+        k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      }
+    } else {
+      k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+    }
     LS_LAUNCHED();
     LS_TRY(mark(s, false));
     return LSFDTD_OK;
@@ -639,8 +694,18 @@ struct Engine final : lsfdtd_engine {
 
   int update_e(cudaStream_t s) override {
     LS_TRY(ghosts(Hflat(), true, s));
+    const YeeArgs<F> a = current_args();
     LS_TRY(mark(s, true));
-    k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(y);
+    if constexpr (std::is_same<F, float>::value) {
+      if (vec_ok()) {
+        const dim3 grid(cdiv(desc.shape[2], 128), cdiv(desc.shape[1], 8), desc.shape[0]);
+        k_update_e_v4<<<grid, dim3(32, 8), 0, s>>>(a, interior());
+      } else {
+        k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      }
+    } else {
+      k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+    }
     LS_LAUNCHED();
     LS_TRY(mark(s, false));
     return LSFDTD_OK;
@@ -743,7 +808,7 @@ struct Engine final : lsfdtd_engine {
 
   int step(cudaStream_t s) override {
     if (scratch_bytes < need_scratch()) return fail(LSFDTD_EINVAL, "scratch not set or too small");
-    if (decide()) {
+    if (decide() && variant == 1) {
       LS_TRY(fused_step(s));
     } else {
       LS_TRY(update_h(s));
@@ -798,7 +863,7 @@ struct Engine final : lsfdtd_engine {
   }
 
   int64_t launches_per_chunk() const override {
-    int64_t per_step = (fused == 1 ? 1 : 2) + 1;  // fused pass or H and E, counter
+    int64_t per_step = (fused == 1 && variant == 1 ? 1 : 2) + 1;  // fused pass or H and E, counter
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
     for (auto& g : groups) per_step += g.n > 0;
@@ -980,7 +1045,7 @@ int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_gr
     }
     LS_CUDA(cudaGraphLaunch(eng->exec[b], s));
     eng->n_host += eng->desc.dft_stride;
-    if (eng->fused == 1 && (eng->desc.dft_stride & 1)) eng->cur ^= 1;
+    if (eng->fused == 1 && eng->variant == 1 && (eng->desc.dft_stride & 1)) eng->cur ^= 1;
   }
   return LSFDTD_OK;
 }
@@ -1038,17 +1103,23 @@ int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma) {
   return LSFDTD_OK;
 }
 
-int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng) { return eng ? (eng->decide() && eng->uses_tma()) : -1; }
+int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng) {
+  return eng ? (eng->decide() && eng->variant == 1 && eng->uses_tma()) : -1;
+}
 
-int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? eng->decide() : -1; }
+int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? (eng->decide() && eng->variant == 1) : -1; }
 
-int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t tile_y, int32_t planes, int32_t stages) {
+int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
+                                 int32_t stages) {
   LS_NEED(eng);
-  if ((tile_y != 8 && tile_y != 16) || planes < 1 || (stages != 4 && stages != 6 && stages != 8))
-    return fail(LSFDTD_EINVAL, "tuning: tile_y 8 or 16, planes >= 1, stages 4, 6 or 8");
+  const bool ok = variant == 0 || variant == 2 ||
+                  (variant == 1 && (tile_y == 8 || tile_y == 16) && (stages == 4 || stages == 6 || stages == 8) &&
+                   planes >= 1);
+  if (!ok)
+    return fail(LSFDTD_EINVAL, "tuning: variant 0 (in-place kernels), 2 (in-place four-node kernels) or 1 (fused "
+                               "pass: CTA tile rows 8 or 16, ring 4, 6 or 8, planes >= 1)");
   if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "tuning must be set before the first graph capture");
-  if (eng->fused >= 0 && eng->tile_y != tile_y)
-    return fail(LSFDTD_EINVAL, "tile rows must be set before the first step");
+  eng->variant = variant;
   eng->tile_y = tile_y;
   eng->planes = planes;
   eng->stages = stages;

@@ -103,14 +103,9 @@ __device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, con
   }
 }
 
-// H update: one thread per node (i, j, k), all three components.
+// H update of node (i, j, k), all three components (in place).
 template <typename F>
-__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArgs<F> g) {
-  using R = typename real_of<F>::type;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= g.n[2] || j >= g.n[1]) return;
+__device__ __forceinline__ void update_h_node(const YeeArgs<F>& g, int i, int j, int k) {
   const int x[3] = {i, j, k};
   const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
   const long long p = i * s0 + j * s1 + k;
@@ -129,14 +124,10 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArg
   }
 }
 
-// E update: one thread per node, all three components.
+// E update of node (i, j, k), all three components (in place).
 template <typename F>
-__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArgs<F> g) {
+__device__ __forceinline__ void update_e_node(const YeeArgs<F>& g, int i, int j, int k) {
   using R = typename real_of<F>::type;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= g.n[2] || j >= g.n[1]) return;
   const int x[3] = {i, j, k};
   const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
   const long long p = i * s0 + j * s1 + k;
@@ -154,6 +145,24 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArg
     apply_cpml<0>(e, g, c, x, a, b, cb);
     g.E[c][p] = e;
   }
+}
+
+// H update: one thread per node (i, j, k), all three components.
+template <typename F>
+__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArgs<F> g) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (k >= g.n[2] || j >= g.n[1]) return;
+  update_h_node(g, blockIdx.z, j, k);
+}
+
+// E update: one thread per node, all three components.
+template <typename F>
+__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArgs<F> g) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (k >= g.n[2] || j >= g.n[1]) return;
+  update_e_node(g, blockIdx.z, j, k);
 }
 
 // Periodic ghost planes of one axis: dst plane <- src plane times a Bloch phase (engine.py:595-611).

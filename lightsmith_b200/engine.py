@@ -491,11 +491,11 @@ class Engine:
         _abi.check(_abi.lib().lsfdtd_engine_status(self._h, self.stream.cuda_stream, C.byref(st)),
                    "lsfdtd_engine_status")
 
-    def set_tuning(self, tile_y: int, planes: int, stages: int = 4) -> None:
-        """Launch shape of the fused pass (before the first graph capture): CTA tile rows, x planes per CTA
-        and depth of the copy ring."""
-        _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(tile_y), int(planes), int(stages)),
-                   "lsfdtd_engine_set_tuning")
+    def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:
+        """Launch shape of the fused pass (before the first graph capture): variant 0 warp-independent tiles
+        (rows 4 or 8, ring 3/4/6) or 1 CTA tiles (rows 8 or 16, ring 4/6/8), x planes per tile, ring depth."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(variant), int(tile_y), int(planes),
+                                                       int(stages)), "lsfdtd_engine_set_tuning")
 
     @property
     def n_host(self) -> int:

@@ -90,7 +90,7 @@ def throughput_plan(n: int | tuple = 640, pml: int = 16, dx: float = 20.0, n_fre
         return np.asarray(inv_eps)[ijk]
     dip = point_dipole(shape, np.zeros(3), dx, dt, ctr, (0.0, 0.0, 1.0), at, omega_c, omega_half, max_steps)
     mon = plane_monitor(shape, shape[2] // 2, om, energy=1)
-    spec = PMLSpec(cells=((pml, pml),) * 3, alpha_max=0.05 * 2 * np.pi / 2000.0, eps_ref=1.0)
+    spec = PMLSpec(cells=((pml, pml),) * 3, alpha_max=0.05 * 2 * np.pi / 2000.0 if pml else 0.0, eps_ref=1.0)
     if hasattr(inv_eps, "detach"):
         # make_plan takes host arrays: a device tensor for 1/eps is put in place afterwards
         plan = _plan_on_device(shape, dx, dt, single, spec, dip, mon, stride or st)
@@ -104,7 +104,7 @@ def _plan_on_device(shape, dx, dt, single, spec, dip, mon, stride):
     plan = make_plan(shape=(3, 3, 3), dx=dx, dt=dt, single=single, inv_eps=np.ones((3, 3, 3)), groups=[],
                      pml=PMLSpec(cells=((0, 0),) * 3), sources=[dip], monitors=[mon], dft_stride=stride)
     plan["shape"] = tuple(shape)
-    plan["pml"] = {"cells": tuple(tuple(c) for c in spec.cells), "m": float(spec.m),
+    plan["pml"] = {"cells": tuple(tuple(int(v) for v in c) for c in spec.cells), "m": float(spec.m),
                    "kappa_max": float(spec.kappa_max), "alpha_max": float(spec.alpha_max),
                    "eps_ref": float(spec.eps_ref), "eps_ref_high": None}
     return plan

@@ -80,15 +80,15 @@ def test_source_waveform_end_raises(golden):
 FUSED_CASES = ["yee_cpml_dipole", "kappa_noncubic", "ade_groups"]
 
 
-@pytest.mark.parametrize("tile_y,planes,stages", [(8, 3, 4), (16, 5, 6), (16, 128, 8), (8, 2, 8)])
+@pytest.mark.parametrize("variant,tile_y,planes,stages", [(1, 8, 3, 4), (1, 16, 5, 6), (1, 16, 128, 8), (1, 8, 2, 8)])
 @pytest.mark.parametrize("case", FUSED_CASES)
-def test_fused_pass_any_launch_shape(case, tile_y, planes, stages, golden):
+def test_fused_pass_any_launch_shape(case, variant, tile_y, planes, stages, golden):
     """The fused pass under launch shapes that split x into several segments (each CTA then recomputes the
     H plane before its segment) still matches lightsmith's engine."""
     d = golden("engine_" + case)
     plan, out = d["plan"], d["out"]
     eng = _engine(plan, "double")
-    eng.set_tuning(tile_y, planes, stages)
+    eng.set_tuning(variant, tile_y, planes, stages)
     assert eng.fused
     for _ in range(out["n_chunks"]):
         eng.chunk(1, use_graph=True)
@@ -105,8 +105,8 @@ def test_fused_pass_equals_in_place_kernels(case, golden):
     plan = golden("engine_" + case)["plan"]
     a = Engine.from_plan(plan, precision="single")
     b = Engine.from_plan(plan, precision="single", fused=False)
+    a.set_tuning(1, 8, 4, 4)
     assert a.fused and not b.fused
-    a.set_tuning(8, 4)
     for _ in range(5):
         a.chunk(1, use_graph=True)
         b.chunk(1, use_graph=True)
@@ -125,8 +125,8 @@ def test_tma_and_cp_async_rings_agree_bit_for_bit(case, golden):
     a = Engine.from_plan(plan, precision="double")
     b = Engine.from_plan(plan, precision="double")
     b.set_copy_engine(False)
-    a.set_tuning(8, 6)
-    b.set_tuning(8, 6)
+    a.set_tuning(1, 8, 6, 4)
+    b.set_tuning(1, 8, 6, 4)
     for _ in range(4):
         a.chunk(1, use_graph=True)
         b.chunk(1, use_graph=True)
@@ -134,5 +134,24 @@ def test_tma_and_cp_async_rings_agree_bit_for_bit(case, golden):
     a.check_status()
     assert np.array_equal(a.E.cpu().numpy(), b.E.cpu().numpy())
     assert np.array_equal(a.H.cpu().numpy(), b.H.cpu().numpy())
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("case", ["yee_cpml_dipole", "line_periodic"])
+def test_vector_kernels_equal_per_node_kernels(case, golden):
+    """The four-node vector kernels (rows of a multiple of four nodes) give the per-node kernels' values."""
+    from lightsmith_b200.engine import Engine
+
+    plan = golden("engine_" + case)["plan"]
+    assert plan["shape"][2] % 4 == 0
+    a = Engine.from_plan(plan, precision="single", fused=False)
+    b = Engine.from_plan(plan, precision="single", fused=False)
+    a.set_tuning(2, 8, 32, 4)
+    for _ in range(5):
+        a.chunk(1, use_graph=True)
+        b.chunk(1, use_graph=True)
+    assert _rel(a.E.cpu().numpy(), b.E.cpu().numpy()) < 1e-6
+    assert _rel(a.H.cpu().numpy(), b.H.cpu().numpy()) < 1e-6
     a.close()
     b.close()

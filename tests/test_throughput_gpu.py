@@ -20,8 +20,8 @@ def test_throughput_case_matches_oracle_at_128():
     ref = OracleEngine(plan, threads=8)
     gpu64 = Engine.from_plan(plan, precision="double")
     gpu32 = Engine.from_plan(plan, precision="single")
-    gpu64.set_tuning(8, 40)  # several x segments per tile column
-    assert gpu64.fused and gpu32.fused
+    gpu64.set_tuning(1, 8, 40, 4)  # the fused pass, several x segments per tile column
+    assert gpu64.fused and not gpu32.fused  # float32 here: the in-place vector kernels
     for _ in range(3):
         ref.chunk()
         gpu64.chunk(1, use_graph=True)
