@@ -262,6 +262,23 @@ int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma);
 int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng);
 /* steps completed so far, as the host has launched them */
 int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng);
+
+/* One running-DFT sample of one monitor, allocating nothing (no counterpart in lightsmith: its engine samples
+ * monitors with array operations of the array library it runs on). For callers that cannot allocate device
+ * memory: a host runtime that only lends the library the buffers it owns, or a process whose device memory
+ * all comes from one external pool. The caller passes the monitor's inputs (sampled arrays, indices,
+ * frequencies) and outputs (accumulators, updated in place) in `m`, the device step counter `step` (the
+ * sample time is step * dt, H at half a step earlier) and `energy`, a device double that receives the
+ * monitor's sum |E|^2 + |H_avg|^2 when m->energy is set and the monitor has H (else it is left alone).
+ * precision / is_complex describe the sampled arrays as for the grid (m->space 1: real arrays).
+ * The energy reduction's scratch is a static device array of 8192 doubles (64 KiB, held by every GPU that
+ * loads the library until exit): a monitor may span at most 8192 blocks of 256 points (E points and H points
+ * rounded up separately), and larger ones are rejected with LSFDTD_EINVAL. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array: calls whose GPU work overlaps (for example on two streams) race on it; nothing
+ * in it needs clearing between calls. */
+int32_t lsfdtd_dft_sample_noalloc(const lsfdtd_monitor_desc* m, int32_t precision, int32_t is_complex,
+                                  const int64_t* step, double dt, double* energy, void* stream);
 /* kernel launches one chunk issues (for launch accounting) */
 int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng);
 

@@ -108,6 +108,7 @@ SIGNATURES = {
     "lsfdtd_engine_set_tuning": (i32, [vp, i32, i32, i32, i32]),
     "lsfdtd_engine_steps": (i64, [vp]),
     "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
+    "lsfdtd_dft_sample_noalloc": (i32, [C.POINTER(MonitorDesc), i32, i32, vp, f64, vp, vp]),
 }
 
 _lib = None

@@ -89,6 +89,11 @@ int slab(const int32_t* shape, const int32_t* periodic, int d, int lo_n, int hi_
 
 }  // namespace
 
+namespace lsfdtd {
+// the error hook of the library's other translation units (lsfdtd_last_error reports it)
+int report_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace lsfdtd
+
 struct lsfdtd_engine {
   lsfdtd_grid_desc desc{};
   int64_t n_host = 0;

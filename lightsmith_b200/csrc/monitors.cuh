@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kMonBlock) k_monitor(MonArgs<S> a) {
 }
 
 // energy[g] = sum of the partials [first, first + count) of each group present (a fixed-order warp sum)
-__global__ void k_energy(const double* partial, long long first0, long long count0, long long first1,
+static __global__ void k_energy(const double* partial, long long first0, long long count0, long long first1,
                          long long count1, double* energy) {
   const int lane = threadIdx.x;
   for (int g = 0; g < 2; ++g) {
