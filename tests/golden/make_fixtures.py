@@ -21,8 +21,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
-sys.path[:0] = [os.path.join(HERE, "shim"), REF_SRC, REPO]
+sys.path[:0] = [HERE, REPO]
+from refsrc import REF_SRC, add_to_path  # noqa: E402
+
+if not add_to_path(sys.argv[1] if len(sys.argv) > 1 else REF_SRC):
+    sys.exit("lightsmith sources not found (pass their src/ directory or set LIGHTSMITH_SRC)")
 
 import lightsmith as ls  # noqa: E402
 from lightsmith.backends._fdtd import engine as ref_engine  # noqa: E402
