@@ -249,7 +249,10 @@ int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
  * same with four-node vector kernels for FP32 rows of a multiple of four nodes (the other arguments are
  * ignored for both). variant 1: the fused single pass where the
  * run allows it (second buffers given, no periodic axis, sources that only correct E): CTA tiles of 32 x
- * tile_y nodes (8 or 16), x planes per tile (>= 1), copy ring of `stages` x planes (4, 6 or 8). */
+ * tile_y nodes (8 or 16), x planes per tile (>= 1), copy ring of `stages` x planes (4, 6 or 8). variant 3:
+ * variant 1 split in two launches where its planes are copied by the Tensor Memory Accelerator: the fused
+ * pass over an interior box that needs no region or CPML tests, and a shell kernel over the CPML slabs and
+ * walls (the same values as variant 1, bit for bit). */
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
                                  int32_t stages);
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting

@@ -71,6 +71,27 @@ template <> __device__ __forceinline__ cplx<double> apply_phase<cplx<double>>(cp
   return v * cplx<double>{re, im};
 }
 
+// Loads through the read-only data path, for arrays no thread writes during the kernel (lets the compiler
+// issue them ahead of the kernel's stores), and stores marked global (no false dependence on shared memory)
+__device__ __forceinline__ float ro(const float* p) { return __ldg(p); }
+__device__ __forceinline__ double ro(const double* p) { return __ldg(p); }
+__device__ __forceinline__ cplx<float> ro(const cplx<float>* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return {v.x, v.y};
+}
+__device__ __forceinline__ cplx<double> ro(const cplx<double>* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return {v.x, v.y};
+}
+__device__ __forceinline__ void st_global(float* p, float v) { __stcg(p, v); }
+__device__ __forceinline__ void st_global(double* p, double v) { __stcg(p, v); }
+__device__ __forceinline__ void st_global(cplx<float>* p, cplx<float> v) {
+  __stcg(reinterpret_cast<float2*>(p), make_float2(v.re, v.im));
+}
+__device__ __forceinline__ void st_global(cplx<double>* p, cplx<double> v) {
+  __stcg(reinterpret_cast<double2*>(p), make_double2(v.re, v.im));
+}
+
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace lsfdtd

@@ -33,6 +33,8 @@ struct FusedArgs {
   int inner_hi[3];     // outside every CPML slab
   int pml_lo[3];       // CPML cells per axis and side (0: none)
   int pml_hi[3];
+  int box_lo[3];       // the interior box of the split step: nodes [box_lo, box_hi) per axis, each of them and
+  int box_hi[3];       // its low-side neighbours inside [inner_lo, inner_hi); box_lo[2] a multiple of four
 };
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {

@@ -1,0 +1,363 @@
+// The fused single pass over the whole grid with lean CPML terms.
+//
+// Same tiling, copy ring and step as k_fused_tma (fused_tma.cuh): a CTA owns a 32 (z) x TY (y) tile, marches
+// through a segment of x planes fed by bulk tensor copies, and computes H^{n+1/2} then E^{n+1} per plane, the
+// halo H of its tile recomputed in place. What differs is how nodes near the boundary are stepped.
+//
+// A warp whose nodes and halo nodes all lie inside every component's stepped region and outside every CPML
+// slab takes the region- and CPML-free path (the whole warp, per plane). Any other warp takes the lean path,
+// in which each node finds its place in the slabs of each axis from small per-CTA tables built once before
+// the x march (rows y0-1 .. y0+TY-1 and columns z0-1 .. z0+31 of the tile, for E and for H) and, along x,
+// from one lookup per plane that is uniform across the CTA. Along an axis d the slabs of the two components
+// with a psi along d have the same extent, so one entry serves both. A CPML term then costs a predicate, an
+// index, a coalesced psi load and store and two multiply-adds; its arithmetic and order are cpml_io's.
+//
+// The region tests are those of a grid without periodic axes (the fused pass serves no other): H_c is stepped
+// where x_a <= n_a - 2 for every a != c, E_c where 1 <= x_a <= n_a - 2 for a != c and x_c <= n_c - 2; other
+// nodes copy the component.
+#pragma once
+
+#include "fused_tma.cuh"
+
+namespace lsfdtd {
+
+// a coordinate's place in the CPML slab of one axis and field
+template <typename R>
+struct SlabInfo {
+  int side;  // -1 none, 0 lo, 1 hi
+  int st;    // first node of the slab along the axis
+  int len;   // its length
+  R b, c, k;  // profile values at the coordinate (k: 1/kappa - 1, zero where kappa is 1 everywhere)
+};
+
+template <int FLD, typename F>
+__device__ __forceinline__ SlabInfo<typename real_of<F>::type> slab_info(const PmlAxis<F>& p, int d, int u) {
+  using R = typename real_of<F>::type;
+  SlabInfo<R> s;
+  s.side = -1;
+  s.st = 0;
+  s.len = 1;
+  s.b = s.c = s.k = R(0);
+  if (!p.on) return s;
+  const int cr = (d + 1) % 3;  // a component with a psi along d (both have the same slab extents)
+#pragma unroll
+  for (int sd = 0; sd < 2; ++sd) {
+    const int st = p.start[FLD][cr][sd], ln = p.len[FLD][cr][sd];
+    if (ln > 0 && u >= st && u < st + ln) {
+      s.side = sd;
+      s.st = st;
+      s.len = ln;
+    }
+  }
+  if (s.side >= 0) {
+    s.b = p.b[FLD][u];
+    s.c = p.c[FLD][u];
+    s.k = p.k[FLD] ? p.k[FLD][u] : R(0);
+  }
+  return s;
+}
+
+template <typename F, int TY>
+struct PmlTables {
+  using R = typename real_of<F>::type;
+  static constexpr int NY = TY + 1, NZ = 33;
+  SlabInfo<R> y[2][NY];  // [E, H][row]: y = y0 - 1 + row
+  SlabInfo<R> z[2][NZ];  // [E, H][col]: z = z0 - 1 + col
+};
+
+template <typename F, int TY, int S>
+constexpr size_t fused_pml_smem_bytes() {
+  return fused_tma_smem_bytes<F, TY, S>() + (sizeof(PmlTables<F, TY>) + 15) / 16 * 16;
+}
+
+// the CPML term along axis d of a value v of field FLD, component c, at node x (psi index from the slab
+// info of that axis); psi_out == nullptr: a halo node, computed but not stored
+template <int FLD, typename F>
+__device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
+                                         int d, int c, const int* x, F der, typename real_of<F>::type scale,
+                                         const F* psi_in, F* psi_out) {
+  using R = typename real_of<F>::type;
+  const int d1 = (c + 1) % 3;
+  R sgn = (d == d1) ? R(1) : R(-1);
+  if (FLD == 1) sgn = -sgn;
+  R s = g.uniform ? scale : scale / g.pml[d].div;
+  s = sgn * s;
+  long long q;
+  if (d == 0)
+    q = ((long long)(x[0] - si.st) * g.n[1] + x[1]) * g.n[2] + x[2];
+  else if (d == 1)
+    q = ((long long)x[0] * si.len + (x[1] - si.st)) * g.n[2] + x[2];
+  else
+    q = ((long long)x[0] * g.n[1] + x[1]) * si.len + (x[2] - si.st);
+  F psi = (FLD == 1 ? ro(psi_in + q) : psi_in[q]) * si.b;
+  if (g.pml[d].k[FLD]) v += (s * si.k) * der;
+  psi += der * (s * si.c);
+  if (psi_out) st_global(psi_out + q, psi);
+  v += psi;
+}
+
+template <typename F, int TY, int S>
+__global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
+  using R = typename real_of<F>::type;
+  using St = TmaStage<F, TY>;
+  using Tab = PmlTables<F, TY>;
+  constexpr int TZ = 32, BZ = St::BZ, NT = 32 * TY;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  F(*sH)[2][TY + 1][TZ] = reinterpret_cast<F(*)[2][TY + 1][TZ]>(smem + S * St::kBytes);
+  unsigned long long* bar =
+      reinterpret_cast<unsigned long long*>(smem + S * St::kBytes + 2 * 2 * (TY + 1) * TZ * sizeof(F));
+  // the tables follow the ring, the H exchange rows and the barriers
+  Tab& tab = *reinterpret_cast<Tab*>(smem + S * St::kBytes + 2 * 2 * (TY + 1) * TZ * sizeof(F) + S * 8);
+
+  const FusedArgs<F>& a = t.f;
+  const YeeArgs<F>& g = a.y;
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
+  const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
+  const int k = z0 + tx, j = y0 + ty;
+  const int xs = blockIdx.z * a.seg;
+  if (xs >= n0) return;
+  const int xe = min(n0, xs + a.seg);
+  const int xb = xs > 0 ? xs - 1 : 0;
+  const bool own = k < n2 && j < n1;
+  const long long s1 = n2, s0 = (long long)n1 * n2;
+
+  auto stE = [&](int s, int c) { return reinterpret_cast<F(*)[BZ]>(smem + s * St::kBytes + c * St::kE); };
+  auto stH = [&](int s, int c) {
+    return reinterpret_cast<F(*)[BZ]>(smem + s * St::kBytes + 3 * St::kE + c * St::kH);
+  };
+  auto stC = [&](int s) { return reinterpret_cast<R(*)[TZ]>(smem + s * St::kBytes + 3 * St::kE + 3 * St::kH); };
+
+  // the slab tables of the tile's rows and columns (halo included)
+  for (int e = tid; e < 2 * (Tab::NY + Tab::NZ); e += NT) {
+    const int f = e / (Tab::NY + Tab::NZ), r = e % (Tab::NY + Tab::NZ);
+    if (r < Tab::NY)
+      tab.y[f][r] = f ? slab_info<1>(g.pml[1], 1, y0 - 1 + r) : slab_info<0>(g.pml[1], 1, y0 - 1 + r);
+    else
+      tab.z[f][r - Tab::NY] = f ? slab_info<1>(g.pml[2], 2, z0 - 1 + r - Tab::NY)
+                                : slab_info<0>(g.pml[2], 2, z0 - 1 + r - Tab::NY);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto produce = [&](int p) {
+    const int s = (p - xb) % S;
+    mbar_expect_tx(&bar[s], St::kTx);
+    for (int c = 0; c < 3; ++c) tma_load_3d(stE(s, c), &t.mE[c], z0 - 4, y0 - 1, p, &bar[s]);
+    for (int c = 0; c < 3; ++c) tma_load_3d(stH(s, c), &t.mH[c], z0 - 4, y0 - 1, p, &bar[s]);
+    tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
+  };
+  auto ready = [&](int p) -> bool {
+    return mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, kWaitBudget);
+  };
+  int issued = xb - 1;
+  if (tid == 0) {
+    for (int p = xb; p < xb + S - 1; ++p) produce(p);
+  }
+  issued = xb + S - 2;
+
+  auto curl = [&](F av, F bv, int d1, int d2) -> F {
+    return g.uniform ? (av - bv) : (av * g.inv_d[d1] - bv * g.inv_d[d2]);
+  };
+  // region- and CPML-free H at stage offset o (row-major in the 40-wide boxes)
+  auto hx_fast = [&](int si, int o) -> F {
+    const F* ey = &stE(si, 1)[0][0];
+    const F* ez = &stE(si, 2)[0][0];
+    return stH(si, 0)[0][o] - curl(ez[o + BZ] - ez[o], ey[o + 1] - ey[o], 1, 2) * g.cH;
+  };
+  auto hy_fast = [&](int si, int sn, int o) -> F {
+    const F* ex = &stE(si, 0)[0][0];
+    const F* ez = &stE(si, 2)[0][0];
+    return stH(si, 1)[0][o] - curl(ex[o + 1] - ex[o], (&stE(sn, 2)[0][0])[o] - ez[o], 2, 0) * g.cH;
+  };
+  auto hz_fast = [&](int si, int sn, int o) -> F {
+    const F* ex = &stE(si, 0)[0][0];
+    const F* ey = &stE(si, 1)[0][0];
+    return stH(si, 2)[0][o] - curl((&stE(sn, 1)[0][0])[o] - ey[o], ex[o + BZ] - ex[o], 0, 1) * g.cH;
+  };
+
+  // H^{n+1/2}_c of the tile node at table row yy (y = y0 - 1 + yy) and column zz (z = z0 - 1 + zz) of plane i,
+  // with region test and CPML terms; xs_h: the plane's x slab info (H); store: an own node (H and psi out)
+  auto h_lean = [&](int c, int si, int sn, int i, int yy, int zz, const SlabInfo<R>& xs_h, bool store) -> F {
+    const int row = yy, col = zz + 3;
+    const int x[3] = {i, y0 - 1 + yy, z0 - 1 + zz};
+    const F h0 = stH(si, c)[row][col];
+    const long long p = i * s0 + (long long)x[1] * s1 + x[2];
+    bool in = true;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax)
+      if (ax != c && x[ax] > g.n[ax] - 2) in = false;
+    if (!in) {
+      if (store) st_global(a.Ho[c] + p, h0);
+      return h0;
+    }
+    F av, bv;
+    if (c == 0) {
+      av = stE(si, 2)[row + 1][col] - stE(si, 2)[row][col];
+      bv = stE(si, 1)[row][col + 1] - stE(si, 1)[row][col];
+    } else if (c == 1) {
+      av = stE(si, 0)[row][col + 1] - stE(si, 0)[row][col];
+      bv = stE(sn, 2)[row][col] - stE(si, 2)[row][col];
+    } else {
+      av = stE(sn, 1)[row][col] - stE(si, 1)[row][col];
+      bv = stE(si, 0)[row + 1][col] - stE(si, 0)[row][col];
+    }
+    const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    F h = h0 - curl(av, bv, d1, d2) * g.cH;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d == c) continue;
+      const SlabInfo<R>& sl = d == 0 ? xs_h : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
+      if (sl.side < 0) continue;
+      const F* pin = g.pml[d].psi[1][c][sl.side];
+      F* pout = store ? a.psiHo[d][c][sl.side] : nullptr;
+      pml_term<1>(h, g, sl, d, c, x, d == d1 ? av : bv, g.cH, pin, pout);
+    }
+    if (store) st_global(a.Ho[c] + p, h);
+    return h;
+  };
+
+  const unsigned full = 0xffffffffu;
+  const int oo = (ty + 1) * BZ + tx + 4;
+  const long long off_jk = (long long)j * s1 + k;
+  auto y_in = [&](int y) { return y >= a.inner_lo[1] && y < a.inner_hi[1]; };
+  // the warp's nodes, its halo column (lane 0: z0 - 1) and, for warp 0, the halo row y0 - 1 are all inner
+  // along y and z (warp-uniform: every lane of a warp shares its row)
+  const bool warp_clean = y_in(j) && (ty != 0 || y_in(y0 - 1)) && z0 - 1 >= a.inner_lo[2] &&
+                          z0 + TZ <= a.inner_hi[2];
+  const bool multi_cb = g.cbE[1] != g.cbE[0] || g.cbE[2] != g.cbE[0];
+
+  F prev_hy = zero<F>(), prev_hz = zero<F>();
+  bool failed = false;
+  int cons = xb - 1;
+#pragma unroll 1
+  for (int i = xb; i < xe; ++i) {
+    const bool ok = ready(i) && ready(i + 1);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    cons = i + 1;
+    if (tid == 0) produce(i + S - 1);
+    issued = i + S - 1;
+    const int si = (i - xb) % S, sn = (i + 1 - xb) % S;
+    const bool fast = warp_clean && i >= a.inner_lo[0] && i < a.inner_hi[0];
+    SlabInfo<R> xs_h, xs_e;
+    if (!fast) {
+      xs_h = slab_info<1>(g.pml[0], 0, i);
+      xs_e = slab_info<0>(g.pml[0], 0, i);
+    }
+    if (i < xs) {  // the plane before the segment: H_y, H_z of the own node, not stored
+      if (own) {
+        if (fast) {
+          prev_hy = hy_fast(si, sn, oo);
+          prev_hz = hz_fast(si, sn, oo);
+        } else {
+          prev_hy = h_lean(1, si, sn, i, ty + 1, tx + 1, xs_h, false);
+          prev_hz = h_lean(2, si, sn, i, ty + 1, tx + 1, xs_h, false);
+        }
+      }
+      continue;
+    }
+    const long long p = i * s0 + off_jk;
+    F hx = zero<F>(), hy = zero<F>(), hz = zero<F>();
+    if (fast) {
+      hx = hx_fast(si, oo);
+      hy = hy_fast(si, sn, oo);
+      hz = hz_fast(si, sn, oo);
+      st_global(a.Ho[0] + p, hx);
+      st_global(a.Ho[1] + p, hy);
+      st_global(a.Ho[2] + p, hz);
+    } else if (own) {
+      hx = h_lean(0, si, sn, i, ty + 1, tx + 1, xs_h, true);
+      hy = h_lean(1, si, sn, i, ty + 1, tx + 1, xs_h, true);
+      hz = h_lean(2, si, sn, i, ty + 1, tx + 1, xs_h, true);
+    }
+    F(&hs)[2][TY + 1][TZ] = sH[i & 1];
+    hs[0][ty + 1][tx] = hx;
+    hs[1][ty + 1][tx] = hz;
+    if (ty == 0 && y0 > 0 && k < n2) {  // the halo row y0 - 1
+      if (fast) {
+        hs[0][0][tx] = hx_fast(si, tx + 4);
+        hs[1][0][tx] = hz_fast(si, sn, tx + 4);
+      } else {
+        hs[0][0][tx] = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false);
+        hs[1][0][tx] = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false);
+      }
+    }
+    F hx_zh = zero<F>(), hy_zh = zero<F>();  // H_x, H_y at (j, z0 - 1), for lane 0
+    if (tx == 0 && z0 > 0 && j < n1) {
+      if (fast) {
+        const int o = (ty + 1) * BZ + 3;
+        hx_zh = hx_fast(si, o);
+        hy_zh = hy_fast(si, sn, o);
+      } else {
+        hx_zh = h_lean(0, si, sn, i, ty + 1, 0, xs_h, false);
+        hy_zh = h_lean(1, si, sn, i, ty + 1, 0, xs_h, false);
+      }
+    }
+    F hx_zm = shfl_up(full, hx), hy_zm = shfl_up(full, hy);
+    if (tx == 0) {
+      hx_zm = hx_zh;
+      hy_zm = hy_zh;
+    }
+    __syncthreads();
+    if (own) {
+      const F hz_ym = hs[1][ty][tx], hx_ym = hs[0][ty][tx];
+      const R cb = stC(si)[ty][tx];
+      const F* ex = &stE(si, 0)[0][0];
+      const F* ey = &stE(si, 1)[0][0];
+      const F* ez = &stE(si, 2)[0][0];
+      const F a0 = hz - hz_ym, b0 = hy - hy_zm;
+      const F a1 = hx - hx_zm, b1 = hz - prev_hz;
+      const F a2 = hy - prev_hy, b2 = hx - hx_ym;
+      if (fast && !multi_cb) {
+        st_global(a.Eo[0] + p, ex[oo] + curl(a0, b0, 1, 2) * cb);
+        st_global(a.Eo[1] + p, ey[oo] + curl(a1, b1, 2, 0) * cb);
+        st_global(a.Eo[2] + p, ez[oo] + curl(a2, b2, 0, 1) * cb);
+      } else {
+        const int x[3] = {i, j, k};
+        const F av[3] = {a0, a1, a2}, bv[3] = {b0, b1, b2};
+        const F* e[3] = {ex, ey, ez};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const F e0 = e[c][oo];
+          bool in = x[c] <= g.n[c] - 2;
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax)
+            if (ax != c && (x[ax] < 1 || x[ax] > g.n[ax] - 2)) in = false;
+          if (!fast && !in) {
+            st_global(a.Eo[c] + p, e0);
+            continue;
+          }
+          const R cbc = c == 0 ? cb : ro(g.cbE[c] + p);
+          F ev = e0 + curl(av[c], bv[c], (c + 1) % 3, (c + 2) % 3) * cbc;
+          if (!fast) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              if (d == c) continue;
+              const SlabInfo<R>& sl = d == 0 ? xs_e : (d == 1 ? tab.y[0][ty + 1] : tab.z[0][tx + 1]);
+              if (sl.side < 0) continue;
+              F* ps = g.pml[d].psi[0][c][sl.side];
+              pml_term<0>(ev, g, sl, d, c, x, d == (c + 1) % 3 ? av[c] : bv[c], cbc, ps, ps);
+            }
+          }
+          st_global(a.Eo[c] + p, ev);
+        }
+      }
+    }
+    prev_hy = hy;
+    prev_hz = hz;
+  }
+  if (tid == 0) {
+    for (int p = cons + 1; p <= issued; ++p) mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, kDrainBudget);
+    if (failed && t.status) atomicExch(t.status, 1);
+  }
+  __syncthreads();
+}
+
+}  // namespace lsfdtd

@@ -7,6 +7,11 @@
 // and the same z range, and the coefficient tile. Each stage has an mbarrier that the copies complete;
 // the other threads do no copy work at all, which is what limited the cp.async ring.
 //
+// With BOX, the kernel steps only the interior box of the split step (FusedArgs::box_lo/box_hi): every node
+// it updates or recomputes lies inside every component's stepped region and outside every CPML slab, so the
+// region and CPML code is compiled out; the nodes outside the box are stepped by k_shell_h and k_shell_e
+// (shell.cuh).
+//
 // Every box starts at z0 - 4 (a multiple of four nodes, so 16-byte aligned in both precisions) and may
 // start before the grid or run past it; the tensor maps fill such nodes with zeros. Waits on an mbarrier are
 // bounded by a clock budget: a CTA that exceeds it (copies that never complete) records status 1, waits a
@@ -92,7 +97,7 @@ constexpr size_t fused_tma_smem_bytes() {
   return 128 + S * TmaStage<F, TY>::kBytes + 2 * 2 * (TY + 1) * 32 * sizeof(F) + S * 8;
 }
 
-template <typename F, int TY, int S>
+template <typename F, int TY, int S, bool BOX>
 __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ TmaArgs<F> t) {
   using R = typename real_of<F>::type;
   using St = TmaStage<F, TY>;
@@ -108,13 +113,14 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
   const YeeArgs<F>& g = a.y;
   const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
-  const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
+  const int z0 = (BOX ? a.box_lo[2] : 0) + blockIdx.x * TZ, y0 = (BOX ? a.box_lo[1] : 0) + blockIdx.y * TY;
   const int k = z0 + tx, j = y0 + ty;
-  const int xs = blockIdx.z * a.seg;
-  if (xs >= n0) return;
-  const int xe = min(n0, xs + a.seg);
+  const int xs = (BOX ? a.box_lo[0] : 0) + blockIdx.z * a.seg;
+  const int xend = BOX ? a.box_hi[0] : n0;
+  if (xs >= xend) return;
+  const int xe = min(xend, xs + a.seg);
   const int xb = xs > 0 ? xs - 1 : 0;
-  const bool own = k < n2 && j < n1;
+  const bool own = BOX ? (k < a.box_hi[2] && j < a.box_hi[1]) : (k < n2 && j < n1);
   const long long s1 = n2, s0 = (long long)n1 * n2;
 
   auto stE = [&](int s, int c) { return reinterpret_cast<F(*)[BZ]>(smem + s * St::kBytes + c * St::kE); };
@@ -153,7 +159,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     const F h0 = stH(si, c)[row][col];
     const long long p = i * s0 + (long long)x[1] * s1 + x[2];
     if (!in_h_region(c, x, g.n, g.periodic)) {
-      if (store) a.Ho[c][p] = h0;
+      if (store) st_global(a.Ho[c] + p, h0);
       return h0;
     }
     F av, bv;
@@ -171,7 +177,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     const F curl = g.uniform ? (av - bv) : (av * g.inv_d[d1] - bv * g.inv_d[d2]);
     F h = h0 - curl * g.cH;
     cpml_io<1>(h, a, c, x, av, bv, g.cH, store);
-    if (store) a.Ho[c][p] = h;
+    if (store) st_global(a.Ho[c] + p, h);
     return h;
   };
   // the same for a node inside every component's stepped region and outside every CPML slab
@@ -218,8 +224,8 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     if (tid == 0) produce(i + S - 1);  // into the stage of plane i - 1, which every thread has finished with
     issued = i + S - 1;
     const int si = (i - xb) % S, sn = (i + 1 - xb) % S;
-    const bool x_in = i >= a.inner_lo[0] && i < a.inner_hi[0];
-    const bool fast = x_in && yz_in;
+    const bool x_in = BOX || (i >= a.inner_lo[0] && i < a.inner_hi[0]);
+    const bool fast = BOX || (x_in && yz_in);
     if (i < xs) {  // the plane before the segment: H_y, H_z of the own node, stored by the CTA owning it
       if (own) {
         if (fast) {
@@ -238,9 +244,11 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
       hx = hx_fast(si, oo);
       hy = hy_fast(si, sn, oo);
       hz = hz_fast(si, sn, oo);
-      a.Ho[0][p] = hx;
-      a.Ho[1][p] = hy;
-      a.Ho[2][p] = hz;
+      if (!BOX || own) {  // without BOX, fast implies own
+        st_global(a.Ho[0] + p, hx);
+        st_global(a.Ho[1] + p, hy);
+        st_global(a.Ho[2] + p, hz);
+      }
     } else if (own) {
       hx = h_checked(0, si, sn, i, ty + 1, tx + 4, true);
       hy = h_checked(1, si, sn, i, ty + 1, tx + 4, true);
@@ -252,7 +260,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     hs[1][ty + 1][tx] = hz;
     if (ty == 0 && y0 > 0 && k < n2) {
       const int o = tx + 4;  // box row 0
-      if (x_in && yh_in) {
+      if (BOX || (x_in && yh_in)) {
         hs[0][0][tx] = hx_fast(si, o);
         hs[1][0][tx] = hz_fast(si, sn, o);
       } else {
@@ -263,7 +271,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     F hx_zh = zero<F>(), hy_zh = zero<F>();  // H_x, H_y at (j, z0 - 1), for lane 0
     if (tx == 0 && z0 > 0 && j < n1) {
       const int o = (ty + 1) * BZ + 3;
-      if (x_in && zh_in) {
+      if (BOX || (x_in && zh_in)) {
         hx_zh = hx_fast(si, o);
         hy_zh = hy_fast(si, sn, o);
       } else {
@@ -288,9 +296,9 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
       const F a1 = hx - hx_zm, b1 = hz - prev_hz;
       const F a2 = hy - prev_hy, b2 = hx - hx_ym;
       if (fast && !multi_cb) {
-        a.Eo[0][p] = ex[oo] + curl(a0, b0, 1, 2) * cb;
-        a.Eo[1][p] = ey[oo] + curl(a1, b1, 2, 0) * cb;
-        a.Eo[2][p] = ez[oo] + curl(a2, b2, 0, 1) * cb;
+        st_global(a.Eo[0] + p, ex[oo] + curl(a0, b0, 1, 2) * cb);
+        st_global(a.Eo[1] + p, ey[oo] + curl(a1, b1, 2, 0) * cb);
+        st_global(a.Eo[2] + p, ez[oo] + curl(a2, b2, 0, 1) * cb);
       } else {
         const int x[3] = {i, j, k};
         const F av[3] = {a0, a1, a2}, bv[3] = {b0, b1, b2};
@@ -299,13 +307,13 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
         for (int c = 0; c < 3; ++c) {
           const F e0 = e[c][oo];
           if (!fast && !in_e_region(c, x, g.n, g.periodic)) {
-            a.Eo[c][p] = e0;
+            st_global(a.Eo[c] + p, e0);
             continue;
           }
           const R cbc = c == 0 ? cb : g.cbE[c][p];
           F ev = e0 + curl(av[c], bv[c], (c + 1) % 3, (c + 2) % 3) * cbc;
           if (!fast) cpml_io<0>(ev, a, c, x, av[c], bv[c], cbc, true);
-          a.Eo[c][p] = ev;
+          st_global(a.Eo[c] + p, ev);
         }
       }
     }

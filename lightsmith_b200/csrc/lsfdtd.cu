@@ -16,7 +16,9 @@
 #include "ade.cuh"
 #include "common.cuh"
 #include "fused.cuh"
+#include "fused_pml.cuh"
 #include "fused_tma.cuh"
+#include "shell.cuh"
 #include "yee_vec.cuh"
 
 #include <cudaTypedefs.h>
@@ -104,7 +106,10 @@ struct lsfdtd_engine {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   int cur = 0;          // buffer holding the current fields
   int fused = -1;       // -1 undecided, 0 in-place kernels, 1 fused single pass
-  int variant = 0;  // 0: in-place H and E kernels; 1: the fused single pass; 2: in-place four-node kernels
+  // 0: in-place H and E kernels; 1: the fused single pass; 2: in-place four-node kernels; 3: the fused pass
+  // split into an interior box without region or CPML code and shell kernels; 4: the fused pass with lean CPML
+  // terms (3 and 4 run as 1 where they do not apply)
+  int variant = 0;
   int tile_y = 8, planes = 32, stages = 4;
   int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
@@ -124,6 +129,7 @@ struct lsfdtd_engine {
   virtual int add_mode(const lsfdtd_mode_source_desc* s) = 0;
   virtual int add_monitor(const lsfdtd_monitor_desc* m) = 0;
   virtual size_t need_scratch() const = 0;
+  bool fused_variant() const { return variant == 1 || variant == 3 || variant == 4; }
   virtual int step(cudaStream_t s) = 0;
   virtual int sample(cudaStream_t s) = 0;
   virtual int update_h(cudaStream_t s) = 0;
@@ -257,18 +263,87 @@ struct Engine final : lsfdtd_engine {
   // 3D tensor maps (z fastest) of the field buffers and the coefficient, boxes as k_fused_tma copies them
   bool uses_tma() const override { return tma_ok; }
 
-  template <int TY, int S>
-  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+  template <int TY, int S, bool BOX>
+  int launch_tma_box(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
       constexpr size_t sm = fused_tma_smem_bytes<F, TY, S>();
       static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
       if (!attr) {
-        LS_CUDA(cudaFuncSetAttribute(k_fused_tma<F, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        LS_CUDA(cudaFuncSetAttribute(k_fused_tma<F, TY, S, BOX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
         attr = true;
       }
-      k_fused_tma<F, TY, S><<<grid, dim3(32, TY), sm, s>>>(ta);
+      k_fused_tma<F, TY, S, BOX><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
+  }
+  template <int TY, int S>
+  int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+    if constexpr (!kComplex) {
+      constexpr size_t sm = fused_pml_smem_bytes<F, TY, S>();
+      static bool attr = false;
+      if (!attr) {
+        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+      }
+      k_fused_pml<F, TY, S><<<grid, dim3(32, TY), sm, s>>>(ta);
+    }
+    return LSFDTD_OK;
+  }
+  // kind 0: the fused pass over the grid, 1: over the interior box of the split step, 2: with lean CPML terms
+  template <int TY, int S>
+  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s, int kind) {
+    if (kind == 2) return launch_pml<TY, S>(grid, ta, s);
+    return kind == 1 ? launch_tma_box<TY, S, true>(grid, ta, s) : launch_tma_box<TY, S, false>(grid, ta, s);
+  }
+  template <int TY, int S>
+  static constexpr size_t tma_smem(int kind) {
+    return kind == 2 ? fused_pml_smem_bytes<F, TY, S>() : fused_tma_smem_bytes<F, TY, S>();
+  }
+
+  // the lean-CPML pass needs its copies by the Tensor Memory Accelerator and, per axis, CPML slabs that do
+  // not overlap
+  bool lean_ok() const {
+    if (variant != 4 || !tma_ok) return false;
+    for (int d = 0; d < 3; ++d) {
+      if (!y.pml[d].on) continue;
+      for (int f = 0; f < 2; ++f) {
+        const int c = (d + 1) % 3;
+        const int lo_end = y.pml[d].start[f][c][0] + y.pml[d].len[f][c][0];
+        if (y.pml[d].len[f][c][0] > 0 && y.pml[d].len[f][c][1] > 0 && lo_end > y.pml[d].start[f][c][1]) return false;
+      }
+    }
+    return true;
+  }
+
+  // nodes [lo, hi) per axis stepped for every component and outside every CPML slab
+  void inner_bounds(int* lo_out, int* hi_out) const {
+    for (int ax = 0; ax < 3; ++ax) {
+      int lo = 1, hi = desc.shape[ax] - 1;
+      if (y.pml[ax].on) {
+        lo = std::max(lo, pml_cells[ax][0] ? pml_cells[ax][0] + 1 : 1);
+        hi = std::min(hi, pml_cells[ax][1] ? desc.shape[ax] - 2 - pml_cells[ax][1] : hi);
+      }
+      lo_out[ax] = lo;
+      hi_out[ax] = std::max(lo, hi);
+    }
+  }
+
+  // the interior box of the split step and its shell; false when the split does not apply (no TMA copies,
+  // an empty box, or a shell of 2^32 nodes or more)
+  bool split_box(int* lo, int* hi, ShellBoxes* sb) const {
+    if (variant != 3 || !tma_ok) return false;
+    int ilo[3], ihi[3];
+    inner_bounds(ilo, ihi);
+    for (int ax = 0; ax < 3; ++ax) {
+      lo[ax] = ilo[ax] + 1;  // the low-side halo node of the box is inner too
+      hi[ax] = ihi[ax];
+    }
+    lo[2] = (lo[2] + 3) / 4 * 4;  // tensor-copy boxes start at z0 - 4 on a 16-byte boundary
+    for (int ax = 0; ax < 3; ++ax)
+      if (hi[ax] <= lo[ax]) return false;
+    *sb = shell_boxes(desc.shape, lo, hi);
+    return sb->total > 0 && sb->total < (1ull << 32);
   }
 
   int make_maps() {
@@ -324,23 +399,25 @@ struct Engine final : lsfdtd_engine {
           fa.psiHo[d][c][sd] = psiH[o][d][c][sd];
         }
     fa.seg = planes;
-    // nodes stepped for every component and outside every CPML slab, per axis
+    inner_bounds(fa.inner_lo, fa.inner_hi);
     for (int ax = 0; ax < 3; ++ax) {
-      int lo = 1, hi = desc.shape[ax] - 1;
-      if (y.pml[ax].on) {
-        lo = std::max(lo, pml_cells[ax][0] ? pml_cells[ax][0] + 1 : 1);
-        hi = std::min(hi, pml_cells[ax][1] ? desc.shape[ax] - 2 - pml_cells[ax][1] : hi);
-      }
-      fa.inner_lo[ax] = lo;
-      fa.inner_hi[ax] = std::max(lo, hi);
       fa.pml_lo[ax] = y.pml[ax].on ? pml_cells[ax][0] : 0;
       fa.pml_hi[ax] = y.pml[ax].on ? pml_cells[ax][1] : 0;
+      fa.box_lo[ax] = 0;
+      fa.box_hi[ax] = desc.shape[ax];
     }
-    // CTA-tile kernels have 8 or 16 rows (warp tiles size their own grid below)
-    const dim3 grid(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], tile_y == 16 ? 16 : 8), cdiv(desc.shape[0], planes));
-    LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
       if (tma_ok && maps_tile_y != tile_y) tma_ok = make_maps() == LSFDTD_OK;
+    }
+    ShellBoxes sb{};
+    const bool split = split_box(fa.box_lo, fa.box_hi, &sb);
+    const int kind = split ? 1 : (lean_ok() ? 2 : 0);
+    const int rows = tile_y == 16 ? 16 : 8;
+    const dim3 grid = split ? dim3(cdiv(fa.box_hi[2] - fa.box_lo[2], 32), cdiv(fa.box_hi[1] - fa.box_lo[1], rows),
+                                   cdiv(fa.box_hi[0] - fa.box_lo[0], planes))
+                            : dim3(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], rows), cdiv(desc.shape[0], planes));
+    LS_TRY(mark(s, true));
+    if constexpr (!kComplex) {
       if (tma_ok) {
         TmaArgs<F> ta;
         ta.f = fa;
@@ -357,15 +434,22 @@ struct Engine final : lsfdtd_engine {
         auto fits = [&](size_t b) { return b <= (size_t)smax; };
         int r = LSFDTD_OK;
         if (tile_y == 16) {
-          if (stages >= 8 && fits(fused_tma_smem_bytes<F, 16, 8>())) r = launch_tma<16, 8>(grid, ta, s);
-          else if (stages >= 6 && fits(fused_tma_smem_bytes<F, 16, 6>())) r = launch_tma<16, 6>(grid, ta, s);
-          else r = launch_tma<16, 4>(grid, ta, s);
+          if (stages >= 8 && fits(tma_smem<16, 8>(kind))) r = launch_tma<16, 8>(grid, ta, s, kind);
+          else if (stages >= 6 && fits(tma_smem<16, 6>(kind))) r = launch_tma<16, 6>(grid, ta, s, kind);
+          else r = launch_tma<16, 4>(grid, ta, s, kind);
         } else {
-          if (stages >= 8 && fits(fused_tma_smem_bytes<F, 8, 8>())) r = launch_tma<8, 8>(grid, ta, s);
-          else if (stages >= 6 && fits(fused_tma_smem_bytes<F, 8, 6>())) r = launch_tma<8, 6>(grid, ta, s);
-          else r = launch_tma<8, 4>(grid, ta, s);
+          if (stages >= 8 && fits(tma_smem<8, 8>(kind))) r = launch_tma<8, 8>(grid, ta, s, kind);
+          else if (stages >= 6 && fits(tma_smem<8, 6>(kind))) r = launch_tma<8, 6>(grid, ta, s, kind);
+          else r = launch_tma<8, 4>(grid, ta, s, kind);
         }
         if (r != LSFDTD_OK) return r;
+        if (split) {
+          LS_LAUNCHED();
+          const unsigned blocks = (unsigned)cdiv((long long)sb.total, 256);
+          k_shell_h<F><<<blocks, 256, 0, s>>>(fa, sb);
+          LS_LAUNCHED();
+          k_shell_e<F><<<blocks, 256, 0, s>>>(fa, sb);
+        }
       } else if (tile_y == 16) {
         constexpr size_t sm = fused_smem_bytes<F, 16, kStages>();  // cp.async ring
         if (!attr_set[1]) {
@@ -813,7 +897,7 @@ struct Engine final : lsfdtd_engine {
 
   int step(cudaStream_t s) override {
     if (scratch_bytes < need_scratch()) return fail(LSFDTD_EINVAL, "scratch not set or too small");
-    if (decide() && variant == 1) {
+    if (decide() && fused_variant()) {
       LS_TRY(fused_step(s));
     } else {
       LS_TRY(update_h(s));
@@ -868,7 +952,12 @@ struct Engine final : lsfdtd_engine {
   }
 
   int64_t launches_per_chunk() const override {
-    int64_t per_step = (fused == 1 && variant == 1 ? 1 : 2) + 1;  // fused pass or H and E, counter
+    int64_t per_step = 2 + 1;  // H and E, counter
+    if (fused == 1 && fused_variant()) {
+      int lo[3], hi[3];
+      ShellBoxes sb{};
+      per_step = (split_box(lo, hi, &sb) ? 3 : 1) + 1;  // fused pass (interior box, shell H and E), counter
+    }
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
     for (auto& g : groups) per_step += g.n > 0;
@@ -1050,7 +1139,7 @@ int32_t lsfdtd_engine_chunk(lsfdtd_engine* eng, int32_t n_chunks, int32_t use_gr
     }
     LS_CUDA(cudaGraphLaunch(eng->exec[b], s));
     eng->n_host += eng->desc.dft_stride;
-    if (eng->fused == 1 && eng->variant == 1 && (eng->desc.dft_stride & 1)) eng->cur ^= 1;
+    if (eng->fused == 1 && eng->fused_variant() && (eng->desc.dft_stride & 1)) eng->cur ^= 1;
   }
   return LSFDTD_OK;
 }
@@ -1109,20 +1198,21 @@ int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma) {
 }
 
 int32_t lsfdtd_engine_uses_tma(lsfdtd_engine* eng) {
-  return eng ? (eng->decide() && eng->variant == 1 && eng->uses_tma()) : -1;
+  return eng ? (eng->decide() && eng->fused_variant() && eng->uses_tma()) : -1;
 }
 
-int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? (eng->decide() && eng->variant == 1) : -1; }
+int32_t lsfdtd_engine_fused(lsfdtd_engine* eng) { return eng ? (eng->decide() && eng->fused_variant()) : -1; }
 
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
                                  int32_t stages) {
   LS_NEED(eng);
   const bool ok = variant == 0 || variant == 2 ||
-                  (variant == 1 && (tile_y == 8 || tile_y == 16) && (stages == 4 || stages == 6 || stages == 8) &&
-                   planes >= 1);
+                  ((variant == 1 || variant == 3 || variant == 4) && (tile_y == 8 || tile_y == 16) &&
+                   (stages == 4 || stages == 6 || stages == 8) && planes >= 1);
   if (!ok)
-    return fail(LSFDTD_EINVAL, "tuning: variant 0 (in-place kernels), 2 (in-place four-node kernels) or 1 (fused "
-                               "pass: CTA tile rows 8 or 16, ring 4, 6 or 8, planes >= 1)");
+    return fail(LSFDTD_EINVAL, "tuning: variant 0 (in-place kernels), 2 (in-place four-node kernels), 1 (fused "
+                               "pass), 3 (fused pass split into interior box and shell) or 4 (fused pass with lean "
+                               "CPML terms); for 1, 3 and 4 CTA tile rows 8 or 16, ring 4, 6 or 8, planes >= 1");
   if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "tuning must be set before the first graph capture");
   eng->variant = variant;
   eng->tile_y = tile_y;

@@ -492,8 +492,9 @@ class Engine:
                    "lsfdtd_engine_status")
 
     def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:
-        """Launch shape of the fused pass (before the first graph capture): variant 0 warp-independent tiles
-        (rows 4 or 8, ring 3/4/6) or 1 CTA tiles (rows 8 or 16, ring 4/6/8), x planes per tile, ring depth."""
+        """Kernel choice and launch shape (before the first graph capture): variant 0 the in-place H and E
+        kernels, 2 their four-node vector form, 1 the fused pass (CTA tile rows 8 or 16, x planes per tile,
+        copy ring 4/6/8), 3 the fused pass split into an interior box and a CPML/wall shell kernel."""
         _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(variant), int(tile_y), int(planes),
                                                        int(stages)), "lsfdtd_engine_set_tuning")
 

@@ -6,7 +6,7 @@ its copy ring. ``tune_engine`` times each candidate on an engine with CUDA event
 the engine on the fastest. ``best_shape`` caches the choice per GPU model and grid shape in a JSON file.
 
     python -m lightsmith_b200.tune --n 640                  # sweep the throughput case, print the best
-    python -m lightsmith_b200.tune --n 384 --shape 8,32,4   # one shape (e.g. under ncu)
+    python -m lightsmith_b200.tune --n 384 --shape 3,8,32,4   # one shape (e.g. under ncu)
 """
 
 from __future__ import annotations
@@ -16,8 +16,10 @@ import json
 import os
 
 # (variant, tile rows, x planes per tile, ring depth): variant 0 the in-place kernels, 2 their four-node
-# vector form, 1 the fused pass
-CANDIDATES = [(0, 8, 32, 4), (2, 8, 32, 4), (1, 8, 32, 4), (1, 16, 32, 4), (1, 8, 64, 4)]
+# vector form, 1 the fused pass, 3 the fused pass split into an interior box and the CPML/wall shell, 4 the
+# fused pass with lean CPML terms
+CANDIDATES = [(0, 8, 32, 4), (2, 8, 32, 4), (1, 8, 32, 4), (1, 16, 32, 4), (3, 8, 32, 4), (3, 16, 32, 4),
+              (4, 8, 32, 4), (4, 16, 32, 4)]
 
 
 def _cache_path() -> str:
@@ -47,7 +49,11 @@ def best_shape(eng, candidates=CANDIDATES, path: str | None = None):
     """The cached best shape for this GPU model and grid shape, tuning (and caching) it on a miss."""
     import torch
 
-    key = f"{torch.cuda.get_device_name(eng.dev)}|{'x'.join(map(str, eng.shape))}|{'f32' if eng.single else 'f64'}"
+    import zlib
+
+    cands = zlib.crc32(repr([tuple(c) for c in candidates]).encode())  # a new candidate list tunes afresh
+    key = (f"{torch.cuda.get_device_name(eng.dev)}|{'x'.join(map(str, eng.shape))}|"
+           f"{'f32' if eng.single else 'f64'}|{cands:08x}")
     path = path or _cache_path()
     cache = {}
     try:

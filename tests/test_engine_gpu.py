@@ -11,6 +11,8 @@ pytestmark = pytest.mark.gpu
 # float64 kernels differ from the reference only by fused multiply-adds and summation order; float32 is the
 # reference GPU precision (lightsmith runs float32 on GPUs), compared with its float64 CPU run
 TOL = {"double": 1e-9, "single": 3e-4}
+# two kernel paths of this library with the same arithmetic per value (fused multiply-adds may differ)
+SAME_ARITHMETIC = {"double": 1e-13, "single": 2e-6}
 
 
 def _rel(a, b):
@@ -80,7 +82,9 @@ def test_source_waveform_end_raises(golden):
 FUSED_CASES = ["yee_cpml_dipole", "kappa_noncubic", "ade_groups"]
 
 
-@pytest.mark.parametrize("variant,tile_y,planes,stages", [(1, 8, 3, 4), (1, 16, 5, 6), (1, 16, 128, 8), (1, 8, 2, 8)])
+@pytest.mark.parametrize("variant,tile_y,planes,stages", [(1, 8, 3, 4), (1, 16, 5, 6), (1, 16, 128, 8), (1, 8, 2, 8),
+                                                          (3, 8, 3, 4), (3, 16, 5, 6), (3, 8, 1, 8),
+                                                          (4, 8, 3, 4), (4, 16, 5, 6), (4, 8, 1, 8)])
 @pytest.mark.parametrize("case", FUSED_CASES)
 def test_fused_pass_any_launch_shape(case, variant, tile_y, planes, stages, golden):
     """The fused pass under launch shapes that split x into several segments (each CTA then recomputes the
@@ -112,6 +116,36 @@ def test_fused_pass_equals_in_place_kernels(case, golden):
         b.chunk(1, use_graph=True)
     assert _rel(a.E.cpu().numpy(), b.E.cpu().numpy()) < 1e-6
     assert _rel(a.H.cpu().numpy(), b.H.cpu().numpy()) < 1e-6
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("variant", [3, 4])
+@pytest.mark.parametrize("precision", ["single", "double"])
+def test_split_and_lean_passes_equal_fused_pass(variant, precision, golden):
+    """The split step (interior box without region or CPML code, then the shell H and E kernels) and the
+    lean-CPML pass give the fused pass's values: the same arithmetic per value, in separately compiled
+    kernels (which may contract a multiply and an add into one fused multiply-add differently), so equal to
+    the last bits."""
+    from lightsmith_b200.engine import Engine
+
+    plan = golden("engine_yee_cpml_dipole")["plan"]
+    a = Engine.from_plan(plan, precision=precision)
+    b = Engine.from_plan(plan, precision=precision)
+    a.set_tuning(1, 8, 4, 4)
+    b.set_tuning(variant, 8, 4, 4)
+    assert a.uses_tma and b.uses_tma
+    extra = 2 if variant == 3 else 0  # the shell H and E kernels of the split step
+    assert b.launches_per_chunk() == a.launches_per_chunk() + extra * plan["stride"]
+    for _ in range(5):
+        a.chunk(1, use_graph=True)
+        b.chunk(1, use_graph=True)
+    b.check_status()
+    assert np.abs(a.E.cpu().numpy()).max() > 0
+    tol = SAME_ARITHMETIC[precision]
+    assert _rel(b.E.cpu().numpy(), a.E.cpu().numpy()) < tol
+    assert _rel(b.H.cpu().numpy(), a.H.cpu().numpy()) < tol
+    assert _rel(b.results(0)[0], a.results(0)[0]) < tol
     a.close()
     b.close()
 

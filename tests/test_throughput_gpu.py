@@ -36,6 +36,37 @@ def test_throughput_case_matches_oracle_at_128():
     np.testing.assert_allclose(gpu32.energy.cpu().numpy()[0], ref.energy[0], rtol=1e-3)
 
 
+@pytest.mark.parametrize("variant", [3, 4])
+@pytest.mark.parametrize("n,pml", [(128, 16), (100, 10), (72, 12)])
+def test_split_and_lean_passes_equal_fused_pass_on_the_throughput_case(n, pml, variant):
+    """Interior box plus shell (3) and the lean-CPML pass (4) against the one-kernel fused pass, on grids
+    whose box and slab edges fall inside tiles and x segments (n = 100, 72) and where they do not (128): the
+    same arithmetic per value, equal to the last bits (the kernels may contract multiply-adds differently)."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+
+    plan = throughput_plan(n, pml=pml, max_steps=2000, seed=5)
+    w = plan["sources"][0].wave
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    plan["sources"][0].wave = np.concatenate([w[first:], np.zeros(first)])
+    a = Engine.from_plan(plan)
+    b = Engine.from_plan(plan)
+    a.set_tuning(1, 8, 24, 4)
+    b.set_tuning(variant, 8, 24, 4)
+    assert a.uses_tma and b.uses_tma
+    for _ in range(3):
+        a.chunk(1, use_graph=True)
+        b.chunk(1, use_graph=True)
+    b.check_status()
+    ea, eb = a.E.cpu().numpy(), b.E.cpu().numpy()
+    assert np.abs(ea).max() > 0
+    assert _rel(eb, ea) < 2e-6
+    assert _rel(b.H.cpu().numpy(), a.H.cpu().numpy()) < 2e-6
+    assert _rel(b.results(0)[0], a.results(0)[0]) < 2e-6
+    a.close()
+    b.close()
+
+
 @pytest.mark.slow
 def test_full_size_run_is_linear_in_the_source_bit_for_bit():
     """Every update is linear in the fields, and scaling by 2 is exact in binary floating point (away from
