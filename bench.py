@@ -60,15 +60,19 @@ def _peak():
         return 6650.0, "fallback"
 
 
-def _ncu_traffic_per_cell():
-    """DRAM bytes per cell update of the bulk kernels from the committed ncu summary, if any."""
-    path = os.path.join(HERE, "profiles", "yee_bulk_throughput.md")
-    try:
-        text = open(path).read()
-    except OSError:
-        return None
-    m = re.search(r"dram_bytes_per_cell_update:\s*([0-9.]+)", text)
-    return float(m.group(1)) if m else None
+def _ncu_traffic_per_cell(variant: int):
+    """DRAM bytes per cell update of the bulk kernels of one variant, from the committed ncu summaries (lines
+    ``dram_bytes_per_cell_update[variant V]: X``), if any."""
+    pattern = re.compile(r"dram_bytes_per_cell_update\[variant (\d)\]:\s*([0-9.]+)")
+    for name in sorted(os.listdir(os.path.join(HERE, "profiles"))):
+        try:
+            text = open(os.path.join(HERE, "profiles", name)).read()
+        except OSError:
+            continue
+        for v, x in pattern.findall(text):
+            if int(v) == variant:
+                return float(x)
+    return None
 
 
 class Clocks:
@@ -243,7 +247,7 @@ def run_b200(args):
     alg_bytes = cells * BYTES_PER_CELL + cells_in_cpml(eng.plan) * BYTES_PER_CPML_PAIR
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     peak, peak_kind = _peak()
-    tpc = _ncu_traffic_per_cell()
+    tpc = _ncu_traffic_per_cell(variant)
 
     # end to end through the C ABI with host buffers: permittivity from pinned host memory, K chunks, the DFT
     # accumulators and the energy back to pinned host memory
@@ -292,8 +296,10 @@ def run_b200(args):
                           "l2": "inputs larger than L2 (about 8 GB of state per replica)",
                           "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
                           "variant": {0: "in-place H and E kernels", 1: "fused single pass",
-                                      2: "in-place four-node H and E kernels"}[variant],
-                          "copy_engine": ("TMA" if eng_tma else "cp.async") if variant == 1 else None},
+                                      2: "in-place four-node H and E kernels",
+                                      3: "fused single pass over the interior box + CPML/wall shell kernels",
+                                      4: "fused single pass with lean CPML terms"}[variant],
+                          "copy_engine": ("TMA" if eng_tma else "cp.async") if variant in (1, 3, 4) else None},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_source": peak_kind,
                             "traffic": None if tpc is None else tpc * cells,

@@ -10,7 +10,8 @@
 // the x march (rows y0-1 .. y0+TY-1 and columns z0-1 .. z0+31 of the tile, for E and for H) and, along x,
 // from one lookup per plane that is uniform across the CTA. Along an axis d the slabs of the two components
 // with a psi along d have the same extent, so one entry serves both. A CPML term then costs a predicate, an
-// index, a coalesced psi load and store and two multiply-adds; its arithmetic and order are cpml_io's.
+// index, a coalesced psi load and store and two multiply-adds; its arithmetic and order are cpml_io's. A lean
+// warp issues all psi loads of its own nodes at the top of each plane, ahead of its wait for the plane.
 //
 // The region tests are those of a grid without periodic axes (the fused pass serves no other): H_c is stepped
 // where x_a <= n_a - 2 for every a != c, E_c where 1 <= x_a <= n_a - 2 for a != c and x_c <= n_c - 2; other
@@ -67,48 +68,53 @@ struct PmlTables {
 
 template <typename F, int TY, int S>
 constexpr size_t fused_pml_smem_bytes() {
-  return fused_tma_smem_bytes<F, TY, S>() + (sizeof(PmlTables<F, TY>) + 15) / 16 * 16;
+  return fused_tma_smem_bytes<F, TY, S>() + (sizeof(PmlTables<F, TY>) + 15) / 16 * 16;  // tables after kUsed
 }
 
-// the CPML term along axis d of a value v of field FLD, component c, at node x (psi index from the slab
-// info of that axis); psi_out == nullptr: a halo node, computed but not stored
+// index of node x in the psi slab of axis d described by si
+template <typename F>
+__device__ __forceinline__ long long pml_index(const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
+                                               int d, const int* x) {
+  if (d == 0) return ((long long)(x[0] - si.st) * g.n[1] + x[1]) * g.n[2] + x[2];
+  if (d == 1) return ((long long)x[0] * si.len + (x[1] - si.st)) * g.n[2] + x[2];
+  return ((long long)x[0] * g.n[1] + x[1]) * si.len + (x[2] - si.st);
+}
+
+// the CPML term along axis d of a value v of field FLD, component c, at psi index q, from psi_prev (the node's
+// psi before this step); psi_out == nullptr: a halo node, computed but not stored
 template <int FLD, typename F>
 __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
-                                         int d, int c, const int* x, F der, typename real_of<F>::type scale,
-                                         const F* psi_in, F* psi_out) {
+                                         int d, int c, long long q, F der, typename real_of<F>::type scale,
+                                         F psi_prev, F* psi_out) {
   using R = typename real_of<F>::type;
   const int d1 = (c + 1) % 3;
   R sgn = (d == d1) ? R(1) : R(-1);
   if (FLD == 1) sgn = -sgn;
   R s = g.uniform ? scale : scale / g.pml[d].div;
   s = sgn * s;
-  long long q;
-  if (d == 0)
-    q = ((long long)(x[0] - si.st) * g.n[1] + x[1]) * g.n[2] + x[2];
-  else if (d == 1)
-    q = ((long long)x[0] * si.len + (x[1] - si.st)) * g.n[2] + x[2];
-  else
-    q = ((long long)x[0] * g.n[1] + x[1]) * si.len + (x[2] - si.st);
-  F psi = (FLD == 1 ? ro(psi_in + q) : psi_in[q]) * si.b;
+  F psi = psi_prev * si.b;
   if (g.pml[d].k[FLD]) v += (s * si.k) * der;
   psi += der * (s * si.c);
   if (psi_out) st_global(psi_out + q, psi);
   v += psi;
 }
 
+// FP32: four CTAs of 8 rows (two of 16) per SM, at most 64 registers per thread, which their shared memory
+// allows; FP64 tiles need twice the shared memory and are not constrained
 template <typename F, int TY, int S>
-__global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
+__global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 1)
+    k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
   using R = typename real_of<F>::type;
   using St = TmaStage<F, TY>;
   using Tab = PmlTables<F, TY>;
   constexpr int TZ = 32, BZ = St::BZ, NT = 32 * TY;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
-  F(*sH)[2][TY + 1][TZ] = reinterpret_cast<F(*)[2][TY + 1][TZ]>(smem + S * St::kBytes);
-  unsigned long long* bar =
-      reinterpret_cast<unsigned long long*>(smem + S * St::kBytes + 2 * 2 * (TY + 1) * TZ * sizeof(F));
-  // the tables follow the ring, the H exchange rows and the barriers
-  Tab& tab = *reinterpret_cast<Tab*>(smem + S * St::kBytes + 2 * 2 * (TY + 1) * TZ * sizeof(F) + S * 8);
+  using L = TmaLayout<F, TY, S>;
+  F(*sH)[2][TY + 1][TZ] = reinterpret_cast<F(*)[2][TY + 1][TZ]>(smem + L::kRing);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + L::kRing + L::kRows);
+  F(*zc)[2][TY] = reinterpret_cast<F(*)[2][TY]>(smem + L::kRing + L::kRows + L::kBars);  // [plane][H_x, H_y][row]
+  Tab& tab = *reinterpret_cast<Tab*>(smem + L::kUsed);
 
   const FusedArgs<F>& a = t.f;
   const YeeArgs<F>& g = a.y;
@@ -182,7 +188,9 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
 
   // H^{n+1/2}_c of the tile node at table row yy (y = y0 - 1 + yy) and column zz (z = z0 - 1 + zz) of plane i,
   // with region test and CPML terms; xs_h: the plane's x slab info (H); store: an own node (H and psi out)
-  auto h_lean = [&](int c, int si, int sn, int i, int yy, int zz, const SlabInfo<R>& xs_h, bool store) -> F {
+  // pre: the node's psi per axis, loaded ahead (own nodes), or nullptr to load it here (halo nodes)
+  auto h_lean = [&](int c, int si, int sn, int i, int yy, int zz, const SlabInfo<R>& xs_h, bool store,
+                    const F* pre) -> F {
     const int row = yy, col = zz + 3;
     const int x[3] = {i, y0 - 1 + yy, z0 - 1 + zz};
     const F h0 = stH(si, c)[row][col];
@@ -213,9 +221,10 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
       if (d == c) continue;
       const SlabInfo<R>& sl = d == 0 ? xs_h : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
       if (sl.side < 0) continue;
-      const F* pin = g.pml[d].psi[1][c][sl.side];
+      const long long q = pml_index(g, sl, d, x);
+      const F prev = pre ? pre[d] : ro(g.pml[d].psi[1][c][sl.side] + q);
       F* pout = store ? a.psiHo[d][c][sl.side] : nullptr;
-      pml_term<1>(h, g, sl, d, c, x, d == d1 ? av : bv, g.cH, pin, pout);
+      pml_term<1>(h, g, sl, d, c, q, d == d1 ? av : bv, g.cH, prev, pout);
     }
     if (store) st_global(a.Ho[c] + p, h);
     return h;
@@ -230,13 +239,59 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
   const bool warp_clean = y_in(j) && (ty != 0 || y_in(y0 - 1)) && z0 - 1 >= a.inner_lo[2] &&
                           z0 + TZ <= a.inner_hi[2];
   const bool multi_cb = g.cbE[1] != g.cbE[0] || g.cbE[2] != g.cbE[0];
+  // the halo column z0 - 1 and all the tile's rows are inner along y and z
+  const bool col_clean = z0 - 1 >= a.inner_lo[2] && z0 - 1 < a.inner_hi[2] && y_in(y0) && y0 + TY <= a.inner_hi[1];
+  constexpr int kColWarp = TY > 1 ? 1 : 0;  // warp 0 computes the halo row, this warp the halo column
+  // own node: components stepped as far as y and z decide (bit c), for H and for E; the x part per plane
+  unsigned yz_hm = 0, yz_em = 0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const bool hy_ok = c == 1 || j <= n1 - 2, hz_ok = c == 2 || k <= n2 - 2;
+    const bool ey_ok = j <= n1 - 2 && (c == 1 || j >= 1), ez_ok = k <= n2 - 2 && (c == 2 || k >= 1);
+    yz_hm |= (hy_ok && hz_ok ? 1u : 0u) << c;
+    yz_em |= (ey_ok && ez_ok ? 1u : 0u) << c;
+  }
 
   F prev_hy = zero<F>(), prev_hz = zero<F>();
   bool failed = false;
   int cons = xb - 1;
 #pragma unroll 1
   for (int i = xb; i < xe; ++i) {
-    const bool ok = ready(i) && ready(i + 1);
+    const bool fast = warp_clean && i >= a.inner_lo[0] && i < a.inner_hi[0];
+    SlabInfo<R> xs_h, xs_e;
+    // a lean warp issues the psi loads of its own nodes for this plane before it waits for the plane's
+    // copies, so that their latency overlaps the wait and each other: [component][axis], with the psi index
+    // per axis (H, E)
+    F pre_h[3][3], pre_e[3][3];
+    long long qh[3] = {0, 0, 0}, qe[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) pre_h[c][d] = pre_e[c][d] = zero<F>();
+    if (!fast) {
+      xs_h = slab_info<1>(g.pml[0], 0, i);
+      xs_e = slab_info<0>(g.pml[0], 0, i);
+      if (own) {
+        const int x[3] = {i, j, k};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const SlabInfo<R>& sh = d == 0 ? xs_h : (d == 1 ? tab.y[1][ty + 1] : tab.z[1][tx + 1]);
+          const SlabInfo<R>& se = d == 0 ? xs_e : (d == 1 ? tab.y[0][ty + 1] : tab.z[0][tx + 1]);
+          const int c1 = (d + 1) % 3, c2 = (d + 2) % 3;  // the components with a psi along d
+          if (sh.side >= 0) {
+            qh[d] = pml_index(g, sh, d, x);
+            pre_h[c1][d] = ro(g.pml[d].psi[1][c1][sh.side] + qh[d]);
+            pre_h[c2][d] = ro(g.pml[d].psi[1][c2][sh.side] + qh[d]);
+          }
+          if (se.side >= 0 && i >= xs) {
+            qe[d] = pml_index(g, se, d, x);
+            pre_e[c1][d] = g.pml[d].psi[0][c1][se.side][qe[d]];
+            pre_e[c2][d] = g.pml[d].psi[0][c2][se.side][qe[d]];
+          }
+        }
+      }
+    }
+    const bool ok = (i > xb || ready(i)) && ready(i + 1);  // plane i was waited for as plane i + 1 before
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -245,37 +300,58 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
     if (tid == 0) produce(i + S - 1);
     issued = i + S - 1;
     const int si = (i - xb) % S, sn = (i + 1 - xb) % S;
-    const bool fast = warp_clean && i >= a.inner_lo[0] && i < a.inner_hi[0];
-    SlabInfo<R> xs_h, xs_e;
-    if (!fast) {
-      xs_h = slab_info<1>(g.pml[0], 0, i);
-      xs_e = slab_info<0>(g.pml[0], 0, i);
-    }
-    if (i < xs) {  // the plane before the segment: H_y, H_z of the own node, not stored
-      if (own) {
-        if (fast) {
-          prev_hy = hy_fast(si, sn, oo);
-          prev_hz = hz_fast(si, sn, oo);
-        } else {
-          prev_hy = h_lean(1, si, sn, i, ty + 1, tx + 1, xs_h, false);
-          prev_hz = h_lean(2, si, sn, i, ty + 1, tx + 1, xs_h, false);
-        }
-      }
-      continue;
-    }
     const long long p = i * s0 + off_jk;
     F hx = zero<F>(), hy = zero<F>(), hz = zero<F>();
     if (fast) {
       hx = hx_fast(si, oo);
       hy = hy_fast(si, sn, oo);
       hz = hz_fast(si, sn, oo);
-      st_global(a.Ho[0] + p, hx);
-      st_global(a.Ho[1] + p, hy);
-      st_global(a.Ho[2] + p, hz);
+      if (i >= xs) {
+        st_global(a.Ho[0] + p, hx);
+        st_global(a.Ho[1] + p, hy);
+        st_global(a.Ho[2] + p, hz);
+      }
     } else if (own) {
-      hx = h_lean(0, si, sn, i, ty + 1, tx + 1, xs_h, true);
-      hy = h_lean(1, si, sn, i, ty + 1, tx + 1, xs_h, true);
-      hz = h_lean(2, si, sn, i, ty + 1, tx + 1, xs_h, true);
+      // the fast formulas, then the region mask and the CPML terms of the axes whose slab holds the node
+      // (x: uniform per plane, y: per warp, z: per lane), in cpml_io's order; nothing stored before xs
+      const bool st = i >= xs;
+      const F* ex = &stE(si, 0)[0][0];
+      const F* ey = &stE(si, 1)[0][0];
+      const F* ez = &stE(si, 2)[0][0];
+      const F av[3] = {ez[oo + BZ] - ez[oo], ex[oo + 1] - ex[oo], (&stE(sn, 1)[0][0])[oo] - ey[oo]};
+      const F bv[3] = {ey[oo + 1] - ey[oo], (&stE(sn, 2)[0][0])[oo] - ez[oo], ex[oo + BZ] - ex[oo]};
+      const unsigned hm = yz_hm & (i <= n0 - 2 ? 7u : 1u);
+      const SlabInfo<R>& yh = tab.y[1][ty + 1];
+      const SlabInfo<R>& zh = tab.z[1][tx + 1];
+      F hv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+        const F h0 = stH(si, c)[0][oo];
+        F h = h0;
+        if (hm >> c & 1u) {
+          h = h0 - curl(av[c], bv[c], d1, d2) * g.cH;
+          if (c != 0 && xs_h.side >= 0)
+            pml_term<1>(h, g, xs_h, 0, c, qh[0], d1 == 0 ? av[c] : bv[c], g.cH, pre_h[c][0],
+                        st ? a.psiHo[0][c][xs_h.side] : nullptr);
+          if (c != 1 && yh.side >= 0)
+            pml_term<1>(h, g, yh, 1, c, qh[1], d1 == 1 ? av[c] : bv[c], g.cH, pre_h[c][1],
+                        st ? a.psiHo[1][c][yh.side] : nullptr);
+          if (c != 2 && zh.side >= 0)
+            pml_term<1>(h, g, zh, 2, c, qh[2], d1 == 2 ? av[c] : bv[c], g.cH, pre_h[c][2],
+                        st ? a.psiHo[2][c][zh.side] : nullptr);
+        }
+        if (st) st_global(a.Ho[c] + p, h);
+        hv[c] = h;
+      }
+      hx = hv[0];
+      hy = hv[1];
+      hz = hv[2];
+    }
+    if (i < xs) {  // the plane before the segment: H_y, H_z of the own node only
+      prev_hy = hy;
+      prev_hz = hz;
+      continue;
     }
     F(&hs)[2][TY + 1][TZ] = sH[i & 1];
     hs[0][ty + 1][tx] = hx;
@@ -285,27 +361,28 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
         hs[0][0][tx] = hx_fast(si, tx + 4);
         hs[1][0][tx] = hz_fast(si, sn, tx + 4);
       } else {
-        hs[0][0][tx] = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false);
-        hs[1][0][tx] = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false);
+        hs[0][0][tx] = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
+        hs[1][0][tx] = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
       }
     }
-    F hx_zh = zero<F>(), hy_zh = zero<F>();  // H_x, H_y at (j, z0 - 1), for lane 0
-    if (tx == 0 && z0 > 0 && j < n1) {
-      if (fast) {
-        const int o = (ty + 1) * BZ + 3;
-        hx_zh = hx_fast(si, o);
-        hy_zh = hy_fast(si, sn, o);
+    // the halo column z0 - 1 (H_x, H_y of every row, for lane 0 of each warp): one warp, lane r for row r
+    if (ty == kColWarp && tx < TY && z0 > 0 && y0 + tx < n1) {
+      if (col_clean && i >= a.inner_lo[0] && i < a.inner_hi[0]) {
+        const int o = (tx + 1) * BZ + 3;
+        zc[i & 1][0][tx] = hx_fast(si, o);
+        zc[i & 1][1][tx] = hy_fast(si, sn, o);
       } else {
-        hx_zh = h_lean(0, si, sn, i, ty + 1, 0, xs_h, false);
-        hy_zh = h_lean(1, si, sn, i, ty + 1, 0, xs_h, false);
+        SlabInfo<R> xc_h = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;  // this warp may be fast itself
+        zc[i & 1][0][tx] = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
+        zc[i & 1][1][tx] = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
       }
     }
     F hx_zm = shfl_up(full, hx), hy_zm = shfl_up(full, hy);
-    if (tx == 0) {
-      hx_zm = hx_zh;
-      hy_zm = hy_zh;
-    }
     __syncthreads();
+    if (tx == 0) {
+      hx_zm = zc[i & 1][0][ty];
+      hy_zm = zc[i & 1][1][ty];
+    }
     if (own) {
       const F hz_ym = hs[1][ty][tx], hx_ym = hs[0][ty][tx];
       const R cb = stC(si)[ty][tx];
@@ -320,31 +397,31 @@ __global__ void __launch_bounds__(32 * TY) k_fused_pml(const __grid_constant__ T
         st_global(a.Eo[1] + p, ey[oo] + curl(a1, b1, 2, 0) * cb);
         st_global(a.Eo[2] + p, ez[oo] + curl(a2, b2, 0, 1) * cb);
       } else {
-        const int x[3] = {i, j, k};
         const F av[3] = {a0, a1, a2}, bv[3] = {b0, b1, b2};
         const F* e[3] = {ex, ey, ez};
+        const unsigned em = fast ? 7u : yz_em & ((i <= n0 - 2 ? 1u : 0u) | (i >= 1 && i <= n0 - 2 ? 6u : 0u));
+        const SlabInfo<R>& ye = tab.y[0][ty + 1];
+        const SlabInfo<R>& ze = tab.z[0][tx + 1];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const F e0 = e[c][oo];
-          bool in = x[c] <= g.n[c] - 2;
-#pragma unroll
-          for (int ax = 0; ax < 3; ++ax)
-            if (ax != c && (x[ax] < 1 || x[ax] > g.n[ax] - 2)) in = false;
-          if (!fast && !in) {
+          if (!(em >> c & 1u)) {
             st_global(a.Eo[c] + p, e0);
             continue;
           }
-          const R cbc = c == 0 ? cb : ro(g.cbE[c] + p);
-          F ev = e0 + curl(av[c], bv[c], (c + 1) % 3, (c + 2) % 3) * cbc;
+          const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+          const R cbc = (c == 0 || !multi_cb) ? cb : ro(g.cbE[c] + p);
+          F ev = e0 + curl(av[c], bv[c], d1, d2) * cbc;
           if (!fast) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              if (d == c) continue;
-              const SlabInfo<R>& sl = d == 0 ? xs_e : (d == 1 ? tab.y[0][ty + 1] : tab.z[0][tx + 1]);
-              if (sl.side < 0) continue;
-              F* ps = g.pml[d].psi[0][c][sl.side];
-              pml_term<0>(ev, g, sl, d, c, x, d == (c + 1) % 3 ? av[c] : bv[c], cbc, ps, ps);
-            }
+            if (c != 0 && xs_e.side >= 0)
+              pml_term<0>(ev, g, xs_e, 0, c, qe[0], d1 == 0 ? av[c] : bv[c], cbc, pre_e[c][0],
+                          g.pml[0].psi[0][c][xs_e.side]);
+            if (c != 1 && ye.side >= 0)
+              pml_term<0>(ev, g, ye, 1, c, qe[1], d1 == 1 ? av[c] : bv[c], cbc, pre_e[c][1],
+                          g.pml[1].psi[0][c][ye.side]);
+            if (c != 2 && ze.side >= 0)
+              pml_term<0>(ev, g, ze, 2, c, qe[2], d1 == 2 ? av[c] : bv[c], cbc, pre_e[c][2],
+                          g.pml[2].psi[0][c][ze.side]);
           }
           st_global(a.Eo[c] + p, ev);
         }

@@ -91,10 +91,21 @@ struct TmaStage {
                                              sizeof(typename real_of<F>::type) * TY * 32);
 };
 
+// dynamic shared memory of the fused passes, from its first 128-byte boundary: the copy ring, the rows of H
+// exchanged between warps (two planes), the ring's mbarriers and the tile's halo column of H (two planes)
+template <typename F, int TY, int S>
+struct TmaLayout {
+  static constexpr size_t kRing = S * TmaStage<F, TY>::kBytes;
+  static constexpr size_t kRows = 2 * 2 * (TY + 1) * 32 * sizeof(F);
+  static constexpr size_t kBars = S * 8;
+  static constexpr size_t kCol = (2 * 2 * TY * sizeof(F) + 15) / 16 * 16;
+  static constexpr size_t kUsed = kRing + kRows + kBars + kCol;
+};
+
 template <typename F, int TY, int S>
 constexpr size_t fused_tma_smem_bytes() {
   // + 128: the ring is placed at the first 128-byte boundary of the dynamic shared memory
-  return 128 + S * TmaStage<F, TY>::kBytes + 2 * 2 * (TY + 1) * 32 * sizeof(F) + S * 8;
+  return 128 + TmaLayout<F, TY, S>::kUsed;
 }
 
 template <typename F, int TY, int S, bool BOX>
@@ -105,9 +116,10 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   // bulk tensor copies need 128-byte aligned destinations
   unsigned char* smem = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
-  F(*sH)[2][TY + 1][TZ] = reinterpret_cast<F(*)[2][TY + 1][TZ]>(smem + S * St::kBytes);
-  unsigned long long* bar =
-      reinterpret_cast<unsigned long long*>(smem + S * St::kBytes + 2 * 2 * (TY + 1) * TZ * sizeof(F));
+  using L = TmaLayout<F, TY, S>;
+  F(*sH)[2][TY + 1][TZ] = reinterpret_cast<F(*)[2][TY + 1][TZ]>(smem + L::kRing);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + L::kRing + L::kRows);
+  F(*zc)[2][TY] = reinterpret_cast<F(*)[2][TY]>(smem + L::kRing + L::kRows + L::kBars);  // [plane][H_x, H_y][row]
 
   const FusedArgs<F>& a = t.f;
   const YeeArgs<F>& g = a.y;
@@ -207,7 +219,10 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
   const long long off_jk = (long long)j * s1 + k;
   const bool yz_in = own && j >= a.inner_lo[1] && j < a.inner_hi[1] && k >= a.inner_lo[2] && k < a.inner_hi[2];
   const bool yh_in = y0 - 1 >= a.inner_lo[1] && y0 - 1 < a.inner_hi[1] && k >= a.inner_lo[2] && k < a.inner_hi[2];
-  const bool zh_in = j >= a.inner_lo[1] && j < a.inner_hi[1] && z0 - 1 >= a.inner_lo[2] && z0 - 1 < a.inner_hi[2];
+  // the halo column's node of row y0 + tx (computed by lane tx of warp kColWarp)
+  const bool col_in = y0 + tx >= a.inner_lo[1] && y0 + tx < a.inner_hi[1] && z0 - 1 >= a.inner_lo[2] &&
+                      z0 - 1 < a.inner_hi[2];
+  constexpr int kColWarp = TY > 1 ? 1 : 0;  // warp 0 computes the halo row
   const bool multi_cb = g.cbE[1] != g.cbE[0] || g.cbE[2] != g.cbE[0];
 
   F prev_hy = zero<F>(), prev_hz = zero<F>();
@@ -215,7 +230,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
   int cons = xb - 1;  // planes up to cons have landed and were waited on by every thread
 #pragma unroll 1
   for (int i = xb; i < xe; ++i) {
-    const bool ok = ready(i) && ready(i + 1);
+    const bool ok = (i > xb || ready(i)) && ready(i + 1);  // plane i was waited for as plane i + 1 before
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -268,23 +283,23 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
         hs[1][0][tx] = h_checked(2, si, sn, i, 0, o, false);
       }
     }
-    F hx_zh = zero<F>(), hy_zh = zero<F>();  // H_x, H_y at (j, z0 - 1), for lane 0
-    if (tx == 0 && z0 > 0 && j < n1) {
-      const int o = (ty + 1) * BZ + 3;
-      if (BOX || (x_in && zh_in)) {
-        hx_zh = hx_fast(si, o);
-        hy_zh = hy_fast(si, sn, o);
+    // the halo column z0 - 1 (H_x, H_y of every row, for lane 0 of each warp): one warp, lane r for row r
+    if (ty == kColWarp && tx < TY && z0 > 0 && y0 + tx < n1) {
+      const int o = (tx + 1) * BZ + 3;
+      if (BOX || (x_in && col_in)) {
+        zc[i & 1][0][tx] = hx_fast(si, o);
+        zc[i & 1][1][tx] = hy_fast(si, sn, o);
       } else {
-        hx_zh = h_checked(0, si, sn, i, ty + 1, 3, false);
-        hy_zh = h_checked(1, si, sn, i, ty + 1, 3, false);
+        zc[i & 1][0][tx] = h_checked(0, si, sn, i, tx + 1, 3, false);
+        zc[i & 1][1][tx] = h_checked(1, si, sn, i, tx + 1, 3, false);
       }
     }
     F hx_zm = shfl_up(full, hx), hy_zm = shfl_up(full, hy);
-    if (tx == 0) {
-      hx_zm = hx_zh;
-      hy_zm = hy_zh;
-    }
     __syncthreads();
+    if (tx == 0) {
+      hx_zm = zc[i & 1][0][ty];
+      hy_zm = zc[i & 1][1][ty];
+    }
     if (own) {
       const F hz_ym = hs[1][ty][tx], hx_ym = hs[0][ty][tx];
       const R cb = stC(si)[ty][tx];
