@@ -285,6 +285,30 @@ int32_t lsfdtd_dft_sample_noalloc(const lsfdtd_monitor_desc* m, int32_t precisio
 /* kernel launches one chunk issues (for launch accounting) */
 int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng);
 
+/* ---- batched Bloch-periodic sweeps ------------------------------------------------------------------
+ * Replaces the sequential loop over oblique runs of lightsmith's periodic driver
+ * (backends/_fdtd/periodic.py:503-518, each run `_run_oblique`, periodic.py:426-459): many independent runs
+ * of uneven grid size advanced by one persistent kernel. Each run is an engine built as usual (complex
+ * fields; periodic x and y, CPML along z only; exactly one Bloch column source; no dispersive groups; at
+ * most four monitors on the grid or the column). The batch keeps the engines' own device state and step
+ * counters: after a batch run each engine is where its own chunks would have left it. */
+typedef struct lsfdtd_batch lsfdtd_batch;
+
+/* a batch of n engines of one precision; last[i]: the step count run i stops at (at most what its source
+ * waveform covers). The runs are spread over the kernel's CTAs longest first. */
+int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out);
+int32_t lsfdtd_batch_destroy(lsfdtd_batch* batch);
+/* device scratch the batch needs (run descriptors and the CTAs' run lists), set once; set_scratch copies
+ * the descriptors in (synchronously) */
+int32_t lsfdtd_batch_scratch_bytes(const lsfdtd_batch* batch, size_t* bytes);
+int32_t lsfdtd_batch_set_scratch(lsfdtd_batch* batch, void* scratch, size_t bytes);
+/* n_launches launches of the persistent kernel on `stream`; in each, every run advances `steps` steps (or to
+ * its last step), sampling its monitors after every dft_stride steps. use_graph: the launch is captured once
+ * as a CUDA graph (per step count) and replayed. */
+int32_t lsfdtd_batch_run(lsfdtd_batch* batch, int32_t steps, int32_t n_launches, int32_t use_graph, void* stream);
+/* CTAs of the persistent kernel (one wave) */
+int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,12 @@ SIGNATURES = {
     "lsfdtd_engine_steps": (i64, [vp]),
     "lsfdtd_engine_launches_per_chunk": (i64, [vp]),
     "lsfdtd_dft_sample_noalloc": (i32, [C.POINTER(MonitorDesc), i32, i32, vp, f64, vp, vp]),
+    "lsfdtd_batch_create": (i32, [C.POINTER(vp), i32, C.POINTER(i64), C.POINTER(vp)]),
+    "lsfdtd_batch_destroy": (i32, [vp]),
+    "lsfdtd_batch_scratch_bytes": (i32, [vp, C.POINTER(C.c_size_t)]),
+    "lsfdtd_batch_set_scratch": (i32, [vp, vp, C.c_size_t]),
+    "lsfdtd_batch_run": (i32, [vp, i32, i32, i32, vp]),
+    "lsfdtd_batch_ctas": (i32, [vp]),
 }
 
 _lib = None

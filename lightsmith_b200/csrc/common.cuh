@@ -7,9 +7,10 @@
 namespace lsfdtd {
 
 // A complex field value laid out as (re, im), the layout of torch.complex64 / complex128 and of
-// std::complex, so field tensors are passed straight through.
+// std::complex, so field tensors are passed straight through. Aligned to its size (as those tensors are),
+// so that a value moves in one 8- or 16-byte access instead of two.
 template <typename R>
-struct cplx {
+struct alignas(2 * sizeof(R)) cplx {
   R re, im;
 };
 

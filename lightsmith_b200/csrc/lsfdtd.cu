@@ -4,7 +4,9 @@
 // lightsmith's Engine.step (backends/_fdtd/engine.py:665-678) with the Yee/CPML updates fused per field, then
 // the sources' hooks, the dispersive groups and the step counter. Nothing here allocates device memory or
 // synchronises the host, so a chunk can be captured once as a CUDA graph and replayed.
+#include <algorithm>
 #include <cmath>
+#include <memory>
 #include <cstring>
 #include <type_traits>
 #include <limits>
@@ -14,6 +16,7 @@
 #include "lsfdtd.h"
 
 #include "ade.cuh"
+#include "batch.cuh"
 #include "common.cuh"
 #include "fused.cuh"
 #include "fused_pml.cuh"
@@ -137,6 +140,9 @@ struct lsfdtd_engine {
   virtual int64_t launches_per_chunk() const = 0;
   virtual int decide() = 0;
   virtual bool uses_tma() const = 0;
+  // the run descriptor of a batched Bloch sweep (BlochRun<F>), run to step `last`
+  virtual size_t bloch_desc_bytes() const = 0;
+  virtual int bloch_desc(void* out, size_t bytes, int64_t last) = 0;
 };
 
 namespace {
@@ -472,6 +478,71 @@ struct Engine final : lsfdtd_engine {
     LS_TRY(mark(s, false));
     cur = o;
     return LSFDTD_OK;
+  }
+
+  size_t bloch_desc_bytes() const override { return kComplex ? sizeof(BlochRun<F>) : 0; }
+
+  int bloch_desc(void* out, size_t bytes, int64_t last) override {
+    if constexpr (!kComplex) {
+      (void)out;
+      (void)bytes;
+      (void)last;
+      return fail(LSFDTD_EUNSUPPORTED, "a batched Bloch run needs complex fields");
+    } else {
+      if (bytes != sizeof(BlochRun<F>)) return fail(LSFDTD_EINVAL, "batch: descriptor size");
+      if (!desc.periodic[0] || !desc.periodic[1] || desc.periodic[2])
+        return fail(LSFDTD_EUNSUPPORTED, "batch: a run must be periodic along x and y, not z");
+      if (y.pml[0].on || y.pml[1].on) return fail(LSFDTD_EUNSUPPORTED, "batch: CPML along z only");
+      if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "batch: dispersive groups have no batched path");
+      if (order.size() != 1 || order[0].first != kColumn)
+        return fail(LSFDTD_EUNSUPPORTED, "batch: a run needs exactly one Bloch column source");
+      if (monitors.size() > (size_t)kBatchMaxMon) return fail(LSFDTD_EUNSUPPORTED, "batch: at most four monitors");
+      for (auto& m : monitors)
+        if (m.space == 1) return fail(LSFDTD_EUNSUPPORTED, "batch: monitors on the grid or the column only");
+      if (last < n_host || last > step_limit)
+        return fail(LSFDTD_ERANGE, "batch: the last step lies before the run's step or past its source waveform");
+      const Column& c = columns[0];
+      auto* col = static_cast<Engine<F>*>(c.col);
+      if (col->desc.shape[2] != desc.shape[2] || col->y.pml[0].on || col->y.pml[1].on || !col->order.empty() ||
+          !col->groups.empty())
+        return fail(LSFDTD_EUNSUPPORTED, "batch: the column must match the grid along z with CPML along z only");
+      if (c.k_src < 1 || c.k_src >= desc.shape[2] - 1 || c.k_launch < 0 || c.k_launch >= desc.shape[2])
+        return fail(LSFDTD_EINVAL, "batch: source planes out of range");
+      BlochRun<F> r{};
+      r.g = y;
+      r.col = col->y;
+      for (int a = 0; a < 2; ++a)
+        for (int sd = 0; sd < 2; ++sd) {
+          r.gph[a][sd] = F{(R)bloch_re[a][sd], (R)bloch_im[a][sd]};
+          r.cph[a][sd] = F{(R)col->bloch_re[a][sd], (R)col->bloch_im[a][sd]};
+        }
+      r.phase = c.phase;
+      r.amp0 = c.amp0;
+      r.amp1 = c.amp1;
+      r.wave = c.wave;
+      r.cE = c.cE;
+      r.cH = c.cH;
+      r.k_src = c.k_src;
+      r.k_launch = c.k_launch;
+      r.stride = desc.dft_stride;
+      r.last = last;
+      r.nstep = reinterpret_cast<long long*>(desc.step);
+      r.div_n2 = udiv_make((unsigned)desc.shape[2]);
+      r.div_ny = udiv_make((unsigned)(desc.shape[1] - 2));
+      r.n_mon = (int)monitors.size();
+      for (size_t i = 0; i < monitors.size(); ++i) {
+        MonArgs<F> m = monitors[i].af;
+        if (monitors[i].space == 0) {
+          m.Esrc = Eflat();
+          m.Hsrc = Hflat();
+        }
+        m.want_energy = 0;
+        m.partial = nullptr;
+        r.mon[i] = m;
+      }
+      std::memcpy(out, &r, sizeof r);
+      return LSFDTD_OK;
+    }
   }
 
   int set_pml(const lsfdtd_pml_desc* p) override {
@@ -975,6 +1046,53 @@ struct Engine final : lsfdtd_engine {
   }
 };
 
+// a batched Bloch sweep: the engines' run descriptors, the CTAs' run lists, the scratch holding them and
+// the captured launch
+struct BatchImpl {
+  int precision = LSFDTD_F32;
+  size_t run_bytes = 0;
+  std::vector<lsfdtd_engine*> engines;
+  std::vector<int64_t> last;
+  std::vector<unsigned char> descs;  // n * run_bytes
+  std::vector<int> order, first;     // runs of CTA b: order[first[b] .. first[b + 1])
+  int ctas = 0;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  size_t off_order = 0, off_first = 0, need = 0;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int graph_steps = -1;
+};
+
+// clusters of the persistent kernel that fit on the device at once
+template <typename F>
+int batch_max_clusters(int* out) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kBatchCluster, 1, 1);
+  cfg.blockDim = dim3(kBatchThreads, 1, 1);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kBatchCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaOccupancyMaxActiveClusters(out, k_bloch_batch<F>, &cfg);
+  if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("batch: cluster occupancy: ") + cudaGetErrorString(e));
+  if (*out < 1) return fail(LSFDTD_EUNSUPPORTED, "batch: no cluster of the persistent kernel fits the device");
+  return LSFDTD_OK;
+}
+
+template <typename F>
+int batch_launch(const BatchImpl& b, int steps, cudaStream_t s) {
+  const auto* runs = static_cast<const BlochRun<F>*>(b.scratch);
+  const int* order = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_order);
+  const int* first = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_first);
+  k_bloch_batch<F><<<b.ctas, kBatchThreads, 0, s>>>(runs, order, first, steps);  // whole clusters
+  LS_LAUNCHED();
+  return LSFDTD_OK;
+}
+
 lsfdtd_engine* make_engine(const lsfdtd_grid_desc& g) {
   if (g.precision == LSFDTD_F32) {
     if (g.is_complex) return new Engine<cplx<float>>(g);
@@ -990,6 +1108,8 @@ int run_chunk(lsfdtd_engine* e, cudaStream_t s) {
 }
 
 }  // namespace
+
+struct lsfdtd_batch : BatchImpl {};
 
 extern "C" {
 
@@ -1224,5 +1344,135 @@ int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t ti
 int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng) { return eng ? eng->n_host : -1; }
 
 int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng) { return eng ? eng->launches_per_chunk() : -1; }
+
+int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out) {
+  LS_NEED(engines && last && out && n > 0);
+  *out = nullptr;
+  auto b = std::make_unique<lsfdtd_batch>();
+  b->precision = engines[0] ? engines[0]->desc.precision : LSFDTD_F32;
+  for (int32_t i = 0; i < n; ++i) {
+    lsfdtd_engine* e = engines[i];
+    if (!e) return fail(LSFDTD_EINVAL, "batch: null engine");
+    if (e->desc.precision != b->precision || !e->desc.is_complex)
+      return fail(LSFDTD_EINVAL, "batch: engines of one precision with complex fields");
+    const size_t rb = e->bloch_desc_bytes();
+    if (b->run_bytes == 0) b->run_bytes = rb;
+    std::vector<unsigned char> d(rb);
+    LS_TRY(e->bloch_desc(d.data(), rb, last[i]));
+    b->descs.insert(b->descs.end(), d.begin(), d.end());
+    b->engines.push_back(e);
+    b->last.push_back(last[i]);
+  }
+  // one wave of clusters; the runs longest first, each to the cluster with the least work so far
+  int clusters = 0;
+  LS_TRY(b->precision == LSFDTD_F32 ? batch_max_clusters<cplx<float>>(&clusters)
+                                    : batch_max_clusters<cplx<double>>(&clusters));
+  clusters = std::max(1, std::min<int>(n, clusters));
+  b->ctas = clusters * kBatchCluster;
+  for (int32_t i = 0; i < n; ++i) {
+    const auto& d = b->engines[i]->desc;
+    if ((double)(d.shape[0] - 2) * (d.shape[1] - 2) * d.shape[2] + d.shape[2] >= 4294967296.0)
+      return fail(LSFDTD_EUNSUPPORTED, "batch: a run of 2^32 nodes or more");
+  }
+  std::vector<double> cost(n);
+  for (int32_t i = 0; i < n; ++i) {
+    const auto& d = b->engines[i]->desc;
+    cost[i] = (double)d.shape[0] * d.shape[1] * d.shape[2] * (double)std::max<int64_t>(0, last[i] - b->engines[i]->n_host);
+  }
+  std::vector<int> idx(n);
+  for (int32_t i = 0; i < n; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+  std::vector<double> load(clusters, 0.0);
+  std::vector<std::vector<int>> lists(clusters);
+  for (int i : idx) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[k] += cost[i];
+    lists[k].push_back(i);
+  }
+  b->first.push_back(0);
+  for (auto& l : lists) {
+    b->order.insert(b->order.end(), l.begin(), l.end());
+    b->first.push_back((int)b->order.size());
+  }
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  b->off_order = up(b->descs.size());
+  b->off_first = b->off_order + up(b->order.size() * sizeof(int));
+  b->need = b->off_first + up(b->first.size() * sizeof(int));
+  *out = b.release();
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_batch_destroy(lsfdtd_batch* batch) {
+  if (!batch) return LSFDTD_OK;
+  if (batch->exec) cudaGraphExecDestroy(batch->exec);
+  if (batch->graph) cudaGraphDestroy(batch->graph);
+  delete batch;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_batch_scratch_bytes(const lsfdtd_batch* batch, size_t* bytes) {
+  LS_NEED(batch && bytes);
+  *bytes = batch->need;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_batch_set_scratch(lsfdtd_batch* batch, void* scratch, size_t bytes) {
+  LS_NEED(batch && scratch);
+  if (bytes < batch->need) return fail(LSFDTD_EINVAL, "batch: scratch too small");
+  if (reinterpret_cast<uintptr_t>(scratch) % 256) return fail(LSFDTD_EINVAL, "batch: scratch must be 256-byte aligned");
+  char* base = static_cast<char*>(scratch);
+  LS_CUDA(cudaMemcpy(base, batch->descs.data(), batch->descs.size(), cudaMemcpyHostToDevice));
+  LS_CUDA(cudaMemcpy(base + batch->off_order, batch->order.data(), batch->order.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  LS_CUDA(cudaMemcpy(base + batch->off_first, batch->first.data(), batch->first.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  batch->scratch = scratch;
+  batch->scratch_bytes = bytes;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_batch_run(lsfdtd_batch* batch, int32_t steps, int32_t n_launches, int32_t use_graph, void* stream) {
+  LS_NEED(batch);
+  if (!batch->scratch) return fail(LSFDTD_EINVAL, "batch: scratch not set");
+  if (steps < 0 || n_launches < 0) return fail(LSFDTD_EINVAL, "batch: negative step or launch count");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto launch = [&](cudaStream_t st) {
+    return batch->precision == LSFDTD_F32 ? batch_launch<cplx<float>>(*batch, steps, st)
+                                          : batch_launch<cplx<double>>(*batch, steps, st);
+  };
+  for (int32_t l = 0; l < n_launches; ++l) {
+    if (!use_graph) {
+      LS_TRY(launch(s));
+    } else {
+      if (!batch->exec || batch->graph_steps != steps) {
+        if (s == nullptr || s == cudaStreamLegacy) return fail(LSFDTD_EINVAL, "graph capture needs a created stream");
+        if (batch->exec) cudaGraphExecDestroy(batch->exec);
+        if (batch->graph) cudaGraphDestroy(batch->graph);
+        batch->exec = nullptr;
+        batch->graph = nullptr;
+        LS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int r = launch(s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (r != LSFDTD_OK) {
+          if (g) cudaGraphDestroy(g);
+          return r;
+        }
+        if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+        batch->graph = g;
+        LS_CUDA(cudaGraphInstantiate(&batch->exec, g, 0));
+        batch->graph_steps = steps;
+      }
+      LS_CUDA(cudaGraphLaunch(batch->exec, s));
+    }
+    for (size_t i = 0; i < batch->engines.size(); ++i) {
+      lsfdtd_engine* e = batch->engines[i];
+      e->n_host = std::min<int64_t>(e->n_host + steps, batch->last[i]);
+    }
+  }
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch) { return batch ? batch->ctas : -1; }
 
 }  // extern "C"

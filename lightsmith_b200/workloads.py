@@ -14,7 +14,7 @@ import math
 
 import numpy as np
 
-from .plan import DFTMonitor, DipoleSource, PMLSpec, flat_index, make_plan
+from .plan import ColumnSource, DFTMonitor, DipoleSource, PMLSpec, flat_index, make_plan
 
 
 def point_dipole(shape, origin, dx: float, dt: float, pos, pdir, inv_eps_at, omega_c: float, omega_half: float,
@@ -118,3 +118,86 @@ def cells_in_cpml(plan) -> int:
         thick = (lo + 1 if lo else 0) + (hi + 1 if hi else 0)
         tot += thick * int(np.prod([shape[a] for a in range(3) if a != d]))
     return tot
+
+
+# --- the batched oblique sweep of a periodic metasurface cell ---------------------------------------------
+
+
+def metasurface_run(period: float, theta_deg: float, phi_deg: float, wavelength: float, pol: str, *,
+                    dz: float = 10.0, nz: int = 200, pml: int = 12, single: bool = True, steps: int = 3000,
+                    n_pillar: float = 2.4, n_sub: float = 1.45, height: float = 600.0) -> dict:
+    """Plan of one fixed-k_par oblique run of a periodic cell (the structure of lightsmith's
+    ``periodic._run_oblique``, ``periodic.py:426-459``): a cylinder of index ``n_pillar``, radius 0.3 x period
+    and ``height`` on a substrate of index ``n_sub``, air above, square period ``period``.
+
+    Cells: ceil(period / 10 nm) per period (spacing period / n, as ``periodic.py:172``), ``dz`` along z, ``nz``
+    nodes (fixed here; lightsmith derives it from gaps), CPML of ``pml`` cells at both ends. Along z: the
+    reflection plane, the TF/SF plane (k_src, fed by the Bloch column, ``tfsf.py:214-296``), the incident probe,
+    the pillar, the substrate and the transmission plane. The permittivity is sampled at the nodes (staircase,
+    isotropic). The pulse is lightsmith's oblique-run pulse: a Gaussian of half-width 0.15 omega around the
+    wavelength (the upper clip of ``periodic._oblique_half_width``)."""
+    n = int(math.ceil(period / 10.0))
+    d = period / n
+    shape = (n + 2, n + 2, nz)
+    spacing = (d, d, dz)
+    dt = 0.99 / math.sqrt(2 / d ** 2 + 1 / dz ** 2)
+    k_r, k_src = pml + 4, pml + 10
+    k_launch, k_probe = k_src - 1, k_src + 3
+    z_top = k_src + 8
+    z_sub = z_top + int(round(height / dz))
+    k_t = nz - pml - 4
+    if not (z_sub < k_t):
+        raise ValueError("the cell is too short for the pillar")
+    # nodes: x, y periodic over the real cells (ghosts repeat them), z as laid out above
+    xi = (np.arange(shape[0]) - 1) % n
+    xc = (xi + 0.5) * d - 0.5 * period
+    r2 = xc[:, None] ** 2 + xc[None, :] ** 2
+    pillar = r2 <= (0.3 * period) ** 2
+    eps = np.ones(shape)
+    eps[:, :, z_sub:] = n_sub ** 2
+    eps[:, :, z_top:z_sub][pillar] = n_pillar ** 2
+    omega = 2 * np.pi / wavelength
+    half = 0.15 * omega
+    th, ph = math.radians(theta_deg), math.radians(phi_deg)
+    kx, ky = omega * math.sin(th) * math.cos(ph), omega * math.sin(th) * math.sin(ph)
+    stride = max(1, int(2 * np.pi / (2 * omega + 4 * half) / dt))
+    pml_main = PMLSpec(cells=((0, 0), (0, 0), (pml, pml)), alpha_max=0.01, eps_ref=1.0, eps_ref_high=n_sub ** 2)
+    pml_col = PMLSpec(cells=((0, 0), (0, 0), (pml, pml)), alpha_max=0.01, eps_ref=1.0, eps_ref_high=None)
+    col = make_plan(shape=(3, 3, nz), dx=spacing, dt=dt, single=single, inv_eps=np.ones((3, 3, 3, nz)), groups=[],
+                    pml=pml_col, sources=[], monitors=[], dft_stride=1, periodic=(True, True, False),
+                    bloch=(kx, ky, 0.0))
+    # the sheet along s = (-Ky, Kx) or p = (Kx, Ky), K the grid wavenumbers (tfsf.py:229-238)
+    K = np.array([2 * math.sin(kx * d / 2) / d, 2 * math.sin(ky * d / 2) / d])
+    u = K / np.linalg.norm(K) if np.linalg.norm(K) > 1e-12 else np.array([math.cos(ph), math.sin(ph)])
+    a = np.array([-u[1], u[0]]) if pol == "s" else u
+    amp = (complex(a[0] * np.exp(0.5j * kx * d)), complex(a[1] * np.exp(0.5j * ky * d)))
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    phase = np.exp(1j * (kx * i * d + ky * j * d))
+    tau = 2.0 / half
+    t0 = 3.5 * tau
+    t = (np.arange(steps + 2) + 1) * dt
+    wave = np.exp(-(((t - t0) / tau) ** 2)) * np.sin(omega * (t - t0))
+    src = ColumnSource(column=col, k_src=k_src, k_launch=k_launch, phase=phase, amp=amp, wave=wave,
+                       cE=dt / dz, cH=dt / dz)
+    cs = (3, 3, nz)
+    probe = DFTMonitor(np.array([omega]), np.array([flat_index(0, 1, 1, k_probe, cs), flat_index(1, 1, 1, k_probe, cs)]),
+                       np.array([flat_index(1, 1, 1, k_probe - 1, cs), flat_index(0, 1, 1, k_probe - 1, cs)]),
+                       np.array([flat_index(1, 1, 1, k_probe, cs), flat_index(0, 1, 1, k_probe, cs)]), source=src)
+    mons = [plane_monitor(shape, k_r, [omega], energy=1), plane_monitor(shape, k_t, [omega], energy=1), probe]
+    return make_plan(shape=shape, dx=spacing, dt=dt, single=single, inv_eps=1.0 / eps, groups=[], pml=pml_main,
+                     sources=[src], monitors=mons, dft_stride=stride, periodic=(True, True, False),
+                     bloch=(kx, ky, 0.0))
+
+
+def metasurface_sweep(n_runs: int = 96, seed: int = 0, **kw) -> list[dict]:
+    """``n_runs`` oblique runs drawn from ``seed``: period U(300, 600) nm, polar angle U(0, 60) deg, azimuth
+    U(0, 90) deg, wavelength U(450, 750) nm, s or p polarisation."""
+    rng = np.random.default_rng(seed)
+    runs = []
+    for _ in range(n_runs):
+        period = float(rng.uniform(300, 600))
+        theta, phi = float(rng.uniform(0, 60)), float(rng.uniform(0, 90))
+        wl = float(rng.uniform(450, 750))
+        pol = "s" if rng.integers(2) == 0 else "p"
+        runs.append(metasurface_run(period, theta, phi, wl, pol, **kw))
+    return runs
