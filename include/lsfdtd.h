@@ -309,6 +309,43 @@ int32_t lsfdtd_batch_run(lsfdtd_batch* batch, int32_t steps, int32_t n_launches,
 /* CTAs of the persistent kernel (one wave) */
 int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch);
 
+/* ---- discrete adjoint ----------------------------------------------------------------------------------
+ * No counterpart in lightsmith (its FDTD has no gradient): the transpose of one FDTD step of an engine with
+ * real fields and no periodic axis, for d(objective)/d(E curl coefficient) of an objective |A|^2 with A a
+ * linear combination of one frequency's DFT samples, A = sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q]. */
+typedef struct lsfdtd_adjoint lsfdtd_adjoint;
+
+typedef struct lsfdtd_adjoint_desc {
+  void* Eb;                          /* adjoint fields (3, n0, n1, n2), the engine's precision, zeroed */
+  void* Hb;
+  void* psi_bar[2][2][3][3][2];      /* [buffer][E, H][axis][component][side]: zeroed slabs shaped as the
+                                        engine's psi (null where the engine has none) */
+  int32_t box_lo[3], box_hi[3];      /* gradient box, outside every CPML slab and source node */
+  void* hist;                        /* hist_slots boxes of H (3, box + 1 along each axis: the low halo) */
+  int32_t hist_slots;
+  double* grad;                      /* (3, box): dJ/dcbE_c, accumulated */
+  const int64_t* e_idx;              /* the objective's E points (flat indices into the fields) */
+  const double* ge;                  /* (re, im) per E point: conj(A) wE_p */
+  int64_t n_e;
+  const int64_t* h_idx1;             /* its H points (the two H samples averaged) */
+  const int64_t* h_idx2;
+  const double* gh;                  /* (re, im) per H point: conj(A) wH_q */
+  int64_t n_h;
+  double omega;
+} lsfdtd_adjoint_desc;
+
+/* sets the engine's host step count (after the caller rewinds its device counter and fields to a saved step,
+ * e.g. a checkpoint of the adjoint's forward recomputation) */
+int32_t lsfdtd_engine_set_steps(lsfdtd_engine* eng, int64_t n);
+int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, lsfdtd_adjoint** out);
+int32_t lsfdtd_adjoint_destroy(lsfdtd_adjoint* adj);
+/* copies the engine's current H over the box (with its low halo) into history slot `slot` */
+int32_t lsfdtd_adjoint_record(lsfdtd_adjoint* adj, int32_t slot, void* stream);
+/* the transpose of forward step n (E^n, H^{n-1/2} -> E^{n+1}, H^{n+1/2}), H^{n+1/2} of the box in history
+ * slot `slot`: adds the objective's adjoint source when the monitor sampled after that step, then the
+ * transposes of the E and H updates, and accumulates the gradient */
+int32_t lsfdtd_adjoint_step(lsfdtd_adjoint* adj, int64_t n, int32_t slot, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,13 @@ class MonitorDesc(C.Structure):
 
 
 # every exported symbol of include/lsfdtd.h with its ctypes signature
+class AdjointDesc(C.Structure):
+    # psi_bar: C's [buffer][E, H][axis][component][side], flat: (((b * 2 + f) * 3 + d) * 3 + c) * 2 + side
+    _fields_ = [("Eb", vp), ("Hb", vp), ("psi_bar", vp * 72), ("box_lo", i32 * 3), ("box_hi", i32 * 3),
+                ("hist", vp), ("hist_slots", i32), ("grad", vp), ("e_idx", vp), ("ge", vp), ("n_e", i64),
+                ("h_idx1", vp), ("h_idx2", vp), ("gh", vp), ("n_h", i64), ("omega", f64)]
+
+
 SIGNATURES = {
     "lsfdtd_abi_version": (i32, []),
     "lsfdtd_last_error": (C.c_char_p, []),
@@ -115,6 +122,11 @@ SIGNATURES = {
     "lsfdtd_batch_set_scratch": (i32, [vp, vp, C.c_size_t]),
     "lsfdtd_batch_run": (i32, [vp, i32, i32, i32, vp]),
     "lsfdtd_batch_ctas": (i32, [vp]),
+    "lsfdtd_engine_set_steps": (i32, [vp, i64]),
+    "lsfdtd_adjoint_create": (i32, [vp, C.POINTER(AdjointDesc), C.POINTER(vp)]),
+    "lsfdtd_adjoint_destroy": (i32, [vp]),
+    "lsfdtd_adjoint_record": (i32, [vp, i32, vp]),
+    "lsfdtd_adjoint_step": (i32, [vp, i64, i32, vp]),
 }
 
 _lib = None

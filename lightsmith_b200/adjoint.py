@@ -1,0 +1,244 @@
+"""Gradients of an FDTD objective by the discrete adjoint, behind ``torch.autograd``.
+
+lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
+the FDTD path: for a run with real fields, no periodic axis and no dispersive groups (a slab waveguide device,
+say), the objective J = |A|^2 with A = sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q] over one frequency of one
+DFT monitor, and its gradient with respect to 1/eps over a design box of nodes.
+
+``AdjointRun.forward`` runs the engine (the CUDA kernels, in-place form) for ``n_steps`` steps, sampling the
+monitors as lightsmith's chunks do, and keeps the state (E, H, CPML psi) every ``checkpoint`` steps.
+``AdjointRun.backward`` walks the segments in reverse: it restores a checkpoint, recomputes the segment's steps
+while recording H of the box at every step (``lsfdtd_adjoint_record``), then applies the transposed steps
+(``lsfdtd_adjoint_step``, ``csrc/adjoint.cuh``) from the segment's end to its start, accumulating
+dJ/dcbE over the box. Sources only add field-independent terms, so they have no adjoint; the ones allowed
+here (point dipoles, port modes, table-fed TF/SF) keep no state of their own, and their nodes must lie
+outside the box (their coefficients are fixed, not functions of the design).
+
+``FDTDObjective.apply(inv_eps_box, run)`` is the ``torch.autograd.Function``: forward returns J, backward
+dJ/d(1/eps) of the box (isotropic: the three E components of a node share its 1/eps, so the gradient is
+cdx times the sum of the three components' dJ/dcbE).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .engine import Engine
+from .plan import DipoleSource, ModeSource, TableSource
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class AdjointRun:
+    """One run's forward and adjoint passes. ``box``: ((x0, x1), (y0, y1), (z0, z1)) node ranges of the design
+    box; ``monitor``/``freq``: the objective's monitor and frequency; ``wE``/``wH``: complex weights of its E
+    and H points (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride)."""
+
+    def __init__(self, plan: dict, box, monitor: int = 0, freq: int = 0, wE=None, wH=None, checkpoint: int = 256,
+                 precision: str | None = None, device="cuda:0"):
+        torch = _torch()
+        if plan["complex"] or any(plan["periodic"]) or plan["groups"]:
+            raise ValueError("the adjoint serves real fields without periodic axes or dispersive groups")
+        for s in plan["sources"]:
+            if not isinstance(s, (DipoleSource, ModeSource, TableSource)):
+                raise ValueError(f"{type(s).__name__} keeps state of its own; the adjoint does not restore it")
+        self.plan = plan
+        self.eng = Engine.from_plan(plan, device=device, precision=precision, fused=False)
+        eng = self.eng
+        if not eng.isotropic:
+            raise ValueError("the adjoint's design box needs isotropic permittivity (one 1/eps per node)")
+        self.dev = eng.dev
+        self.stride = eng.stride
+        self.K = max(self.stride, int(checkpoint) // self.stride * self.stride)
+        self.box = tuple((int(a), int(b)) for a, b in box)
+        self.box_sl = tuple(slice(a, b) for a, b in self.box)
+        bshape = tuple(b - a for a, b in self.box)
+        mon = plan["monitors"][monitor]
+        self.monitor, self.freq = monitor, freq
+        self.omega = float(mon["omega"][freq])
+        cd = torch.complex128
+        self.wE = torch.as_tensor(np.zeros(len(mon["e_idx"])) if wE is None else np.asarray(wE), dtype=cd,
+                                  device=self.dev)
+        self.wH = None
+        if mon["h_idx1"] is not None:
+            self.wH = torch.as_tensor(np.zeros(len(mon["h_idx1"])) if wH is None else np.asarray(wH), dtype=cd,
+                                      device=self.dev)
+        for s in plan["sources"]:
+            nodes = s.idx if isinstance(s, DipoleSource) else (np.concatenate([s.h_idx, s.e_idx]) if isinstance(
+                s, ModeSource) else np.concatenate([s.E.node, s.H.node]))
+            rest = np.asarray(nodes) % int(np.prod(eng.shape))
+            ijk = np.stack(np.unravel_index(rest, eng.shape), axis=1)
+            inside = np.all((ijk >= [a for a, _ in self.box]) & (ijk < [b for _, b in self.box]), axis=1)
+            if inside.any():
+                raise ValueError("a source node lies in the design box")
+        rdt = eng.rdt
+        self.Eb = torch.zeros_like(eng.E)
+        self.Hb = torch.zeros_like(eng.H)
+        self.psi_bar = [[{}, {}], [{}, {}]]  # [buffer][E, H]: {(c, d, side): tensor}
+        d = _abi.AdjointDesc()
+        d.Eb, d.Hb = self.Eb.data_ptr(), self.Hb.data_ptr()
+        for (kind, comp, ax, side), t in eng.psi.items():
+            f = 0 if kind == "E" else 1
+            for b in range(2):
+                z = torch.zeros_like(t)
+                self.psi_bar[b][f][(comp, ax, side)] = z
+                d.psi_bar[(((b * 2 + f) * 3 + ax) * 3 + comp) * 2 + side] = z.data_ptr()
+        d.box_lo[:] = [a for a, _ in self.box]
+        d.box_hi[:] = [b for _, b in self.box]
+        self.hist = torch.zeros((self.K, 3) + tuple(n + 1 for n in bshape), dtype=rdt, device=self.dev)
+        d.hist, d.hist_slots = self.hist.data_ptr(), self.K
+        self.grad = torch.zeros((3,) + bshape, dtype=torch.float64, device=self.dev)
+        d.grad = self.grad.data_ptr()
+        i64 = torch.int64
+        self.e_idx = torch.as_tensor(mon["e_idx"], dtype=i64, device=self.dev)
+        self.ge = torch.zeros((len(mon["e_idx"]), 2), dtype=torch.float64, device=self.dev)
+        d.e_idx, d.ge, d.n_e = self.e_idx.data_ptr(), self.ge.data_ptr(), len(mon["e_idx"])
+        if self.wH is not None:
+            self.h1 = torch.as_tensor(mon["h_idx1"], dtype=i64, device=self.dev)
+            self.h2 = torch.as_tensor(mon["h_idx2"], dtype=i64, device=self.dev)
+            self.gh = torch.zeros((len(mon["h_idx1"]), 2), dtype=torch.float64, device=self.dev)
+            d.h_idx1, d.h_idx2, d.gh, d.n_h = self.h1.data_ptr(), self.h2.data_ptr(), self.gh.data_ptr(), len(
+                mon["h_idx1"])
+        d.omega = self.omega
+        self._desc = d
+        h = C.c_void_p()
+        _abi.check(_abi.lib().lsfdtd_adjoint_create(eng._h, C.byref(d), C.byref(h)), "lsfdtd_adjoint_create")
+        self._h = h
+        self.A = None
+        self.n_steps = 0
+        self._ckpt = []
+
+    # --- state ----------------------------------------------------------------------------------------------
+    def _state(self):
+        eng = self.eng
+        return [eng.E, eng.H] + list(eng.psi.values())
+
+    def _save(self):
+        return [t.clone() for t in self._state()]
+
+    def _restore(self, saved, n: int):
+        eng = self.eng
+        for dst, src in zip(self._state(), saved):
+            dst.copy_(src)
+        eng.n.fill_(n)
+        _abi.check(_abi.lib().lsfdtd_engine_set_steps(eng._h, int(n)), "lsfdtd_engine_set_steps")
+        _torch().cuda.synchronize(self.dev)  # the engine's stream starts from the restored state
+
+    def _reset(self):
+        for t in self._state():
+            t.zero_()
+        for m in self.eng.monitors:
+            m["acc_e"].zero_()
+            if m["acc_h"] is not None:
+                m["acc_h"].zero_()
+        self._restore(self._save(), 0)
+
+    def set_inv_eps_box(self, inv_eps_box) -> None:
+        """1/eps over the box (the engine's shared E curl coefficient there becomes cdx / eps)."""
+        eng = self.eng
+        torch = _torch()
+        cb = eng.cbE[0]
+        cb[self.box_sl] = (torch.as_tensor(inv_eps_box, device=self.dev, dtype=torch.float64) * eng.cdx).to(cb.dtype)
+        torch.cuda.synchronize(self.dev)
+
+    # --- passes -----------------------------------------------------------------------------------------------
+    def forward(self, n_steps: int):
+        """Runs n_steps steps from rest (a multiple of dft_stride); returns (J, A)."""
+        torch = _torch()
+        eng = self.eng
+        if n_steps % self.stride:
+            raise ValueError("n_steps must be a multiple of dft_stride")
+        self._reset()
+        self._ckpt = [self._save()]
+        for n in range(n_steps):
+            eng.step(1)
+            if (n + 1) % self.stride == 0:
+                eng.sample()
+            if (n + 1) % self.K == 0 and n + 1 < n_steps:
+                self._ckpt.append(self._save())
+        self.n_steps = n_steps
+        m = eng.monitors[self.monitor]
+        A = (self.wE * m["acc_e"][self.freq]).sum()
+        if self.wH is not None:
+            A = A + (self.wH * m["acc_h"][self.freq]).sum()
+        self.A = A
+        torch.cuda.synchronize(self.dev)
+        return float(abs(A.item()) ** 2), complex(A.item())
+
+    def backward(self):
+        """dJ/d(1/eps) over the box, as float64 (x, y, z) after forward()."""
+        torch = _torch()
+        eng = self.eng
+        L = _abi.lib()
+        cA = torch.conj(self.A)
+        self.ge.copy_(torch.view_as_real(2 * cA * self.wE))
+        if self.wH is not None:
+            self.gh.copy_(torch.view_as_real(2 * cA * self.wH))
+        self.Eb.zero_()
+        self.Hb.zero_()
+        for b in range(2):
+            for f in range(2):
+                for t in self.psi_bar[b][f].values():
+                    t.zero_()
+        self.grad.zero_()
+        torch.cuda.synchronize(self.dev)
+        h = self._h
+        stream = eng.stream
+        for k in reversed(range(len(self._ckpt))):
+            n0 = k * self.K
+            n1 = min(n0 + self.K, self.n_steps)
+            self._restore(self._ckpt[k], n0)
+            torch.cuda.synchronize(self.dev)
+            for i in range(n1 - n0):
+                eng.step(1)
+                _abi.check(L.lsfdtd_adjoint_record(h, i, stream.cuda_stream), "lsfdtd_adjoint_record")
+            for i in reversed(range(n1 - n0)):
+                _abi.check(L.lsfdtd_adjoint_step(h, n0 + i, i, stream.cuda_stream), "lsfdtd_adjoint_step")
+            torch.cuda.synchronize(self.dev)
+        return self.grad.sum(0) * eng.cdx
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _abi.lib().lsfdtd_adjoint_destroy(h)
+            self._h = C.c_void_p()
+        self.eng.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 (interpreter shutdown)
+            pass
+
+
+def _function():
+    torch = _torch()
+
+    class FDTDObjective(torch.autograd.Function):
+        """J(1/eps of the design box) of an ``AdjointRun``, differentiable by the discrete adjoint."""
+
+        @staticmethod
+        def forward(ctx, inv_eps_box, run: AdjointRun, n_steps: int):
+            run.set_inv_eps_box(inv_eps_box.detach())
+            J, _ = run.forward(n_steps)
+            ctx.run = run
+            return torch.tensor(J, dtype=torch.float64, device=inv_eps_box.device)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            g = ctx.run.backward().to(gJ.device)
+            return gJ * g, None, None
+
+    return FDTDObjective
+
+
+def fdtd_objective(inv_eps_box, run: AdjointRun, n_steps: int):
+    """J as a differentiable function of 1/eps over the design box."""
+    return _function().apply(inv_eps_box, run, n_steps)

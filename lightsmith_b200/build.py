@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 SOURCES = [os.path.join(HERE, "csrc", "lsfdtd.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "yee.cuh", "yee_vec.cuh", "fused.cuh",
-                                                   "fused_tma.cuh", "fused_pml.cuh", "shell.cuh", "batch.cuh", "ade.cuh", "sources.cuh",
+                                                   "fused_tma.cuh", "fused_pml.cuh", "shell.cuh", "batch.cuh", "adjoint.cuh", "ade.cuh", "sources.cuh",
                                                    "monitors.cuh")] + \
     [os.path.join(REPO, "include", "lsfdtd.h")]
 OUT = os.path.join(HERE, "liblsfdtd.so")

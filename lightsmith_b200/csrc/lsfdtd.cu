@@ -16,6 +16,7 @@
 #include "lsfdtd.h"
 
 #include "ade.cuh"
+#include "adjoint.cuh"
 #include "batch.cuh"
 #include "common.cuh"
 #include "fused.cuh"
@@ -143,6 +144,8 @@ struct lsfdtd_engine {
   // the run descriptor of a batched Bloch sweep (BlochRun<F>), run to step `last`
   virtual size_t bloch_desc_bytes() const = 0;
   virtual int bloch_desc(void* out, size_t bytes, int64_t last) = 0;
+  // the coefficients of the adjoint (YeeArgs of a real engine) and the current H array
+  virtual int adjoint_args(void* yee, size_t bytes, void** H) = 0;
 };
 
 namespace {
@@ -481,6 +484,18 @@ struct Engine final : lsfdtd_engine {
   }
 
   size_t bloch_desc_bytes() const override { return kComplex ? sizeof(BlochRun<F>) : 0; }
+
+  int adjoint_args(void* yee, size_t bytes, void** H) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
+    if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
+      return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
+    if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "adjoint: dispersive groups have no adjoint here");
+    if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
+    const YeeArgs<F> a = current_args();
+    std::memcpy(yee, &a, sizeof a);
+    *H = Hflat();
+    return LSFDTD_OK;
+  }
 
   int bloch_desc(void* out, size_t bytes, int64_t last) override {
     if constexpr (!kComplex) {
@@ -1111,6 +1126,78 @@ int run_chunk(lsfdtd_engine* e, cudaStream_t s) {
 
 struct lsfdtd_batch : BatchImpl {};
 
+struct lsfdtd_adjoint {
+  lsfdtd_engine* eng = nullptr;
+  int precision = LSFDTD_F32;
+  lsfdtd_adjoint_desc d{};
+  std::vector<unsigned char> yee;  // YeeArgs of the engine's precision
+  int buf = 0;                     // psibar buffer holding the current (old) values
+  size_t slot_elems = 0;
+};
+
+namespace {
+
+template <typename R>
+int adjoint_record(lsfdtd_adjoint* a, int slot, cudaStream_t s) {
+  const auto& y = *reinterpret_cast<const YeeArgs<R>*>(a->yee.data());
+  void* Hv = nullptr;
+  std::vector<unsigned char> tmp(sizeof(YeeArgs<R>));
+  LS_TRY(a->eng->adjoint_args(tmp.data(), tmp.size(), &Hv));  // the current H (a fused engine alternates)
+  const long long cells = (long long)y.n[0] * y.n[1] * y.n[2];
+  const R* H = static_cast<const R*>(Hv);
+  const int h0 = a->d.box_hi[0] - a->d.box_lo[0] + 1, h1 = a->d.box_hi[1] - a->d.box_lo[1] + 1,
+            h2 = a->d.box_hi[2] - a->d.box_lo[2] + 1;
+  R* dst = static_cast<R*>(a->d.hist) + (size_t)slot * a->slot_elems;
+  k_adj_hist<R><<<cdiv(3LL * h0 * h1 * h2, 256), 256, 0, s>>>(H, H + cells, H + 2 * cells, dst, y.n[1], y.n[2],
+                                                            a->d.box_lo[0], a->d.box_lo[1], a->d.box_lo[2], h0,
+                                                            h1, h2);
+  LS_LAUNCHED();
+  return LSFDTD_OK;
+}
+
+template <typename R>
+int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
+  AdjArgs<R> A{};
+  A.y = *reinterpret_cast<const YeeArgs<R>*>(a->yee.data());
+  const long long cells = (long long)A.y.n[0] * A.y.n[1] * A.y.n[2];
+  for (int c = 0; c < 3; ++c) {
+    A.Eb[c] = static_cast<R*>(a->d.Eb) + c * cells;
+    A.Hb[c] = static_cast<R*>(a->d.Hb) + c * cells;
+  }
+  const int o = a->buf, w = a->buf ^ 1;
+  for (int d = 0; d < 3; ++d)
+    for (int c = 0; c < 3; ++c)
+      for (int sd = 0; sd < 2; ++sd) {
+        A.pe_old[d][c][sd] = static_cast<R*>(a->d.psi_bar[o][0][d][c][sd]);
+        A.pe_new[d][c][sd] = static_cast<R*>(a->d.psi_bar[w][0][d][c][sd]);
+        A.ph_old[d][c][sd] = static_cast<R*>(a->d.psi_bar[o][1][d][c][sd]);
+        A.ph_new[d][c][sd] = static_cast<R*>(a->d.psi_bar[w][1][d][c][sd]);
+      }
+  for (int ax = 0; ax < 3; ++ax) {
+    A.box_lo[ax] = a->d.box_lo[ax];
+    A.box_hi[ax] = a->d.box_hi[ax];
+  }
+  A.hist = static_cast<const R*>(a->d.hist) + (size_t)slot * a->slot_elems;
+  A.grad = a->d.grad;
+  const auto& desc = a->eng->desc;
+  if ((n + 1) % desc.dft_stride == 0 && a->d.n_e + a->d.n_h > 0) {
+    k_adj_inject<R><<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(
+        A.Eb[0], A.Hb[0], reinterpret_cast<const long long*>(a->d.e_idx), a->d.ge, a->d.n_e,
+        reinterpret_cast<const long long*>(a->d.h_idx1), reinterpret_cast<const long long*>(a->d.h_idx2), a->d.gh,
+        a->d.n_h, a->d.omega, desc.dt, n + 1);
+    LS_LAUNCHED();
+  }
+  const dim3 grid(cdiv(A.y.n[2], 32), cdiv(A.y.n[1], 8), A.y.n[0]);
+  k_adj_e<R><<<grid, dim3(32, 8), 0, s>>>(A);
+  LS_LAUNCHED();
+  k_adj_h<R><<<grid, dim3(32, 8), 0, s>>>(A);
+  LS_LAUNCHED();
+  a->buf = w;
+  return LSFDTD_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int32_t lsfdtd_abi_version(void) { return LSFDTD_ABI_VERSION; }
@@ -1474,5 +1561,74 @@ int32_t lsfdtd_batch_run(lsfdtd_batch* batch, int32_t steps, int32_t n_launches,
 }
 
 int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch) { return batch ? batch->ctas : -1; }
+
+int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, lsfdtd_adjoint** out) {
+  LS_NEED(eng && d && out && d->Eb && d->Hb && d->grad && d->hist && d->hist_slots > 0);
+  *out = nullptr;
+  auto a = std::make_unique<lsfdtd_adjoint>();
+  a->eng = eng;
+  a->precision = eng->desc.precision;
+  a->d = *d;
+  a->yee.resize(a->precision == LSFDTD_F32 ? sizeof(YeeArgs<float>) : sizeof(YeeArgs<double>));
+  void* H = nullptr;
+  LS_TRY(eng->adjoint_args(a->yee.data(), a->yee.size(), &H));
+  if ((d->n_e > 0 && (!d->e_idx || !d->ge)) || (d->n_h > 0 && (!d->h_idx1 || !d->h_idx2 || !d->gh)))
+    return fail(LSFDTD_EINVAL, "adjoint: objective arrays missing");
+  const int32_t* n = eng->desc.shape;
+  for (int ax = 0; ax < 3; ++ax)
+    if (d->box_lo[ax] < 1 || d->box_hi[ax] > n[ax] - 1 || d->box_hi[ax] <= d->box_lo[ax])
+      return fail(LSFDTD_EINVAL, "adjoint: gradient box out of range");
+  // every E node of the box outside every E slab (there the E update's coefficient enters only through the
+  // curl term; the H values of the box and its halo are recorded, wherever they lie)
+  auto slabs_ok = [&](const auto& y) {
+    for (int dd = 0; dd < 3; ++dd) {
+      if (!y.pml[dd].on) continue;
+      for (int f = 0; f < 2; ++f)
+        for (int c = 0; c < 3; ++c)
+          for (int sd = 0; sd < 2; ++sd) {
+            const int st = y.pml[dd].start[f][c][sd], ln = y.pml[dd].len[f][c][sd];
+            if (f == 0 && ln > 0 && d->box_lo[dd] < st + ln && d->box_hi[dd] > st) return false;
+            const bool need = ln > 0;
+            for (int b = 0; b < 2; ++b)
+              if (need && !d->psi_bar[b][f][dd][c][sd]) return false;
+          }
+    }
+    return true;
+  };
+  const bool ok = a->precision == LSFDTD_F32 ? slabs_ok(*reinterpret_cast<const YeeArgs<float>*>(a->yee.data()))
+                                             : slabs_ok(*reinterpret_cast<const YeeArgs<double>*>(a->yee.data()));
+  if (!ok) return fail(LSFDTD_EINVAL, "adjoint: the box overlaps a CPML slab, or a psibar slab is missing");
+  a->slot_elems = 3ull * (d->box_hi[0] - d->box_lo[0] + 1) * (d->box_hi[1] - d->box_lo[1] + 1) *
+                  (d->box_hi[2] - d->box_lo[2] + 1);
+  *out = a.release();
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_set_steps(lsfdtd_engine* eng, int64_t n) {
+  LS_NEED(eng);
+  if (n < 0 || n > eng->step_limit) return fail(LSFDTD_ERANGE, "step count out of range");
+  eng->n_host = n;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_adjoint_destroy(lsfdtd_adjoint* adj) {
+  delete adj;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_adjoint_record(lsfdtd_adjoint* adj, int32_t slot, void* stream) {
+  LS_NEED(adj);
+  if (slot < 0 || slot >= adj->d.hist_slots) return fail(LSFDTD_EINVAL, "adjoint: history slot out of range");
+  auto s = static_cast<cudaStream_t>(stream);
+  return adj->precision == LSFDTD_F32 ? adjoint_record<float>(adj, slot, s) : adjoint_record<double>(adj, slot, s);
+}
+
+int32_t lsfdtd_adjoint_step(lsfdtd_adjoint* adj, int64_t n, int32_t slot, void* stream) {
+  LS_NEED(adj);
+  if (slot < 0 || slot >= adj->d.hist_slots) return fail(LSFDTD_EINVAL, "adjoint: history slot out of range");
+  if (n < 0) return fail(LSFDTD_EINVAL, "adjoint: negative step");
+  auto s = static_cast<cudaStream_t>(stream);
+  return adj->precision == LSFDTD_F32 ? adjoint_step<float>(adj, n, slot, s) : adjoint_step<double>(adj, n, slot, s);
+}
 
 }  // extern "C"

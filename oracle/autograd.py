@@ -1,0 +1,136 @@
+"""A plain-PyTorch restatement of the FDTD step, differentiated by torch.autograd: TEST INFRASTRUCTURE ONLY.
+
+The checker of ``lightsmith_b200.adjoint``: the same update equations as ``oracle/engine.py`` (lightsmith's
+``engine.py:613-663`` curl updates over the stepped regions, ``engine.py:344-418`` CPML terms in their order,
+``emission.py:130-140`` point-current corrections after the E update), for real fields, no periodic axes, no
+dispersive groups and point-dipole sources, written out of place so that autograd can differentiate the DFT
+objective |sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q]|^2 with respect to 1/eps over a box of nodes.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from lightsmith_b200.plan import DipoleSource, cpml_profiles, cpml_terms, e_range, h_range
+
+from .engine import _Spec
+
+
+def _put(F, region, delta):
+    """F with delta added over region (out of place)."""
+    Z = torch.zeros_like(F)
+    Z[region] = delta
+    return F + Z
+
+
+def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_steps: int):
+    """J (float64 tensor) after n_steps steps from rest, differentiable in inv_eps_box (the box's 1/eps)."""
+    dt = torch.float64
+    shape = tuple(plan["shape"])
+    spacing = tuple(plan["spacing"])
+    step_dt = float(plan["dt"])
+    stride = int(plan["stride"])
+    uniform = len(set(spacing)) == 1
+    cdx = step_dt / spacing[0] if uniform else step_dt
+    inv_d = [1.0 / s for s in spacing]
+    per = (False, False, False)
+    inv0 = np.asarray(plan["inv_eps"], float)
+    if inv0.ndim != 3:
+        raise ValueError("isotropic permittivity only")
+    bsl = tuple(slice(a, b) for a, b in box)
+    full = torch.as_tensor(inv0, dtype=dt).clone()
+    full[bsl] = inv_eps_box
+    RE = [tuple(e_range(c, a, shape[a], per[a]) for a in range(3)) for c in range(3)]
+    RH = [tuple(h_range(c, a, shape[a], per[a]) for a in range(3)) for c in range(3)]
+    sl = lambda R: tuple(slice(r[0], r[1]) for r in R)  # noqa: E731
+    cb = [cdx * full[sl(RE[c])] for c in range(3)]
+    cH = cdx
+
+    # CPML terms (oracle/engine.py:_build_pml)
+    spec = _Spec(plan["pml"])
+    prof = cpml_profiles(spec, shape, spacing, step_dt)
+    terms = {"E": [], "H": []}
+    for t in cpml_terms(spec, shape, per):
+        d, fld = t["d"], t["field"]
+        a, b = t["region"][d]
+        bb, cc, kk = (v[a:b] for v in prof[d][2][fld])
+        bshape = [1, 1, 1]
+        bshape[d] = b - a
+        reg = sl(t["region"])
+        scale = cdx * full[reg] if fld == "E" else torch.full([r[1] - r[0] for r in t["region"]], cdx, dtype=dt)
+        if not uniform:
+            scale = scale / spacing[d]
+        cp = t["sgn"] * scale * torch.as_tensor(cc.reshape(bshape), dtype=dt)
+        kp = t["sgn"] * scale * torch.as_tensor((1 / kk - 1).reshape(bshape), dtype=dt) if np.any(kk > 1) else None
+        terms[fld].append({**t, "reg": reg, "b": torch.as_tensor(bb.reshape(bshape), dtype=dt), "cp": cp, "kp": kp,
+                           "psi": torch.zeros(cp.shape, dtype=dt)})
+
+    def shifted(R, d, s):
+        R = list(R)
+        R[d] = slice(R[d].start + s, R[d].stop + s)
+        return tuple(R)
+
+    def curl(F, c, R, forward):
+        d1, d2 = (c + 1) % 3, (c + 2) % 3
+        if forward:
+            a = F[d2][shifted(R, d1, 1)] - F[d2][R]
+            b = F[d1][shifted(R, d2, 1)] - F[d1][R]
+        else:
+            a = F[d2][R] - F[d2][shifted(R, d1, -1)]
+            b = F[d1][R] - F[d1][shifted(R, d2, -1)]
+        if not uniform:
+            a, b = a * inv_d[d1], b * inv_d[d2]
+        return a - b
+
+    def pml(tgt, src, kind):
+        out = list(tgt)
+        for t in terms[kind]:
+            R, d, s = t["reg"], t["d"], t["src"]
+            if kind == "H":
+                der = src[s][shifted(R, d, 1)] - src[s][R]
+            else:
+                der = src[s][R] - src[s][shifted(R, d, -1)]
+            psi = t["psi"] * t["b"]
+            delta = torch.zeros_like(der)
+            if t["kp"] is not None:
+                delta = delta + t["kp"] * der
+            psi = psi + der * t["cp"]
+            t["psi"] = psi
+            out[t["c"]] = _put(out[t["c"]], R, delta + psi)
+        return out
+
+    E = [torch.zeros(shape, dtype=dt) for _ in range(3)]
+    H = [torch.zeros(shape, dtype=dt) for _ in range(3)]
+    dips = [s for s in plan["sources"] if isinstance(s, DipoleSource)]
+    if len(dips) != len(plan["sources"]):
+        raise ValueError("point dipoles only")
+    mon = plan["monitors"][monitor]
+    omega = float(mon["omega"][freq])
+    wE = torch.as_tensor(np.asarray(wE), dtype=torch.complex128)
+    wH = None if wH is None else torch.as_tensor(np.asarray(wH), dtype=torch.complex128)
+    e_idx = torch.as_tensor(mon["e_idx"])
+    h1 = None if mon["h_idx1"] is None else torch.as_tensor(mon["h_idx1"])
+    h2 = None if mon["h_idx2"] is None else torch.as_tensor(mon["h_idx2"])
+    A = torch.zeros((), dtype=torch.complex128)
+    cells = int(np.prod(shape))
+    for n in range(n_steps):
+        H = [_put(H[c], sl(RH[c]), -curl(E, c, sl(RH[c]), True) * cH) for c in range(3)]
+        H = pml(H, E, "H")
+        E = [_put(E[c], sl(RE[c]), curl(H, c, sl(RE[c]), False) * cb[c]) for c in range(3)]
+        E = pml(E, H, "E")
+        for s in dips:  # E_flat[idx] -= coef * wave[n] (after the E update)
+            flat = torch.cat([e.reshape(-1) for e in E])
+            upd = torch.zeros_like(flat).index_add(0, torch.as_tensor(s.idx),
+                                                   torch.as_tensor(s.coef * s.wave[n], dtype=dt))
+            flat = flat - upd
+            E = [flat[c * cells:(c + 1) * cells].reshape(shape) for c in range(3)]
+        if (n + 1) % stride == 0:
+            t_e = (n + 1) * step_dt
+            flat_e = torch.cat([e.reshape(-1) for e in E])
+            A = A + np.exp(1j * omega * t_e) * (wE * flat_e[e_idx].to(torch.complex128)).sum()
+            if wH is not None:
+                flat_h = torch.cat([h.reshape(-1) for h in H])
+                havg = ((flat_h[h1] + flat_h[h2]) * 0.5).to(torch.complex128)
+                A = A + np.exp(1j * omega * (t_e - 0.5 * step_dt)) * (wH * havg).sum()
+    return (A * A.conj()).real

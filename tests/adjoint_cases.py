@@ -1,0 +1,42 @@
+"""Small seeded runs for the adjoint tests: a random-permittivity grid with CPML on every face, a point
+dipole near the low-x face, a DFT plane monitor, and a design box between them (outside the CPML slabs and
+away from the source nodes)."""
+
+import math
+
+import numpy as np
+
+from lightsmith_b200.plan import PMLSpec, make_plan
+from lightsmith_b200.workloads import plane_monitor, point_dipole
+
+SHAPE = (22, 18, 16)
+BOX = ((10, 15), (6, 12), (5, 9))
+DX = 20.0
+
+
+def small_case(seed: int = 4, n_chunks: int = 4):
+    """(plan, n_steps, weights of the monitor's E and H points)."""
+    dt = 0.99 * DX / math.sqrt(3)
+    rng = np.random.default_rng(seed)
+    inv_eps = 1.0 / rng.uniform(1.0, 4.0, size=SHAPE)
+    omega = 2 * np.pi / 300.0
+    stride = 7
+    n_steps = n_chunks * stride
+
+    def at(flat):
+        rest = np.asarray(flat) % int(np.prod(SHAPE))
+        return inv_eps[np.unravel_index(rest, SHAPE)]
+
+    dip = point_dipole(SHAPE, np.zeros(3), DX, dt, np.array([6.37, 9.37, 8.37]) * DX, (0.3, 1.0, 0.2), at,
+                       omega, 0.4 * omega, n_steps + 400)
+    w = dip.wave
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    dip.wave = np.concatenate([w[first:], np.zeros(first)])
+    mon = plane_monitor(SHAPE, 12, [omega], energy=1)
+    pml = PMLSpec(cells=((4, 4),) * 3, alpha_max=0.02, eps_ref=1.5)
+    plan = make_plan(shape=SHAPE, dx=DX, dt=dt, single=False, inv_eps=inv_eps, groups=[], pml=pml, sources=[dip],
+                     monitors=[mon], dft_stride=stride)
+    m = len(mon.e_idx)
+    wE = rng.normal(size=m) + 1j * rng.normal(size=m)
+    wH = 0.3 * (rng.normal(size=m) + 1j * rng.normal(size=m))
+    return plan, n_steps, wE, wH

@@ -1,0 +1,92 @@
+"""The discrete adjoint on the GPU (lightsmith_b200.adjoint): its objective against the oracle's, its gradient
+against torch autograd through the plain-PyTorch restatement (oracle/autograd.py) and against central finite
+differences of the CUDA forward, with checkpoints every K steps for several K."""
+
+import numpy as np
+import pytest
+import torch
+
+from adjoint_cases import BOX, small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _autograd(plan, n_steps, wE, wH):
+    from oracle.autograd import objective
+
+    base = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in BOX)])
+    x = base.clone().requires_grad_(True)
+    J = objective(plan, x, BOX, 0, 0, wE, wH, n_steps)
+    (g,) = torch.autograd.grad(J, x)
+    return float(J.detach()), g.numpy(), base
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def test_adjoint_gradient_matches_autograd_in_double():
+    from lightsmith_b200.adjoint import AdjointRun
+
+    plan, n_steps, wE, wH = small_case()
+    J_ref, g_ref, base = _autograd(plan, n_steps, wE, wH)
+    run = AdjointRun(plan, BOX, wE=wE, wH=wH, checkpoint=2 * plan["stride"], precision="double")
+    run.set_inv_eps_box(base)
+    J, _ = run.forward(n_steps)
+    g = run.backward().cpu().numpy()
+    run.close()
+    assert abs(J - J_ref) / J_ref < 1e-11
+    assert np.abs(g_ref).max() > 0
+    assert _rel(g, g_ref) < 1e-9
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    from lightsmith_b200.adjoint import AdjointRun
+
+    plan, n_steps, wE, wH = small_case()
+    grads = []
+    for K in (plan["stride"], 3 * plan["stride"], n_steps):
+        run = AdjointRun(plan, BOX, wE=wE, wH=wH, checkpoint=K, precision="double")
+        run.forward(n_steps)
+        grads.append(run.backward().cpu().numpy())
+        run.close()
+    assert np.array_equal(grads[0], grads[1]) and np.array_equal(grads[0], grads[2])
+
+
+def test_autograd_function_and_single_precision():
+    """fdtd_objective as a torch.autograd.Function (float32 engine) against the float64 autograd reference."""
+    from lightsmith_b200.adjoint import AdjointRun, fdtd_objective
+
+    plan, n_steps, wE, wH = small_case()
+    J_ref, g_ref, base = _autograd(plan, n_steps, wE, wH)
+    run = AdjointRun(plan, BOX, wE=wE, wH=wH, checkpoint=2 * plan["stride"], precision="single")
+    x = base.clone().to("cuda").requires_grad_(True)
+    J = fdtd_objective(x, run, n_steps)
+    J.backward()
+    run.close()
+    assert abs(float(J.detach()) - J_ref) / J_ref < 1e-4
+    assert _rel(x.grad.cpu().numpy(), g_ref) < 1e-3
+
+
+def test_adjoint_gradient_matches_central_differences():
+    from lightsmith_b200.adjoint import AdjointRun
+
+    plan, n_steps, wE, wH = small_case()
+    run = AdjointRun(plan, BOX, wE=wE, wH=wH, checkpoint=2 * plan["stride"], precision="double")
+    base = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in BOX)])
+    run.set_inv_eps_box(base)
+    run.forward(n_steps)
+    g = run.backward().cpu().numpy()
+    h = 1e-6
+    for flat in np.argsort(-np.abs(g).reshape(-1))[:4]:
+        idx = tuple(int(v) for v in np.unravel_index(flat, g.shape))
+        vals = []
+        for sgn in (1, -1):
+            x = base.clone()
+            x[idx] += sgn * h
+            run.set_inv_eps_box(x)
+            vals.append(run.forward(n_steps)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
+    run.close()
