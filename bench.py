@@ -49,7 +49,7 @@ def _args():
     ap.add_argument("--tile-y", type=int, default=8, help="fused pass: tile rows along y")
     ap.add_argument("--planes", type=int, default=32, help="fused pass: x planes per CTA")
     ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring")
-    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep"],
+    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint"],
                     help="sweep: the batched oblique-incidence sweep (96 Bloch-periodic runs) against the same "
                          "runs one after another")
     ap.add_argument("--runs", type=int, default=96, help="sweep: number of runs")
@@ -401,12 +401,63 @@ def run_sweep(args):
     print(json.dumps(out), flush=True)
 
 
+def run_adjoint(args):
+    """The inverse-design gradient: the slab device (200 x 200 x 120 cells of 20 nm, CPML 12, FP32, 100 x 100
+    x 11 design box of a projected Gaussian random field), 8000 steps, checkpoints every 256 steps. Times the
+    forward run (J) and the gradient (recomputation from checkpoints plus the reverse steps) on the device
+    clock; the gradient is taken with respect to the design density rho (chain rule through eps)."""
+    import numpy as np
+    import torch
+
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import slab_device_plan
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    plan, box, wE, info = slab_device_plan(n_steps=8000)
+    run = AdjointRun(plan, box, wE=wE, checkpoint=256)
+    rho = info["rho"]
+    eps = info["eps_clad"] + rho[:, :, None] * (info["eps_core"] - info["eps_clad"])
+    inv_box = np.broadcast_to(1.0 / eps, tuple(b - a for a, b in box))
+    run.set_inv_eps_box(inv_box)
+    run.forward(10 * plan["stride"])  # warm-up (kernels, allocator)
+    run.backward()
+    clocks = Clocks(_gpu_uuid(torch, dev))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize(dev)
+    ev[0].record()
+    J, _ = run.forward(info["n_steps"])
+    ev[1].record()
+    g_inv = run.backward()
+    ev[2].record()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    t_fwd, t_grad = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    d_inv = -(info["eps_core"] - info["eps_clad"]) / torch.as_tensor(eps, device=dev) ** 2
+    g_rho = (g_inv * d_inv).sum(dim=2)
+    cells = int(np.prod(plan["shape"]))
+    run.close()
+    out = {"metric": "FDTD adjoint gradient time / forward time", "value": t_grad / t_fwd, "unit": "ratio",
+           "n_gpus": 1, "steps": info["n_steps"], "warmup": 1, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "220 nm Si slab in SiO2, 200 x 200 x 120 cells of 20 nm, CPML 12, 2 x 2 um design "
+                                  "region (100 x 100 x 11 nodes) of a seeded Gaussian random field (corr. 100 nm, tanh "
+                                  "projection beta 8), TE0 slab-mode pulse at 1550 nm, |DFT overlap|^2 on the output "
+                                  "plane", "checkpoint_steps": 256},
+           "forward_ms": t_fwd, "gradient_ms": t_grad,
+           "forward_gcells": cells * info["n_steps"] / (t_fwd / 1e3) / 1e9,
+           "objective": J, "grad_rho_absmax": float(g_rho.abs().max()), "clocks": clk}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "sweep":
         run_sweep(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_b200(args)
 

@@ -150,7 +150,6 @@ class Engine:
             _abi.check(L.lsfdtd_engine_set_scratch(self._h, _ptr(self.scratch), int(nbytes.value)),
                        "lsfdtd_engine_set_scratch")
         self._graph_used = False
-        self._primed = False
 
     def _dev(self, a, dtype):
         t = _torch().as_tensor(np.ascontiguousarray(a)).to(device=self.dev, dtype=dtype).contiguous()
@@ -394,10 +393,10 @@ class Engine:
 
     # --- running ---------------------------------------------------------------------------------------------
     def _prime(self):
+        """The engine's stream waits for the caller's: whatever the caller did to the engine's arrays on its own
+        stream (writes, or reads such as a checkpoint's copy) comes before the engine's next kernels."""
         torch = _torch()
-        if not self._primed:
-            self.stream.wait_stream(torch.cuda.current_stream(self.dev))
-            self._primed = True
+        self.stream.wait_stream(torch.cuda.current_stream(self.dev))
 
     def _finish(self):
         _torch().cuda.current_stream(self.dev).wait_stream(self.stream)

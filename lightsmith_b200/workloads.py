@@ -201,3 +201,101 @@ def metasurface_sweep(n_runs: int = 96, seed: int = 0, **kw) -> list[dict]:
         pol = "s" if rng.integers(2) == 0 else "p"
         runs.append(metasurface_run(period, theta, phi, wl, pol, **kw))
     return runs
+
+
+# --- the adjoint workload: a slab waveguide device with a design region ---------------------------------
+
+
+def slab_te0(n_core: float, n_clad: float, thickness: float, wavelength: float):
+    """(beta, profile(z)) of the fundamental TE mode of a symmetric slab: E_y = cos(kappa z) in the core
+    (|z| <= t/2), cos(kappa t/2) exp(-gamma (|z| - t/2)) outside, from kappa tan(kappa t/2) = gamma (bisection
+    on kappa in (0, pi/t))."""
+    k0 = 2 * np.pi / wavelength
+    V = k0 * math.sqrt(n_core ** 2 - n_clad ** 2)
+    lo, hi = 1e-12, min(math.pi / thickness, V) * (1 - 1e-12)
+
+    def f(kap):
+        return kap * math.tan(kap * thickness / 2) - math.sqrt(max(V * V - kap * kap, 0.0))
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(lo) * f(mid) <= 0:
+            hi = mid
+        else:
+            lo = mid
+    kap = 0.5 * (lo + hi)
+    gam = math.sqrt(V * V - kap * kap)
+    beta = math.sqrt((n_core * k0) ** 2 - kap ** 2)
+
+    def profile(z):
+        z = np.abs(np.asarray(z, float))
+        inside = z <= thickness / 2
+        return np.where(inside, np.cos(kap * z), math.cos(kap * thickness / 2) * np.exp(-gam * (z - thickness / 2)))
+    return beta, profile
+
+
+def design_field(shape2, corr_cells: float, seed: int, beta: float = 8.0, eta: float = 0.5) -> np.ndarray:
+    """rho in [0, 1] over a 2D design region: white noise from ``seed`` filtered by a Gaussian of correlation
+    length ``corr_cells`` (FFT), normalised, then the tanh projection with steepness beta about eta."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape2)
+    kx = np.fft.fftfreq(shape2[0])[:, None]
+    ky = np.fft.fftfreq(shape2[1])[None, :]
+    g = np.real(np.fft.ifft2(np.fft.fft2(w) * np.exp(-2 * (np.pi * corr_cells) ** 2 * (kx ** 2 + ky ** 2))))
+    g = (g - g.mean()) / (g.std() + 1e-30)
+    x = 1 / (1 + np.exp(-g))  # into (0, 1) about 0.5
+    num = np.tanh(beta * eta) + np.tanh(beta * (x - eta))
+    return num / (np.tanh(beta * eta) + np.tanh(beta * (1 - eta)))
+
+
+def slab_device_plan(shape=(200, 200, 120), dx: float = 20.0, pml: int = 12, design=(100, 100),
+                     thickness: float = 220.0, n_core: float = 3.48, n_clad: float = 1.44,
+                     wavelength: float = 1550.0, n_steps: int = 8000, stride: int = 10, seed: int = 0,
+                     single: bool = True):
+    """The inverse-design workload: a ``thickness`` slab of index n_core in n_clad filling the grid along x and
+    y (the input and output waveguides), a ``design`` (cells) region of it in the middle whose permittivity is
+    eps = n_clad^2 + rho (n_core^2 - n_clad^2) for a seeded Gaussian random field rho (correlation 100 nm, tanh
+    projection beta = 8), the slab's TE0 mode launched by an E_y current sheet on a plane before the design
+    region (a Gaussian pulse at ``wavelength``) and the objective's monitor, E_y on a plane after it.
+
+    Returns (plan, box, wE, info): the design box (node ranges), the overlap weights of the monitor's points
+    (the mode profile times the cell area) and the pieces that map rho to 1/eps."""
+    n0, n1, n2 = shape
+    dt = 0.99 * dx / math.sqrt(3)
+    zc = n2 // 2
+    z = (np.arange(n2) - zc) * dx
+    core = np.abs(z) <= thickness / 2
+    eps = np.full(shape, n_clad ** 2)
+    eps[:, :, core] = n_core ** 2
+    x0 = (n0 - design[0]) // 2
+    y0 = (n1 - design[1]) // 2
+    box = ((x0, x0 + design[0]), (y0, y0 + design[1]), (int(np.nonzero(core)[0][0]), int(np.nonzero(core)[0][-1]) + 1))
+    rho = design_field(design, 100.0 / dx, seed)
+    eps[box[0][0]:box[0][1], box[1][0]:box[1][1], box[2][0]:box[2][1]] = (
+        n_clad ** 2 + rho[:, :, None] * (n_core ** 2 - n_clad ** 2))
+    inv_eps = 1.0 / eps
+    beta, prof = slab_te0(n_core, n_clad, thickness, wavelength)
+    # E_y nodes of the source and monitor planes: y over the non-CPML range, z within the mode's extent
+    ys = np.arange(pml + 2, n1 - pml - 2)
+    zs = np.arange(n2)[np.abs(z) <= thickness / 2 + 3 * wavelength / (2 * np.pi * math.sqrt(n_core ** 2 - n_clad ** 2))]
+    zs = zs[(zs > pml + 1) & (zs < n2 - pml - 2)]
+    Y, Z = np.meshgrid(ys, zs, indexing="ij")
+    amp = prof((Z.ravel() - zc) * dx)
+    x_src, x_out = pml + 6, n0 - pml - 7
+    src_idx = flat_index(1, np.full(Y.size, x_src), Y.ravel(), Z.ravel(), shape).astype(np.int64)
+    omega = 2 * np.pi / wavelength
+    half = 0.1 * omega
+    tau = 2.0 / half
+    t0 = 3.5 * tau
+    t = np.arange(n_steps + 3) * dt
+    gpulse = np.exp(-(((t - t0) / tau) ** 2)) * np.sin(omega * (t - t0))
+    flat_inv = inv_eps.reshape(-1)
+    coef = dt * flat_inv[src_idx % (n0 * n1 * n2)] * amp
+    src = DipoleSource(idx=src_idx, coef=coef, wave=np.diff(gpulse) / (omega * dt))
+    mon_idx = flat_index(1, np.full(Y.size, x_out), Y.ravel(), Z.ravel(), shape).astype(np.int64)
+    mon = DFTMonitor(np.array([omega]), mon_idx, None, None, energy=0)
+    spec = PMLSpec(cells=((pml, pml),) * 3, alpha_max=0.05 * omega, eps_ref=n_clad ** 2)
+    plan = make_plan(shape=shape, dx=dx, dt=dt, single=single, inv_eps=inv_eps, groups=[], pml=spec, sources=[src],
+                     monitors=[mon], dft_stride=stride)
+    wE = amp * dx * dx
+    info = {"rho": rho, "eps_clad": n_clad ** 2, "eps_core": n_core ** 2, "n_steps": n_steps}
+    return plan, box, wE, info

@@ -14,7 +14,7 @@ BOX = ((10, 15), (6, 12), (5, 9))
 DX = 20.0
 
 
-def small_case(seed: int = 4, n_chunks: int = 4):
+def small_case(seed: int = 4, n_chunks: int = 4, pml_cells: int = 4):
     """(plan, n_steps, weights of the monitor's E and H points)."""
     dt = 0.99 * DX / math.sqrt(3)
     rng = np.random.default_rng(seed)
@@ -33,7 +33,7 @@ def small_case(seed: int = 4, n_chunks: int = 4):
     first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
     dip.wave = np.concatenate([w[first:], np.zeros(first)])
     mon = plane_monitor(SHAPE, 12, [omega], energy=1)
-    pml = PMLSpec(cells=((4, 4),) * 3, alpha_max=0.02, eps_ref=1.5)
+    pml = PMLSpec(cells=((pml_cells, pml_cells),) * 3, alpha_max=0.02, eps_ref=1.5)
     plan = make_plan(shape=SHAPE, dx=DX, dt=dt, single=False, inv_eps=inv_eps, groups=[], pml=pml, sources=[dip],
                      monitors=[mon], dft_stride=stride)
     m = len(mon.e_idx)

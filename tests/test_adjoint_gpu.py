@@ -90,3 +90,42 @@ def test_adjoint_gradient_matches_central_differences():
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
     run.close()
+
+
+@pytest.mark.slow
+def test_slab_device_gradient_in_rho_matches_finite_differences_on_32_cells():
+    """The inverse-design workload at reduced size (float64): dJ/drho of the extruded design density by the
+    adjoint against central differences on 32 random design cells."""
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import slab_device_plan
+
+    plan, box, wE, info = slab_device_plan(shape=(64, 64, 48), pml=8, design=(24, 24), n_steps=1200, stride=10,
+                                           single=False)
+    run = AdjointRun(plan, box, wE=wE, checkpoint=200, precision="double")
+    nz = box[2][1] - box[2][0]
+    a, b = info["eps_clad"], info["eps_core"]
+
+    def J_of(rho):
+        eps = a + rho[:, :, None] * (b - a)
+        run.set_inv_eps_box(torch.as_tensor(np.broadcast_to(1.0 / eps, rho.shape + (nz,)).copy()))
+        return run.forward(info["n_steps"])[0]
+
+    rho = info["rho"]
+    J0 = J_of(rho)
+    g_inv = run.backward().cpu().numpy()
+    eps = a + rho[:, :, None] * (b - a)
+    g = (g_inv * (-(b - a) / eps ** 2)).sum(axis=2)
+    assert J0 > 0 and np.abs(g).max() > 0
+    rng = np.random.default_rng(1)
+    cells = rng.choice(rho.size, 32, replace=False)
+    h = 1e-5
+    errs = []
+    for c in cells:
+        i, j = np.unravel_index(c, rho.shape)
+        rp, rm = rho.copy(), rho.copy()
+        rp[i, j] += h
+        rm[i, j] -= h
+        fd = (J_of(rp) - J_of(rm)) / (2 * h)
+        errs.append(abs(fd - g[i, j]) / max(np.abs(g).max(), 1e-300))
+    run.close()
+    assert max(errs) < 1e-5, max(errs)
