@@ -157,11 +157,12 @@ class AdjointRun:
             raise ValueError("n_steps must be a multiple of dft_stride")
         self._reset()
         self._ckpt = [self._save()]
-        for n in range(n_steps):
-            eng.step(1)
-            if (n + 1) % self.stride == 0:
-                eng.sample()
-            if (n + 1) % self.K == 0 and n + 1 < n_steps:
+        done = 0
+        while done < n_steps:  # chunks (dft_stride steps and a sample) replayed as CUDA graphs
+            seg = min(self.K, n_steps - done)
+            eng.chunk(seg // self.stride, use_graph=True)
+            done += seg
+            if done < n_steps:
                 self._ckpt.append(self._save())
         self.n_steps = n_steps
         m = eng.monitors[self.monitor]
@@ -189,18 +190,17 @@ class AdjointRun:
                     t.zero_()
         self.grad.zero_()
         torch.cuda.synchronize(self.dev)
-        h = self._h
-        stream = eng.stream
+        h, he = self._h, eng._h
+        st = eng.stream.cuda_stream  # every launch below on the engine's stream, in order
         for k in reversed(range(len(self._ckpt))):
             n0 = k * self.K
             n1 = min(n0 + self.K, self.n_steps)
             self._restore(self._ckpt[k], n0)
-            torch.cuda.synchronize(self.dev)
             for i in range(n1 - n0):
-                eng.step(1)
-                _abi.check(L.lsfdtd_adjoint_record(h, i, stream.cuda_stream), "lsfdtd_adjoint_record")
+                _abi.check(L.lsfdtd_engine_step(he, 1, st), "lsfdtd_engine_step")
+                _abi.check(L.lsfdtd_adjoint_record(h, i, st), "lsfdtd_adjoint_record")
             for i in reversed(range(n1 - n0)):
-                _abi.check(L.lsfdtd_adjoint_step(h, n0 + i, i, stream.cuda_stream), "lsfdtd_adjoint_step")
+                _abi.check(L.lsfdtd_adjoint_step(h, n0 + i, i, st), "lsfdtd_adjoint_step")
             torch.cuda.synchronize(self.dev)
         return self.grad.sum(0) * eng.cdx
 

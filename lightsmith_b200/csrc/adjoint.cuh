@@ -35,6 +35,8 @@ struct AdjArgs {
   R* ph_old[3][3][2];       // psibar of H
   R* ph_new[3][3][2];
   int box_lo[3], box_hi[3];  // gradient box (nodes)
+  int ein_lo[3], ein_hi[3];  // nodes stepped for every E component and outside every E slab, per axis
+  int hin_lo[3], hin_hi[3];  // the same for H
   const R* hist;            // H^{n+1/2} over [box_lo - 1, box_hi) per component
   double* grad;             // dJ/dcbE per component over the box
 };
@@ -61,16 +63,18 @@ __device__ __forceinline__ bool adj_in_grid(const int* x, const int* n) {
 }
 
 // adjoint of difference `which` (0: a, along d1; 1: b, along d2) of component c's E update at node x
-template <typename R>
+// FAST: x is known to be stepped for every component and outside every slab (no tests, no CPML term)
+template <bool FAST, typename R>
 __device__ __forceinline__ R adj_e_diff(const AdjArgs<R>& A, int c, int which, const int* x) {
   const YeeArgs<R>& g = A.y;
-  if (!adj_in_grid(x, g.n) || !in_e_region(c, x, g.n, g.periodic)) return R(0);
+  if (!FAST && (!adj_in_grid(x, g.n) || !in_e_region(c, x, g.n, g.periodic))) return R(0);
   const long long p = ((long long)x[0] * g.n[1] + x[1]) * g.n[2] + x[2];
   const int d1 = (c + 1) % 3, d2 = (c + 2) % 3, d = which ? d2 : d1;
   const R eb = A.Eb[c][p];
   const R cb = g.cbE[c][p];
   R v = which ? -(eb * cb) : eb * cb;
   if (!g.uniform) v = v * g.inv_d[d];
+  if (FAST) return v;
   int side;
   const long long q = adj_slab<0>(g.pml[d], d, c, x, g.n, &side);
   if (q >= 0) {
@@ -86,15 +90,16 @@ __device__ __forceinline__ R adj_e_diff(const AdjArgs<R>& A, int c, int which, c
 }
 
 // the same for the H update (forward differences, coefficient -cH, H's CPML signs)
-template <typename R>
+template <bool FAST, typename R>
 __device__ __forceinline__ R adj_h_diff(const AdjArgs<R>& A, int c, int which, const int* x) {
   const YeeArgs<R>& g = A.y;
-  if (!adj_in_grid(x, g.n) || !in_h_region(c, x, g.n, g.periodic)) return R(0);
+  if (!FAST && (!adj_in_grid(x, g.n) || !in_h_region(c, x, g.n, g.periodic))) return R(0);
   const long long p = ((long long)x[0] * g.n[1] + x[1]) * g.n[2] + x[2];
   const int d1 = (c + 1) % 3, d2 = (c + 2) % 3, d = which ? d2 : d1;
   const R hb = A.Hb[c][p];
   R v = which ? hb * g.cH : -(hb * g.cH);
   if (!g.uniform) v = v * g.inv_d[d];
+  if (FAST) return v;
   int side;
   const long long q = adj_slab<1>(g.pml[d], d, c, x, g.n, &side);
   if (q >= 0) {
@@ -117,24 +122,58 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
   if (k >= g.n[2] || j >= g.n[1]) return;
   const int x[3] = {i, j, k};
   const long long p = ((long long)i * g.n[1] + j) * g.n[2] + k;
+  // the node and its +1 neighbours along every axis are E-inner: every difference adjoint is test-free
+  bool fast = true;
 #pragma unroll
-  for (int jj = 0; jj < 3; ++jj) {
-    const int ca = (jj + 1) % 3, da = (jj + 2) % 3;  // the component whose difference a reads H_jj along da
-    const int cb = (jj + 2) % 3, db = (jj + 1) % 3;  // and whose difference b reads it along db
-    int xa[3] = {i, j, k}, xb[3] = {i, j, k};
-    xa[da] += 1;
-    xb[db] += 1;
-    const R acc = (adj_e_diff(A, ca, 0, x) - adj_e_diff(A, ca, 0, xa)) +
-                  (adj_e_diff(A, cb, 1, x) - adj_e_diff(A, cb, 1, xb));
-    A.Hb[jj][p] += acc;
+  for (int ax = 0; ax < 3; ++ax) fast = fast && x[ax] >= A.ein_lo[ax] && x[ax] + 1 < A.ein_hi[ax];
+  R acc[3];
+  if (fast) {
+    // Ebar_c cbE_c at the node and at its +1 neighbours, every load before the first store
+    const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
+    R u0[3], u1[3][3];  // u0[c]: at the node; u1[c][d]: at the node + e_d
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      u0[c] = A.Eb[c][p] * g.cbE[c][p];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d != c) u1[c][d] = A.Eb[c][p + st[d]] * g.cbE[c][p + st[d]];
+    }
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) {
+      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
+      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
+      R va0 = u0[ca], va1 = u1[ca][da], vb0 = -u0[cb], vb1 = -u1[cb][db];
+      if (!g.uniform) {
+        va0 = va0 * g.inv_d[da];
+        va1 = va1 * g.inv_d[da];
+        vb0 = vb0 * g.inv_d[db];
+        vb1 = vb1 * g.inv_d[db];
+      }
+      acc[jj] = (va0 - va1) + (vb0 - vb1);
+    }
+  } else {
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) {
+      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;  // the component whose difference a reads H_jj along da
+      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;  // and whose difference b reads it along db
+      int xa[3] = {i, j, k}, xb[3] = {i, j, k};
+      xa[da] += 1;
+      xb[db] += 1;
+      acc[jj] = (adj_e_diff<false>(A, ca, 0, x) - adj_e_diff<false>(A, ca, 0, xa)) +
+                (adj_e_diff<false>(A, cb, 1, x) - adj_e_diff<false>(A, cb, 1, xb));
+    }
   }
+  const R hb0 = A.Hb[0][p], hb1 = A.Hb[1][p], hb2 = A.Hb[2][p];
+  A.Hb[0][p] = hb0 + acc[0];
+  A.Hb[1][p] = hb1 + acc[1];
+  A.Hb[2][p] = hb2 + acc[2];
   // this node's E psibar, and the gradient
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (!in_e_region(c, x, g.n, g.periodic)) continue;
     const R eb = A.Eb[c][p];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3 && !fast; ++d) {  // an inner node lies in no slab
       if (d == c) continue;
       int side;
       const long long q = adj_slab<0>(g.pml[d], d, c, x, g.n, &side);
@@ -170,23 +209,58 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
   if (k >= g.n[2] || j >= g.n[1]) return;
   const int x[3] = {i, j, k};
   const long long p = ((long long)i * g.n[1] + j) * g.n[2] + k;
+  // the node and its -1 neighbours along every axis are H-inner
+  bool fast = true;
 #pragma unroll
-  for (int jj = 0; jj < 3; ++jj) {
-    const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
-    const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
-    int xa[3] = {i, j, k}, xb[3] = {i, j, k};
-    xa[da] -= 1;
-    xb[db] -= 1;
-    const R acc = (adj_h_diff(A, ca, 0, xa) - adj_h_diff(A, ca, 0, x)) +
-                  (adj_h_diff(A, cb, 1, xb) - adj_h_diff(A, cb, 1, x));
-    A.Eb[jj][p] += acc;
+  for (int ax = 0; ax < 3; ++ax) fast = fast && x[ax] - 1 >= A.hin_lo[ax] && x[ax] < A.hin_hi[ax];
+  R acc[3];
+  if (fast) {
+    // Hbar_c at the node and at its -1 neighbours, every load before the first store
+    const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
+    R h0[3], hm[3][3];  // h0[c]: at the node; hm[c][d]: at the node - e_d
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      h0[c] = A.Hb[c][p];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d != c) hm[c][d] = A.Hb[c][p - st[d]];
+    }
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) {
+      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
+      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
+      // a of H_ca: -Hbar cH (along da); b of H_cb: +Hbar cH (along db)
+      R va1 = -(hm[ca][da] * g.cH), va0 = -(h0[ca] * g.cH), vb1 = hm[cb][db] * g.cH, vb0 = h0[cb] * g.cH;
+      if (!g.uniform) {
+        va1 = va1 * g.inv_d[da];
+        va0 = va0 * g.inv_d[da];
+        vb1 = vb1 * g.inv_d[db];
+        vb0 = vb0 * g.inv_d[db];
+      }
+      acc[jj] = (va1 - va0) + (vb1 - vb0);
+    }
+  } else {
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) {
+      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
+      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
+      int xa[3] = {i, j, k}, xb[3] = {i, j, k};
+      xa[da] -= 1;
+      xb[db] -= 1;
+      acc[jj] = (adj_h_diff<false>(A, ca, 0, xa) - adj_h_diff<false>(A, ca, 0, x)) +
+                (adj_h_diff<false>(A, cb, 1, xb) - adj_h_diff<false>(A, cb, 1, x));
+    }
   }
+  const R eb0 = A.Eb[0][p], eb1 = A.Eb[1][p], eb2 = A.Eb[2][p];
+  A.Eb[0][p] = eb0 + acc[0];
+  A.Eb[1][p] = eb1 + acc[1];
+  A.Eb[2][p] = eb2 + acc[2];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (!in_h_region(c, x, g.n, g.periodic)) continue;
     const R hb = A.Hb[c][p];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3 && !fast; ++d) {  // an inner node lies in no slab
       if (d == c) continue;
       int side;
       const long long q = adj_slab<1>(g.pml[d], d, c, x, g.n, &side);

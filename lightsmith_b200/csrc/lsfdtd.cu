@@ -1179,6 +1179,25 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
   }
   A.hist = static_cast<const R*>(a->d.hist) + (size_t)slot * a->slot_elems;
   A.grad = a->d.grad;
+  // inner node ranges per axis: in every component's stepped region and past every slab of the field
+  for (int ax = 0; ax < 3; ++ax) {
+    const int n = A.y.n[ax];
+    int elo = 1, ehi = n - 1, hlo = 0, hhi = n - 1;
+    const PmlAxis<R>& pm = A.y.pml[ax];
+    if (pm.on) {
+      const int c = (ax + 1) % 3;  // a component with slabs along ax (both share their extent)
+      for (int f = 0; f < 2; ++f) {
+        int& lo = f ? hlo : elo;
+        int& hi = f ? hhi : ehi;
+        if (pm.len[f][c][0] > 0) lo = std::max(lo, pm.start[f][c][0] + pm.len[f][c][0]);
+        if (pm.len[f][c][1] > 0) hi = std::min(hi, pm.start[f][c][1]);
+      }
+    }
+    A.ein_lo[ax] = elo;
+    A.ein_hi[ax] = ehi;
+    A.hin_lo[ax] = hlo;
+    A.hin_hi[ax] = hhi;
+  }
   const auto& desc = a->eng->desc;
   if ((n + 1) % desc.dft_stride == 0 && a->d.n_e + a->d.n_h > 0) {
     k_adj_inject<R><<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(
