@@ -13,6 +13,8 @@
 // gathers, for H node q: Hbar_j(q) += abar(j+1, q) - abar(j+1, q + e_{j+2}) + bbar(j+2, q) - bbar(j+2,
 // q + e_{j+1}) (indices mod 3). The H update's transpose is the same with forward differences. psibar is
 // double buffered (each kernel reads the step's old values, also at neighbours, and writes the new ones).
+// A warp whose nodes and neighbours are all interior (stepped, in no slab) takes the plain stencil; any
+// other warp takes the stencil with the stepped-region tests as masks plus the slab terms per axis.
 //
 // The objective's adjoint source (the DFT samples' weights times e^{i omega t}) is added to Ebar and Hbar at
 // the steps the monitor sampled, before that step's reverse. The gradient with respect to the E curl
@@ -41,77 +43,88 @@ struct AdjArgs {
   double* grad;             // dJ/dcbE per component over the box
 };
 
-// psi index of node x in the slab of axis d (field FLD, component c), or -1 when x is not in it
+// slab of axis d holding coordinate u (sides share the extent of both components c != d), or -1
 template <int FLD, typename R>
-__device__ __forceinline__ long long adj_slab(const PmlAxis<R>& p, int d, int c, const int* x, const int* n,
-                                              int* side) {
-  if (!p.on) return -1;
-  const int u = x[d];
-#pragma unroll
-  for (int sd = 0; sd < 2; ++sd) {
-    const int st = p.start[FLD][c][sd], ln = p.len[FLD][c][sd];
-    if (ln > 0 && u >= st && u < st + ln) {
-      *side = sd;
-      return psi_index(x, n, d, u - st, ln);
-    }
-  }
+__device__ __forceinline__ int adj_side(const PmlAxis<R>& pm, int c, int u) {
+  if (pm.len[FLD][c][0] > 0 && u >= pm.start[FLD][c][0] && u < pm.start[FLD][c][0] + pm.len[FLD][c][0]) return 0;
+  if (pm.len[FLD][c][1] > 0 && u >= pm.start[FLD][c][1] && u < pm.start[FLD][c][1] + pm.len[FLD][c][1]) return 1;
   return -1;
 }
 
-__device__ __forceinline__ bool adj_in_grid(const int* x, const int* n) {
-  return x[0] >= 0 && x[0] < n[0] && x[1] >= 0 && x[1] < n[1] && x[2] >= 0 && x[2] < n[2];
-}
-
-// adjoint of difference `which` (0: a, along d1; 1: b, along d2) of component c's E update at node x
-// FAST: x is known to be stepped for every component and outside every slab (no tests, no CPML term)
-template <bool FAST, typename R>
-__device__ __forceinline__ R adj_e_diff(const AdjArgs<R>& A, int c, int which, const int* x) {
+// Transposed E update at H node x for a warp with any node outside the interior: the curl stencil with the
+// stepped-region tests as masks (non-periodic grids), then, per axis d whose slab holds x or x + e_d, the CPML
+// terms of the two components c != d (warp-uniform branches for d = 0, 1), and x's own E psibar.
+template <typename R>
+__device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
+                                           R* acc) {
   const YeeArgs<R>& g = A.y;
-  if (!FAST && (!adj_in_grid(x, g.n) || !in_e_region(c, x, g.n, g.periodic))) return R(0);
-  const long long p = ((long long)x[0] * g.n[1] + x[1]) * g.n[2] + x[2];
-  const int d1 = (c + 1) % 3, d2 = (c + 2) % 3, d = which ? d2 : d1;
-  const R eb = A.Eb[c][p];
-  const R cb = g.cbE[c][p];
-  R v = which ? -(eb * cb) : eb * cb;
-  if (!g.uniform) v = v * g.inv_d[d];
-  if (FAST) return v;
-  int side;
-  const long long q = adj_slab<0>(g.pml[d], d, c, x, g.n, &side);
-  if (q >= 0) {
-    const PmlAxis<R>& pm = g.pml[d];
-    const R sgn = which ? R(-1) : R(1);
-    R s = g.uniform ? cb : cb / pm.div;
-    s = sgn * s;
-    const R tot = A.pe_old[d][c][side][q] + eb;
-    v += tot * (s * pm.c[0][x[d]]);
-    if (pm.k[0]) v += eb * (s * pm.k[0][x[d]]);
+  bool okc[3], oko[3], nb[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    okc[a] = x[a] < g.n[a] - 1;  // along the component's own axis
+    oko[a] = x[a] >= 1 && okc[a];
+    nb[a] = x[a] + 1 < g.n[a] - 1;
   }
-  return v;
-}
-
-// the same for the H update (forward differences, coefficient -cH, H's CPML signs)
-template <bool FAST, typename R>
-__device__ __forceinline__ R adj_h_diff(const AdjArgs<R>& A, int c, int which, const int* x) {
-  const YeeArgs<R>& g = A.y;
-  if (!FAST && (!adj_in_grid(x, g.n) || !in_h_region(c, x, g.n, g.periodic))) return R(0);
-  const long long p = ((long long)x[0] * g.n[1] + x[1]) * g.n[2] + x[2];
-  const int d1 = (c + 1) % 3, d2 = (c + 2) % 3, d = which ? d2 : d1;
-  const R hb = A.Hb[c][p];
-  R v = which ? hb * g.cH : -(hb * g.cH);
-  if (!g.uniform) v = v * g.inv_d[d];
-  if (FAST) return v;
-  int side;
-  const long long q = adj_slab<1>(g.pml[d], d, c, x, g.n, &side);
-  if (q >= 0) {
-    const PmlAxis<R>& pm = g.pml[d];
-    const R sgn = which ? R(1) : R(-1);
-    R s = g.uniform ? g.cH : g.cH / pm.div;
-    s = sgn * s;
-    const R tot = A.ph_old[d][c][side][q] + hb;
-    v += tot * (s * pm.c[1][x[d]]);
-    if (pm.k[1]) v += hb * (s * pm.k[1][x[d]]);
+  R eb0[3], cb0[3], eb1[3][3], cb1[3][3];
+  bool m0[3], m1[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+    m0[c] = okc[c] && oko[d1] && oko[d2];
+    eb0[c] = m0[c] ? A.Eb[c][p] : R(0);
+    cb0[c] = m0[c] ? g.cbE[c][p] : R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d == c) continue;
+      m1[c][d] = nb[d] && okc[c] && oko[3 - c - d];
+      eb1[c][d] = m1[c][d] ? A.Eb[c][p + st[d]] : R(0);
+      cb1[c][d] = m1[c][d] ? g.cbE[c][p + st[d]] : R(0);
+    }
   }
-  return v;
+  acc[0] = acc[1] = acc[2] = R(0);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) continue;
+      const int jh = 3 - c - d;
+      R v = eb0[c] * cb0[c] - eb1[c][d] * cb1[c][d];
+      if (!g.uniform) v = v * g.inv_d[d];
+      acc[jh] += d == (c + 1) % 3 ? v : -v;
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const PmlAxis<R>& pm = g.pml[d];
+    if (!pm.on) continue;
+    const int cr = (d + 1) % 3;
+    const int s0 = adj_side<0>(pm, cr, x[d]), s1 = adj_side<0>(pm, cr, x[d] + 1);
+    if (s0 < 0 && s1 < 0) continue;
+    const int u = x[d];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) continue;
+      const int jh = 3 - c - d;
+      R t = R(0);
+      if (s0 >= 0 && m0[c]) {
+        const long long q = psi_index(x, g.n, d, u - pm.start[0][c][s0], pm.len[0][c][s0]);
+        const R tot = A.pe_old[d][c][s0][q] + eb0[c];
+        A.pe_new[d][c][s0][q] = tot * pm.b[0][u];
+        R w = tot * pm.c[0][u];
+        if (pm.k[0]) w += eb0[c] * pm.k[0][u];
+        t += g.uniform ? cb0[c] * w : (cb0[c] / pm.div) * w;
+      }
+      if (s1 >= 0 && m1[c][d]) {
+        int y[3] = {x[0], x[1], x[2]};
+        y[d] += 1;
+        const long long q = psi_index(y, g.n, d, u + 1 - pm.start[0][c][s1], pm.len[0][c][s1]);
+        R w = (A.pe_old[d][c][s1][q] + eb1[c][d]) * pm.c[0][u + 1];
+        if (pm.k[0]) w += eb1[c][d] * pm.k[0][u + 1];
+        t -= g.uniform ? cb1[c][d] * w : (cb1[c][d] / pm.div) * w;
+      }
+      acc[jh] += d == (c + 1) % 3 ? t : -t;
+    }
+  }
 }
 
 // transpose of the E update: Hbar += (dE^{n+1}/dH^{n+1/2})^T Ebar; psibar_E to the step before; gradient
@@ -122,14 +135,14 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
   if (k >= g.n[2] || j >= g.n[1]) return;
   const int x[3] = {i, j, k};
   const long long p = ((long long)i * g.n[1] + j) * g.n[2] + k;
+  const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
   // the node and its +1 neighbours along every axis are E-inner: every difference adjoint is test-free
   bool fast = true;
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) fast = fast && x[ax] >= A.ein_lo[ax] && x[ax] + 1 < A.ein_hi[ax];
   R acc[3];
-  if (fast) {
+  if (__all_sync(__activemask(), fast)) {
     // Ebar_c cbE_c at the node and at its +1 neighbours, every load before the first store
-    const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
     R u0[3], u1[3][3];  // u0[c]: at the node; u1[c][d]: at the node + e_d
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -152,51 +165,106 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
       acc[jj] = (va0 - va1) + (vb0 - vb1);
     }
   } else {
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) {
-      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;  // the component whose difference a reads H_jj along da
-      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;  // and whose difference b reads it along db
-      int xa[3] = {i, j, k}, xb[3] = {i, j, k};
-      xa[da] += 1;
-      xb[db] += 1;
-      acc[jj] = (adj_e_diff<false>(A, ca, 0, x) - adj_e_diff<false>(A, ca, 0, xa)) +
-                (adj_e_diff<false>(A, cb, 1, x) - adj_e_diff<false>(A, cb, 1, xb));
-    }
+    adj_e_lean(A, x, p, st, acc);  // also this node's E psibar
   }
   const R hb0 = A.Hb[0][p], hb1 = A.Hb[1][p], hb2 = A.Hb[2][p];
   A.Hb[0][p] = hb0 + acc[0];
   A.Hb[1][p] = hb1 + acc[1];
   A.Hb[2][p] = hb2 + acc[2];
-  // this node's E psibar, and the gradient
+  // the gradient over the box (inside every component's stepped region, outside every E slab)
+  if (i >= A.box_lo[0] && i < A.box_hi[0] && j >= A.box_lo[1] && j < A.box_hi[1] && k >= A.box_lo[2] &&
+      k < A.box_hi[2]) {
+    const int h0 = A.box_hi[0] - A.box_lo[0] + 1, h1 = A.box_hi[1] - A.box_lo[1] + 1,
+              h2 = A.box_hi[2] - A.box_lo[2] + 1;
+    const long long hs = (long long)h0 * h1 * h2;
+    auto H = [&](int comp, int dx, int dy, int dz) {
+      const long long o = ((long long)(i - A.box_lo[0] + 1 + dx) * h1 + (j - A.box_lo[1] + 1 + dy)) * h2 +
+                          (k - A.box_lo[2] + 1 + dz);
+      return A.hist[comp * hs + o];
+    };
+    const int b0 = A.box_hi[0] - A.box_lo[0], b1 = A.box_hi[1] - A.box_lo[1], b2 = A.box_hi[2] - A.box_lo[2];
+    const long long o = ((long long)(i - A.box_lo[0]) * b1 + (j - A.box_lo[1])) * b2 + (k - A.box_lo[2]);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (!in_e_region(c, x, g.n, g.periodic)) continue;
-    const R eb = A.Eb[c][p];
-#pragma unroll
-    for (int d = 0; d < 3 && !fast; ++d) {  // an inner node lies in no slab
-      if (d == c) continue;
-      int side;
-      const long long q = adj_slab<0>(g.pml[d], d, c, x, g.n, &side);
-      if (q >= 0) A.pe_new[d][c][side][q] = (A.pe_old[d][c][side][q] + eb) * g.pml[d].b[0][x[d]];
-    }
-    if (i >= A.box_lo[0] && i < A.box_hi[0] && j >= A.box_lo[1] && j < A.box_hi[1] && k >= A.box_lo[2] &&
-        k < A.box_hi[2]) {
-      const int h0 = A.box_hi[0] - A.box_lo[0] + 1, h1 = A.box_hi[1] - A.box_lo[1] + 1,
-                h2 = A.box_hi[2] - A.box_lo[2] + 1;
-      const long long hs = (long long)h0 * h1 * h2;
-      auto H = [&](int comp, int dx, int dy, int dz) {
-        const long long o = ((long long)(i - A.box_lo[0] + 1 + dx) * h1 + (j - A.box_lo[1] + 1 + dy)) * h2 +
-                            (k - A.box_lo[2] + 1 + dz);
-        return A.hist[comp * hs + o];
-      };
+    for (int c = 0; c < 3; ++c) {
       const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
       const int s1[3] = {d1 == 0, d1 == 1, d1 == 2}, s2[3] = {d2 == 0, d2 == 1, d2 == 2};
       const R a = H(d2, 0, 0, 0) - H(d2, -s1[0], -s1[1], -s1[2]);
       const R b = H(d1, 0, 0, 0) - H(d1, -s2[0], -s2[1], -s2[2]);
       const R curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
-      const int b0 = A.box_hi[0] - A.box_lo[0], b1 = A.box_hi[1] - A.box_lo[1], b2 = A.box_hi[2] - A.box_lo[2];
-      const long long o = ((long long)(i - A.box_lo[0]) * b1 + (j - A.box_lo[1])) * b2 + (k - A.box_lo[2]);
-      A.grad[(long long)c * b0 * b1 * b2 + o] += (double)eb * (double)curl;
+      A.grad[(long long)c * b0 * b1 * b2 + o] += (double)A.Eb[c][p] * (double)curl;
+    }
+  }
+}
+
+// Transposed H update at E node x for a warp with any node outside the interior (backward neighbours, H's
+// stepped region and CPML signs), with x's own H psibar.
+template <typename R>
+__device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
+                                           R* acc) {
+  const YeeArgs<R>& g = A.y;
+  bool lt[3], ge1[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lt[a] = x[a] < g.n[a] - 1;
+    ge1[a] = x[a] >= 1;
+  }
+  R hb0[3], hb1[3][3];
+  bool m0[3], m1[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    m0[c] = lt[(c + 1) % 3] && lt[(c + 2) % 3];
+    hb0[c] = m0[c] ? A.Hb[c][p] : R(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d == c) continue;
+      m1[c][d] = ge1[d] && lt[3 - c - d];
+      hb1[c][d] = m1[c][d] ? A.Hb[c][p - st[d]] : R(0);
+    }
+  }
+  acc[0] = acc[1] = acc[2] = R(0);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) continue;
+      const int jh = 3 - c - d;
+      R v = hb1[c][d] * g.cH - hb0[c] * g.cH;
+      if (!g.uniform) v = v * g.inv_d[d];
+      acc[jh] += d == (c + 1) % 3 ? -v : v;
+    }
+  }
+  const R sH = g.cH;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const PmlAxis<R>& pm = g.pml[d];
+    if (!pm.on) continue;
+    const int cr = (d + 1) % 3;
+    const int s0 = adj_side<1>(pm, cr, x[d]), s1 = adj_side<1>(pm, cr, x[d] - 1);
+    if (s0 < 0 && s1 < 0) continue;
+    const int u = x[d];
+    const R sc = g.uniform ? sH : sH / pm.div;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) continue;
+      const int jh = 3 - c - d;
+      R t = R(0);
+      if (s1 >= 0 && m1[c][d]) {
+        int y[3] = {x[0], x[1], x[2]};
+        y[d] -= 1;
+        const long long q = psi_index(y, g.n, d, u - 1 - pm.start[1][c][s1], pm.len[1][c][s1]);
+        R w = (A.ph_old[d][c][s1][q] + hb1[c][d]) * pm.c[1][u - 1];
+        if (pm.k[1]) w += hb1[c][d] * pm.k[1][u - 1];
+        t += sc * w;
+      }
+      if (s0 >= 0 && m0[c]) {
+        const long long q = psi_index(x, g.n, d, u - pm.start[1][c][s0], pm.len[1][c][s0]);
+        const R tot = A.ph_old[d][c][s0][q] + hb0[c];
+        A.ph_new[d][c][s0][q] = tot * pm.b[1][u];
+        R w = tot * pm.c[1][u];
+        if (pm.k[1]) w += hb0[c] * pm.k[1][u];
+        t -= sc * w;
+      }
+      acc[jh] += d == (c + 1) % 3 ? -t : t;
     }
   }
 }
@@ -209,14 +277,14 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
   if (k >= g.n[2] || j >= g.n[1]) return;
   const int x[3] = {i, j, k};
   const long long p = ((long long)i * g.n[1] + j) * g.n[2] + k;
+  const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
   // the node and its -1 neighbours along every axis are H-inner
   bool fast = true;
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) fast = fast && x[ax] - 1 >= A.hin_lo[ax] && x[ax] < A.hin_hi[ax];
   R acc[3];
-  if (fast) {
+  if (__all_sync(__activemask(), fast)) {
     // Hbar_c at the node and at its -1 neighbours, every load before the first store
-    const long long st[3] = {(long long)g.n[1] * g.n[2], g.n[2], 1};
     R h0[3], hm[3][3];  // h0[c]: at the node; hm[c][d]: at the node - e_d
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -240,33 +308,12 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
       acc[jj] = (va1 - va0) + (vb1 - vb0);
     }
   } else {
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) {
-      const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
-      const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
-      int xa[3] = {i, j, k}, xb[3] = {i, j, k};
-      xa[da] -= 1;
-      xb[db] -= 1;
-      acc[jj] = (adj_h_diff<false>(A, ca, 0, xa) - adj_h_diff<false>(A, ca, 0, x)) +
-                (adj_h_diff<false>(A, cb, 1, xb) - adj_h_diff<false>(A, cb, 1, x));
-    }
+    adj_h_lean(A, x, p, st, acc);  // also this node's H psibar
   }
   const R eb0 = A.Eb[0][p], eb1 = A.Eb[1][p], eb2 = A.Eb[2][p];
   A.Eb[0][p] = eb0 + acc[0];
   A.Eb[1][p] = eb1 + acc[1];
   A.Eb[2][p] = eb2 + acc[2];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    if (!in_h_region(c, x, g.n, g.periodic)) continue;
-    const R hb = A.Hb[c][p];
-#pragma unroll
-    for (int d = 0; d < 3 && !fast; ++d) {  // an inner node lies in no slab
-      if (d == c) continue;
-      int side;
-      const long long q = adj_slab<1>(g.pml[d], d, c, x, g.n, &side);
-      if (q >= 0) A.ph_new[d][c][side][q] = (A.ph_old[d][c][side][q] + hb) * g.pml[d].b[1][x[d]];
-    }
-  }
 }
 
 // the objective's adjoint source at one sample (after n steps): Ebar[e_idx] += Re(ge e^{i w t_e}),
