@@ -251,8 +251,12 @@ int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
  * run allows it (second buffers given, no periodic axis, sources that only correct E): CTA tiles of 32 x
  * tile_y nodes (8 or 16), x planes per tile (>= 1), copy ring of `stages` x planes (4, 6 or 8). variant 3:
  * variant 1 split in two launches where its planes are copied by the Tensor Memory Accelerator: the fused
- * pass over an interior box that needs no region or CPML tests, and a shell kernel over the CPML slabs and
- * walls (the same values as variant 1, bit for bit). */
+ * pass over an interior box that needs no region or CPML tests, and shell kernels over the CPML slabs and
+ * walls. variant 4: variant 1 with region tests as bit masks and each axis's CPML terms under warp-uniform
+ * branches. Variants 3 and 4 compute the values of variant 1 up to the contraction of multiplies and adds
+ * into fused multiply-adds. planes 0 chooses per grid: 32, or fewer where 32 would leave fewer than about
+ * three waves of CTAs. Default: variant 4, tile_y 8, planes 0, ring 4 (the in-place kernels where the fused
+ * pass does not apply). */
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
                                  int32_t stages);
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting

@@ -5,8 +5,9 @@ the FDTD path: for a run with real fields, no periodic axis and no dispersive gr
 say), the objective J = |A|^2 with A = sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q] over one frequency of one
 DFT monitor, and its gradient with respect to 1/eps over a design box of nodes.
 
-``AdjointRun.forward`` runs the engine (the CUDA kernels, in-place form) for ``n_steps`` steps, sampling the
-monitors as lightsmith's chunks do, and keeps the state (E, H, CPML psi) every ``checkpoint`` steps.
+``AdjointRun.forward`` runs the engine (the CUDA kernels: the fused pass where the run allows it, as a plain
+solve would) for ``n_steps`` steps, sampling the monitors as lightsmith's chunks do, and keeps the state (E, H,
+CPML psi of the current buffer parity) every ``checkpoint`` steps.
 ``AdjointRun.backward`` walks the segments in reverse: it restores a checkpoint, recomputes the segment's steps
 while recording H of the box at every step (``lsfdtd_adjoint_record``), then applies the transposed steps
 (``lsfdtd_adjoint_step``, ``csrc/adjoint.cuh``) from the segment's end to its start, accumulating
@@ -50,7 +51,7 @@ class AdjointRun:
             if not isinstance(s, (DipoleSource, ModeSource, TableSource)):
                 raise ValueError(f"{type(s).__name__} keeps state of its own; the adjoint does not restore it")
         self.plan = plan
-        self.eng = Engine.from_plan(plan, device=device, precision=precision, fused=False)
+        self.eng = Engine.from_plan(plan, device=device, precision=precision)
         eng = self.eng
         if not eng.isotropic:
             raise ValueError("the adjoint's design box needs isotropic permittivity (one 1/eps per node)")
@@ -117,8 +118,7 @@ class AdjointRun:
 
     # --- state ----------------------------------------------------------------------------------------------
     def _state(self):
-        eng = self.eng
-        return [eng.E, eng.H] + list(eng.psi.values())
+        return self.eng.state()
 
     def _save(self):
         return [t.clone() for t in self._state()]
@@ -132,7 +132,7 @@ class AdjointRun:
         _torch().cuda.synchronize(self.dev)  # the engine's stream starts from the restored state
 
     def _reset(self):
-        for t in self._state():
+        for t in self.eng.all_state():
             t.zero_()
         for m in self.eng.monitors:
             m["acc_e"].zero_()
@@ -149,8 +149,9 @@ class AdjointRun:
         torch.cuda.synchronize(self.dev)
 
     # --- passes -----------------------------------------------------------------------------------------------
-    def forward(self, n_steps: int):
-        """Runs n_steps steps from rest (a multiple of dft_stride); returns (J, A)."""
+    def forward(self, n_steps: int, keep: bool = True):
+        """Runs n_steps steps from rest (a multiple of dft_stride); returns (J, A). ``keep=False`` saves no
+        checkpoints (J alone, e.g. for a line search); ``backward`` then needs another forward first."""
         torch = _torch()
         eng = self.eng
         if n_steps % self.stride:
@@ -162,9 +163,9 @@ class AdjointRun:
             seg = min(self.K, n_steps - done)
             eng.chunk(seg // self.stride, use_graph=True)
             done += seg
-            if done < n_steps:
+            if done < n_steps and keep:
                 self._ckpt.append(self._save())
-        self.n_steps = n_steps
+        self.n_steps = n_steps if keep else 0
         m = eng.monitors[self.monitor]
         A = (self.wE * m["acc_e"][self.freq]).sum()
         if self.wH is not None:
@@ -175,6 +176,8 @@ class AdjointRun:
 
     def backward(self):
         """dJ/d(1/eps) over the box, as float64 (x, y, z) after forward()."""
+        if not self.n_steps:
+            raise RuntimeError("backward needs a forward run that kept its checkpoints")
         torch = _torch()
         eng = self.eng
         L = _abi.lib()

@@ -167,6 +167,7 @@ class Engine:
         shp = (C.c_int32 * 3)(*self.shape)
         per = (C.c_int32 * 3)(*[int(p) for p in self.periodic])
         self.psi = {}
+        self.psi_alt = {}  # the H slabs that go with the second field buffers of the fused pass
         for d, (lo_n, hi_n, pr) in prof.items():
             if self.periodic[d]:
                 raise ValueError("a periodic axis cannot have a PML")
@@ -189,7 +190,9 @@ class Engine:
                             self.psi[(kind, comp, d, side)] = t
                             p.psi[f][comp][side] = _ptr(t)
                             if kind == "H" and self.double_buffered:
-                                p.psi_alt[comp][side] = _ptr(self._zeros(dims, self.fdt))
+                                alt = self._zeros(dims, self.fdt)
+                                self.psi_alt[(kind, comp, d, side)] = alt
+                                p.psi_alt[comp][side] = _ptr(alt)
             _abi.check(L.lsfdtd_engine_set_pml(self._h, C.byref(p)), "lsfdtd_engine_set_pml")
 
     def _build_group(self, gr, L):
@@ -461,6 +464,17 @@ class Engine:
     def H(self):
         return self._H[int(_abi.lib().lsfdtd_engine_buffer(self._h))]
 
+    def state(self) -> list:
+        """The fields and CPML psi of the current step, in a fixed order (E, H, then psi in ``self.psi``'s
+        order): on the fused path, the buffers of the current parity."""
+        b = int(_abi.lib().lsfdtd_engine_buffer(self._h))
+        return [self._E[b], self._H[b]] + [self.psi_alt[k] if b and k in self.psi_alt else t
+                                           for k, t in self.psi.items()]
+
+    def all_state(self) -> list:
+        """Every state buffer of both parities (for clearing the state)."""
+        return self._E + self._H + list(self.psi.values()) + list(self.psi_alt.values())
+
     @property
     def E_flat(self):
         return self.E.view(-1)
@@ -493,7 +507,10 @@ class Engine:
     def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:
         """Kernel choice and launch shape (before the first graph capture): variant 0 the in-place H and E
         kernels, 2 their four-node vector form, 1 the fused pass (CTA tile rows 8 or 16, x planes per tile,
-        copy ring 4/6/8), 3 the fused pass split into an interior box and a CPML/wall shell kernel."""
+        copy ring 4/6/8), 3 the fused pass split into an interior box and CPML/wall shell kernels, 4 the fused
+        pass with lean CPML terms (the default, with tile rows 8, planes per grid and ring 4; runs the fused pass
+        does not serve take the in-place kernels). ``planes=0`` chooses per grid: 32, or fewer on grids too
+        small for about three waves of CTAs."""
         _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(variant), int(tile_y), int(planes),
                                                        int(stages)), "lsfdtd_engine_set_tuning")
 

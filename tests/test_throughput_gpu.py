@@ -21,7 +21,8 @@ def test_throughput_case_matches_oracle_at_128():
     gpu64 = Engine.from_plan(plan, precision="double")
     gpu32 = Engine.from_plan(plan, precision="single")
     gpu64.set_tuning(1, 8, 40, 4)  # the fused pass, several x segments per tile column
-    assert gpu64.fused and not gpu32.fused  # float32 here: the in-place vector kernels
+    gpu32.set_tuning(0, 8, 32, 4)  # float32 here: the in-place kernels
+    assert gpu64.fused and not gpu32.fused
     for _ in range(3):
         ref.chunk()
         gpu64.chunk(1, use_graph=True)
