@@ -81,8 +81,9 @@ __device__ __forceinline__ long long pml_index(const YeeArgs<F>& g, const SlabIn
 }
 
 // the CPML term along axis d of a value v of field FLD, component c, at psi index q, from psi_prev (the node's
-// psi before this step); psi_out == nullptr: a halo node, computed but not stored
-template <int FLD, typename F>
+// psi before this step); psi_out == nullptr: a halo node, computed but not stored. UNI: cubic cells (the
+// grid's uniform flag, known when the kernel is compiled)
+template <int FLD, bool UNI, typename F>
 __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
                                          int d, int c, long long q, F der, typename real_of<F>::type scale,
                                          F psi_prev, F* psi_out) {
@@ -90,7 +91,7 @@ __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabIn
   const int d1 = (c + 1) % 3;
   R sgn = (d == d1) ? R(1) : R(-1);
   if (FLD == 1) sgn = -sgn;
-  R s = g.uniform ? scale : scale / g.pml[d].div;
+  R s = UNI ? scale : scale / g.pml[d].div;
   s = sgn * s;
   F psi = psi_prev * si.b;
   if (g.pml[d].k[FLD]) v += (s * si.k) * der;
@@ -100,8 +101,9 @@ __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabIn
 }
 
 // FP32: four CTAs of 8 rows (two of 16) per SM, at most 64 registers per thread, which their shared memory
-// allows; FP64 tiles need twice the shared memory and are not constrained
-template <typename F, int TY, int S>
+// allows; FP64 tiles need twice the shared memory and are not constrained. UNI: cubic cells, so the curl
+// differences and CPML coefficients carry no per-axis spacing (one instantiation each way)
+template <typename F, int TY, int S, bool UNI>
 __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 1)
     k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
   using R = typename real_of<F>::type;
@@ -151,14 +153,15 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   __syncthreads();
 
   auto produce = [&](int p) {
-    const int s = (p - xb) % S;
+    const int s = (int)((unsigned)(p - xb) % S);  // p >= xb: unsigned, so the ring slot is a mask or a multiply
     mbar_expect_tx(&bar[s], St::kTx);
     for (int c = 0; c < 3; ++c) tma_load_3d(stE(s, c), &t.mE[c], z0 - 4, y0 - 1, p, &bar[s]);
     for (int c = 0; c < 3; ++c) tma_load_3d(stH(s, c), &t.mH[c], z0 - 4, y0 - 1, p, &bar[s]);
     tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
   };
   auto ready = [&](int p) -> bool {
-    return mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, kWaitBudget);
+    const unsigned r = (unsigned)(p - xb);
+    return mbar_wait_bounded(&bar[r % S], (r / S) & 1, kWaitBudget);
   };
   int issued = xb - 1;
   if (tid == 0) {
@@ -167,7 +170,8 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   issued = xb + S - 2;
 
   auto curl = [&](F av, F bv, int d1, int d2) -> F {
-    return g.uniform ? (av - bv) : (av * g.inv_d[d1] - bv * g.inv_d[d2]);
+    if constexpr (UNI) return av - bv;
+    else return av * g.inv_d[d1] - bv * g.inv_d[d2];
   };
   // region- and CPML-free H at stage offset o (row-major in the 40-wide boxes)
   auto hx_fast = [&](int si, int o) -> F {
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       const long long q = pml_index(g, sl, d, x);
       const F prev = pre ? pre[d] : ro(g.pml[d].psi[1][c][sl.side] + q);
       F* pout = store ? a.psiHo[d][c][sl.side] : nullptr;
-      pml_term<1>(h, g, sl, d, c, q, d == d1 ? av : bv, g.cH, prev, pout);
+      pml_term<1, UNI>(h, g, sl, d, c, q, d == d1 ? av : bv, g.cH, prev, pout);
     }
     if (store) st_global(a.Ho[c] + p, h);
     return h;
@@ -299,7 +303,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     cons = i + 1;
     if (tid == 0) produce(i + S - 1);
     issued = i + S - 1;
-    const int si = (i - xb) % S, sn = (i + 1 - xb) % S;
+    const int si = (int)((unsigned)(i - xb) % S), sn = (int)((unsigned)(i + 1 - xb) % S);
     const long long p = i * s0 + off_jk;
     F hx = zero<F>(), hy = zero<F>(), hz = zero<F>();
     if (fast) {
@@ -332,13 +336,13 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         if (hm >> c & 1u) {
           h = h0 - curl(av[c], bv[c], d1, d2) * g.cH;
           if (c != 0 && xs_h.side >= 0)
-            pml_term<1>(h, g, xs_h, 0, c, qh[0], d1 == 0 ? av[c] : bv[c], g.cH, pre_h[c][0],
+            pml_term<1, UNI>(h, g, xs_h, 0, c, qh[0], d1 == 0 ? av[c] : bv[c], g.cH, pre_h[c][0],
                         st ? a.psiHo[0][c][xs_h.side] : nullptr);
           if (c != 1 && yh.side >= 0)
-            pml_term<1>(h, g, yh, 1, c, qh[1], d1 == 1 ? av[c] : bv[c], g.cH, pre_h[c][1],
+            pml_term<1, UNI>(h, g, yh, 1, c, qh[1], d1 == 1 ? av[c] : bv[c], g.cH, pre_h[c][1],
                         st ? a.psiHo[1][c][yh.side] : nullptr);
           if (c != 2 && zh.side >= 0)
-            pml_term<1>(h, g, zh, 2, c, qh[2], d1 == 2 ? av[c] : bv[c], g.cH, pre_h[c][2],
+            pml_term<1, UNI>(h, g, zh, 2, c, qh[2], d1 == 2 ? av[c] : bv[c], g.cH, pre_h[c][2],
                         st ? a.psiHo[2][c][zh.side] : nullptr);
         }
         if (st) st_global(a.Ho[c] + p, h);
@@ -414,13 +418,13 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
           F ev = e0 + curl(av[c], bv[c], d1, d2) * cbc;
           if (!fast) {
             if (c != 0 && xs_e.side >= 0)
-              pml_term<0>(ev, g, xs_e, 0, c, qe[0], d1 == 0 ? av[c] : bv[c], cbc, pre_e[c][0],
+              pml_term<0, UNI>(ev, g, xs_e, 0, c, qe[0], d1 == 0 ? av[c] : bv[c], cbc, pre_e[c][0],
                           g.pml[0].psi[0][c][xs_e.side]);
             if (c != 1 && ye.side >= 0)
-              pml_term<0>(ev, g, ye, 1, c, qe[1], d1 == 1 ? av[c] : bv[c], cbc, pre_e[c][1],
+              pml_term<0, UNI>(ev, g, ye, 1, c, qe[1], d1 == 1 ? av[c] : bv[c], cbc, pre_e[c][1],
                           g.pml[1].psi[0][c][ye.side]);
             if (c != 2 && ze.side >= 0)
-              pml_term<0>(ev, g, ze, 2, c, qe[2], d1 == 2 ? av[c] : bv[c], cbc, pre_e[c][2],
+              pml_term<0, UNI>(ev, g, ze, 2, c, qe[2], d1 == 2 ? av[c] : bv[c], cbc, pre_e[c][2],
                           g.pml[2].psi[0][c][ze.side]);
           }
           st_global(a.Eo[c] + p, ev);
@@ -431,7 +435,8 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     prev_hz = hz;
   }
   if (tid == 0) {
-    for (int p = cons + 1; p <= issued; ++p) mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, kDrainBudget);
+    for (int p = cons + 1; p <= issued; ++p)
+      mbar_wait_bounded(&bar[(unsigned)(p - xb) % S], ((unsigned)(p - xb) / S) & 1, kDrainBudget);
     if (failed && t.status) atomicExch(t.status, 1);
   }
   __syncthreads();

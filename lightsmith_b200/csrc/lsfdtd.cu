@@ -291,12 +291,21 @@ struct Engine final : lsfdtd_engine {
   int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
       constexpr size_t sm = fused_pml_smem_bytes<F, TY, S>();
-      static bool attr = false;
-      if (!attr) {
-        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        attr = true;
+      static bool attr[2] = {false, false};  // per instantiation (cubic cells or not)
+      const int u = y.uniform ? 1 : 0;
+      if (!attr[u]) {
+        if (u)
+          LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+        else
+          LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+        attr[u] = true;
       }
-      k_fused_pml<F, TY, S><<<grid, dim3(32, TY), sm, s>>>(ta);
+      if (u)
+        k_fused_pml<F, TY, S, true><<<grid, dim3(32, TY), sm, s>>>(ta);
+      else
+        k_fused_pml<F, TY, S, false><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
   }
