@@ -203,7 +203,9 @@ def run_b200(args):
     K, W = args.steps, args.warmup
     R = max(1, min(K, 6))  # chunks of the kernel-timing pass
     _, _, _, _, stride = throughput_band()
-    total_chunks = W + 2 * K + R + 2 + 30  # the tuner's eager chunks too
+    from lightsmith_b200.tune import CANDIDATES
+
+    total_chunks = W + 2 * K + R + 2 + 3 * len(CANDIDATES) + 2  # the tuner's eager chunks (3 per candidate) too
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234)
     inv = 1.0 / (torch.rand(shape, generator=gen, device=dev, dtype=torch.float32) * 11.25 + 1.0)
@@ -215,8 +217,9 @@ def run_b200(args):
         tuned, _ = tune_engine(eng)
         variant = tuned[0]
     else:
+        tuned = (args.variant, args.tile_y, args.planes, args.stages)
         variant = args.variant
-        eng.set_tuning(args.variant, args.tile_y, args.planes, args.stages)
+        eng.set_tuning(*tuned)
     inv_host = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     inv_host.copy_(inv)
     del inv, plan["inv_eps"]
@@ -300,6 +303,8 @@ def run_b200(args):
                           "step": f"one chunk = {stride} FDTD steps + one DFT sample, CUDA graph replay",
                           "l2": "inputs larger than L2 (about 8 GB of state per replica)",
                           "parallelism": f"{world} independent replicas" if world > 1 else "single GPU",
+                          "launch_shape": {"variant": tuned[0], "tile_y": tuned[1],
+                                           "planes": tuned[2] or "per grid", "ring": tuned[3]},
                           "variant": {0: "in-place H and E kernels", 1: "fused single pass",
                                       2: "in-place four-node H and E kernels",
                                       3: "fused single pass over the interior box + CPML/wall shell kernels",

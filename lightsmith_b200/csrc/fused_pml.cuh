@@ -273,8 +273,15 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
 #pragma unroll
       for (int d = 0; d < 3; ++d) pre_h[c][d] = pre_e[c][d] = zero<F>();
     if (!fast) {
-      xs_h = slab_info<1>(g.pml[0], 0, i);
-      xs_e = slab_info<0>(g.pml[0], 0, i);
+      if (i >= a.inner_lo[0] && i < a.inner_hi[0]) {  // a plane outside the x slabs (most lean planes)
+        xs_h.side = xs_e.side = -1;
+        xs_h.st = xs_e.st = 0;
+        xs_h.len = xs_e.len = 1;
+        xs_h.b = xs_h.c = xs_h.k = xs_e.b = xs_e.c = xs_e.k = R(0);
+      } else {
+        xs_h = slab_info<1>(g.pml[0], 0, i);
+        xs_e = slab_info<0>(g.pml[0], 0, i);
+      }
       if (own) {
         const int x[3] = {i, j, k};
 #pragma unroll
