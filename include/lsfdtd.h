@@ -315,9 +315,14 @@ int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch);
 
 /* ---- discrete adjoint ----------------------------------------------------------------------------------
  * No counterpart in lightsmith (its FDTD has no gradient): the transpose of one FDTD step of an engine with
- * real fields and no periodic axis, for d(objective)/d(E curl coefficient) of an objective |A|^2 with A a
- * linear combination of one frequency's DFT samples, A = sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q]. */
+ * real fields, no periodic axis and pure (staircase) dispersive groups, for d(objective)/d(E curl
+ * coefficient) of a real objective J of one monitor's DFT accumulators. The caller gives J's adjoint source
+ * as G = 2 dJ/d(acc) (the Wirtinger derivative: the conjugate of the gradient torch reports for a complex
+ * tensor) per frequency and point; the E samples then receive sum_f Re(G_e[f, p] e^{i w_f t}) at each
+ * sampled step. */
 typedef struct lsfdtd_adjoint lsfdtd_adjoint;
+
+#define LSFDTD_ADJ_MAX_GROUPS 8
 
 typedef struct lsfdtd_adjoint_desc {
   void* Eb;                          /* adjoint fields (3, n0, n1, n2), the engine's precision, zeroed */
@@ -329,13 +334,16 @@ typedef struct lsfdtd_adjoint_desc {
   int32_t hist_slots;
   double* grad;                      /* (3, box): dJ/dcbE_c, accumulated */
   const int64_t* e_idx;              /* the objective's E points (flat indices into the fields) */
-  const double* ge;                  /* (re, im) per E point: conj(A) wE_p */
+  const double* ge;                  /* (re, im) per [frequency][E point]: G_e */
   int64_t n_e;
   const int64_t* h_idx1;             /* its H points (the two H samples averaged) */
   const int64_t* h_idx2;
-  const double* gh;                  /* (re, im) per H point: conj(A) wH_q */
+  const double* gh;                  /* (re, im) per [frequency][H point]: G_h */
   int64_t n_h;
-  double omega;
+  const double* omega;               /* (n_freq) angular frequencies, host memory (copied at create) */
+  int32_t n_freq;
+  int32_t n_groups;                  /* the engine's dispersive groups, in the order they were added */
+  void* group_bar[LSFDTD_ADJ_MAX_GROUPS]; /* adjoint state per group, shaped as its forward state, zeroed */
 } lsfdtd_adjoint_desc;
 
 /* sets the engine's host step count (after the caller rewinds its device counter and fields to a saved step,

@@ -82,7 +82,8 @@ class AdjointDesc(C.Structure):
     # psi_bar: C's [buffer][E, H][axis][component][side], flat: (((b * 2 + f) * 3 + d) * 3 + c) * 2 + side
     _fields_ = [("Eb", vp), ("Hb", vp), ("psi_bar", vp * 72), ("box_lo", i32 * 3), ("box_hi", i32 * 3),
                 ("hist", vp), ("hist_slots", i32), ("grad", vp), ("e_idx", vp), ("ge", vp), ("n_e", i64),
-                ("h_idx1", vp), ("h_idx2", vp), ("gh", vp), ("n_h", i64), ("omega", f64)]
+                ("h_idx1", vp), ("h_idx2", vp), ("gh", vp), ("n_h", i64), ("omega", vp), ("n_freq", i32),
+                ("n_groups", i32), ("group_bar", vp * 8)]
 
 
 SIGNATURES = {

@@ -1,9 +1,11 @@
 """Gradients of an FDTD objective by the discrete adjoint, behind ``torch.autograd``.
 
 lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
-the FDTD path: for a run with real fields, no periodic axis and no dispersive groups (a slab waveguide device,
-say), the objective J = |A|^2 with A = sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q] over one frequency of one
-DFT monitor, and its gradient with respect to 1/eps over a design box of nodes.
+the FDTD path: for a run with real fields, no periodic axis and pure (staircase) dispersive groups at most (a
+slab waveguide device, a metal nanoparticle cluster), a real objective J of one DFT monitor's accumulators,
+and its gradient with respect to 1/eps over a design box of non-dispersive nodes. J is either
+|sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2 at one frequency f, or any torch function of the
+accumulators (a flux spectrum, say): its adjoint source G = 2 dJ/d(acc) comes from torch autograd on J.
 
 ``AdjointRun.forward`` runs the engine (the CUDA kernels: the fused pass where the run allows it, as a plain
 solve would) for ``n_steps`` steps, sampling the monitors as lightsmith's chunks do, and keeps the state (E, H,
@@ -13,7 +15,9 @@ while recording H of the box at every step (``lsfdtd_adjoint_record``), then app
 (``lsfdtd_adjoint_step``, ``csrc/adjoint.cuh``) from the segment's end to its start, accumulating
 dJ/dcbE over the box. Sources only add field-independent terms, so they have no adjoint; the ones allowed
 here (point dipoles, port modes, table-fed TF/SF) keep no state of their own, and their nodes must lie
-outside the box (their coefficients are fixed, not functions of the design).
+outside the box (their coefficients are fixed, not functions of the design). A dispersive group's step (D, E
+of the previous step and the poles' P) is linear too: its transpose (``k_adj_ade``) runs before the E
+update's, and its state is part of each checkpoint.
 
 ``FDTDObjective.apply(inv_eps_box, run)`` is the ``torch.autograd.Function``: forward returns J, backward
 dJ/d(1/eps) of the box (isotropic: the three E components of a node share its 1/eps, so the gradient is
@@ -39,14 +43,18 @@ def _torch():
 
 class AdjointRun:
     """One run's forward and adjoint passes. ``box``: ((x0, x1), (y0, y1), (z0, z1)) node ranges of the design
-    box; ``monitor``/``freq``: the objective's monitor and frequency; ``wE``/``wH``: complex weights of its E
-    and H points (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride)."""
+    box; ``monitor``: the objective's monitor; ``objective``: J(acc_e, acc_h) -> real torch scalar, with acc_e
+    (n_freq, n_e) and acc_h (n_freq, n_h) or None the monitor's accumulators as complex128 tensors; or, when
+    it is None, J = |A|^2 at frequency ``freq`` with ``wE``/``wH`` the complex weights of the E and H points
+    (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride)."""
 
     def __init__(self, plan: dict, box, monitor: int = 0, freq: int = 0, wE=None, wH=None, checkpoint: int = 256,
-                 precision: str | None = None, device="cuda:0"):
+                 precision: str | None = None, device="cuda:0", objective=None):
         torch = _torch()
-        if plan["complex"] or any(plan["periodic"]) or plan["groups"]:
-            raise ValueError("the adjoint serves real fields without periodic axes or dispersive groups")
+        if plan["complex"] or any(plan["periodic"]):
+            raise ValueError("the adjoint serves real fields without periodic axes")
+        if any(g["w"] is not None for g in plan["groups"]):
+            raise ValueError("the adjoint serves pure (staircase) dispersive groups, not mixed (subpixel) ones")
         for s in plan["sources"]:
             if not isinstance(s, (DipoleSource, ModeSource, TableSource)):
                 raise ValueError(f"{type(s).__name__} keeps state of its own; the adjoint does not restore it")
@@ -63,14 +71,25 @@ class AdjointRun:
         bshape = tuple(b - a for a, b in self.box)
         mon = plan["monitors"][monitor]
         self.monitor, self.freq = monitor, freq
-        self.omega = float(mon["omega"][freq])
+        self.omegas = np.asarray(mon["omega"], float)
+        nf = len(self.omegas)
         cd = torch.complex128
-        self.wE = torch.as_tensor(np.zeros(len(mon["e_idx"])) if wE is None else np.asarray(wE), dtype=cd,
-                                  device=self.dev)
-        self.wH = None
-        if mon["h_idx1"] is not None:
-            self.wH = torch.as_tensor(np.zeros(len(mon["h_idx1"])) if wH is None else np.asarray(wH), dtype=cd,
-                                      device=self.dev)
+        self.has_h = mon["h_idx1"] is not None
+        if objective is None:
+            wE_t = torch.as_tensor(np.zeros(len(mon["e_idx"])) if wE is None else np.asarray(wE), dtype=cd,
+                                   device=self.dev)
+            wH_t = None
+            if self.has_h:
+                wH_t = torch.as_tensor(np.zeros(len(mon["h_idx1"])) if wH is None else np.asarray(wH), dtype=cd,
+                                       device=self.dev)
+
+            def objective(acc_e, acc_h, f=freq, wE_t=wE_t, wH_t=wH_t):
+                A = (wE_t * acc_e[f]).sum()
+                if wH_t is not None:
+                    A = A + (wH_t * acc_h[f]).sum()
+                return (A * A.conj()).real
+
+        self.objective = objective
         for s in plan["sources"]:
             nodes = s.idx if isinstance(s, DipoleSource) else (np.concatenate([s.h_idx, s.e_idx]) if isinstance(
                 s, ModeSource) else np.concatenate([s.E.node, s.H.node]))
@@ -80,6 +99,7 @@ class AdjointRun:
             if inside.any():
                 raise ValueError("a source node lies in the design box")
         rdt = eng.rdt
+        self.group_bar = [torch.zeros_like(g["state"]) for g in eng.groups]
         self.Eb = torch.zeros_like(eng.E)
         self.Hb = torch.zeros_like(eng.H)
         self.psi_bar = [[{}, {}], [{}, {}]]  # [buffer][E, H]: {(c, d, side): tensor}
@@ -99,20 +119,27 @@ class AdjointRun:
         d.grad = self.grad.data_ptr()
         i64 = torch.int64
         self.e_idx = torch.as_tensor(mon["e_idx"], dtype=i64, device=self.dev)
-        self.ge = torch.zeros((len(mon["e_idx"]), 2), dtype=torch.float64, device=self.dev)
+        self.ge = torch.zeros((nf, len(mon["e_idx"]), 2), dtype=torch.float64, device=self.dev)
         d.e_idx, d.ge, d.n_e = self.e_idx.data_ptr(), self.ge.data_ptr(), len(mon["e_idx"])
-        if self.wH is not None:
+        if self.has_h:
             self.h1 = torch.as_tensor(mon["h_idx1"], dtype=i64, device=self.dev)
             self.h2 = torch.as_tensor(mon["h_idx2"], dtype=i64, device=self.dev)
-            self.gh = torch.zeros((len(mon["h_idx1"]), 2), dtype=torch.float64, device=self.dev)
+            self.gh = torch.zeros((nf, len(mon["h_idx1"]), 2), dtype=torch.float64, device=self.dev)
             d.h_idx1, d.h_idx2, d.gh, d.n_h = self.h1.data_ptr(), self.h2.data_ptr(), self.gh.data_ptr(), len(
                 mon["h_idx1"])
-        d.omega = self.omega
+        om = (C.c_double * nf)(*self.omegas.tolist())
+        d.omega = C.cast(om, C.c_void_p)
+        d.n_freq = nf
+        if len(self.group_bar) > 8:
+            raise ValueError("the adjoint serves at most 8 dispersive groups")
+        d.n_groups = len(self.group_bar)
+        for gi, t in enumerate(self.group_bar):
+            d.group_bar[gi] = t.data_ptr()
         self._desc = d
         h = C.c_void_p()
         _abi.check(_abi.lib().lsfdtd_adjoint_create(eng._h, C.byref(d), C.byref(h)), "lsfdtd_adjoint_create")
         self._h = h
-        self.A = None
+        self.acc = None
         self.n_steps = 0
         self._ckpt = []
 
@@ -167,12 +194,13 @@ class AdjointRun:
                 self._ckpt.append(self._save())
         self.n_steps = n_steps if keep else 0
         m = eng.monitors[self.monitor]
-        A = (self.wE * m["acc_e"][self.freq]).sum()
-        if self.wH is not None:
-            A = A + (self.wH * m["acc_h"][self.freq]).sum()
-        self.A = A
         torch.cuda.synchronize(self.dev)
-        return float(abs(A.item()) ** 2), complex(A.item())
+        acc_e = m["acc_e"].to(torch.complex128).clone()
+        acc_h = m["acc_h"].to(torch.complex128).clone() if self.has_h else None
+        self.acc = (acc_e, acc_h)
+        with torch.no_grad():
+            J = self.objective(acc_e, acc_h)
+        return float(J), (acc_e, acc_h)
 
     def backward(self):
         """dJ/d(1/eps) over the box, as float64 (x, y, z) after forward()."""
@@ -181,12 +209,21 @@ class AdjointRun:
         torch = _torch()
         eng = self.eng
         L = _abi.lib()
-        cA = torch.conj(self.A)
-        self.ge.copy_(torch.view_as_real(2 * cA * self.wE))
-        if self.wH is not None:
-            self.gh.copy_(torch.view_as_real(2 * cA * self.wH))
+        # the adjoint source: G = 2 dJ/d(acc) = conj of the gradient torch gives for a complex tensor
+        acc_e = self.acc[0].detach().clone().requires_grad_(True)
+        acc_h = self.acc[1].detach().clone().requires_grad_(True) if self.has_h else None
+        with torch.enable_grad():
+            J = self.objective(acc_e, acc_h)
+            grads = torch.autograd.grad(J, [acc_e] + ([acc_h] if acc_h is not None else []), allow_unused=True)
+        g_e = grads[0] if grads[0] is not None else torch.zeros_like(acc_e)
+        self.ge.copy_(torch.view_as_real(g_e.conj().resolve_conj()))
+        if self.has_h:
+            g_h = grads[1] if grads[1] is not None else torch.zeros_like(acc_h)
+            self.gh.copy_(torch.view_as_real(g_h.conj().resolve_conj()))
         self.Eb.zero_()
         self.Hb.zero_()
+        for t in self.group_bar:
+            t.zero_()
         for b in range(2):
             for f in range(2):
                 for t in self.psi_bar[b][f].values():

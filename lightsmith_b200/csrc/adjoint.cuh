@@ -22,6 +22,7 @@
 // box of nodes away from the CPML slabs, from H^{n+1/2} of the box (with its low halo) recomputed forward.
 #pragma once
 
+#include "ade.cuh"
 #include "common.cuh"
 #include "yee.cuh"
 
@@ -316,26 +317,78 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
   A.Eb[2][p] = eb2 + acc[2];
 }
 
-// the objective's adjoint source at one sample (after n steps): Ebar[e_idx] += Re(ge e^{i w t_e}),
-// Hbar[h1], Hbar[h2] += Re(gh e^{i w t_h}) / 2 each (the monitor's H sample is the mean of the two)
+constexpr int kAdjMaxFreq = 128;
+
+// the objective's frequencies, passed by value
+struct AdjFreqs {
+  double omega[kAdjMaxFreq];
+  int nf;
+};
+
+// the objective's adjoint source at one sample (after n steps): Ebar[e_idx[p]] += sum_f Re(G_e[f][p]
+// e^{i w_f t_e}); Hbar[h1[q]], Hbar[h2[q]] += sum_f Re(G_h[f][q] e^{i w_f t_h}) / 2 each (the monitor's H
+// sample is the mean of the two)
 template <typename R>
 __global__ void k_adj_inject(R* Eb, R* Hb, const long long* e_idx, const double* ge, long long ne,
-                             const long long* h1, const long long* h2, const double* gh, long long nh, double omega,
-                             double dt, long long n) {
+                             const long long* h1, const long long* h2, const double* gh, long long nh,
+                             const __grid_constant__ AdjFreqs fr, double dt, long long n) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double te = (double)n * dt, th = te - 0.5 * dt;
   if (t < ne) {
-    double sn, cs;
-    sincos(omega * te, &sn, &cs);
-    atomicAdd(Eb + e_idx[t], (R)(ge[2 * t] * cs - ge[2 * t + 1] * sn));
+    double v = 0.0;
+    for (int f = 0; f < fr.nf; ++f) {
+      double sn, cs;
+      sincos(fr.omega[f] * te, &sn, &cs);
+      const double* gp = ge + 2 * ((long long)f * ne + t);
+      v += gp[0] * cs - gp[1] * sn;
+    }
+    atomicAdd(Eb + e_idx[t], (R)v);
   } else if (t < ne + nh) {
     const long long q = t - ne;
-    double sn, cs;
-    sincos(omega * th, &sn, &cs);
-    const R v = (R)(0.5 * (gh[2 * q] * cs - gh[2 * q + 1] * sn));
-    atomicAdd(Hb + h1[q], v);
-    atomicAdd(Hb + h2[q], v);
+    double v = 0.0;
+    for (int f = 0; f < fr.nf; ++f) {
+      double sn, cs;
+      sincos(fr.omega[f] * th, &sn, &cs);
+      const double* gp = gh + 2 * ((long long)f * nh + q);
+      v += gp[0] * cs - gp[1] * sn;
+    }
+    const R h = (R)(0.5 * v);
+    atomicAdd(Hb + h1[q], h);
+    atomicAdd(Hb + h2[q], h);
   }
+}
+
+// the transpose of a pure dispersive group's step (k_ade) at each of its nodes. Forward, with e the node's E
+// after the curl update: D' = D + (e - E_prev); P_k' = c1 P_k + c2 Pp_k + c3 E_prev; Pp_k' = P_k;
+// e' = (D' - sum_k P_k') / eps_inf; E' = E_prev' = e'. Backward, from the adjoints of the outputs (Ebar at the
+// node, and the adjoint state Dbar, Epbar, Pbar_k, Ppbar_k of the step after): g = Ebar + Epbar; Dbar +=
+// g / eps_inf; Phat_k = Pbar_k - g / eps_inf; Epbar = -Dbar + sum_k c3 Phat_k; Pbar_k = c1 Phat_k + Ppbar_k;
+// Ppbar_k = c2 Phat_k; and the adjoint of e (the new Ebar at the node) is Dbar. The state's layout is k_ade's.
+template <typename R>
+__global__ void k_adj_ade(const AdeArgs<R> g, R* Eb, R* bar) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.n) return;
+  const long long n = g.n;
+  R* Db = bar;
+  R* Epb = bar + n;
+  R* Pb = bar + 2 * n;
+  const long long node = g.idx[t];
+  const R inv = g.inv_inf[0];
+  const R gs = Eb[node] + Epb[t];
+  const R dbar = Db[t] + inv * gs;
+  R epb = -dbar;
+  for (int k = 0; k < g.n_poles[0]; ++k) {
+    R* pk = Pb + (2 * k) * n;
+    R* pp = Pb + (2 * k + 1) * n;
+    const R ph = pk[t] - inv * gs;
+    epb += g.c3[0][k] * ph;
+    const R npk = g.c1[0][k] * ph + pp[t];
+    pp[t] = g.c2[0][k] * ph;
+    pk[t] = npk;
+  }
+  Db[t] = dbar;
+  Epb[t] = epb;
+  Eb[node] = dbar;
 }
 
 // H over the gradient box and its low halo: dst[c][x - lo + 1][y - lo + 1][z - lo + 1]

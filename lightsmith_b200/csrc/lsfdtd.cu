@@ -147,6 +147,9 @@ struct lsfdtd_engine {
   virtual int bloch_desc(void* out, size_t bytes, int64_t last) = 0;
   // the coefficients of the adjoint (YeeArgs of a real engine) and the current H array
   virtual int adjoint_args(void* yee, size_t bytes, void** H) = 0;
+  // the dispersive groups (AdeArgs of a real engine), for the adjoint
+  virtual int adjoint_n_groups() const = 0;
+  virtual int adjoint_group(int gi, void* out, size_t bytes) = 0;
 };
 
 namespace {
@@ -513,11 +516,21 @@ struct Engine final : lsfdtd_engine {
 
   size_t bloch_desc_bytes() const override { return kComplex ? sizeof(BlochRun<F>) : 0; }
 
+  int adjoint_n_groups() const override { return (int)groups.size(); }
+  int adjoint_group(int gi, void* out, size_t bytes) override {
+    if (gi < 0 || gi >= (int)groups.size() || bytes != sizeof(AdeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: group");
+    AdeArgs<F> ga = groups[gi];
+    ga.E = Eflat();
+    std::memcpy(out, &ga, sizeof ga);
+    return LSFDTD_OK;
+  }
+
   int adjoint_args(void* yee, size_t bytes, void** H) override {
     if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
     if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
-    if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "adjoint: dispersive groups have no adjoint here");
+    for (auto& gr : groups)
+      if (gr.mixed) return fail(LSFDTD_EUNSUPPORTED, "adjoint: mixed (subpixel) dispersive groups have no adjoint");
     if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
     const YeeArgs<F> a = current_args();
     std::memcpy(yee, &a, sizeof a);
@@ -1161,6 +1174,8 @@ struct lsfdtd_adjoint {
   std::vector<unsigned char> yee;  // YeeArgs of the engine's precision
   int buf = 0;                     // psibar buffer holding the current (old) values
   size_t slot_elems = 0;
+  AdjFreqs freqs{};                // the objective's frequencies
+  std::vector<std::vector<unsigned char>> groups;  // AdeArgs of the engine's dispersive groups
 };
 
 namespace {
@@ -1231,7 +1246,14 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
     k_adj_inject<R><<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(
         A.Eb[0], A.Hb[0], reinterpret_cast<const long long*>(a->d.e_idx), a->d.ge, a->d.n_e,
         reinterpret_cast<const long long*>(a->d.h_idx1), reinterpret_cast<const long long*>(a->d.h_idx2), a->d.gh,
-        a->d.n_h, a->d.omega, desc.dt, n + 1);
+        a->d.n_h, a->freqs, desc.dt, n + 1);
+    LS_LAUNCHED();
+  }
+  // the dispersive groups ran after the E curl update: their transposes come first
+  for (size_t gi = 0; gi < a->groups.size(); ++gi) {
+    const auto& ga = *reinterpret_cast<const AdeArgs<R>*>(a->groups[gi].data());
+    if (ga.n <= 0) continue;
+    k_adj_ade<R><<<cdiv(ga.n, 256), 256, 0, s>>>(ga, A.Eb[0], static_cast<R*>(a->d.group_bar[gi]));
     LS_LAUNCHED();
   }
   const dim3 grid(cdiv(A.y.n[2], 32), cdiv(A.y.n[1], 8), A.y.n[0]);
@@ -1621,6 +1643,23 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
   LS_TRY(eng->adjoint_args(a->yee.data(), a->yee.size(), &H));
   if ((d->n_e > 0 && (!d->e_idx || !d->ge)) || (d->n_h > 0 && (!d->h_idx1 || !d->h_idx2 || !d->gh)))
     return fail(LSFDTD_EINVAL, "adjoint: objective arrays missing");
+  if (d->n_e + d->n_h > 0) {
+    if (!d->omega || d->n_freq < 1 || d->n_freq > kAdjMaxFreq)
+      return fail(LSFDTD_EINVAL, "adjoint: 1 to " + std::to_string(kAdjMaxFreq) + " objective frequencies");
+    for (int f = 0; f < d->n_freq; ++f) a->freqs.omega[f] = d->omega[f];
+    a->freqs.nf = d->n_freq;
+  }
+  a->d.omega = nullptr;  // copied: the caller's array need not outlive this call
+  if (d->n_groups != eng->adjoint_n_groups() || d->n_groups > LSFDTD_ADJ_MAX_GROUPS)
+    return fail(LSFDTD_EINVAL, "adjoint: n_groups must equal the engine's dispersive groups");
+  for (int gi = 0; gi < d->n_groups; ++gi) {
+    std::vector<unsigned char> ga(a->precision == LSFDTD_F32 ? sizeof(AdeArgs<float>) : sizeof(AdeArgs<double>));
+    LS_TRY(eng->adjoint_group(gi, ga.data(), ga.size()));
+    const long long gn = a->precision == LSFDTD_F32 ? reinterpret_cast<const AdeArgs<float>*>(ga.data())->n
+                                                    : reinterpret_cast<const AdeArgs<double>*>(ga.data())->n;
+    if (gn > 0 && !d->group_bar[gi]) return fail(LSFDTD_EINVAL, "adjoint: a group's adjoint state is missing");
+    a->groups.push_back(std::move(ga));
+  }
   const int32_t* n = eng->desc.shape;
   for (int ax = 0; ax < 3; ++ax)
     if (d->box_lo[ax] < 1 || d->box_hi[ax] > n[ax] - 1 || d->box_hi[ax] <= d->box_lo[ax])

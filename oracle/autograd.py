@@ -2,9 +2,10 @@
 
 The checker of ``lightsmith_b200.adjoint``: the same update equations as ``oracle/engine.py`` (lightsmith's
 ``engine.py:613-663`` curl updates over the stepped regions, ``engine.py:344-418`` CPML terms in their order,
-``emission.py:130-140`` point-current corrections after the E update), for real fields, no periodic axes, no
-dispersive groups and point-dipole sources, written out of place so that autograd can differentiate the DFT
-objective |sum_p wE_p acc_e[p] + sum_q wH_q acc_h[q]|^2 with respect to 1/eps over a box of nodes.
+``emission.py:130-140`` point-current corrections after the E update, ``engine.py:769-775`` pure D-form ADE
+groups after the sources), for real fields, no periodic axes and point-dipole sources, written out of place so
+that autograd can differentiate a DFT objective (|sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2, or any
+function of the accumulators) with respect to 1/eps over a box of nodes.
 """
 
 from __future__ import annotations
@@ -12,8 +13,9 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from lightsmith_b200.plan import DipoleSource, cpml_profiles, cpml_terms, e_range, h_range
+from lightsmith_b200.plan import DipoleSource, cpml_profiles, cpml_terms, e_range, h_range, pole_coefficients
 
+from .engine import _P as _Pole
 from .engine import _Spec
 
 
@@ -24,8 +26,10 @@ def _put(F, region, delta):
     return F + Z
 
 
-def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_steps: int):
-    """J (float64 tensor) after n_steps steps from rest, differentiable in inv_eps_box (the box's 1/eps)."""
+def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_steps: int, J=None):
+    """J (float64 tensor) after n_steps steps from rest, differentiable in inv_eps_box (the box's 1/eps). J:
+    a function of the monitor's accumulators (acc_e (n_freq, n_e), acc_h or None, complex128); None: the
+    |A|^2 of weights wE, wH at frequency index freq."""
     dt = torch.float64
     shape = tuple(plan["shape"])
     spacing = tuple(plan["spacing"])
@@ -106,14 +110,25 @@ def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_s
     if len(dips) != len(plan["sources"]):
         raise ValueError("point dipoles only")
     mon = plan["monitors"][monitor]
-    omega = float(mon["omega"][freq])
-    wE = torch.as_tensor(np.asarray(wE), dtype=torch.complex128)
-    wH = None if wH is None else torch.as_tensor(np.asarray(wH), dtype=torch.complex128)
+    omegas = torch.as_tensor(np.asarray(mon["omega"], float))
     e_idx = torch.as_tensor(mon["e_idx"])
     h1 = None if mon["h_idx1"] is None else torch.as_tensor(mon["h_idx1"])
     h2 = None if mon["h_idx2"] is None else torch.as_tensor(mon["h_idx2"])
-    A = torch.zeros((), dtype=torch.complex128)
+    acc_e = torch.zeros((len(omegas), len(e_idx)), dtype=torch.complex128)
+    acc_h = None if h1 is None else torch.zeros((len(omegas), len(h1)), dtype=torch.complex128)
     cells = int(np.prod(shape))
+
+    # pure dispersive groups (oracle/engine.py:_Group): D, E_prev and (P, P') per pole, out of place
+    groups = []
+    for g in plan["groups"]:
+        if g["w"] is not None:
+            raise ValueError("pure dispersive groups only")
+        (m,) = g["media"]
+        idx = torch.as_tensor(np.asarray(g["idx"], np.int64))
+        z = torch.zeros(len(idx), dtype=dt)
+        coef = [pole_coefficients(_Pole(*p), step_dt) for p in m["poles"]]
+        groups.append({"idx": idx, "D": z, "Ep": z, "P": [(z, z) for _ in coef], "coef": coef,
+                       "inv_inf": 1.0 / m["eps_inf"]})
     for n in range(n_steps):
         H = [_put(H[c], sl(RH[c]), -curl(E, c, sl(RH[c]), True) * cH) for c in range(3)]
         H = pml(H, E, "H")
@@ -125,12 +140,34 @@ def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_s
                                                    torch.as_tensor(s.coef * s.wave[n], dtype=dt))
             flat = flat - upd
             E = [flat[c * cells:(c + 1) * cells].reshape(shape) for c in range(3)]
+        if groups:  # D += E - E_prev; P <- c1 P + c2 P' + c3 E_prev; E = (D - sum P) / eps_inf; E_prev = E
+            flat = torch.cat([e.reshape(-1) for e in E])
+            for g in groups:
+                e_now = flat[g["idx"]]
+                g["D"] = g["D"] + (e_now - g["Ep"])
+                tot, newP = None, []
+                for (P, Pp), (c1, c2, c3) in zip(g["P"], g["coef"]):
+                    nw = c1 * P + c2 * Pp + c3 * g["Ep"]
+                    newP.append((nw, P))
+                    tot = nw if tot is None else tot + nw
+                g["P"] = newP
+                e_new = (g["D"] - tot) * g["inv_inf"]
+                g["Ep"] = e_new
+                flat = flat.index_put((g["idx"],), e_new)
+            E = [flat[c * cells:(c + 1) * cells].reshape(shape) for c in range(3)]
         if (n + 1) % stride == 0:
             t_e = (n + 1) * step_dt
             flat_e = torch.cat([e.reshape(-1) for e in E])
-            A = A + np.exp(1j * omega * t_e) * (wE * flat_e[e_idx].to(torch.complex128)).sum()
-            if wH is not None:
+            ph_e = torch.exp(1j * omegas * t_e)[:, None]
+            acc_e = acc_e + ph_e * flat_e[e_idx].to(torch.complex128)[None, :]
+            if acc_h is not None:
                 flat_h = torch.cat([h.reshape(-1) for h in H])
                 havg = ((flat_h[h1] + flat_h[h2]) * 0.5).to(torch.complex128)
-                A = A + np.exp(1j * omega * (t_e - 0.5 * step_dt)) * (wH * havg).sum()
+                acc_h = acc_h + torch.exp(1j * omegas * (t_e - 0.5 * step_dt))[:, None] * havg[None, :]
+    if J is not None:
+        return J(acc_e, acc_h)
+    wE = torch.as_tensor(np.asarray(wE), dtype=torch.complex128)
+    A = (wE * acc_e[freq]).sum()
+    if wH is not None and acc_h is not None:
+        A = A + (torch.as_tensor(np.asarray(wH), dtype=torch.complex128) * acc_h[freq]).sum()
     return (A * A.conj()).real
