@@ -49,11 +49,14 @@ def _args():
     ap.add_argument("--tile-y", type=int, default=8, help="fused pass: tile rows along y")
     ap.add_argument("--planes", type=int, default=0, help="fused pass: x planes per CTA (0: chosen per grid)")
     ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring")
-    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint"],
+    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint", "clusters"],
                     help="sweep: the batched oblique-incidence sweep (96 Bloch-periodic runs) against the same "
-                         "runs one after another")
+                         "runs one after another; adjoint: the slab device's gradient against its forward run; "
+                         "clusters: forward + gradient over dispersive sphere clusters, with FP64 errors")
     ap.add_argument("--runs", type=int, default=96, help="sweep: number of runs")
     ap.add_argument("--sweep-steps", type=int, default=3000, help="sweep: FDTD steps per run")
+    ap.add_argument("--instances", type=int, default=24, help="clusters: number of instances")
+    ap.add_argument("--cluster-steps", type=int, default=2000, help="clusters: FDTD steps per instance")
     return ap.parse_args()
 
 
@@ -462,6 +465,76 @@ def run_adjoint(args):
     print(json.dumps(out), flush=True)
 
 
+def run_clusters(args):
+    """Forward + adjoint over dispersive clusters: ``--instances`` seeded instances of 3-12 silver spheres
+    (Drude + 2 Lorentz poles, radii U(10, 40) nm, 2 nm grid, 96^3-256^3 cells sized to the cluster), each
+    excited by a point dipole just outside a 60 nm shell, objective the power out of a closed box at 24
+    wavelengths in 350-700 nm, gradient with respect to the background index of the shell's cells. Each
+    instance runs forward (checkpoints every 256 steps) and backward in FP32 on the device clock; the same
+    in FP64 gives the errors of each spectrum and each gradient. The instances run one after another (each
+    is a whole-GPU grid)."""
+    import numpy as np
+    import torch
+
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import cluster_instance
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    clocks = Clocks(_gpu_uuid(torch, dev))
+    rows, t_f_tot, t_g_tot, cell_steps = [], 0.0, 0.0, 0
+    for seed in range(args.instances):
+        out = {}
+        for prec in ("single", "double"):
+            plan, info = cluster_instance(seed, n_steps=args.cluster_steps, single=prec == "single")
+            run = AdjointRun(plan, info["box"], objective=info["objective"], checkpoint=256, precision=prec)
+            if prec == "single":  # untimed warm-up of this instance's kernels and graphs
+                run.forward(2 * plan["stride"])
+                run.backward()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize(dev)
+            ev[0].record()
+            J, (acc_e, acc_h) = run.forward(info["n_steps"])
+            ev[1].record()
+            g = run.backward()
+            ev[2].record()
+            torch.cuda.synchronize(dev)
+            s = torch.as_tensor(info["sign"], device=acc_e.device)
+            spectrum = (0.5 * (acc_e * acc_h.conj() * s).real.sum(dim=1)).cpu().numpy()
+            n_bg = info["n_bg"]
+            shell = torch.as_tensor(info["shell"], device=g.device)
+            g_n = (g * (-2.0 / n_bg ** 3))[shell].cpu().numpy()  # dJ/dn per shell cell (1/eps = 1/n^2)
+            out[prec] = (ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), spectrum, g_n, J)
+            run.close()
+            del run, g, acc_e, acc_h
+            torch.cuda.empty_cache()
+        tf, tg, s32, g32, J32 = out["single"]
+        _, _, s64, g64, J64 = out["double"]
+        cells = info["cells"]
+        t_f_tot += tf
+        t_g_tot += tg
+        cell_steps += cells * info["n_steps"]
+        rows.append({"seed": seed, "grid": plan["shape"][0], "spheres": len(info["spheres"]),
+                     "shell_cells": int(info["shell"].sum()), "forward_ms": round(tf, 2), "gradient_ms": round(tg, 2),
+                     "spectrum_err_vs_fp64": float(np.abs(s32 - s64).max() / max(np.abs(s64).max(), 1e-300)),
+                     "gradient_err_vs_fp64": float(np.abs(g32 - g64).max() / max(np.abs(g64).max(), 1e-300))})
+    clk = clocks.stop()
+    value = cell_steps / ((t_f_tot + t_g_tot) / 1e3) / 1e9
+    out = {"metric": "FDTD forward + adjoint gradient over dispersive clusters, Gcell-updates/s of the forward "
+                     "steps per second of forward + gradient", "value": value, "unit": UNIT, "n_gpus": 1,
+           "steps": args.cluster_steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"{args.instances} seeded clusters of 3-12 silver spheres (Drude + 2 Lorentz, "
+                                  "radii U(10, 40) nm) in n = 1.33, 2 nm grid, CPML 12, dipole outside a 60 nm "
+                                  "shell, power out of a closed box at 24 wavelengths in 350-700 nm, gradient in "
+                                  "the shell's background index", "checkpoint_steps": 256},
+           "forward_ms_total": t_f_tot, "gradient_ms_total": t_g_tot, "gradient_over_forward": t_g_tot / t_f_tot,
+           "max_spectrum_err_vs_fp64": max(r["spectrum_err_vs_fp64"] for r in rows),
+           "max_gradient_err_vs_fp64": max(r["gradient_err_vs_fp64"] for r in rows),
+           "instances": rows, "clocks": clk}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = _args()
     if args.impl == "reference":
@@ -470,6 +543,8 @@ def main():
         run_sweep(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "clusters":
+        run_clusters(args)
     else:
         run_b200(args)
 

@@ -117,6 +117,7 @@ struct lsfdtd_engine {
   int tile_y = 8, planes = 0, stages = 4;  // planes 0: chosen per grid (Engine::auto_planes)
   int sm_count = 0;
   int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
+  bool tuned = false;   // a kernel choice was set explicitly (lsfdtd_engine_set_tuning)
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
@@ -268,8 +269,13 @@ struct Engine final : lsfdtd_engine {
         for (int sd = 0; sd < 2; ++sd)
           if (y.pml[d].len[1][c][sd] > 0 && !psiH[1][d][c][sd]) return 0;
     }
-    fused = 1;
     tma_ok = use_tma && make_maps() == LSFDTD_OK;
+    // rows the copies cannot take (not a multiple of 16 bytes): the cp.async ring of the fused pass runs
+    // slower than the in-place kernels (measured on B200, CPML 12: 607 against 296 us per step at 214^3, 226
+    // against 74 us at 129^3), so the default steps in place there; an explicit kernel choice or copy engine
+    // keeps the fused pass
+    if (use_tma && !tma_ok && !tuned) return 0;
+    fused = 1;
     return 1;
   }
 
@@ -1491,6 +1497,7 @@ int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t ti
                                "CPML terms); for 1, 3 and 4 CTA tile rows 8 or 16, ring 4, 6 or 8, planes >= 1 (0: per grid)");
   if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "tuning must be set before the first graph capture");
   eng->variant = variant;
+  eng->tuned = true;
   eng->tile_y = tile_y;
   eng->planes = planes;
   eng->stages = stages;

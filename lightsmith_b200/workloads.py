@@ -14,7 +14,8 @@ import math
 
 import numpy as np
 
-from .plan import ColumnSource, DFTMonitor, DipoleSource, PMLSpec, flat_index, make_plan
+from .plan import (ColumnSource, DFTMonitor, DipoleSource, DispersiveGroup, Medium, PMLSpec, Pole, flat_index,
+                   make_plan)
 
 
 def point_dipole(shape, origin, dx: float, dt: float, pos, pdir, inv_eps_at, omega_c: float, omega_half: float,
@@ -299,3 +300,135 @@ def slab_device_plan(shape=(200, 200, 120), dx: float = 20.0, pml: int = 12, des
     wE = amp * dx * dx
     info = {"rho": rho, "eps_clad": n_clad ** 2, "eps_core": n_core ** 2, "n_steps": n_steps}
     return plan, box, wE, info
+
+
+# --- dispersive clusters (forward + adjoint over many instances) ------------------------------------------
+
+EV_NM = 197.3269804  # hbar c in eV nm: photon energies to angular frequencies in rad/nm (c = 1)
+
+
+def drude_lorentz(eps_inf: float, wp_ev: float, gamma_ev: float, lorentz) -> Medium:
+    """A Drude pole and Lorentz poles (d_eps, omega0 eV, width eV) in engine units, as lightsmith's media
+    converts them (``media.py:68-75``): Drude sigma = wp^2, omega0 = 0; Lorentz sigma = d_eps omega0^2."""
+    poles = [Pole((wp_ev / EV_NM) ** 2, 0.0, gamma_ev / EV_NM)]
+    poles += [Pole(de * (w0 / EV_NM) ** 2, w0 / EV_NM, g / EV_NM) for de, w0, g in lorentz]
+    return Medium(eps_inf, tuple(poles))
+
+
+# silver of the cluster workload: eps_inf 3.7, wp 9.2 eV, gamma 0.02 eV, and the two Lorentz poles of the
+# sphere benchmark (1.3 at 2.6 eV, width 0.6 eV; 1.5 at 3.7 eV, width 1.0 eV)
+SILVER = drude_lorentz(3.7, 9.2, 0.02, [(1.3, 2.6, 0.6), (1.5, 3.7, 1.0)])
+
+
+def box_flux_monitor(shape, lo, hi, omega):
+    """The six faces of the node box [lo, hi] as one monitor: per face normal to axis a at index k, the two
+    tangential E components on the face's nodes, each with the H component it pairs with averaged over planes
+    k - 1 and k along a (plane_monitor's layout per face). Returns (monitor, s): the power out of the box is
+    0.5 Re sum_p s_p acc_e[f, p] conj(acc_h[f, p]) (s: +-1 by pairing and outward normal)."""
+    e, h1, h2, sg = [], [], [], []
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        rng_b = np.arange(lo[b], hi[b] + 1)
+        rng_c = np.arange(lo[c], hi[c] + 1)
+        B, Cc = (v.ravel() for v in np.meshgrid(rng_b, rng_c, indexing="ij"))
+        for side, k in ((-1, lo[a]), (1, hi[a])):
+            def at(comp, kk):
+                x = [None] * 3
+                x[a], x[b], x[c] = np.full(B.size, kk), B, Cc
+                return flat_index(comp, x[0], x[1], x[2], shape)
+            # flux_a = E_b H_c* - E_c H_b*
+            e += [at(b, k), at(c, k)]
+            h1 += [at(c, k - 1), at(b, k - 1)]
+            h2 += [at(c, k), at(b, k)]
+            sg += [np.full(B.size, float(side)), np.full(B.size, -float(side))]
+    mon = DFTMonitor(np.asarray(omega, float), np.concatenate(e).astype(np.int64),
+                     np.concatenate(h1).astype(np.int64), np.concatenate(h2).astype(np.int64), energy=0)
+    return mon, np.concatenate(sg)
+
+
+def cluster_instance(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int = 24, lam=(350.0, 700.0),
+                     n_steps: int = 2000, shell_nm: float = 60.0, pml: int = 12, single: bool = True,
+                     stride: int = 16, n_min: int = 96, n_max: int = 256):
+    """One instance of the dispersive-cluster workload: 3-12 silver spheres (radii U(10, 40) nm) at random
+    non-overlapping positions in a background of index n_bg on a cubic grid of dx, sized to the cluster
+    (n_min^3 .. n_max^3 cells); node-centred staircase spheres (every E component of a node whose centre lies
+    in a sphere belongs to one pure D-form group, with 1/eps = 1 there); a point dipole just outside the
+    60 nm shell around the spheres; the power out of a closed box around the shell at n_freq wavelengths in
+    lam as the objective. Returns (plan, info) with info: box (the shell's bounding box of nodes, the
+    gradient's design box), shell (a bool mask over that box: background nodes within shell_nm of a sphere),
+    objective (J of the accumulators), the spheres and the step count."""
+    rng = np.random.default_rng(seed)
+    n_sph = int(rng.integers(3, 13))
+    radii = rng.uniform(10.0, 40.0, n_sph)
+    side = 2.2 * float(np.sum(radii ** 3)) ** (1 / 3) + 2 * radii.max()
+    centres = []
+    for _ in range(200):
+        centres = []
+        for r in radii:
+            for _try in range(2000):
+                c = rng.uniform(-side / 2 + r, side / 2 - r, 3)
+                if all(np.linalg.norm(c - c2) >= r + r2 + 2 * dx for c2, r2 in centres):
+                    centres.append((c, r))
+                    break
+            else:
+                break
+        if len(centres) == n_sph:
+            break
+        side *= 1.1
+    lo_nm = np.min([c - r for c, r in centres], axis=0) - shell_nm
+    hi_nm = np.max([c + r for c, r in centres], axis=0) + shell_nm
+    margin = 14  # cells: dipole and flux box outside the shell, then the CPML
+    n = int(np.clip(math.ceil(float(np.max(hi_nm - lo_nm)) / dx) + 2 * (margin + pml + 2), n_min, n_max))
+    n = min(n_max, -(-n // 4) * 4)  # rows of a multiple of 16 bytes: the fused pass's tensor copies apply
+    shape = (n, n, n)
+    mid = 0.5 * (lo_nm + hi_nm)
+    origin = mid - (n // 2) * dx  # node i sits at origin + i dx
+    pos = origin[:, None] + dx * np.arange(n)[None, :]
+    X, Y, Z = np.meshgrid(pos[0], pos[1], pos[2], indexing="ij")
+    inside = np.zeros(shape, bool)
+    dist = np.full(shape, np.inf)
+    for c, r in centres:
+        d = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r
+        inside |= d < 0
+        dist = np.minimum(dist, d)
+    inv_eps = np.full(shape, 1.0 / n_bg ** 2)
+    inv_eps[inside] = 1.0
+    cells = n ** 3
+    node = np.flatnonzero(inside.reshape(-1))
+    idx = np.concatenate([cc * cells + node for cc in range(3)]).astype(np.int64)
+    group = DispersiveGroup(idx=idx, media=[SILVER], frac=np.ones((1, len(idx))), w=None)
+    blo = np.maximum(np.floor((lo_nm - origin) / dx).astype(int), pml + 3)
+    bhi = np.minimum(np.ceil((hi_nm - origin) / dx).astype(int) + 1, n - pml - 3)
+    box = tuple((int(a), int(b)) for a, b in zip(blo, bhi))
+    bsl = tuple(slice(a, b) for a, b in box)
+    shell = (~inside[bsl]) & (dist[bsl] <= shell_nm)
+    dt = 0.99 * dx / math.sqrt(3)
+    wl = np.linspace(lam[0], lam[1], n_freq)
+    om = 2 * np.pi / wl  # vacuum wavelengths (c = 1)
+    omega_c = 0.5 * (om.min() + om.max())
+    dip_node = np.array([bhi[0] + 3, (blo[1] + bhi[1]) // 2, (blo[2] + bhi[2]) // 2])
+    pdir = rng.normal(size=3)
+    pdir /= np.linalg.norm(pdir)
+
+    def at(flat):
+        rest = np.asarray(flat) % cells
+        return inv_eps.reshape(-1)[rest]
+
+    dip = point_dipole(shape, np.zeros(3), dx, dt, (dip_node + 0.3) * dx, tuple(pdir), at, omega_c, 0.6 * omega_c,
+                       n_steps + 8)
+    flo = [int(v) - 6 for v in blo]
+    fhi = [int(v) + 6 for v in bhi]
+    mon, sgn = box_flux_monitor(shape, flo, fhi, om)
+    spec = PMLSpec(cells=((pml, pml),) * 3, alpha_max=0.05 * omega_c, eps_ref=n_bg ** 2)
+    plan = make_plan(shape=shape, dx=dx, dt=dt, single=single, inv_eps=inv_eps, groups=[group], pml=spec,
+                     sources=[dip], monitors=[mon], dft_stride=stride)
+
+    def objective(acc_e, acc_h, sgn=sgn):
+        import torch
+
+        s = torch.as_tensor(sgn, dtype=torch.float64, device=acc_e.device)
+        return 0.5 * (acc_e * acc_h.conj() * s).real.sum()
+
+    info = {"box": box, "shell": shell, "objective": objective, "sign": sgn, "spheres": centres,
+            "n_steps": int(n_steps), "n_bg": n_bg, "wavelengths": wl, "cells": cells}
+    return plan, info

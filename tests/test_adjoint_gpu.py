@@ -169,3 +169,33 @@ def test_dispersive_group_and_flux_objective():
     assert np.abs(g_ref.numpy()).max() > 0
     assert _rel(grads[0], g_ref.numpy()) < 1e-9
     assert np.array_equal(grads[0], grads[1])
+
+
+def test_cluster_instance_gradient_matches_finite_differences():
+    """A reduced instance of the dispersive-cluster workload (silver spheres as one pure D-form group, 4 nm
+    grid, 12 nm shell, 800 steps), float64: dJ/d(1/eps) of the closed-box power on the shell's largest
+    entries against central differences of the CUDA forward."""
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import cluster_instance
+
+    plan, info = cluster_instance(1, dx=4.0, shell_nm=12.0, n_steps=800, n_min=40, n_max=128, single=False)
+    box = info["box"]
+    run = AdjointRun(plan, box, objective=info["objective"], checkpoint=128, precision="double")
+    base = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in box)]).clone()
+    run.set_inv_eps_box(base)
+    J0, _ = run.forward(info["n_steps"])
+    g = run.backward().cpu().numpy()
+    assert J0 != 0 and np.abs(g[info["shell"]]).max() > 0
+    gs = np.where(info["shell"], np.abs(g), 0)
+    h = 1e-6
+    for flat in np.argsort(-gs.reshape(-1))[:4]:
+        idx = tuple(int(v) for v in np.unravel_index(flat, g.shape))
+        vals = []
+        for sgn in (1, -1):
+            x = base.clone()
+            x[idx] += sgn * h
+            run.set_inv_eps_box(x)
+            vals.append(run.forward(info["n_steps"], keep=False)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
+    run.close()
