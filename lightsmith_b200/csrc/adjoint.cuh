@@ -55,7 +55,7 @@ __device__ __forceinline__ int adj_side(const PmlAxis<R>& pm, int c, int u) {
 // Transposed E update at H node x for a warp with any node outside the interior: the curl stencil with the
 // stepped-region tests as masks (non-periodic grids), then, per axis d whose slab holds x or x + e_d, the CPML
 // terms of the two components c != d (warp-uniform branches for d = 0, 1), and x's own E psibar.
-template <typename R>
+template <bool UNI, typename R>
 __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
@@ -90,7 +90,7 @@ __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, lo
       if (c == d) continue;
       const int jh = 3 - c - d;
       R v = eb0[c] * cb0[c] - eb1[c][d] * cb1[c][d];
-      if (!g.uniform) v = v * g.inv_d[d];
+      if (!UNI) v = v * g.inv_d[d];
       acc[jh] += d == (c + 1) % 3 ? v : -v;
     }
   }
@@ -113,7 +113,7 @@ __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, lo
         A.pe_new[d][c][s0][q] = tot * pm.b[0][u];
         R w = tot * pm.c[0][u];
         if (pm.k[0]) w += eb0[c] * pm.k[0][u];
-        t += g.uniform ? cb0[c] * w : (cb0[c] / pm.div) * w;
+        t += UNI ? cb0[c] * w : (cb0[c] / pm.div) * w;
       }
       if (s1 >= 0 && m1[c][d]) {
         int y[3] = {x[0], x[1], x[2]};
@@ -121,16 +121,17 @@ __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, lo
         const long long q = psi_index(y, g.n, d, u + 1 - pm.start[0][c][s1], pm.len[0][c][s1]);
         R w = (A.pe_old[d][c][s1][q] + eb1[c][d]) * pm.c[0][u + 1];
         if (pm.k[0]) w += eb1[c][d] * pm.k[0][u + 1];
-        t -= g.uniform ? cb1[c][d] * w : (cb1[c][d] / pm.div) * w;
+        t -= UNI ? cb1[c][d] * w : (cb1[c][d] / pm.div) * w;
       }
       acc[jh] += d == (c + 1) % 3 ? t : -t;
     }
   }
 }
 
-// transpose of the E update: Hbar += (dE^{n+1}/dH^{n+1/2})^T Ebar; psibar_E to the step before; gradient
-template <typename R>
-__global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R> A) {
+// transpose of the E update: Hbar += (dE^{n+1}/dH^{n+1/2})^T Ebar; psibar_E to the step before; gradient.
+// UNI: cubic cells (one instantiation per cell shape). Latency-bound: five CTAs per SM (at most 51 registers)
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256, 5) k_adj_e(const __grid_constant__ AdjArgs<R> A) {
   const YeeArgs<R>& g = A.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
   if (k >= g.n[2] || j >= g.n[1]) return;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
       const int ca = (jj + 1) % 3, da = (jj + 2) % 3;
       const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
       R va0 = u0[ca], va1 = u1[ca][da], vb0 = -u0[cb], vb1 = -u1[cb][db];
-      if (!g.uniform) {
+      if (!UNI) {
         va0 = va0 * g.inv_d[da];
         va1 = va1 * g.inv_d[da];
         vb0 = vb0 * g.inv_d[db];
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
       acc[jj] = (va0 - va1) + (vb0 - vb1);
     }
   } else {
-    adj_e_lean(A, x, p, st, acc);  // also this node's E psibar
+    adj_e_lean<UNI>(A, x, p, st, acc);  // also this node's E psibar
   }
   const R hb0 = A.Hb[0][p], hb1 = A.Hb[1][p], hb2 = A.Hb[2][p];
   A.Hb[0][p] = hb0 + acc[0];
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
       const int s1[3] = {d1 == 0, d1 == 1, d1 == 2}, s2[3] = {d2 == 0, d2 == 1, d2 == 2};
       const R a = H(d2, 0, 0, 0) - H(d2, -s1[0], -s1[1], -s1[2]);
       const R b = H(d1, 0, 0, 0) - H(d1, -s2[0], -s2[1], -s2[2]);
-      const R curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+      const R curl = UNI ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
       A.grad[(long long)c * b0 * b1 * b2 + o] += (double)A.Eb[c][p] * (double)curl;
     }
   }
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ AdjArgs<R
 
 // Transposed H update at E node x for a warp with any node outside the interior (backward neighbours, H's
 // stepped region and CPML signs), with x's own H psibar.
-template <typename R>
+template <bool UNI, typename R>
 __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
@@ -230,7 +231,7 @@ __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, lo
       if (c == d) continue;
       const int jh = 3 - c - d;
       R v = hb1[c][d] * g.cH - hb0[c] * g.cH;
-      if (!g.uniform) v = v * g.inv_d[d];
+      if (!UNI) v = v * g.inv_d[d];
       acc[jh] += d == (c + 1) % 3 ? -v : v;
     }
   }
@@ -243,7 +244,7 @@ __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, lo
     const int s0 = adj_side<1>(pm, cr, x[d]), s1 = adj_side<1>(pm, cr, x[d] - 1);
     if (s0 < 0 && s1 < 0) continue;
     const int u = x[d];
-    const R sc = g.uniform ? sH : sH / pm.div;
+    const R sc = UNI ? sH : sH / pm.div;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (c == d) continue;
@@ -271,8 +272,8 @@ __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, lo
 }
 
 // transpose of the H update: Ebar += (dH^{n+1/2}/dE^n)^T Hbar; psibar_H to the step before
-template <typename R>
-__global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R> A) {
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AdjArgs<R> A) {
   const YeeArgs<R>& g = A.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
   if (k >= g.n[2] || j >= g.n[1]) return;
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
       const int cb = (jj + 2) % 3, db = (jj + 1) % 3;
       // a of H_ca: -Hbar cH (along da); b of H_cb: +Hbar cH (along db)
       R va1 = -(hm[ca][da] * g.cH), va0 = -(h0[ca] * g.cH), vb1 = hm[cb][db] * g.cH, vb0 = h0[cb] * g.cH;
-      if (!g.uniform) {
+      if (!UNI) {
         va1 = va1 * g.inv_d[da];
         va0 = va0 * g.inv_d[da];
         vb1 = vb1 * g.inv_d[db];
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ AdjArgs<R
       acc[jj] = (va1 - va0) + (vb1 - vb0);
     }
   } else {
-    adj_h_lean(A, x, p, st, acc);  // also this node's H psibar
+    adj_h_lean<UNI>(A, x, p, st, acc);  // also this node's H psibar
   }
   const R eb0 = A.Eb[0][p], eb1 = A.Eb[1][p], eb2 = A.Eb[2][p];
   A.Eb[0][p] = eb0 + acc[0];

@@ -895,6 +895,17 @@ struct Engine final : lsfdtd_engine {
     return false;
   }
 
+  // the in-place H (or E) kernel, instantiated for the grid's cell shape
+  void launch_inplace(bool h, const YeeArgs<F>& a, cudaStream_t s) {
+    if (a.uniform) {
+      if (h) k_update_h<F, 1><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      else k_update_e<F, 1><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+    } else {
+      if (h) k_update_h<F, 0><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      else k_update_e<F, 0><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+    }
+  }
+
   int update_h(cudaStream_t s) override {
     LS_TRY(ghosts(Eflat(), false, s));
     const YeeArgs<F> a = current_args();
@@ -904,10 +915,10 @@ struct Engine final : lsfdtd_engine {
         const dim3 grid(cdiv(desc.shape[2], 128), cdiv(desc.shape[1], 8), desc.shape[0]);
         k_update_h_v4<<<grid, dim3(32, 8), 0, s>>>(a, interior());
       } else {
-        k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+        launch_inplace(true, a, s);
       }
     } else {
-      k_update_h<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      launch_inplace(true, a, s);
     }
     LS_LAUNCHED();
     LS_TRY(mark(s, false));
@@ -923,10 +934,10 @@ struct Engine final : lsfdtd_engine {
         const dim3 grid(cdiv(desc.shape[2], 128), cdiv(desc.shape[1], 8), desc.shape[0]);
         k_update_e_v4<<<grid, dim3(32, 8), 0, s>>>(a, interior());
       } else {
-        k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+        launch_inplace(false, a, s);
       }
     } else {
-      k_update_e<F><<<bulk_grid(), dim3(32, 8), 0, s>>>(a);
+      launch_inplace(false, a, s);
     }
     LS_LAUNCHED();
     LS_TRY(mark(s, false));
@@ -1263,9 +1274,15 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
     LS_LAUNCHED();
   }
   const dim3 grid(cdiv(A.y.n[2], 32), cdiv(A.y.n[1], 8), A.y.n[0]);
-  k_adj_e<R><<<grid, dim3(32, 8), 0, s>>>(A);
-  LS_LAUNCHED();
-  k_adj_h<R><<<grid, dim3(32, 8), 0, s>>>(A);
+  if (A.y.uniform) {
+    k_adj_e<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
+    LS_LAUNCHED();
+    k_adj_h<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
+  } else {
+    k_adj_e<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
+    LS_LAUNCHED();
+    k_adj_h<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
+  }
   LS_LAUNCHED();
   a->buf = w;
   return LSFDTD_OK;

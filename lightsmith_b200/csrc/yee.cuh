@@ -72,7 +72,8 @@ __device__ __forceinline__ long long psi_index(const int* x, const int* n, int d
 
 // F += CPML terms of component c along every axis d != c. der1 / der2 are the raw differences along
 // d1 / d2; scale is the curl coefficient of this node (cH, or cbE of the node), FLD 0 = E, 1 = H.
-template <int FLD, typename F>
+// UNI: 1 cubic cells, 0 not, -1 as the grid's uniform flag says (known when the caller is compiled or not)
+template <int FLD, int UNI = -1, typename F>
 __device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, const int* x, F der1, F der2,
                                            typename real_of<F>::type scale) {
   using R = typename real_of<F>::type;
@@ -87,7 +88,8 @@ __device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, con
     R sgn = (d == d1) ? R(1) : R(-1);
     if (FLD == 1) sgn = -sgn;
     const int u = x[d];
-    R s = g.uniform ? scale : scale / p.div;
+    const bool uni = UNI < 0 ? (bool)g.uniform : UNI == 1;
+    R s = uni ? scale : scale / p.div;
     s = sgn * s;
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
@@ -103,9 +105,10 @@ __device__ __forceinline__ void apply_cpml(F& v, const YeeArgs<F>& g, int c, con
   }
 }
 
-// H update of node (i, j, k), all three components (in place).
-template <typename F>
+// H update of node (i, j, k), all three components (in place); UNI as apply_cpml's
+template <typename F, int UNI = -1>
 __device__ __forceinline__ void update_h_node(const YeeArgs<F>& g, int i, int j, int k) {
+  const bool uni = UNI < 0 ? (bool)g.uniform : UNI == 1;
   const int x[3] = {i, j, k};
   const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
   const long long p = i * s0 + j * s1 + k;
@@ -116,18 +119,19 @@ __device__ __forceinline__ void update_h_node(const YeeArgs<F>& g, int i, int j,
     const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const F a = g.E[d2][p + step[d1]] - g.E[d2][p];
     const F b = g.E[d1][p + step[d2]] - g.E[d1][p];
-    F curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+    F curl = uni ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
     F h = g.H[c][p];
     h = h - curl * g.cH;
-    apply_cpml<1>(h, g, c, x, a, b, g.cH);
+    apply_cpml<1, UNI>(h, g, c, x, a, b, g.cH);
     g.H[c][p] = h;
   }
 }
 
-// E update of node (i, j, k), all three components (in place).
-template <typename F>
+// E update of node (i, j, k), all three components (in place); UNI as apply_cpml's
+template <typename F, int UNI = -1>
 __device__ __forceinline__ void update_e_node(const YeeArgs<F>& g, int i, int j, int k) {
   using R = typename real_of<F>::type;
+  const bool uni = UNI < 0 ? (bool)g.uniform : UNI == 1;
   const int x[3] = {i, j, k};
   const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
   const long long p = i * s0 + j * s1 + k;
@@ -138,31 +142,32 @@ __device__ __forceinline__ void update_e_node(const YeeArgs<F>& g, int i, int j,
     const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const F a = g.H[d2][p] - g.H[d2][p - step[d1]];
     const F b = g.H[d1][p] - g.H[d1][p - step[d2]];
-    F curl = g.uniform ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+    F curl = uni ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
     const R cb = g.cbE[c][p];
     F e = g.E[c][p];
     e = e + curl * cb;
-    apply_cpml<0>(e, g, c, x, a, b, cb);
+    apply_cpml<0, UNI>(e, g, c, x, a, b, cb);
     g.E[c][p] = e;
   }
 }
 
-// H update: one thread per node (i, j, k), all three components.
-template <typename F>
+// H update: one thread per node (i, j, k), all three components; one instantiation per cell shape (UNI 1:
+// cubic cells)
+template <typename F, int UNI>
 __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArgs<F> g) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.n[2] || j >= g.n[1]) return;
-  update_h_node(g, blockIdx.z, j, k);
+  update_h_node<F, UNI>(g, blockIdx.z, j, k);
 }
 
-// E update: one thread per node, all three components.
-template <typename F>
+// E update: one thread per node, all three components
+template <typename F, int UNI>
 __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArgs<F> g) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.n[2] || j >= g.n[1]) return;
-  update_e_node(g, blockIdx.z, j, k);
+  update_e_node<F, UNI>(g, blockIdx.z, j, k);
 }
 
 // Periodic ghost planes of one axis: dst plane <- src plane times a Bloch phase (engine.py:595-611).
