@@ -189,3 +189,28 @@ def test_vector_kernels_equal_per_node_kernels(case, golden):
     assert _rel(a.H.cpu().numpy(), b.H.cpu().numpy()) < 1e-6
     a.close()
     b.close()
+
+
+def test_rows_without_tensor_copies_step_in_place_by_default():
+    """Rows of 30 FP32 nodes (120 bytes, not a multiple of 16): the engine's default steps in place (faster
+    there than the fused pass's cp.async ring), and an explicit kernel choice keeps the fused pass; the two give
+    the same values up to fused multiply-add contraction."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+
+    plan = throughput_plan(30, pml=4, max_steps=600, seed=4)
+    w = plan["sources"][0].wave
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    plan["sources"][0].wave = np.concatenate([w[first:], np.zeros(first)])
+    a = Engine.from_plan(plan)
+    b = Engine.from_plan(plan)
+    b.set_tuning(1, 8, 4, 4)
+    assert not a.fused and b.fused and not b.uses_tma
+    for _ in range(4):
+        a.chunk(1, use_graph=True)
+        b.chunk(1, use_graph=True)
+    assert np.abs(a.E.cpu().numpy()).max() > 0
+    assert _rel(b.E.cpu().numpy(), a.E.cpu().numpy()) < SAME_ARITHMETIC["single"]
+    assert _rel(b.results(0)[0], a.results(0)[0]) < SAME_ARITHMETIC["single"]
+    a.close()
+    b.close()
