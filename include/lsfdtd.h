@@ -61,6 +61,11 @@ typedef struct {
    * (lsfdtd_engine_buffer tells which holds the current fields); NULL: in-place kernels */
   void* E_alt;
   void* H_alt;
+  /* mirror plane per axis at node 1 (engine.py:47-60, the `mirror` argument of lightsmith's Engine): 0 none,
+   * +1 symmetric (PMC: tangential H's ghost plane 0 is refreshed as minus plane 1 before each E update), -1
+   * antisymmetric (PEC: tangential E vanishes on plane 1); on a non-periodic axis without PML on its low
+   * side. Such runs step in place. */
+  int32_t mirror[3];
 } lsfdtd_grid_desc;
 
 /* One CPML axis (Engine._build_pml, engine.py:344-418). Profiles have one entry per node position along the

@@ -26,7 +26,8 @@ f64 = C.c_double
 class GridDesc(C.Structure):
     _fields_ = [("shape", i32 * 3), ("precision", i32), ("is_complex", i32), ("periodic", i32 * 3),
                 ("spacing", f64 * 3), ("dt", f64), ("bloch", f64 * 3), ("dft_stride", i32),
-                ("E", vp), ("H", vp), ("cbE", vp * 3), ("step", vp), ("energy", vp), ("E_alt", vp), ("H_alt", vp)]
+                ("E", vp), ("H", vp), ("cbE", vp * 3), ("step", vp), ("energy", vp), ("E_alt", vp), ("H_alt", vp),
+                ("mirror", i32 * 3)]
 
 
 class PmlDesc(C.Structure):

@@ -12,7 +12,7 @@ It is lightsmith's ``NativeFDTD`` with one part swapped: on a CUDA device, the p
 (setup.py:722-773) and the post-processing (cross sections, orders, S-parameters) are lightsmith's own.
 
 On a CPU device the class is ``NativeFDTD`` unchanged: this package adds no CPU path. On a CUDA device there is
-no fallback: a problem that needs a feature with no CUDA path here (graded grids, mirror planes, conformal
+no fallback: a problem that needs a feature with no CUDA path here (graded grids, conformal
 off-diagonal terms, time monitors, substrates, Gaussian beams) is rejected by ``supports`` or raises
 ``ValueError`` when its engine is built, and a missing or unloadable ``liblsfdtd.so`` raises from the engine.
 """

@@ -221,6 +221,7 @@ struct Engine final : lsfdtd_engine {
     for (int a = 0; a < 3; ++a) {
       y.n[a] = g.shape[a];
       y.periodic[a] = g.periodic[a];
+      y.mirror[a] = g.mirror[a];
       y.inv_d[a] = R(1.0 / g.spacing[a]);
       y.E[a] = static_cast<F*>(g.E) + a * cells;
       y.H[a] = static_cast<F*>(g.H) + a * cells;
@@ -260,7 +261,7 @@ struct Engine final : lsfdtd_engine {
     fused = 0;
     if (kComplex || !Ebuf[1] || !Hbuf[1]) return 0;  // Bloch fields come with periodic axes
     for (int a = 0; a < 3; ++a)
-      if (desc.periodic[a]) return 0;
+      if (desc.periodic[a] || desc.mirror[a]) return 0;  // the fused pass's region tests know neither
     for (auto& o : order)
       if (o.first != kDipole) return 0;
     for (int d = 0; d < 3; ++d) {
@@ -533,6 +534,8 @@ struct Engine final : lsfdtd_engine {
 
   int adjoint_args(void* yee, size_t bytes, void** H) override {
     if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
+    if (desc.mirror[0] || desc.mirror[1] || desc.mirror[2])
+      return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
     if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
     for (auto& gr : groups)
@@ -554,6 +557,7 @@ struct Engine final : lsfdtd_engine {
       if (bytes != sizeof(BlochRun<F>)) return fail(LSFDTD_EINVAL, "batch: descriptor size");
       if (!desc.periodic[0] || !desc.periodic[1] || desc.periodic[2])
         return fail(LSFDTD_EUNSUPPORTED, "batch: a run must be periodic along x and y, not z");
+      if (desc.mirror[2]) return fail(LSFDTD_EUNSUPPORTED, "batch: no mirror plane");
       if (y.pml[0].on || y.pml[1].on) return fail(LSFDTD_EUNSUPPORTED, "batch: CPML along z only");
       if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "batch: dispersive groups have no batched path");
       if (order.size() != 1 || order[0].first != kColumn)
@@ -611,6 +615,7 @@ struct Engine final : lsfdtd_engine {
     const int d = p->axis;
     if (d < 0 || d > 2) return fail(LSFDTD_EINVAL, "pml axis out of range");
     if (desc.periodic[d]) return fail(LSFDTD_EINVAL, "a periodic axis cannot have a PML");
+    if (desc.mirror[d] && p->cells_lo) return fail(LSFDTD_EINVAL, "a mirror axis cannot have a PML on its low side");
     PmlAxis<F>& q = y.pml[d];
     q.on = 1;
     pml_cells[d][0] = p->cells_lo;
@@ -927,6 +932,15 @@ struct Engine final : lsfdtd_engine {
 
   int update_e(cudaStream_t s) override {
     LS_TRY(ghosts(Hflat(), true, s));
+    const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
+    for (int a = 0; a < 3; ++a) {  // symmetric mirror planes: tangential H's ghost plane, after the periodic ones
+      if (desc.mirror[a] <= 0) continue;
+      const long long plane = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2] / desc.shape[a];
+      F* h = Hflat();
+      k_mirror_ghost<F><<<cdiv(2 * plane, 256), 256, 0, s>>>(h, h + cells, h + 2 * cells, desc.shape[0],
+                                                              desc.shape[1], desc.shape[2], a);
+      LS_LAUNCHED();
+    }
     const YeeArgs<F> a = current_args();
     LS_TRY(mark(s, true));
     if constexpr (std::is_same<F, float>::value) {
@@ -1104,6 +1118,7 @@ struct Engine final : lsfdtd_engine {
     }
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
+    for (int a = 0; a < 3; ++a) per_step += desc.mirror[a] > 0;  // mirror ghost planes
     for (auto& g : groups) per_step += g.n > 0;
     for (auto& o : order) {
       switch (o.first) {
@@ -1320,6 +1335,8 @@ int32_t lsfdtd_engine_create(const lsfdtd_grid_desc* grid, lsfdtd_engine** out) 
     if (grid->shape[a] < 3) return fail(LSFDTD_EINVAL, "every axis needs at least 3 nodes");
     if (!(grid->spacing[a] > 0)) return fail(LSFDTD_EINVAL, "spacing must be positive");
     if (grid->bloch[a] != 0 && !grid->periodic[a]) return fail(LSFDTD_EINVAL, "a Bloch wavevector needs a periodic axis");
+    if (grid->mirror[a] < -1 || grid->mirror[a] > 1) return fail(LSFDTD_EINVAL, "mirror must be -1, 0 or +1");
+    if (grid->mirror[a] && grid->periodic[a]) return fail(LSFDTD_EINVAL, "a mirror axis cannot be periodic");
   }
   const bool any_bloch = grid->bloch[0] != 0 || grid->bloch[1] != 0 || grid->bloch[2] != 0;
   if (any_bloch && !grid->is_complex) return fail(LSFDTD_EINVAL, "a Bloch wavevector needs complex fields");

@@ -32,6 +32,7 @@ struct YeeArgs {
   using R = typename real_of<F>::type;
   int n[3];
   int periodic[3];
+  int mirror[3];   // per axis: 0, or +1 / -1 for a symmetric / antisymmetric mirror plane at node 1
   int uniform;     // cubic cells: coefficients carry dt/dx and differences are not rescaled
   R inv_d[3];
   R cH;
@@ -41,20 +42,27 @@ struct YeeArgs {
   PmlAxis<F> pml[3];
 };
 
-__device__ __forceinline__ bool in_e_region(int c, const int* x, const int* n, const int* per) {
+// mir: the mirror planes (null: none); along a mirror axis E_c starts at node 2 when it is tangential to an
+// antisymmetric plane, else at 1 (engine.py:41-60)
+__device__ __forceinline__ bool in_e_region(int c, const int* x, const int* n, const int* per,
+                                            const int* mir = nullptr) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     int lo = (per[a] || a != c) ? 1 : 0;
+    if (mir && mir[a]) lo = (mir[a] < 0 && a != c) ? 2 : 1;
     if (x[a] < lo || x[a] >= n[a] - 1) return false;
   }
   return true;
 }
 
-__device__ __forceinline__ bool in_h_region(int c, const int* x, const int* n, const int* per) {
+// H_c along a mirror axis starts at node 2 when it is normal to an antisymmetric plane, else at 1
+__device__ __forceinline__ bool in_h_region(int c, const int* x, const int* n, const int* per,
+                                            const int* mir = nullptr) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     int lo = per[a] ? 1 : 0;
     int hi = per[a] ? n[a] - 1 : (a == c ? n[a] : n[a] - 1);
+    if (mir && mir[a]) lo = (mir[a] < 0 && a == c) ? 2 : 1;
     if (x[a] < lo || x[a] >= hi) return false;
   }
   return true;
@@ -115,7 +123,7 @@ __device__ __forceinline__ void update_h_node(const YeeArgs<F>& g, int i, int j,
   const long long step[3] = {s0, s1, 1};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if (!in_h_region(c, x, g.n, g.periodic)) continue;
+    if (!in_h_region(c, x, g.n, g.periodic, g.mirror)) continue;
     const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const F a = g.E[d2][p + step[d1]] - g.E[d2][p];
     const F b = g.E[d1][p + step[d2]] - g.E[d1][p];
@@ -138,7 +146,7 @@ __device__ __forceinline__ void update_e_node(const YeeArgs<F>& g, int i, int j,
   const long long step[3] = {s0, s1, 1};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if (!in_e_region(c, x, g.n, g.periodic)) continue;
+    if (!in_e_region(c, x, g.n, g.periodic, g.mirror)) continue;
     const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
     const F a = g.H[d2][p] - g.H[d2][p - step[d1]];
     const F b = g.H[d1][p] - g.H[d1][p - step[d2]];
@@ -189,6 +197,32 @@ __global__ void k_ghost(F* f0, F* f1, F* f2, int n0, int n1, int n2, int axis, i
   const long long pd = ((long long)xd[0] * n1 + xd[1]) * n2 + xd[2];
   const long long ps = ((long long)xs[0] * n1 + xs[1]) * n2 + xs[2];
   f[pd] = apply_phase<F>(f[ps], ph_re, ph_im);
+}
+
+// Symmetric (PMC) mirror plane along `axis`: the two tangential H components' ghost plane 0 set to minus
+// plane 1, before an E update (engine.py:290-298, 649-650). One thread per node of the plane and component.
+template <typename F>
+__global__ void k_mirror_ghost(F* h0, F* h1, F* h2, int n0, int n1, int n2, int axis) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = axis == 0 ? n1 : n0, nb = axis == 2 ? n1 : n2;  // the plane's two other axes, in order
+  const long long per = (long long)na * nb;
+  if (t >= 2 * per) return;
+  const int comp = (axis + 1 + (int)(t / per)) % 3;  // a tangential component
+  const long long r = t % per;
+  const int u = (int)(r / nb), v = (int)(r % nb);
+  long long pg, ps;  // the node on plane 0 along axis, and its image on plane 1
+  if (axis == 0) {
+    pg = (long long)u * n2 + v;
+    ps = (long long)n1 * n2 + pg;
+  } else if (axis == 1) {
+    pg = (long long)u * n1 * n2 + v;
+    ps = pg + n2;
+  } else {
+    pg = ((long long)u * n1 + v) * n2;
+    ps = pg + 1;
+  }
+  F* f = comp == 0 ? h0 : (comp == 1 ? h1 : h2);
+  f[pg] = zero<F>() - f[ps];
 }
 
 }  // namespace lsfdtd

@@ -96,7 +96,9 @@ class Engine:
             self._H = [torch.zeros((3,) + self.shape, dtype=self.fdt, device=self.dev)]
             # the fused single-pass step alternates between two field buffers; it serves runs without periodic
             # axes whose sources only correct E (point dipoles)
+            self.mirror = tuple(int(m) for m in plan.get("mirror", (0, 0, 0)))
             self.double_buffered = (fused is not False and not any(self.periodic) and not self.complex and
+                                    not any(self.mirror) and
                                     all(isinstance(s, DipoleSource) for s in plan["sources"]))
             if self.double_buffered:
                 self._E.append(torch.zeros_like(self._E[0]))
@@ -125,6 +127,7 @@ class Engine:
             g.precision = _abi.F32 if self.single else _abi.F64
             g.is_complex = int(self.complex)
             g.periodic[:] = [int(p) for p in self.periodic]
+            g.mirror[:] = list(self.mirror)
             g.spacing[:] = list(self.spacing)
             g.dt = self.dt
             g.bloch[:] = list(plan["bloch"])

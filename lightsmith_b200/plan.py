@@ -95,16 +95,27 @@ class DFTMonitor:
 # --- region helpers ----------------------------------------------------------------------------------
 
 
-def e_range(c: int, a: int, n: int, periodic: bool) -> tuple[int, int]:
-    """Stepped index range [lo, hi) of E_c along axis a (``engine.py:47-60``, no mirror planes): tangential E
-    stays 0 on the outer (PEC) planes; periodic axes step the real cells 1..n-2 between two ghost planes."""
+def _mirror_start(c: int, a: int, m: int, kind: str) -> int:
+    """First stepped index along a mirror axis (``engine.py:41-44``): 1, or 2 for the fields that vanish on an
+    antisymmetric plane (tangential E, normal H)."""
+    return 2 if m < 0 and (c != a) == (kind == "E") else 1
+
+
+def e_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[int, int]:
+    """Stepped index range [lo, hi) of E_c along axis a (``engine.py:47-60``): tangential E stays 0 on the
+    outer (PEC) planes; periodic axes step the real cells 1..n-2 between two ghost planes; on a mirror axis
+    (mirror = +1 or -1, the plane at node 1, a ghost plane at 0) the range starts at 1 or 2."""
+    if mirror:
+        return _mirror_start(c, a, mirror, "E"), n - 1
     if periodic or a != c:
         return 1, n - 1
     return 0, n - 1
 
 
-def h_range(c: int, a: int, n: int, periodic: bool) -> tuple[int, int]:
-    """Stepped index range of H_c along axis a (``engine.py:63-66``, no mirror planes)."""
+def h_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[int, int]:
+    """Stepped index range of H_c along axis a (``engine.py:63-66``)."""
+    if mirror:
+        return _mirror_start(c, a, mirror, "H"), (n if a == c else n - 1)
     if periodic:
         return 1, n - 1
     return (0, n) if a == c else (0, n - 1)
@@ -158,7 +169,7 @@ def cpml_profiles(pml, shape, spacing, dt):
     return out
 
 
-def cpml_terms(pml, shape, periodic):
+def cpml_terms(pml, shape, periodic, mirror=(0, 0, 0)):
     """The CPML correction terms in lightsmith's order (``engine.py:373-418``): per axis d, per field (E then
     H), per component c != d, per side (low, high) a slab of c's stepped region restricted along d.
 
@@ -181,7 +192,7 @@ def cpml_terms(pml, shape, periodic):
                 if fld == "H":
                     sgn = -sgn
                 rng = e_range if fld == "E" else h_range
-                R = [rng(c, a, shape[a], periodic[a]) for a in range(3)]
+                R = [rng(c, a, shape[a], periodic[a], mirror[a]) for a in range(3)]
                 start, stop = R[d]
                 sides = []
                 if lo_n:
@@ -396,14 +407,16 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
               mirror=(0, 0, 0), widths=None) -> dict:
     """The plan of lightsmith's ``Engine(...)`` keyword arguments (``engine.py:231-241``).
 
-    Graded grids, mirror planes and the conformal off-diagonal / vertex-tensor terms have no CUDA path here and
-    are rejected."""
+    Graded grids and the conformal off-diagonal / vertex-tensor terms have no CUDA path here and are rejected.
+    Mirror planes (``mirror`` per axis: +1 symmetric, -1 antisymmetric, at node 1) are kept."""
     shape = tuple(int(n) for n in shape)
     spacing = tuple(float(v) for v in np.broadcast_to(np.asarray(dx, dtype=float), (3,)))
     if widths is not None and any(w is not None for w in widths):
         raise NotImplementedError("graded grids have no CUDA path in lightsmith-b200")
-    if any(int(np.sign(m)) for m in mirror):
-        raise NotImplementedError("mirror planes have no CUDA path in lightsmith-b200")
+    mirror = tuple(int(np.sign(m)) for m in mirror)
+    for a, m in enumerate(mirror):  # engine.py:259-261
+        if m and (bool(periodic[a]) or int(pml.cells[a][0])):
+            raise ValueError("a mirror plane needs a non-periodic axis without PML on its low side")
     if offdiag is not None and len(getattr(offdiag, "comp", ())):
         raise NotImplementedError("conformal off-diagonal terms have no CUDA path in lightsmith-b200")
     if time_monitors:
@@ -429,6 +442,8 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
         "groups": grp,
         "sources": [source_plan(s, shape, single) for s in sources],
     }
+    if any(mirror):  # only then (plans without mirror planes keep their earlier form)
+        plan["mirror"] = mirror
     mons = []
     for m in monitors:
         space = _monitor_space(m.source, sources, plan["sources"])

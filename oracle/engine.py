@@ -52,8 +52,19 @@ class OracleEngine:
         self.H = np.zeros((3, n0, n1, n2), self.fdt)
         self.n = 0
         P = self.periodic
-        self.RE = [tuple(e_range(c, a, self.shape[a], P[a]) for a in range(3)) for c in range(3)]
-        self.RH = [tuple(h_range(c, a, self.shape[a], P[a]) for a in range(3)) for c in range(3)]
+        M = self.mirror = tuple(plan.get("mirror", (0, 0, 0)))
+        self.RE = [tuple(e_range(c, a, self.shape[a], P[a], M[a]) for a in range(3)) for c in range(3)]
+        self.RH = [tuple(h_range(c, a, self.shape[a], P[a], M[a]) for a in range(3)) for c in range(3)]
+        # symmetric (PMC) mirror planes: tangential H's ghost plane 0 is minus its image, plane 1, before every
+        # E update (engine.py:290-298, 649-650)
+        self._mirror_ghosts = []
+        for a, m in enumerate(M):
+            if m > 0:
+                for t in range(3):
+                    if t != a:
+                        g, s = [slice(None)] * 3, [slice(None)] * 3
+                        g[a], s[a] = slice(0, 1), slice(1, 2)
+                        self._mirror_ghosts.append((t, tuple(g), tuple(s)))
         # uniform cubic cells fold dt/dx into the coefficients; otherwise differences are scaled by 1/d_axis and
         # the coefficients carry dt alone (engine.py:274-276, 622-627)
         cdx = self.dt / self.spacing[0] if self.uniform else self.dt
@@ -78,7 +89,7 @@ class OracleEngine:
     def _build_pml(self, inv_eps, cdx):
         prof = cpml_profiles(_Spec(self.plan["pml"]), self.shape, self.spacing, self.dt)
         self.pml = {"E": [], "H": []}
-        for t in cpml_terms(_Spec(self.plan["pml"]), self.shape, self.periodic):
+        for t in cpml_terms(_Spec(self.plan["pml"]), self.shape, self.periodic, self.mirror):
             d, fld = t["d"], t["field"]
             a, b = t["region"][d]
             bb, cc, kk = (v[a:b] for v in prof[d][2][fld])
@@ -208,6 +219,8 @@ class OracleEngine:
     def update_E(self):
         if any(self.periodic):
             self._ghosts(self.H, low=True)
+        for t, g, s in self._mirror_ghosts:
+            self.H[t][g] = -self.H[t][s]
         self._parallel(lambda a, b: self._update("E", a, b), 0, self.shape[0])
 
     # --- step order (engine.py:665-683) -----------------------------------------------------------------

@@ -134,6 +134,23 @@ def case_kappa_noncubic():
     run_engine_case("kappa_noncubic", kw, 8, snap=2)
 
 
+def case_mirror():
+    """Mirror planes at node 1 (engine.py:47-60): symmetric (PMC) along x and z, antisymmetric (PEC) along y;
+    CPML on the high sides only."""
+    rng = np.random.default_rng(8)
+    shape, dx = (14, 15, 16), 5.0
+    dt = 0.99 * dx / np.sqrt(3)
+    ie = 1.0 / rng.uniform(1.0, 6.0, size=(3,) + shape)
+    pml = ref_engine.PMLSpec(cells=((0, 3), (0, 3), (0, 3)), alpha_max=0.02, eps_ref=1.5)
+    om = 2 * np.pi / np.array([300.0, 450.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(22.3, 31.7, 41.2), pdir=(0.6, 0.3, 0.7),
+                      inv_eps=ie, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    mons = [plane_monitor(shape, 9, om, 1)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[dip],
+              monitors=mons, dft_stride=3, mirror=(1, -1, 1))
+    run_engine_case("mirror", kw, 10, snap=2)
+
+
 def sphere_slot_fn(center, radius, slot=1):
     c = np.asarray(center, float)
 
@@ -338,7 +355,7 @@ def sphere_problem(mesh: str):
 
 CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_noncubic,
          "ade_groups": case_ade_groups, "tfsf_table": case_tfsf_table, "line_periodic": case_line_periodic,
-         "bloch_column": case_bloch_column, "mode_source": case_mode_source,
+         "bloch_column": case_bloch_column, "mode_source": case_mode_source, "mirror": case_mirror,
          "solve_sphere_staircase": lambda: solve_case("sphere_staircase", sphere_problem("staircase")),
          "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel"))}
 

@@ -112,10 +112,21 @@ def test_solve_hands_lightsmiths_plan_to_the_cuda_engine(monkeypatch, golden):
             np.testing.assert_array_equal(got[k], want[k], err_msg=k)
 
 
-def test_features_without_a_cuda_path_raise_value_error():
-    """symmetry='auto' gives this sphere mirror planes, which the CUDA engine lacks: lightsmith's error."""
-    with pytest.raises(ValueError, match="mirror planes"):
+def test_mirror_planes_reach_the_cuda_engine(monkeypatch):
+    """symmetry='auto' gives this sphere mirror planes: the driver hands the CUDA engine a plan that keeps them
+    (a half or quarter grid stepped with PEC/PMC planes at node 1)."""
+    seen = {}
+
+    class Recorder:
+        def __init__(self, device, **kw):
+            seen["plan"] = P.make_plan(**kw)
+            raise _Recorded
+
+    monkeypatch.setattr(B._engine, "Engine", Recorder)
+    with pytest.raises(_Recorded):
         B.B200FDTD.solve(sphere(symmetry="auto"), CUDA0)
+    mirror = seen["plan"].get("mirror", (0, 0, 0))
+    assert any(mirror) and all(m in (-1, 0, 1) for m in mirror)
 
 
 def test_solve_on_cuda_without_a_gpu_fails_loudly():
