@@ -30,6 +30,7 @@ if not add_to_path(sys.argv[1] if len(sys.argv) > 1 else REF_SRC):
 import lightsmith as ls  # noqa: E402
 from lightsmith.backends._fdtd import engine as ref_engine  # noqa: E402
 from lightsmith.backends._fdtd import scattering as ref_scattering  # noqa: E402
+from lightsmith.backends._fdtd import symmetry as ref_symmetry  # noqa: E402
 from lightsmith.backends._fdtd.emission import PointDipole  # noqa: E402
 from lightsmith.backends._fdtd.layered import ObliqueLayeredPlaneWave  # noqa: E402
 from lightsmith.backends._fdtd.media import Medium, Pole  # noqa: E402
@@ -330,7 +331,8 @@ def solve_case(name: str, sim):
     src = kw["sources"][0]
     omega = 2 * np.pi / sim.wavelength_array()
     sca, tot = boxes
-    post = {"omega": omega, "n_sym": 1.0, "n_inc": float(src.n_inc), "sca_coeff": sca[3], "tot_coeff": tot[3],
+    n_sym = float(ref_symmetry.factor(kw.get("mirror", (0, 0, 0))))
+    post = {"omega": omega, "n_sym": n_sym, "n_inc": float(src.n_inc), "sca_coeff": sca[3], "tot_coeff": tot[3],
             "unit": src.incident_reference(omega), "bg_e": src.background(omega, tot[0], "E"),
             "bg_h": 0.5 * (src.background(omega, tot[1], "H") + src.background(omega, tot[2], "H")),
             "steps": int(res.provenance["steps"])}
@@ -342,13 +344,13 @@ def solve_case(name: str, sim):
     print(name, rec["plan"]["shape"], "steps", post["steps"], "C_ext", out["c_ext"])
 
 
-def sphere_problem(mesh: str):
+def sphere_problem(mesh: str, symmetry: str = "off"):
     mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
                           poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
                                  {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
     return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=mat)], medium_index=1.33,
                          wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
-                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry="off", mesh_refinement=mesh,
+                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry=symmetry, mesh_refinement=mesh,
                                                padding_nm=8.0, pml_gap_nm=8.0, dft_stride=10,
                                                run_time_fs=399.5 * 2.2863 / 299.792458)})
 
@@ -357,7 +359,8 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "ade_groups": case_ade_groups, "tfsf_table": case_tfsf_table, "line_periodic": case_line_periodic,
          "bloch_column": case_bloch_column, "mode_source": case_mode_source, "mirror": case_mirror,
          "solve_sphere_staircase": lambda: solve_case("sphere_staircase", sphere_problem("staircase")),
-         "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel"))}
+         "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel")),
+         "solve_sphere_symmetric": lambda: solve_case("sphere_symmetric", sphere_problem("staircase", "auto"))}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)
