@@ -221,6 +221,19 @@ int32_t lsfdtd_engine_create(const lsfdtd_grid_desc* grid, lsfdtd_engine** out);
 int32_t lsfdtd_engine_destroy(lsfdtd_engine* eng);
 int32_t lsfdtd_engine_set_pml(lsfdtd_engine* eng, const lsfdtd_pml_desc* pml);
 int32_t lsfdtd_engine_add_group(lsfdtd_engine* eng, const lsfdtd_group_desc* g);
+
+/* Conformal off-diagonal 1/eps terms (Engine._build_offdiag and _update_E, engine.py:421-518, 653-655): row r
+ * adds sum_k w[r][k] * H_flat[h[r][k]] to E_flat[e[r]] after each E curl update, before the sources' E
+ * corrections. The tables are built on the host (lightsmith_b200/plan.py:offdiag_tables restates the
+ * reference's construction). At most one set per engine. */
+typedef struct {
+  const int64_t* e;  /* device (n): distinct flat E indices */
+  const int64_t* h;  /* device (n, width): flat H indices */
+  const void* w;     /* device (n, width): weights in the field precision (complex under a Bloch wavevector) */
+  int64_t n;
+  int32_t width;
+} lsfdtd_offdiag_desc;
+int32_t lsfdtd_engine_add_offdiag(lsfdtd_engine* eng, const lsfdtd_offdiag_desc* d);
 /* sources act in the order they are added (Engine.step, engine.py:665-678) */
 int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s);
 int32_t lsfdtd_engine_add_dipole(lsfdtd_engine* eng, const lsfdtd_dipole_desc* s);

@@ -30,6 +30,10 @@ class GridDesc(C.Structure):
                 ("mirror", i32 * 3)]
 
 
+class OffdiagDesc(C.Structure):
+    _fields_ = [("e", vp), ("h", vp), ("w", vp), ("n", i64), ("width", i32)]
+
+
 class PmlDesc(C.Structure):
     _fields_ = [("axis", i32), ("cells_lo", i32), ("cells_hi", i32), ("b", vp * 2), ("c", vp * 2), ("k", vp * 2),
                 ("psi", ((vp * 2) * 3) * 2), ("psi_alt", (vp * 2) * 3)]
@@ -97,6 +101,7 @@ SIGNATURES = {
     "lsfdtd_engine_destroy": (i32, [vp]),
     "lsfdtd_engine_set_pml": (i32, [vp, C.POINTER(PmlDesc)]),
     "lsfdtd_engine_add_group": (i32, [vp, C.POINTER(GroupDesc)]),
+    "lsfdtd_engine_add_offdiag": (i32, [vp, C.POINTER(OffdiagDesc)]),
     "lsfdtd_engine_add_table_source": (i32, [vp, C.POINTER(TableSourceDesc)]),
     "lsfdtd_engine_add_dipole": (i32, [vp, C.POINTER(DipoleDesc)]),
     "lsfdtd_engine_add_line_source": (i32, [vp, C.POINTER(LineSourceDesc)]),

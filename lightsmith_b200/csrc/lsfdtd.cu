@@ -128,6 +128,7 @@ struct lsfdtd_engine {
   }
   virtual int set_pml(const lsfdtd_pml_desc* p) = 0;
   virtual int add_group(const lsfdtd_group_desc* g) = 0;
+  virtual int add_offdiag(const lsfdtd_offdiag_desc* d) = 0;
   virtual int add_table(const lsfdtd_table_source_desc* s) = 0;
   virtual int add_dipole(const lsfdtd_dipole_desc* s) = 0;
   virtual int add_line(const lsfdtd_line_source_desc* s) = 0;
@@ -536,6 +537,7 @@ struct Engine final : lsfdtd_engine {
     if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
     if (desc.mirror[0] || desc.mirror[1] || desc.mirror[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
+    if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no conformal off-diagonal terms");
     if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
     for (auto& gr : groups)
@@ -558,6 +560,7 @@ struct Engine final : lsfdtd_engine {
       if (!desc.periodic[0] || !desc.periodic[1] || desc.periodic[2])
         return fail(LSFDTD_EUNSUPPORTED, "batch: a run must be periodic along x and y, not z");
       if (desc.mirror[2]) return fail(LSFDTD_EUNSUPPORTED, "batch: no mirror plane");
+      if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "batch: no conformal off-diagonal terms");
       if (y.pml[0].on || y.pml[1].on) return fail(LSFDTD_EUNSUPPORTED, "batch: CPML along z only");
       if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "batch: dispersive groups have no batched path");
       if (order.size() != 1 || order[0].first != kColumn)
@@ -640,6 +643,41 @@ struct Engine final : lsfdtd_engine {
           }
         }
     }
+    return LSFDTD_OK;
+  }
+
+  // conformal off-diagonal gather (at most one set)
+  const long long* od_e = nullptr;
+  const long long* od_h = nullptr;
+  const F* od_w = nullptr;
+  long long od_n = 0;
+  int od_width = 0;
+  int add_offdiag(const lsfdtd_offdiag_desc* d) override {
+    if (od_n) return fail(LSFDTD_EINVAL, "offdiag: one set per engine");
+    if (d->n < 0 || d->width < 1 || (d->n > 0 && (!d->e || !d->h || !d->w)))
+      return fail(LSFDTD_EINVAL, "offdiag: arrays missing or sizes out of range");
+    // index ranges checked here, once (the kernel trusts them)
+    const long long flat = 3LL * desc.shape[0] * desc.shape[1] * desc.shape[2];
+    std::vector<long long> he(d->n), hh(d->n * (long long)d->width);
+    if (d->n > 0) {
+      LS_CUDA(cudaMemcpy(he.data(), d->e, he.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+      LS_CUDA(cudaMemcpy(hh.data(), d->h, hh.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    }
+    for (long long v : he)
+      if (v < 0 || v >= flat) return fail(LSFDTD_ERANGE, "offdiag: an E index out of range");
+    for (long long v : hh)
+      if (v < 0 || v >= flat) return fail(LSFDTD_ERANGE, "offdiag: an H index out of range");
+    od_e = reinterpret_cast<const long long*>(d->e);
+    od_h = reinterpret_cast<const long long*>(d->h);
+    od_w = static_cast<const F*>(d->w);
+    od_n = d->n;
+    od_width = d->width;
+    return LSFDTD_OK;
+  }
+  int offdiag(cudaStream_t s) {
+    if (od_n <= 0) return LSFDTD_OK;
+    k_offdiag<F><<<cdiv(od_n, 256), 256, 0, s>>>(od_e, od_h, od_w, od_n, od_width, Eflat(), Hflat());
+    LS_LAUNCHED();
     return LSFDTD_OK;
   }
 
@@ -1063,6 +1101,7 @@ struct Engine final : lsfdtd_engine {
       LS_TRY(hook(1, s));
       LS_TRY(update_e(s));
     }
+    LS_TRY(offdiag(s));
     LS_TRY(hook(2, s));
     for (auto& g : groups) {
       if (g.n <= 0) continue;
@@ -1119,6 +1158,7 @@ struct Engine final : lsfdtd_engine {
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
     for (int a = 0; a < 3; ++a) per_step += desc.mirror[a] > 0;  // mirror ghost planes
+    per_step += od_n > 0;  // the off-diagonal gather
     for (auto& g : groups) per_step += g.n > 0;
     for (auto& o : order) {
       switch (o.first) {
@@ -1367,6 +1407,10 @@ int32_t lsfdtd_engine_set_pml(lsfdtd_engine* eng, const lsfdtd_pml_desc* p) {
 int32_t lsfdtd_engine_add_group(lsfdtd_engine* eng, const lsfdtd_group_desc* g) {
   LS_NEED(eng && g);
   return eng->add_group(g);
+}
+int32_t lsfdtd_engine_add_offdiag(lsfdtd_engine* eng, const lsfdtd_offdiag_desc* d) {
+  LS_NEED(eng && d);
+  return eng->add_offdiag(d);
 }
 int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s) {
   LS_NEED(eng && s);

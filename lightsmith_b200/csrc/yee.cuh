@@ -199,6 +199,20 @@ __global__ void k_ghost(F* f0, F* f1, F* f2, int n0, int n1, int n2, int axis, i
   f[pd] = apply_phase<F>(f[ps], ph_re, ph_im);
 }
 
+// Conformal off-diagonal 1/eps terms (engine.py:653-655): row t adds sum_k w[t][k] H[h[t][k]] to E[e[t]]; the
+// targets are distinct, so one thread per row needs no atomics. E and H are the flat component-stacked fields.
+template <typename F>
+__global__ void k_offdiag(const long long* e, const long long* h, const F* w, long long n, int width, F* E,
+                          const F* H) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long* hr = h + t * width;
+  const F* wr = w + t * width;
+  F acc = zero<F>();
+  for (int k = 0; k < width; ++k) acc = acc + wr[k] * H[hr[k]];
+  E[e[t]] = E[e[t]] + acc;
+}
+
 // Symmetric (PMC) mirror plane along `axis`: the two tangential H components' ghost plane 0 set to minus
 // plane 1, before an E update (engine.py:290-298, 649-650). One thread per node of the plane and component.
 template <typename F>

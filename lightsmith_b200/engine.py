@@ -142,6 +142,16 @@ class Engine:
             self._h = h
             self._build_pml(plan, L)
             self.groups = [self._build_group(gr, L) for gr in plan["groups"]]
+            od = plan.get("offdiag")
+            if od is not None and len(od["e"]):  # conformal off-diagonal terms (engine.py:421-518, 653-655)
+                torch = _torch()
+                o = _abi.OffdiagDesc()
+                ee = self._dev(np.asarray(od["e"], np.int64), torch.int64)
+                hh = self._dev(np.ascontiguousarray(od["h"], np.int64), torch.int64)
+                ww = self._dev(np.ascontiguousarray(od["w"]), self.fdt)
+                o.e, o.h, o.w = _ptr(ee), _ptr(hh), _ptr(ww)
+                o.n, o.width = len(od["e"]), int(np.asarray(od["h"]).shape[1])
+                _abi.check(L.lsfdtd_engine_add_offdiag(self._h, C.byref(o)), "lsfdtd_engine_add_offdiag")
             self._src_state = [self._build_source(s, L) for s in plan["sources"]]
             self.monitors = []
             objs = monitor_objs if monitor_objs is not None else [None] * len(plan["monitors"])

@@ -402,6 +402,126 @@ def _inv_eps(inv_eps, shape):
     return np.asarray(a, dtype=float).reshape((3,) + tuple(shape))
 
 
+def _mirror_fold(comp, idx3, mirror):
+    """Nodes on the ghost side of mirror planes mapped to their stepped images (``engine.py:75-90``): (idx3,
+    sign), sign the image's parity, 0 for a node that vanishes on an antisymmetric plane."""
+    idx3 = np.array(idx3, dtype=np.int64)
+    comp = np.broadcast_to(np.asarray(comp), (len(idx3),))
+    sign = np.ones(len(idx3), dtype=np.int64)
+    for a, m in enumerate(mirror):
+        if not m:
+            continue
+        normal = comp == a
+        j = idx3[:, a]
+        ghost = j <= 0
+        idx3[:, a] = np.where(ghost, np.where(normal, 1 - j, 2 - j), j)
+        sign = np.where(ghost, sign * np.where(normal, -m, m), sign)
+        sign = np.where((m < 0) & ~normal & (idx3[:, a] == 1), 0, sign)
+    return idx3, sign
+
+
+def _mirror_rows(idx3, comp, coef, mirror):
+    """Off-diagonal rows plus their images across every mirror plane (``engine.py:540-553``): rows on a plane
+    (tangential components at node 1) are their own images; an image's (1/eps)_cd changes sign when exactly one
+    of c, d is the mirror axis."""
+    for a, m in enumerate(mirror):
+        if not m:
+            continue
+        normal = comp == a
+        new = normal | (idx3[:, a] != 1)
+        im = idx3[new].copy()
+        im[:, a] = np.where(normal[new], 1 - im[:, a], 2 - im[:, a])
+        flip = np.where((np.arange(3)[None, :] == a) != normal[new][:, None], -1.0, 1.0)
+        idx3 = np.concatenate([idx3, im])
+        comp = np.concatenate([comp, comp[new]])
+        coef = np.concatenate([coef, coef[new] * flip])
+    return idx3, comp, coef
+
+
+def offdiag_tables(od, shape, spacing, dt, periodic, bloch, mirror, group_idx, complex_fields):
+    """Gather tables of the conformal off-diagonal 1/eps terms (``engine.py:421-518``, cubic or rectangular
+    cells, no graded axes): (targets (n,), h (n, 4 W), w (n, 4 W)); row r adds sum_k w[r, k] H_flat[h[r, k]] to
+    E_flat[targets[r]] after the E curl update.
+
+    E_c at node p couples to curl_d H at the four E_d nodes q around it (p + e_c (0 or 1) - e_d (0 or 1)); the
+    coupling is symmetrised, (1/eps)_cd(p) / 8 from q to p and its conjugate / 8 from p to q; periodic axes
+    wrap q onto the real cells with the Bloch phase of the period crossed; along other axes q must lie in
+    E_d's stepped range (mirror axes: any index, folded below). With mirror planes the rows' images are added,
+    couplings into ghost-side targets dropped, and ghost-side sources act through their images with the parity
+    sign. Pairs touching a dispersive node are dropped, equal pairs merged, and each pair's source D_d (the time
+    integral of curl_d H) expanded into its four H differences with dt / dx along each difference's axis."""
+    shape = tuple(int(n) for n in shape)
+    ncell = int(np.prod(shape))
+    nflat = 3 * ncell
+    idx3 = np.asarray(od.idx3, np.int64)
+    comp = np.asarray(od.comp, np.int64)
+    coef = np.asarray(od.coef, float)
+    if any(mirror):
+        idx3, comp, coef = _mirror_rows(idx3, comp, coef, mirror)
+    eye = np.eye(3, dtype=np.int64)
+    tc, ti, sc, si, fwd, bwd = [], [], [], [], [], []
+    for d in range(3):
+        for corner in range(4):
+            q = idx3 + eye[comp] * (corner & 1)
+            q[:, d] -= corner >> 1
+            phase = np.ones(len(q), complex)
+            ok = (comp != d) & (coef[:, d] != 0)
+            for a in range(3):
+                n = shape[a]
+                if periodic[a]:
+                    kl = bloch[a] * (n - 2) * spacing[a]
+                    lo, hi = q[:, a] == 0, q[:, a] == n - 1
+                    q[lo, a], q[hi, a] = n - 2, 1
+                    phase[lo] *= np.exp(-1j * kl)
+                    phase[hi] *= np.exp(1j * kl)
+                else:
+                    start, stop = e_range(d, a, n, False)
+                    ok &= (q[:, a] < stop) & ((q[:, a] >= start) | bool(mirror[a]))
+            tc.append(comp[ok])
+            ti.append(idx3[ok])
+            sc.append(np.full(int(ok.sum()), d))
+            si.append(q[ok])
+            fwd.append(coef[ok, d] * phase[ok] / 8)
+            bwd.append(np.conj(coef[ok, d] * phase[ok]) / 8)
+    tc, ti, sc, si, f = (np.concatenate(x) for x in (tc, ti, sc, si, fwd))
+    tc, sc = np.concatenate([tc, sc]), np.concatenate([sc, tc])
+    ti, si = np.concatenate([ti, si]), np.concatenate([si, ti])
+    v = np.concatenate([f, np.concatenate(bwd)])
+    if any(mirror):
+        ti_f, t_sign = _mirror_fold(tc, ti, mirror)
+        si, s_sign = _mirror_fold(sc, si, mirror)
+        keep = (np.all(ti_f == ti, axis=1) & (t_sign != 0) & (s_sign != 0) &
+                np.all(si < np.asarray(shape) - 1, axis=1))
+        tc, ti, sc, si, v = tc[keep], ti[keep], sc[keep], si[keep], v[keep] * s_sign[keep]
+    t = flat_index(tc, ti[:, 0], ti[:, 1], ti[:, 2], shape)
+    src = flat_index(sc, si[:, 0], si[:, 1], si[:, 2], shape)
+    if len(group_idx):
+        keep = ~(np.isin(t, group_idx) | np.isin(src, group_idx))
+        t, src, v = t[keep], src[keep], v[keep]
+    if not len(t):
+        return None
+    key, inv = np.unique(t * nflat + src, return_inverse=True)
+    v = np.bincount(inv, v.real, len(key)) + 1j * np.bincount(inv, v.imag, len(key))
+    t, src = key // nflat, key % nflat
+    targets, first, count = np.unique(t, return_index=True, return_counts=True)
+    slot = np.arange(len(t)) - np.repeat(first, count)
+    row = np.repeat(np.arange(len(targets)), count)
+    width = int(count.max())
+    h = np.ones((len(targets), 4 * width), np.int64)  # padding: any valid index, weight 0
+    w = np.zeros((len(targets), 4 * width), complex)
+    d, rest = np.divmod(src, ncell)
+    q = np.stack(np.unravel_index(rest, shape), axis=1)
+    d1, d2 = (d + 1) % 3, (d + 2) % 3
+    inv_d = 1.0 / np.asarray(spacing, float)
+    # curl_d H at q = (H_d2[q] - H_d2[q - e_d1]) / dx_d1 - (H_d1[q] - H_d1[q - e_d2]) / dx_d2
+    for k, (cmp, back, sgn, ax) in enumerate(((d2, None, 1.0, d1), (d2, d1, -1.0, d1),
+                                               (d1, None, -1.0, d2), (d1, d2, 1.0, d2))):
+        pp = q if back is None else q - eye[back]
+        h[row, 4 * slot + k] = flat_index(cmp, pp[:, 0], pp[:, 1], pp[:, 2], shape)
+        w[row, 4 * slot + k] = dt * sgn * inv_d[ax] * v
+    return targets.astype(np.int64), h, (w if complex_fields else w.real)
+
+
 def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors, dft_stride,
               periodic=(False, False, False), bloch=(0.0, 0.0, 0.0), offdiag=None, time_monitors=(),
               mirror=(0, 0, 0), widths=None) -> dict:
@@ -417,8 +537,6 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
     for a, m in enumerate(mirror):  # engine.py:259-261
         if m and (bool(periodic[a]) or int(pml.cells[a][0])):
             raise ValueError("a mirror plane needs a non-periodic axis without PML on its low side")
-    if offdiag is not None and len(getattr(offdiag, "comp", ())):
-        raise NotImplementedError("conformal off-diagonal terms have no CUDA path in lightsmith-b200")
     if time_monitors:
         raise NotImplementedError("time monitors have no CUDA path in lightsmith-b200")
     periodic = tuple(bool(p) for p in periodic)
@@ -444,6 +562,11 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
     }
     if any(mirror):  # only then (plans without mirror planes keep their earlier form)
         plan["mirror"] = mirror
+    if offdiag is not None and len(getattr(offdiag, "comp", ())):
+        gidx = np.concatenate([g["idx"] for g in grp]) if grp else np.zeros(0, np.int64)
+        tab = offdiag_tables(offdiag, shape, spacing, dt, periodic, bloch, mirror, gidx, any(bloch))
+        if tab is not None:
+            plan["offdiag"] = {"e": tab[0], "h": tab[1], "w": tab[2]}
     mons = []
     for m in monitors:
         space = _monitor_space(m.source, sources, plan["sources"])

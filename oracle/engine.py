@@ -222,6 +222,11 @@ class OracleEngine:
         for t, g, s in self._mirror_ghosts:
             self.H[t][g] = -self.H[t][s]
         self._parallel(lambda a, b: self._update("E", a, b), 0, self.shape[0])
+        od = self.plan.get("offdiag")
+        if od is not None:  # conformal off-diagonal terms (engine.py:653-655; added here after the CPML terms,
+            # which changes only the order of the additions)
+            Ef, Hf = self.E.reshape(-1), self.H.reshape(-1)
+            Ef[od["e"]] += np.sum(np.asarray(od["w"]) * Hf[od["h"]], axis=1)
 
     # --- step order (engine.py:665-683) -----------------------------------------------------------------
     def step(self):

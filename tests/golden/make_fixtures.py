@@ -83,6 +83,8 @@ def run_engine_case(name: str, kw: dict, n_chunks: int, snap: int = 1):
            "n_chunks": n_chunks, "snap": snap, **snaps,
            "acc_e": [np.asarray(m.acc_e) for m in kw["monitors"]],
            "acc_h": [np.zeros(0) if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]}
+    if getattr(eng, "od", None) is not None:  # the reference's off-diagonal gather tables
+        out["od_e"], out["od_h"], out["od_w"] = (np.asarray(x) for x in eng.od)
     for src in kw["sources"]:
         if hasattr(src, "col"):
             out["col_E"], out["col_H"] = np.asarray(src.col.E), np.asarray(src.col.H)
@@ -150,6 +152,58 @@ def case_mirror():
     kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[dip],
               monitors=mons, dft_stride=3, mirror=(1, -1, 1))
     run_engine_case("mirror", kw, 10, snap=2)
+
+
+def _offdiag_rows(rng, shape, n):
+    """n random conformal rows: E_comp at interior nodes, small random (1/eps)_cd with column comp zero."""
+    idx3 = np.stack([rng.integers(2, s - 3, n) for s in shape], axis=1)
+    comp = rng.integers(0, 3, n)
+    coef = rng.uniform(-0.06, 0.06, (n, 3))
+    coef[np.arange(n), comp] = 0.0
+    return ref_engine.OffDiagonal(idx3, comp, coef)
+
+
+def case_offdiag():
+    """Conformal off-diagonal 1/eps terms (engine.py:421-518, 653-655) on random rows, with a pure Drude-Lorentz
+    group overlapping some of them (their couplings are dropped) and CPML on every face."""
+    rng = np.random.default_rng(9)
+    shape, dx = (16, 15, 14), 5.0
+    dt = 0.99 * dx / np.sqrt(3)
+    ie = 1.0 / rng.uniform(1.0, 6.0, size=(3,) + shape)
+    pml = ref_engine.PMLSpec(cells=((3, 3), (3, 3), (3, 3)), alpha_max=0.02, eps_ref=1.5)
+    om = 2 * np.pi / np.array([300.0, 450.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(31.3, 33.7, 26.2), pdir=(0.4, 0.8, 0.3),
+                      inv_eps=ie, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    cells = int(np.prod(shape))
+    node = np.ravel_multi_index(np.meshgrid(np.arange(9, 11), np.arange(5, 7), np.arange(6, 8), indexing="ij"),
+                                shape).ravel()
+    idx = np.concatenate([c * cells + node for c in range(3)])
+    ie.reshape(3, -1)[:, node] = 1.0
+    grp = ref_engine.DispersiveGroup(idx=idx, media=[METAL], frac=np.ones((1, len(idx))), w=None)
+    mons = [plane_monitor(shape, 8, om, 1)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[grp], pml=pml, sources=[dip],
+              monitors=mons, dft_stride=3, offdiag=_offdiag_rows(rng, shape, 240))
+    run_engine_case("offdiag", kw, 10, snap=2)
+
+
+def case_offdiag_mirror():
+    """Off-diagonal terms with mirror planes (symmetric along x, antisymmetric along y): the rows' images and
+    the folded sources (engine.py:475-483, 540-553)."""
+    rng = np.random.default_rng(10)
+    shape, dx = (14, 15, 16), 5.0
+    dt = 0.99 * dx / np.sqrt(3)
+    ie = 1.0 / rng.uniform(1.0, 6.0, size=(3,) + shape)
+    pml = ref_engine.PMLSpec(cells=((0, 3), (0, 3), (3, 3)), alpha_max=0.02, eps_ref=1.5)
+    om = 2 * np.pi / np.array([300.0, 450.0])
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(22.3, 31.7, 41.2), pdir=(0.6, 0.3, 0.7),
+                      inv_eps=ie, omega_c=om.mean(), omega_half=0.5 * np.ptp(om), max_steps=20000)
+    od = _offdiag_rows(rng, shape, 200)
+    od.idx3[:40, 0] = 1  # rows on the symmetric plane
+    od.idx3[40:70, 1] = 1  # and on the antisymmetric one
+    mons = [plane_monitor(shape, 9, om, 1)]
+    kw = dict(shape=shape, dx=dx, dt=dt, single=False, inv_eps=ie, groups=[], pml=pml, sources=[dip],
+              monitors=mons, dft_stride=3, mirror=(1, -1, 0), offdiag=od)
+    run_engine_case("offdiag_mirror", kw, 10, snap=2)
 
 
 def sphere_slot_fn(center, radius, slot=1):
@@ -355,12 +409,23 @@ def sphere_problem(mesh: str, symmetry: str = "off"):
                                                run_time_fs=399.5 * 2.2863 / 299.792458)})
 
 
+def dielectric_sphere_problem():
+    """A non-dispersive sphere (n = 2, radius 16 nm) in n = 1.33 with conformal interfaces (off-diagonal 1/eps)."""
+    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
+                         medium_index=1.33, wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
+                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry="off",
+                                               mesh_refinement="conformal", padding_nm=8.0, pml_gap_nm=8.0,
+                                               dft_stride=10, run_time_fs=399.5 * 2.2863 / 299.792458)})
+
+
 CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_noncubic,
          "ade_groups": case_ade_groups, "tfsf_table": case_tfsf_table, "line_periodic": case_line_periodic,
          "bloch_column": case_bloch_column, "mode_source": case_mode_source, "mirror": case_mirror,
+         "offdiag": case_offdiag, "offdiag_mirror": case_offdiag_mirror,
          "solve_sphere_staircase": lambda: solve_case("sphere_staircase", sphere_problem("staircase")),
          "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel")),
-         "solve_sphere_symmetric": lambda: solve_case("sphere_symmetric", sphere_problem("staircase", "auto"))}
+         "solve_sphere_symmetric": lambda: solve_case("sphere_symmetric", sphere_problem("staircase", "auto")),
+         "solve_dielectric_conformal": lambda: solve_case("dielectric_conformal", dielectric_sphere_problem())}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

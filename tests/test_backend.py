@@ -136,3 +136,30 @@ def test_solve_on_cuda_without_a_gpu_fails_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError, match="CUDA"):
         B.B200FDTD.solve(sphere(), CUDA0)
+
+
+def dielectric_sphere(mesh="conformal"):
+    """A non-dispersive sphere (n = 2) in n = 1.33: conformal interfaces take off-diagonal 1/eps terms."""
+    fdtd = dict(spacing_nm=4.0, pml_cells=8, symmetry="off", mesh_refinement=mesh, padding_nm=8.0,
+                pml_gap_nm=8.0, dft_stride=10, run_time_fs=399.5 * 2.2863 / 299.792458)
+    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
+                         medium_index=1.33, wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
+                         options={"fdtd": fdtd})
+
+
+def test_conformal_dielectric_reaches_the_cuda_engine_with_its_offdiagonal_terms(monkeypatch):
+    """mesh_refinement='conformal' on a dielectric: supported, and the driver's OffDiagonal rows arrive as the
+    plan's gather tables."""
+    assert B.B200FDTD.supports(dielectric_sphere()) == (True, "")
+    seen = {}
+
+    class Recorder:
+        def __init__(self, device, **kw):
+            seen["plan"] = P.make_plan(**kw)
+            raise _Recorded
+
+    monkeypatch.setattr(B._engine, "Engine", Recorder)
+    with pytest.raises(_Recorded):
+        B.B200FDTD.solve(dielectric_sphere(), CUDA0)
+    od = seen["plan"]["offdiag"]
+    assert len(od["e"]) > 0 and od["h"].shape == od["w"].shape and od["h"].shape[1] % 4 == 0

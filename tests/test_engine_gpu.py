@@ -79,7 +79,7 @@ def test_source_waveform_end_raises(golden):
 
 
 # cases the fused single pass serves (no periodic axis, point-dipole sources)
-FUSED_CASES = ["yee_cpml_dipole", "kappa_noncubic", "ade_groups"]
+FUSED_CASES = ["yee_cpml_dipole", "kappa_noncubic", "ade_groups", "offdiag"]
 
 
 @pytest.mark.parametrize("variant,tile_y,planes,stages", [(1, 8, 3, 4), (1, 16, 5, 6), (1, 16, 128, 8), (1, 8, 2, 8),

@@ -60,3 +60,15 @@ def test_oracle_detects_a_planted_mistake(golden):
     for _ in range(d["out"]["n_chunks"]):
         eng.chunk()
     assert _rel(eng.H, d["out"]["H"]) > 1e-6
+
+
+@pytest.mark.parametrize("case", ["offdiag", "offdiag_mirror"])
+def test_offdiag_gather_tables_equal_the_reference(case, golden):
+    """The plan builder's conformal off-diagonal gather tables (targets, H indices, weights) against the ones
+    lightsmith's engine built from the same rows (engine.py:421-518), mirror planes and a dispersive group
+    included."""
+    d = golden("engine_" + case)
+    od, out = d["plan"]["offdiag"], d["out"]
+    assert np.array_equal(od["e"], out["od_e"])
+    assert np.array_equal(od["h"], out["od_h"])
+    assert np.array_equal(od["w"], out["od_w"])
