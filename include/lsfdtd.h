@@ -234,6 +234,44 @@ typedef struct {
   int32_t width;
 } lsfdtd_offdiag_desc;
 int32_t lsfdtd_engine_add_offdiag(lsfdtd_engine* eng, const lsfdtd_offdiag_desc* d);
+
+/* The vertex-tensor ADE of conformal interfaces with dispersive media (TensorMesh and _Tensor,
+ * engine.py:140-175, 796-923), stepped after the D-form groups, as index tables
+ * (lightsmith_b200/plan.py:tensor_plan): nodes (their flat E indices), vertices (each one's six d-node numbers
+ * with their phase and parity, and its normal), tensor slots (output position, vertex, vertex * 3 + c, the node
+ * position among the vertex's six, the normal's component, the conjugate phase, the vertex's medium fractions)
+ * and plain slots (output position, node, medium). Device arrays in the field's (real) precision where not
+ * int64; `state` is zeroed, lsfdtd_tensor_state_len() field scalars. At most one mesh per engine. */
+typedef struct {
+  const int64_t* idx;
+  int64_t n_nodes;
+  const int64_t* vn;      /* (n_vert * 6) */
+  const void* scale;      /* (n_vert * 6) field precision, or NULL (no Bloch phase and no mirror) */
+  const void* normal;     /* (n_vert * 3) real */
+  int64_t n_vert;
+  const int64_t* t_pos;   /* (n_tslots) */
+  const int64_t* t_v;
+  const int64_t* t_vc;
+  const int64_t* t_g;
+  const void* t_nc;       /* (n_tslots) real */
+  const void* t_conj;     /* (n_tslots) field precision, or NULL for real fields */
+  const void* frac;       /* (n_media, n_tslots) real */
+  int64_t n_tslots;
+  const int64_t* p_pos;   /* (n_pslots) */
+  const int64_t* p_node;
+  const int64_t* p_medium;
+  int64_t n_pslots;
+  int32_t n_media;
+  int32_t n_poles[LSFDTD_MAX_MEDIA];
+  double eps_inf[LSFDTD_MAX_MEDIA];
+  double c1[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  double c2[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  double c3[LSFDTD_MAX_MEDIA][LSFDTD_MAX_POLES];
+  void* state;
+} lsfdtd_tensor_desc;
+int64_t lsfdtd_tensor_state_len(int64_t n_nodes, int64_t n_vert, int64_t n_tslots, int64_t n_pslots,
+                                int32_t n_media, const int32_t* n_poles);
+int32_t lsfdtd_engine_add_tensor(lsfdtd_engine* eng, const lsfdtd_tensor_desc* d);
 /* sources act in the order they are added (Engine.step, engine.py:665-678) */
 int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s);
 int32_t lsfdtd_engine_add_dipole(lsfdtd_engine* eng, const lsfdtd_dipole_desc* s);

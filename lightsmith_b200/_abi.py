@@ -34,6 +34,15 @@ class OffdiagDesc(C.Structure):
     _fields_ = [("e", vp), ("h", vp), ("w", vp), ("n", i64), ("width", i32)]
 
 
+class TensorDesc(C.Structure):
+    _fields_ = [("idx", vp), ("n_nodes", i64), ("vn", vp), ("scale", vp), ("normal", vp), ("n_vert", i64),
+                ("t_pos", vp), ("t_v", vp), ("t_vc", vp), ("t_g", vp), ("t_nc", vp), ("t_conj", vp), ("frac", vp),
+                ("n_tslots", i64), ("p_pos", vp), ("p_node", vp), ("p_medium", vp), ("n_pslots", i64),
+                ("n_media", i32), ("n_poles", i32 * MAX_MEDIA), ("eps_inf", f64 * MAX_MEDIA),
+                ("c1", (f64 * MAX_POLES) * MAX_MEDIA), ("c2", (f64 * MAX_POLES) * MAX_MEDIA),
+                ("c3", (f64 * MAX_POLES) * MAX_MEDIA), ("state", vp)]
+
+
 class PmlDesc(C.Structure):
     _fields_ = [("axis", i32), ("cells_lo", i32), ("cells_hi", i32), ("b", vp * 2), ("c", vp * 2), ("k", vp * 2),
                 ("psi", ((vp * 2) * 3) * 2), ("psi_alt", (vp * 2) * 3)]
@@ -102,6 +111,8 @@ SIGNATURES = {
     "lsfdtd_engine_set_pml": (i32, [vp, C.POINTER(PmlDesc)]),
     "lsfdtd_engine_add_group": (i32, [vp, C.POINTER(GroupDesc)]),
     "lsfdtd_engine_add_offdiag": (i32, [vp, C.POINTER(OffdiagDesc)]),
+    "lsfdtd_engine_add_tensor": (i32, [vp, C.POINTER(TensorDesc)]),
+    "lsfdtd_tensor_state_len": (i64, [i64, i64, i64, i64, i32, C.POINTER(i32)]),
     "lsfdtd_engine_add_table_source": (i32, [vp, C.POINTER(TableSourceDesc)]),
     "lsfdtd_engine_add_dipole": (i32, [vp, C.POINTER(DipoleDesc)]),
     "lsfdtd_engine_add_line_source": (i32, [vp, C.POINTER(LineSourceDesc)]),

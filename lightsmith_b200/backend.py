@@ -12,8 +12,8 @@ It is lightsmith's ``NativeFDTD`` with one part swapped: on a CUDA device, the p
 (setup.py:722-773) and the post-processing (cross sections, orders, S-parameters) are lightsmith's own.
 
 On a CPU device the class is ``NativeFDTD`` unchanged: this package adds no CPU path. On a CUDA device there is
-no fallback: a problem that needs a feature with no CUDA path here (graded grids, conformal interfaces of
-dispersive media (vertex-tensor ADE), time monitors, substrates, Gaussian beams) is rejected by ``supports`` or raises
+no fallback: a problem that needs a feature with no CUDA path here (graded grids, time monitors, substrates,
+Gaussian beams) is rejected by ``supports`` or raises
 ``ValueError`` when its engine is built, and a missing or unloadable ``liblsfdtd.so`` raises from the engine.
 """
 
@@ -61,25 +61,8 @@ def _engine_swapped():
                 m.Engine = e
 
 
-def _dispersive(material, wavelengths) -> bool:
-    """Whether lightsmith integrates a material with ADE poles (media.py:94-120); unknown counts as yes."""
-    from lightsmith.backends._fdtd.media import to_medium
-
-    try:
-        return bool(to_medium(material, wavelengths, []).poles)
-    except Exception:  # noqa: BLE001 (a material the conversion cannot take is rejected, not run)
-        return True
-
-
 def _static_rejection(sim, opts) -> str:
     """Features known from the problem and its options alone that have no CUDA path here ('' if none)."""
-    if opts.mesh_refinement == "conformal" and isinstance(sim, Simulation):
-        # dielectric interfaces take off-diagonal 1/eps terms (built here); a dispersive particle's interface
-        # takes lightsmith's vertex-tensor ADE (setup.py:254, 325-420), which has no CUDA path
-        wl = sim.wavelength_array()
-        if any(_dispersive(p.material, wl) for p in sim.particles):
-            return ("does not support mesh_refinement='conformal' with dispersive particles (vertex-tensor ADE) "
-                    "on the GPU")
     if isinstance(sim, (Simulation, DeviceProblem)) and _scattering_driver.graded(opts):
         return "does not support graded grids (grid='auto', mesh_override) on the GPU"
     if isinstance(sim, Simulation):

@@ -23,6 +23,7 @@
 #include "fused_pml.cuh"
 #include "fused_tma.cuh"
 #include "shell.cuh"
+#include "tensor.cuh"
 #include "yee_vec.cuh"
 
 #include <cudaTypedefs.h>
@@ -129,6 +130,7 @@ struct lsfdtd_engine {
   virtual int set_pml(const lsfdtd_pml_desc* p) = 0;
   virtual int add_group(const lsfdtd_group_desc* g) = 0;
   virtual int add_offdiag(const lsfdtd_offdiag_desc* d) = 0;
+  virtual int add_tensor(const lsfdtd_tensor_desc* d) = 0;
   virtual int add_table(const lsfdtd_table_source_desc* s) = 0;
   virtual int add_dipole(const lsfdtd_dipole_desc* s) = 0;
   virtual int add_line(const lsfdtd_line_source_desc* s) = 0;
@@ -538,6 +540,7 @@ struct Engine final : lsfdtd_engine {
     if (desc.mirror[0] || desc.mirror[1] || desc.mirror[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
     if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no conformal off-diagonal terms");
+    if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no vertex-tensor mesh");
     if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
     for (auto& gr : groups)
@@ -561,6 +564,7 @@ struct Engine final : lsfdtd_engine {
         return fail(LSFDTD_EUNSUPPORTED, "batch: a run must be periodic along x and y, not z");
       if (desc.mirror[2]) return fail(LSFDTD_EUNSUPPORTED, "batch: no mirror plane");
       if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "batch: no conformal off-diagonal terms");
+      if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "batch: no vertex-tensor mesh");
       if (y.pml[0].on || y.pml[1].on) return fail(LSFDTD_EUNSUPPORTED, "batch: CPML along z only");
       if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "batch: dispersive groups have no batched path");
       if (order.size() != 1 || order[0].first != kColumn)
@@ -677,6 +681,128 @@ struct Engine final : lsfdtd_engine {
   int offdiag(cudaStream_t s) {
     if (od_n <= 0) return LSFDTD_OK;
     k_offdiag<F><<<cdiv(od_n, 256), 256, 0, s>>>(od_e, od_h, od_w, od_n, od_width, Eflat(), Hflat());
+    LS_LAUNCHED();
+    return LSFDTD_OK;
+  }
+
+  // the vertex-tensor mesh (at most one)
+  bool has_tensor = false;
+  TensorArgs<F> tm{};
+  int add_tensor(const lsfdtd_tensor_desc* d) override {
+    if (has_tensor) return fail(LSFDTD_EINVAL, "tensor: one mesh per engine");
+    if (d->n_media < 1 || d->n_media > kMaxMedia) return fail(LSFDTD_EINVAL, "tensor: media count out of range");
+    if (d->n_nodes < 0 || d->n_vert < 0 || d->n_tslots < 0 || d->n_pslots < 0)
+      return fail(LSFDTD_EINVAL, "tensor: sizes out of range");
+    if (d->n_nodes > 0 && (!d->idx || !d->state)) return fail(LSFDTD_EINVAL, "tensor: arrays missing");
+    if (d->n_vert > 0 && (!d->vn || !d->normal)) return fail(LSFDTD_EINVAL, "tensor: vertex arrays missing");
+    if (d->n_tslots > 0 && (!d->t_pos || !d->t_v || !d->t_vc || !d->t_g || !d->t_nc || !d->frac))
+      return fail(LSFDTD_EINVAL, "tensor: slot arrays missing");
+    if (d->n_pslots > 0 && (!d->p_pos || !d->p_node || !d->p_medium))
+      return fail(LSFDTD_EINVAL, "tensor: plain slot arrays missing");
+    if (kComplex && d->n_tslots > 0 && !d->t_conj) return fail(LSFDTD_EINVAL, "tensor: complex fields need t_conj");
+    // index ranges, once (the kernels trust them)
+    const long long flat = 3LL * desc.shape[0] * desc.shape[1] * desc.shape[2];
+    auto check = [&](const int64_t* a, long long n, long long hi, const char* what) -> int {
+      if (n <= 0) return LSFDTD_OK;
+      std::vector<long long> h(n);
+      LS_CUDA(cudaMemcpy(h.data(), a, n * sizeof(long long), cudaMemcpyDeviceToHost));
+      for (long long v : h)
+        if (v < 0 || v >= hi) return fail(LSFDTD_ERANGE, std::string("tensor: an index out of range: ") + what);
+      return LSFDTD_OK;
+    };
+    LS_TRY(check(d->idx, d->n_nodes, flat, "idx"));
+    LS_TRY(check(d->vn, 6 * d->n_vert, d->n_nodes, "vn"));
+    LS_TRY(check(d->t_pos, d->n_tslots, 2 * d->n_nodes, "t_pos"));
+    LS_TRY(check(d->t_v, d->n_tslots, d->n_vert, "t_v"));
+    LS_TRY(check(d->t_vc, d->n_tslots, 3 * d->n_vert, "t_vc"));
+    LS_TRY(check(d->t_g, d->n_tslots, 6 * d->n_vert, "t_g"));
+    LS_TRY(check(d->p_pos, d->n_pslots, 2 * d->n_nodes, "p_pos"));
+    LS_TRY(check(d->p_node, d->n_pslots, d->n_nodes, "p_node"));
+    LS_TRY(check(d->p_medium, d->n_pslots, d->n_media, "p_medium"));
+    TensorArgs<F> a{};
+    a.idx = reinterpret_cast<const long long*>(d->idx);
+    a.nN = d->n_nodes;
+    a.nV = d->n_vert;
+    a.nT = d->n_tslots;
+    a.nP = d->n_pslots;
+    a.vn = reinterpret_cast<const long long*>(d->vn);
+    a.scale = static_cast<const F*>(d->scale);
+    a.normal = static_cast<const R*>(d->normal);
+    a.t_pos = reinterpret_cast<const long long*>(d->t_pos);
+    a.t_v = reinterpret_cast<const long long*>(d->t_v);
+    a.t_vc = reinterpret_cast<const long long*>(d->t_vc);
+    a.t_g = reinterpret_cast<const long long*>(d->t_g);
+    a.t_nc = static_cast<const R*>(d->t_nc);
+    a.t_conj = static_cast<const F*>(d->t_conj);
+    a.frac = static_cast<const R*>(d->frac);
+    a.p_pos = reinterpret_cast<const long long*>(d->p_pos);
+    a.p_node = reinterpret_cast<const long long*>(d->p_node);
+    a.p_medium = reinterpret_cast<const long long*>(d->p_medium);
+    a.n_media = d->n_media;
+    for (int s = 0; s < d->n_media; ++s) {
+      if (d->n_poles[s] < 0 || d->n_poles[s] > kMaxPoles) return fail(LSFDTD_EINVAL, "tensor: pole count out of range");
+      if (!(d->eps_inf[s] > 0)) return fail(LSFDTD_EINVAL, "tensor: eps_inf must be positive");
+      a.n_poles[s] = d->n_poles[s];
+      a.eps_inf[s] = R(d->eps_inf[s]);
+      a.inv_inf[s] = R(1.0 / d->eps_inf[s]);
+      for (int k = 0; k < d->n_poles[s]; ++k) {
+        a.c1[s][k] = R(d->c1[s][k]);
+        a.c2[s][k] = R(d->c2[s][k]);
+        a.c3[s][k] = R(d->c3[s][k]);
+      }
+    }
+    // the state buffer, in lsfdtd_tensor_state_len's order
+    F* st = static_cast<F*>(d->state);
+    a.D = st;
+    st += a.nN;
+    a.Ep = st;
+    st += a.nN;
+    a.out = st;
+    st += 2 * a.nN;
+    a.dbar = st;
+    st += 3 * a.nV;
+    a.sv = st;
+    st += a.nV;
+    for (int s = 0; s < a.n_media; ++s) {
+      a.ha_E[s] = st;
+      st += a.nT;
+      a.ha_P[s] = st;
+      st += 2LL * a.n_poles[s] * a.nT;
+    }
+    a.ar_y = st;
+    st += a.nT;
+    for (int s = 0; s < a.n_media; ++s) {
+      a.ar_P[s] = st;
+      st += 2LL * a.n_poles[s] * a.nT;
+    }
+    for (int s = 0; s < a.n_media; ++s) {
+      a.pl_E[s] = st;
+      st += a.nP;
+      a.pl_P[s] = st;
+      st += 2LL * a.n_poles[s] * a.nP;
+    }
+    tm = a;
+    has_tensor = a.nN > 0;
+    return LSFDTD_OK;
+  }
+  int tensor_step(cudaStream_t s) {
+    TensorArgs<F> a = tm;
+    a.E = Eflat();
+    k_tm_nodes_d<F><<<cdiv(a.nN, 256), 256, 0, s>>>(a);
+    LS_LAUNCHED();
+    if (a.nV > 0) {
+      k_tm_vertices<F><<<cdiv(a.nV, 256), 256, 0, s>>>(a);
+      LS_LAUNCHED();
+    }
+    if (a.nT > 0) {
+      k_tm_slots<F><<<cdiv(a.nT, 256), 256, 0, s>>>(a);
+      LS_LAUNCHED();
+    }
+    if (a.nP > 0) {
+      k_tm_plain<F><<<cdiv(a.nP, 256), 256, 0, s>>>(a);
+      LS_LAUNCHED();
+    }
+    k_tm_nodes_e<F><<<cdiv(a.nN, 256), 256, 0, s>>>(a);
     LS_LAUNCHED();
     return LSFDTD_OK;
   }
@@ -1110,6 +1236,7 @@ struct Engine final : lsfdtd_engine {
       k_ade<F><<<cdiv(ga.n, 128), 128, 0, s>>>(ga);
       LS_LAUNCHED();
     }
+    if (has_tensor) LS_TRY(tensor_step(s));
     LS_TRY(hook(3, s));
     k_bump<<<1, 32, 0, s>>>(reinterpret_cast<long long*>(desc.step));
     LS_LAUNCHED();
@@ -1159,6 +1286,7 @@ struct Engine final : lsfdtd_engine {
     per_step += 2 * nper;
     for (int a = 0; a < 3; ++a) per_step += desc.mirror[a] > 0;  // mirror ghost planes
     per_step += od_n > 0;  // the off-diagonal gather
+    if (has_tensor) per_step += 2 + (tm.nV > 0) + (tm.nT > 0) + (tm.nP > 0);
     for (auto& g : groups) per_step += g.n > 0;
     for (auto& o : order) {
       switch (o.first) {
@@ -1411,6 +1539,21 @@ int32_t lsfdtd_engine_add_group(lsfdtd_engine* eng, const lsfdtd_group_desc* g) 
 int32_t lsfdtd_engine_add_offdiag(lsfdtd_engine* eng, const lsfdtd_offdiag_desc* d) {
   LS_NEED(eng && d);
   return eng->add_offdiag(d);
+}
+int64_t lsfdtd_tensor_state_len(int64_t n_nodes, int64_t n_vert, int64_t n_tslots, int64_t n_pslots, int32_t n_media,
+                                const int32_t* n_poles) {
+  if (n_media < 1 || n_media > kMaxMedia || !n_poles || n_nodes < 0 || n_vert < 0 || n_tslots < 0 || n_pslots < 0)
+    return -1;
+  int64_t len = 4 * n_nodes + 4 * n_vert + n_tslots;
+  for (int s = 0; s < n_media; ++s) {
+    if (n_poles[s] < 0 || n_poles[s] > kMaxPoles) return -1;
+    len += n_tslots * (1 + 2LL * n_poles[s]) + n_tslots * 2LL * n_poles[s] + n_pslots * (1 + 2LL * n_poles[s]);
+  }
+  return len;
+}
+int32_t lsfdtd_engine_add_tensor(lsfdtd_engine* eng, const lsfdtd_tensor_desc* d) {
+  LS_NEED(eng && d);
+  return eng->add_tensor(d);
 }
 int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s) {
   LS_NEED(eng && s);

@@ -142,6 +142,8 @@ class Engine:
             self._h = h
             self._build_pml(plan, L)
             self.groups = [self._build_group(gr, L) for gr in plan["groups"]]
+            if plan.get("tensor") is not None:  # conformal interfaces of dispersive media (engine.py:838-923)
+                self._build_tensor(plan["tensor"], L)
             od = plan.get("offdiag")
             if od is not None and len(od["e"]):  # conformal off-diagonal terms (engine.py:421-518, 653-655)
                 torch = _torch()
@@ -255,6 +257,52 @@ class Engine:
         g.state = _ptr(state)
         _abi.check(L.lsfdtd_engine_add_group(self._h, C.byref(g)), "lsfdtd_engine_add_group")
         return {"idx": idx, "state": state, "mixed": bool(g.mixed)}
+
+    def _build_tensor(self, t, L):
+        """The vertex-tensor mesh's tables (plan.py:tensor_plan) on the device and its zeroed state."""
+        torch = _torch()
+        i64 = torch.int64
+        d = _abi.TensorDesc()
+        keep = {}
+
+        def arr(name, dtype):
+            a = t[name]
+            if a is None or not len(a):
+                return None
+            keep[name] = self._dev(np.asarray(a), dtype)
+            return _ptr(keep[name])
+
+        d.idx, d.n_nodes = arr("idx", i64), int(t["n_nodes"])
+        d.vn, d.scale, d.normal = arr("vn", i64), arr("scale", self.fdt), arr("normal", self.rdt)
+        d.n_vert = len(np.asarray(t["normal"])) // 3
+        for k in ("t_pos", "t_v", "t_vc", "t_g"):
+            setattr(d, k, arr(k, i64))
+        d.t_nc, d.t_conj = arr("t_nc", self.rdt), arr("t_conj", self.fdt)
+        d.frac = arr("frac", self.rdt)
+        d.n_tslots = len(t["t_pos"])
+        d.p_pos, d.p_node, d.p_medium = arr("p_pos", i64), arr("p_node", i64), arr("p_medium", i64)
+        d.n_pslots = len(t["p_pos"])
+        media = t["media"]
+        if len(media) > _abi.MAX_MEDIA:
+            raise ValueError(f"at most {_abi.MAX_MEDIA} media in a vertex-tensor mesh")
+        d.n_media = len(media)
+        npoles = []
+        for s, m in enumerate(media):
+            if len(m["poles"]) > _abi.MAX_POLES:
+                raise ValueError(f"at most {_abi.MAX_POLES} poles per medium")
+            npoles.append(len(m["poles"]))
+            d.n_poles[s] = len(m["poles"])
+            d.eps_inf[s] = float(m["eps_inf"])
+            for k, pole in enumerate(m["poles"]):
+                d.c1[s][k], d.c2[s][k], d.c3[s][k] = pole_coefficients(_Pole(*pole), self.dt)
+        arr_np = (C.c_int32 * _abi.MAX_MEDIA)(*(npoles + [0] * (_abi.MAX_MEDIA - len(npoles))))
+        n = int(L.lsfdtd_tensor_state_len(d.n_nodes, d.n_vert, d.n_tslots, d.n_pslots, d.n_media, arr_np))
+        if n < 0:
+            raise ValueError("vertex-tensor mesh sizes out of range")
+        state = self._zeros((max(n, 1),), self.fdt)
+        d.state = _ptr(state)
+        _abi.check(L.lsfdtd_engine_add_tensor(self._h, C.byref(d)), "lsfdtd_engine_add_tensor")
+        self.tensor = {"state": state, **keep}
 
     def _points(self, pts, fields):
         """CSR device arrays of a TablePoints/LinePoints (fields: its per-entry arrays and their dtypes)."""

@@ -522,6 +522,42 @@ def offdiag_tables(od, shape, spacing, dt, periodic, bloch, mirror, group_idx, c
     return targets.astype(np.int64), h, (w if complex_fields else w.real)
 
 
+def tensor_plan(tm, shape, spacing, bloch, complex_fields) -> dict:
+    """The vertex-tensor ADE of conformal interfaces with dispersive media (``TensorMesh``, ``_Tensor``,
+    ``engine.py:140-175, 838-923``) as flat index tables, cubic or rectangular cells (no graded axes).
+
+    Per step: each node's D += E - E_prev; per vertex v the mean D~ of its two d-nodes for every d (their
+    values times a Bloch phase and mirror parity, ``scale``) and s = n . D~; per tensor slot (a node next to
+    v) sigma = s + n_c (D_p - D~_c) and out = (1/2) (b[D_p - n_c sigma] + n_c a[sigma]) (times the conjugate
+    phase under a Bloch wavevector), a (``_Harmonic``) and b (``_Arithmetic``) with their own pole states and
+    the vertex's medium fractions; per plain slot out = (1/2) medium[D] of its one medium; a node's E is the sum
+    of its two slots."""
+    nN, nV = len(tm.node_comp), len(tm.normal)
+    idx = np.asarray(tm.idx, np.int64)
+    L = np.array([(n - 2) * d for n, d in zip(shape, spacing)])
+    ph = np.exp(1j * (np.asarray(tm.shift) * (np.asarray(bloch, float) * L)).sum(-1))  # (nV, 3, 2)
+    scale = ph if complex_fields else np.ones(ph.shape)
+    if tm.sign is not None:
+        scale = scale * np.asarray(tm.sign, float)
+    sv = np.asarray(tm.slot_vert)
+    tk, tnode = np.nonzero((sv >= 0).T)  # slots ordered (k, node)
+    tv = sv[tnode, tk]
+    tc = np.asarray(tm.node_comp)[tnode]
+    side = 1 - tk
+    nrm = np.asarray(tm.normal, float)
+    pk, pnode = np.nonzero((sv < 0).T)
+    out = {"idx": idx, "n_nodes": nN, "vn": np.asarray(tm.vert_nodes, np.int64).reshape(-1),
+           "normal": nrm.reshape(-1), "t_pos": (tk * nN + tnode).astype(np.int64), "t_v": tv.astype(np.int64),
+           "t_vc": (tv * 3 + tc).astype(np.int64), "t_g": ((tv * 3 + tc) * 2 + side).astype(np.int64),
+           "t_nc": nrm[tv, tc], "frac": np.asarray(tm.frac, float)[:, tv],
+           "p_pos": (pk * nN + pnode).astype(np.int64), "p_node": pnode.astype(np.int64),
+           "p_medium": np.asarray(tm.slot_medium, np.int64)[pnode, pk], "media": _media_plan(tm.media)}
+    scaled = complex_fields or tm.sign is not None
+    out["scale"] = (scale.reshape(-1) if complex_fields else scale.real.reshape(-1)) if scaled else None
+    out["t_conj"] = np.conj(ph[tv, tc, side]) if complex_fields else None
+    return out
+
+
 def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors, dft_stride,
               periodic=(False, False, False), bloch=(0.0, 0.0, 0.0), offdiag=None, time_monitors=(),
               mirror=(0, 0, 0), widths=None) -> dict:
@@ -543,10 +579,13 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
     bloch = tuple(float(k) for k in bloch)
     if any(k and not p for k, p in zip(bloch, periodic)):
         raise ValueError("a Bloch wavevector needs a periodic axis")
-    grp = []
+    grp, tensor = [], None
     for g in groups:
         if type(g).__name__ == "TensorMesh":
-            raise NotImplementedError("vertex-tensor (conformal metal) groups have no CUDA path in lightsmith-b200")
+            if tensor is not None:
+                raise NotImplementedError("more than one vertex-tensor mesh")
+            tensor = g
+            continue
         grp.append({"idx": np.asarray(g.idx, np.int64), "media": _media_plan(g.media),
                     "frac": np.asarray(g.frac, float), "w": None if g.w is None else np.asarray(g.w, float)})
     plan = {
@@ -562,8 +601,11 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
     }
     if any(mirror):  # only then (plans without mirror planes keep their earlier form)
         plan["mirror"] = mirror
+    if tensor is not None:
+        plan["tensor"] = tensor_plan(tensor, shape, spacing, bloch, any(bloch))
     if offdiag is not None and len(getattr(offdiag, "comp", ())):
-        gidx = np.concatenate([g["idx"] for g in grp]) if grp else np.zeros(0, np.int64)
+        gidx = [g["idx"] for g in grp] + ([plan["tensor"]["idx"]] if tensor is not None else [])
+        gidx = np.concatenate(gidx) if gidx else np.zeros(0, np.int64)
         tab = offdiag_tables(offdiag, shape, spacing, dt, periodic, bloch, mirror, gidx, any(bloch))
         if tab is not None:
             plan["offdiag"] = {"e": tab[0], "h": tab[1], "w": tab[2]}

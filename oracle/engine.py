@@ -76,6 +76,8 @@ class OracleEngine:
         self.inv_d = tuple(1.0 / d for d in self.spacing)
         self._build_pml(inv_eps, cdx)
         self.groups = [_Group(self, g) for g in plan["groups"]]
+        if plan.get("tensor") is not None:  # the vertex-tensor mesh steps after the D-form groups
+            self.groups.append(_TensorMesh(self, plan["tensor"]))
         self.sources = [self._bind_source(s) for s in plan["sources"]]
         self.monitors = []
         for m in plan["monitors"]:
@@ -373,6 +375,103 @@ class _Group:
                 self.Ea[...] = acc * self.inv_a
                 parts.append((1 - self.w) * self.Ea)
             e_new = parts[0] if len(parts) == 1 else parts[0] + parts[1]
+        Ef[self.idx] = e_new
+        self.E_prev[...] = e_new
+
+
+class _Harmonic:
+    """<1/eps>[u] over slots with medium fractions F (S, n) (engine.py:796-818): y = sum_s F_s E_s with
+    E_s = (u - P_s) / eps_inf_s, each dispersive medium's poles driven by its own E_s of the step before."""
+
+    def __init__(self, eng, media, F):
+        n = F.shape[1]
+        self.h0 = sum(F[s] / m["eps_inf"] for s, m in enumerate(media) if not m["poles"]) + 0 * F[0]
+        self.disp = [s for s, m in enumerate(media) if m["poles"] and np.any(F[s] > 0)]
+        self.f = {s: F[s] for s in self.disp}
+        self.inv = {s: 1.0 / media[s]["eps_inf"] for s in self.disp}
+        self.coef = {s: [pole_coefficients(_P(*p), eng.dt) for p in media[s]["poles"]] for s in self.disp}
+        z = lambda: np.zeros(n, eng.fdt)  # noqa: E731
+        self.E = {s: z() for s in self.disp}
+        self.P = {s: [(z(), z()) for _ in media[s]["poles"]] for s in self.disp}
+
+    def __call__(self, u):
+        y = u * self.h0
+        for s in self.disp:
+            tot = _Group._poles(self.P[s], self.coef[s], self.E[s])
+            self.E[s][...] = (u - tot) * self.inv[s]
+            y = y + self.f[s] * self.E[s]
+        return y
+
+
+class _Arithmetic:
+    """(1/<eps>)[u] (engine.py:820-835): y = (u - sum_s F_s P_s) / sum_s F_s eps_inf_s, every pole driven by the
+    y of the step before."""
+
+    def __init__(self, eng, media, F):
+        n = F.shape[1]
+        self.disp = [s for s, m in enumerate(media) if m["poles"] and np.any(F[s] > 0)]
+        self.f = {s: F[s] for s in self.disp}
+        self.inv_a = 1.0 / sum(F[s] * m["eps_inf"] for s, m in enumerate(media))
+        self.coef = {s: [pole_coefficients(_P(*p), eng.dt) for p in media[s]["poles"]] for s in self.disp}
+        z = lambda: np.zeros(n, eng.fdt)  # noqa: E731
+        self.y = z()
+        self.P = {s: [(z(), z()) for _ in media[s]["poles"]] for s in self.disp}
+
+    def __call__(self, u):
+        acc = u
+        for s in self.disp:
+            acc = acc - self.f[s] * _Group._poles(self.P[s], self.coef[s], self.y)
+        self.y[...] = acc * self.inv_a
+        return self.y
+
+
+class _TensorMesh:
+    """The D-form update of a vertex-tensor mesh's nodes (engine.py:838-923), from the plan's index tables
+    (lightsmith_b200/plan.py:tensor_plan)."""
+
+    def __init__(self, eng, t):
+        self.eng = eng
+        self.idx = np.asarray(t["idx"], np.int64)
+        nN = self.nN = int(t["n_nodes"])
+        self.D = np.zeros(nN, eng.fdt)
+        self.E_prev = np.zeros(nN, eng.fdt)
+        self.out = np.zeros(2 * nN, eng.fdt)
+        self.vn = np.asarray(t["vn"], np.int64)
+        self.scale = None if t["scale"] is None else np.asarray(t["scale"])
+        self.n = np.asarray(t["normal"], float).reshape(-1, 3)
+        self.nV = len(self.n)
+        self.t_pos, self.t_v, self.t_vc, self.t_g = (np.asarray(t[k], np.int64) for k in ("t_pos", "t_v", "t_vc", "t_g"))
+        self.t_nc = np.asarray(t["t_nc"], float)
+        self.t_conj = None if t["t_conj"] is None else np.asarray(t["t_conj"])
+        media = t["media"]
+        F = np.asarray(t["frac"], float)
+        self.a = _Harmonic(eng, media, F)
+        self.b = _Arithmetic(eng, media, F)
+        self.p_pos, self.p_node = np.asarray(t["p_pos"], np.int64), np.asarray(t["p_node"], np.int64)
+        onehot = np.zeros((len(media), len(self.p_node)))
+        onehot[np.asarray(t["p_medium"], np.int64), np.arange(len(self.p_node))] = 1.0
+        self.plain = _Harmonic(eng, media, onehot)
+
+    def step(self):
+        Ef = self.eng.E.reshape(-1)
+        e_now = Ef[self.idx]
+        self.D += e_now - self.E_prev
+        dv = self.D[self.vn]
+        if self.scale is not None:
+            dv = dv * self.scale
+        dv = dv.reshape(self.nV, 3, 2)
+        dbar = 0.5 * (dv[..., 0] + dv[..., 1])
+        s = np.sum(self.n * dbar, axis=1)
+        dp = dv.reshape(-1)[self.t_g]
+        nc = self.t_nc
+        sigma = s[self.t_v] + nc * (dp - dbar.reshape(-1)[self.t_vc])
+        contrib = 0.5 * (self.b(dp - nc * sigma) + nc * self.a(sigma))
+        if self.t_conj is not None:
+            contrib = contrib * self.t_conj
+        self.out[self.t_pos] = contrib
+        if len(self.p_node):
+            self.out[self.p_pos] = 0.5 * self.plain(self.D[self.p_node])
+        e_new = self.out[:self.nN] + self.out[self.nN:]
         Ef[self.idx] = e_new
         self.E_prev[...] = e_new
 

@@ -60,7 +60,6 @@ def test_entry_point_replaces_the_builtin_backend(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("extra, why", [
-    (dict(mesh_refinement="conformal"), "conformal"),
     (dict(grid="auto"), "graded"),
 ])
 def test_supports_rejects_options_without_a_cuda_path(extra, why):
@@ -77,7 +76,7 @@ def test_supports_rejects_resonances_output():
 
 
 def test_supports_accepts_the_sphere_problem():
-    for mesh in ("staircase", "subpixel", "volume_average"):
+    for mesh in ("staircase", "subpixel", "volume_average", "conformal"):
         assert B.B200FDTD.supports(sphere(mesh)) == (True, "")
 
 

@@ -14,7 +14,7 @@ import pytest
 
 from oracle.post import cross_sections
 
-CASES = ["sphere_staircase", "sphere_subpixel", "sphere_symmetric", "dielectric_conformal"]
+CASES = ["sphere_staircase", "sphere_subpixel", "sphere_symmetric", "dielectric_conformal", "sphere_conformal"]
 RTOL_F64 = 1e-9  # float64 on the GPU: the same arithmetic, a different summation order at shared nodes
 RTOL_F32 = 1e-4  # float32 on the GPU against lightsmith's float64 CPU run (lightsmith's own GPU-vs-CPU bar)
 
