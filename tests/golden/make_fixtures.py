@@ -426,7 +426,8 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "solve_sphere_subpixel": lambda: solve_case("sphere_subpixel", sphere_problem("subpixel")),
          "solve_sphere_symmetric": lambda: solve_case("sphere_symmetric", sphere_problem("staircase", "auto")),
          "solve_dielectric_conformal": lambda: solve_case("dielectric_conformal", dielectric_sphere_problem()),
-         "solve_sphere_conformal": lambda: solve_case("sphere_conformal", sphere_problem("conformal"))}
+         "solve_sphere_conformal": lambda: solve_case("sphere_conformal", sphere_problem("conformal")),
+         "solve_sphere_defaults": lambda: solve_case("sphere_defaults", sphere_problem("conformal", "auto"))}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

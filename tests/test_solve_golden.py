@@ -3,9 +3,10 @@
 Each ``solve_sphere_*.npz`` fixture holds the plan lightsmith's scattering driver handed to its engine (a
 16 nm Drude-Lorentz sphere in n = 1.33, 49^3 cells at 4 nm, CPML 8, table-fed TF/SF, two flux boxes and the
 incident reference view; staircase and subpixel meshing, and with symmetry="auto" a quarter grid of 26 x 26 x 49
-cells between a PEC and a PMC mirror plane; and a non-dispersive n = 2 sphere with conformal interfaces, whose
-off-diagonal 1/eps terms the plan carries as gather tables), the driver's post-processing inputs, and
-lightsmith's own accumulators and cross sections (float64). The run is replayed for the recorded number of steps, and
+cells between a PEC and a PMC mirror plane; a non-dispersive n = 2 sphere with conformal interfaces, whose
+off-diagonal 1/eps terms the plan carries as gather tables; the metal sphere with conformal interfaces (the
+vertex-tensor ADE), and with lightsmith's default options, conformal and symmetry="auto" together), the
+driver's post-processing inputs, and lightsmith's own accumulators and cross sections (float64). The run is replayed for the recorded number of steps, and
 C_ext, C_sca and C_abs are formed by the oracle's restatement of the driver's post-processing.
 """
 
@@ -14,7 +15,8 @@ import pytest
 
 from oracle.post import cross_sections
 
-CASES = ["sphere_staircase", "sphere_subpixel", "sphere_symmetric", "dielectric_conformal", "sphere_conformal"]
+CASES = ["sphere_staircase", "sphere_subpixel", "sphere_symmetric", "dielectric_conformal", "sphere_conformal",
+         "sphere_defaults"]
 RTOL_F64 = 1e-9  # float64 on the GPU: the same arithmetic, a different summation order at shared nodes
 RTOL_F32 = 1e-4  # float32 on the GPU against lightsmith's float64 CPU run (lightsmith's own GPU-vs-CPU bar)
 
