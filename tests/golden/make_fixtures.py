@@ -30,6 +30,8 @@ if not add_to_path(sys.argv[1] if len(sys.argv) > 1 else REF_SRC):
 import lightsmith as ls  # noqa: E402
 from lightsmith.backends._fdtd import engine as ref_engine  # noqa: E402
 from lightsmith.backends._fdtd import scattering as ref_scattering  # noqa: E402
+from lightsmith.backends._fdtd import emission as ref_emission  # noqa: E402
+from lightsmith.backends._fdtd import periodic as ref_periodic  # noqa: E402
 from lightsmith.backends._fdtd import symmetry as ref_symmetry  # noqa: E402
 from lightsmith.backends._fdtd.emission import PointDipole  # noqa: E402
 from lightsmith.backends._fdtd.layered import ObliqueLayeredPlaneWave  # noqa: E402
@@ -409,6 +411,55 @@ def sphere_problem(mesh: str, symmetry: str = "off"):
                                                run_time_fs=399.5 * 2.2863 / 299.792458)})
 
 
+# --- every engine a problem driver builds, through ls.solve ----------------------------------------------
+
+
+def driver_case(name: str, problem, module):
+    """Every Engine a lightsmith driver builds in ``ls.solve(problem, "fdtd", "cpu")`` (a periodic solve builds
+    one per incidence and polarisation): its plan, step count, final DFT accumulators and energy."""
+    runs = []
+    Base = module.Engine
+
+    class Recording(Base):
+        def __init__(self, device, **kw):
+            plan = P.make_plan(**kw)  # before the engine binds the sources
+            super().__init__(device, **kw)
+            runs.append((plan, kw, self))
+
+    module.Engine = Recording
+    try:
+        ls.solve(problem, "fdtd", "cpu")
+    finally:
+        module.Engine = Base
+    out = []
+    for plan, kw, eng in runs:
+        out.append({"plan": plan, "n": int(eng.n[0]), "energy": np.asarray(eng.energy),
+                    "acc_e": [np.asarray(m.acc_e) for m in kw["monitors"]],
+                    "acc_h": [np.zeros(0) if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]})
+    P.save(os.path.join(HERE, f"driver_{name}.npz"), {"runs": out})
+    print(name, [(r["plan"]["shape"], r["n"], r["plan"]["complex"]) for r in out])
+
+
+def periodic_problem(theta: float, phi: float, pol: str):
+    """A square lattice (300 nm) of TiO2-like pillars (n = 2, radius 80 nm, 120 nm tall) on glass, 15 nm cells."""
+    from lightsmith.problems import Circle, Incidence, PatternedLayer, PeriodicProblem, Structure2D
+    CI = ls.ConstantIndex
+    return PeriodicProblem(
+        lattice_a1_nm=(300, 0), lattice_a2_nm=(0, 300), superstrate=CI(n_real=1.0), substrate=CI(n_real=1.45),
+        layers=[PatternedLayer(thickness_nm=120, background=CI(n_real=1.0),
+                               shapes=[Structure2D(profile=Circle(radius_nm=80), material=CI(n_real=2.0))])],
+        wavelengths=[500.0, 650.0], incidence=Incidence(theta_deg=theta, phi_deg=phi, polarizations=[pol]),
+        options={"fdtd": {"spacing_nm": 15.0, "run_time_fs": 6.0}})
+
+
+def emission_problem():
+    """A dipole 15 nm off an n = 2 sphere (radius 30 nm) in vacuum, 4 nm cells."""
+    from lightsmith.problems import Dipole, EmissionProblem
+    return EmissionProblem(particles=[ls.Particle(shape=ls.Sphere(radius_nm=30), material=ls.ConstantIndex(n_real=2.0))],
+                           wavelengths=[500.0, 700.0], dipole=Dipole(position_nm=(0, 0, 45), orientation=(1, 0, 1)),
+                           options={"fdtd": {"spacing_nm": 4.0, "run_time_fs": 2.0}})
+
+
 def dielectric_sphere_problem():
     """A non-dispersive sphere (n = 2, radius 16 nm) in n = 1.33 with conformal interfaces (off-diagonal 1/eps)."""
     return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
@@ -427,7 +478,12 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "solve_sphere_symmetric": lambda: solve_case("sphere_symmetric", sphere_problem("staircase", "auto")),
          "solve_dielectric_conformal": lambda: solve_case("dielectric_conformal", dielectric_sphere_problem()),
          "solve_sphere_conformal": lambda: solve_case("sphere_conformal", sphere_problem("conformal")),
-         "solve_sphere_defaults": lambda: solve_case("sphere_defaults", sphere_problem("conformal", "auto"))}
+         "solve_sphere_defaults": lambda: solve_case("sphere_defaults", sphere_problem("conformal", "auto")),
+         "driver_periodic_normal": lambda: driver_case("periodic_normal", periodic_problem(0.0, 0.0, "s"),
+                                                       ref_periodic),
+         "driver_periodic_oblique": lambda: driver_case("periodic_oblique", periodic_problem(30.0, 10.0, "p"),
+                                                        ref_periodic),
+         "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission)}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)
