@@ -30,6 +30,7 @@ if not add_to_path(sys.argv[1] if len(sys.argv) > 1 else REF_SRC):
 import lightsmith as ls  # noqa: E402
 from lightsmith.backends._fdtd import engine as ref_engine  # noqa: E402
 from lightsmith.backends._fdtd import scattering as ref_scattering  # noqa: E402
+from lightsmith.backends._fdtd import device as ref_device  # noqa: E402
 from lightsmith.backends._fdtd import emission as ref_emission  # noqa: E402
 from lightsmith.backends._fdtd import periodic as ref_periodic  # noqa: E402
 from lightsmith.backends._fdtd import symmetry as ref_symmetry  # noqa: E402
@@ -460,6 +461,30 @@ def emission_problem():
                            options={"fdtd": {"spacing_nm": 4.0, "run_time_fs": 2.0}})
 
 
+def device_problem(dimension: int):
+    """A silicon waveguide width step (500 -> 700 nm) in silica between two x-normal ports: 2D at 25 nm cells
+    (TE), or a 220 nm thick wire in 3D at 40 nm cells."""
+    from lightsmith.problems import Box, DeviceProblem, Port, Prism, Rectangle, Structure
+    si, sio2 = ls.ConstantIndex(n_real=3.48), ls.ConstantIndex(n_real=1.44)
+    if dimension == 2:
+        def rect(cx, sy):
+            return Structure(geometry=Prism(profile=Rectangle(center_nm=(cx, 0), size_nm=(2000, sy)), z_min_nm=-110,
+                                            z_max_nm=110), material=si)
+        return DeviceProblem(
+            dimension=2, background=sio2, structures=[rect(-1000, 500), rect(1000, 700)],
+            domain_size_nm=(2000, 2400, 0), wavelengths=[1500.0, 1600.0],
+            ports=[Port(name="o1", center_nm=(-800, 0, 0), size_nm=(0, 2000, 1), direction="+"),
+                   Port(name="o2", center_nm=(800, 0, 0), size_nm=(0, 2000, 1), direction="-")],
+            options={"fdtd": {"spacing_nm": 25.0, "polarization": "te", "precision": "double", "run_time_fs": 30.0}})
+    return DeviceProblem(
+        structures=[Structure(geometry=Box(center_nm=(-600, 0, 0), size_nm=(1200, 500, 220)), material=si),
+                    Structure(geometry=Box(center_nm=(600, 0, 0), size_nm=(1200, 700, 220)), material=si)],
+        background=sio2, domain_size_nm=(1200, 1600, 1200), wavelengths=[1500.0, 1600.0],
+        ports=[Port(name="o1", center_nm=(-600, 0, 0), size_nm=(0, 1600, 1200), direction="+"),
+               Port(name="o2", center_nm=(600, 0, 0), size_nm=(0, 1600, 1200), direction="-")],
+        options={"fdtd": {"spacing_nm": 40.0, "run_time_fs": 20.0}})
+
+
 def dielectric_sphere_problem():
     """A non-dispersive sphere (n = 2, radius 16 nm) in n = 1.33 with conformal interfaces (off-diagonal 1/eps)."""
     return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
@@ -483,7 +508,9 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
                                                        ref_periodic),
          "driver_periodic_oblique": lambda: driver_case("periodic_oblique", periodic_problem(30.0, 10.0, "p"),
                                                         ref_periodic),
-         "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission)}
+         "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission),
+         "driver_device_2d": lambda: driver_case("device_2d", device_problem(2), ref_device),
+         "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device)}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

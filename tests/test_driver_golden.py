@@ -9,7 +9,10 @@ that plan, the number of steps the run took and lightsmith's own DFT accumulator
 * ``periodic_oblique``: the same lattice at theta = 30, phi = 10 degrees, p polarisation, one complex-valued
   Bloch-periodic run per wavelength (22 x 22 x 90 cells);
 * ``emission``: a dipole 15 nm off an n = 2 sphere, the scene run and the run in the medium alone
-  (69 x 69 x 75 cells at 4 nm, the point-dipole current source, flux box and far-field monitors).
+  (69 x 69 x 75 cells at 4 nm, the point-dipole current source, flux box and far-field monitors);
+* ``device_2d``, ``device_3d``: a silicon waveguide width step (500 -> 700 nm) in silica between two ports, one
+  run per port with its mode source; 2D TE at 25 nm (123 x 139 x 3 cells) and a 220 nm wire in 3D at 40 nm
+  (73 x 83 x 73 cells).
 
 Each run is replayed for its recorded number of steps and every monitor's accumulators are compared with
 lightsmith's, norm-wise per monitor.
@@ -19,7 +22,7 @@ import numpy as np
 import pytest
 
 CASES = [("periodic_normal", 0), ("periodic_oblique", 0), ("periodic_oblique", 1), ("emission", 0),
-         ("emission", 1)]
+         ("emission", 1), ("device_2d", 0), ("device_2d", 1), ("device_3d", 0), ("device_3d", 1)]
 RTOL_F64 = 1e-9  # float64 on the GPU: the same arithmetic, a different summation order at shared nodes
 RTOL_F32 = 2e-4  # float32 on the GPU against lightsmith's float64 CPU run
 
@@ -38,7 +41,8 @@ def _check(eng_results, run, rtol, label):
 
 
 def test_driver_fixtures_cover_the_drivers(golden):
-    for name, runs in (("periodic_normal", 1), ("periodic_oblique", 2), ("emission", 2)):
+    for name, runs in (("periodic_normal", 1), ("periodic_oblique", 2), ("emission", 2), ("device_2d", 2),
+                       ("device_3d", 2)):
         d = golden("driver_" + name)
         assert len(d["runs"]) == runs
         for run in d["runs"]:
@@ -49,6 +53,8 @@ def test_driver_fixtures_cover_the_drivers(golden):
     assert oblique["complex"] and any(oblique["periodic"])
     emission = golden("driver_emission")["runs"][0]["plan"]
     assert type(emission["sources"][0]).__name__ == "DipoleSource"
+    for name in ("device_2d", "device_3d"):
+        assert type(golden("driver_" + name)["runs"][0]["plan"]["sources"][0]).__name__ == "ModeSource"
 
 
 @pytest.mark.slow
