@@ -43,13 +43,16 @@ def _torch():
 
 class AdjointRun:
     """One run's forward and adjoint passes. ``box``: ((x0, x1), (y0, y1), (z0, z1)) node ranges of the design
-    box; ``monitor``: the objective's monitor; ``objective``: J(acc_e, acc_h) -> real torch scalar, with acc_e
-    (n_freq, n_e) and acc_h (n_freq, n_h) or None the monitor's accumulators as complex128 tensors; or, when
-    it is None, J = |A|^2 at frequency ``freq`` with ``wE``/``wH`` the complex weights of the E and H points
-    (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride)."""
+    box; ``monitor``: the objective's monitor, or a list of monitors with the same frequencies, whose points
+    the objective sees concatenated (in list order); ``objective``: J(acc_e, acc_h) -> real torch scalar, with
+    acc_e (n_freq, n_e) and acc_h (n_freq, n_h) or None the monitors' accumulators as complex128 tensors; or,
+    when it is None, J = |A|^2 at frequency ``freq`` with ``wE``/``wH`` the complex weights of the E and H
+    points (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride).
+    ``sources_in_box``: allow source nodes inside the box, whose injection then stays as the plan built it
+    (the gradient there is that of the field update alone)."""
 
-    def __init__(self, plan: dict, box, monitor: int = 0, freq: int = 0, wE=None, wH=None, checkpoint: int = 256,
-                 precision: str | None = None, device="cuda:0", objective=None):
+    def __init__(self, plan: dict, box, monitor=0, freq: int = 0, wE=None, wH=None, checkpoint: int = 256,
+                 precision: str | None = None, device="cuda:0", objective=None, sources_in_box: bool = False):
         torch = _torch()
         if plan["complex"] or any(plan["periodic"]):
             raise ValueError("the adjoint serves real fields without periodic axes")
@@ -61,20 +64,29 @@ class AdjointRun:
         self.plan = plan
         self.eng = Engine.from_plan(plan, device=device, precision=precision)
         eng = self.eng
-        if not eng.isotropic:
-            raise ValueError("the adjoint's design box needs isotropic permittivity (one 1/eps per node)")
         self.dev = eng.dev
         self.stride = eng.stride
         self.K = max(self.stride, int(checkpoint) // self.stride * self.stride)
         self.box = tuple((int(a), int(b)) for a, b in box)
         self.box_sl = tuple(slice(a, b) for a, b in self.box)
         bshape = tuple(b - a for a, b in self.box)
-        mon = plan["monitors"][monitor]
-        self.monitor, self.freq = monitor, freq
-        self.omegas = np.asarray(mon["omega"], float)
+        self.monitors = [int(monitor)] if np.ndim(monitor) == 0 else [int(k) for k in monitor]
+        mons = [plan["monitors"][k] for k in self.monitors]
+        self.monitor, self.freq = self.monitors[0], freq
+        self.omegas = np.asarray(mons[0]["omega"], float)
+        if any(not np.array_equal(np.asarray(m["omega"], float), self.omegas) for m in mons):
+            raise ValueError("the objective's monitors must share their frequencies")
         nf = len(self.omegas)
         cd = torch.complex128
-        self.has_h = mon["h_idx1"] is not None
+        self.has_h = mons[0]["h_idx1"] is not None
+        if any((m["h_idx1"] is not None) != self.has_h for m in mons):
+            raise ValueError("the objective's monitors must all record H, or none")
+
+        def cat(key):
+            return np.concatenate([np.asarray(m[key], np.int64) for m in mons])
+        mon = {"e_idx": cat("e_idx")}
+        if self.has_h:
+            mon["h_idx1"], mon["h_idx2"] = cat("h_idx1"), cat("h_idx2")
         if objective is None:
             wE_t = torch.as_tensor(np.zeros(len(mon["e_idx"])) if wE is None else np.asarray(wE), dtype=cd,
                                    device=self.dev)
@@ -96,7 +108,7 @@ class AdjointRun:
             rest = np.asarray(nodes) % int(np.prod(eng.shape))
             ijk = np.stack(np.unravel_index(rest, eng.shape), axis=1)
             inside = np.all((ijk >= [a for a, _ in self.box]) & (ijk < [b for _, b in self.box]), axis=1)
-            if inside.any():
+            if inside.any() and not sources_in_box:
                 raise ValueError("a source node lies in the design box")
         rdt = eng.rdt
         self.group_bar = [torch.zeros_like(g["state"]) for g in eng.groups]
@@ -168,11 +180,19 @@ class AdjointRun:
         self._restore(self._save(), 0)
 
     def set_inv_eps_box(self, inv_eps_box) -> None:
-        """1/eps over the box (the engine's shared E curl coefficient there becomes cdx / eps)."""
+        """1/eps over the box, one value per node (x, y, z) or one per E component (3, x, y, z); the E curl
+        coefficient of each component there becomes cdx / eps."""
         eng = self.eng
         torch = _torch()
-        cb = eng.cbE[0]
-        cb[self.box_sl] = (torch.as_tensor(inv_eps_box, device=self.dev, dtype=torch.float64) * eng.cdx).to(cb.dtype)
+        v = torch.as_tensor(inv_eps_box, device=self.dev, dtype=torch.float64) * eng.cdx
+        shared = eng.cbE[0] is eng.cbE[1] and eng.cbE[1] is eng.cbE[2]
+        if v.dim() == 3:
+            v = v.expand(3, *v.shape)
+        elif shared and not (torch.equal(v[0], v[1]) and torch.equal(v[0], v[2])):
+            raise ValueError("this engine shares one 1/eps array between the E components; give one value per node")
+        for c in range(1 if shared else 3):
+            cb = eng.cbE[c]
+            cb[self.box_sl] = v[c].to(cb.dtype)
         torch.cuda.synchronize(self.dev)
 
     # --- passes -----------------------------------------------------------------------------------------------
@@ -193,17 +213,18 @@ class AdjointRun:
             if done < n_steps and keep:
                 self._ckpt.append(self._save())
         self.n_steps = n_steps if keep else 0
-        m = eng.monitors[self.monitor]
+        ms = [eng.monitors[k] for k in self.monitors]
         torch.cuda.synchronize(self.dev)
-        acc_e = m["acc_e"].to(torch.complex128).clone()
-        acc_h = m["acc_h"].to(torch.complex128).clone() if self.has_h else None
+        acc_e = torch.cat([m["acc_e"].to(torch.complex128) for m in ms], dim=1)
+        acc_h = torch.cat([m["acc_h"].to(torch.complex128) for m in ms], dim=1) if self.has_h else None
         self.acc = (acc_e, acc_h)
         with torch.no_grad():
             J = self.objective(acc_e, acc_h)
         return float(J), (acc_e, acc_h)
 
-    def backward(self):
-        """dJ/d(1/eps) over the box, as float64 (x, y, z) after forward()."""
+    def backward(self, per_component: bool = False):
+        """dJ/d(1/eps) over the box after forward(), as float64: (x, y, z) for a 1/eps shared by the node's
+        three E components, or per component (3, x, y, z)."""
         if not self.n_steps:
             raise RuntimeError("backward needs a forward run that kept its checkpoints")
         torch = _torch()
@@ -242,7 +263,7 @@ class AdjointRun:
             for i in reversed(range(n1 - n0)):
                 _abi.check(L.lsfdtd_adjoint_step(h, n0 + i, i, st), "lsfdtd_adjoint_step")
             torch.cuda.synchronize(self.dev)
-        return self.grad.sum(0) * eng.cdx
+        return self.grad * eng.cdx if per_component else self.grad.sum(0) * eng.cdx
 
     def close(self):
         h = getattr(self, "_h", None)

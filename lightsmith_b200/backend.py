@@ -20,6 +20,8 @@ Gaussian beams) is rejected by ``supports`` or raises
 from __future__ import annotations
 
 import threading
+
+import numpy as np
 from contextlib import contextmanager
 
 from lightsmith.backends._fdtd import device as _device_driver
@@ -75,13 +77,198 @@ def _static_rejection(sim, opts) -> str:
     return ""
 
 
+def _port_rows(tables, omega, e_counts, h_counts) -> list[dict]:
+    """The port amplitudes of every port mode as linear functionals of its monitor's DFT accumulators.
+
+    ``ModeTable.amplitudes`` (ports.py:265-280) forms p1 = <E, h> and p2 = <e, H> (unconjugated overlaps with
+    the weights wa, wb), X = (p1 / u2 + p2) / (2 c N), Y = (u2 p1 - p2) / (2 c N) with u2 = exp(i beta s / 2),
+    c = cos(beta s / 2), N = <e, h>, and moves them to the reference plane (exp(+-i beta ds)). Every step is
+    linear in (E, H), so each amplitude is sum(kE E) + sum(kH H); the rows hold kE and kH, (n_w, points), for
+    the incoming and the outgoing amplitude, and the offsets of the monitor's points in the concatenation of
+    all port monitors."""
+    e_off = np.concatenate([[0], np.cumsum(e_counts)])
+    h_off = np.concatenate([[0], np.cumsum(h_counts)])
+    rows = []
+    for fi, tab in enumerate(tables):
+        fr = tab.frame
+        e, h, beta = tab.at(omega)
+        for mm in range(fr.num_modes):
+            em, hm, b = e[:, mm], h[:, mm], beta[:, mm]
+            N = tab.overlap(em, hm)
+            kE = np.stack([tab.wa * hm[:, 1], -tab.wb * hm[:, 0]], axis=1)  # p1 = sum kE E
+            kH = np.stack([-tab.wb * em[:, 1], tab.wa * em[:, 0]], axis=1)  # p2 = sum kH H
+            u2 = np.exp(0.5j * b * tab.spacing)
+            c = np.cos(0.5 * b * tab.spacing)
+            ds = fr.s_ref - fr.s_m
+            x = (np.exp(1j * b * ds) / (2 * c * N))[:, None, None, None]
+            y = (np.exp(-1j * b * ds) / (2 * c * N))[:, None, None, None]
+            fwd = (kE * x / u2[:, None, None, None], kH * x)
+            bwd = (kE * y * u2[:, None, None, None], -kH * y)
+            inc, out = (fwd, bwd) if fr.delta > 0 else (bwd, fwd)
+            nw = len(omega)
+            rows.append({"e_off": int(e_off[fi]), "h_off": int(h_off[fi]),
+                         "in_e": inc[0].reshape(nw, -1), "in_h": inc[1].reshape(nw, -1),
+                         "out_e": out[0].reshape(nw, -1), "out_h": out[1].reshape(nw, -1)})
+    return rows
+
+
+def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: bool = False) -> dict:
+    """The runs lightsmith's device driver makes for ``problem`` (backends/_fdtd/device.py:475-561), as the
+    plain description ``lightsmith_b200.differentiable.DeviceSolver`` solves: one plan per port mode (its mode
+    source and one DFT monitor per port), the driver's 1/eps, the port-amplitude rows, the design grid's node
+    coordinates and the step count.
+
+    The set-up is lightsmith's own (plan, voxelisation, mode tables, pulse band, CPML), with two choices the
+    adjoint needs: the mesh is staircase where a dispersive medium is present (its D-form groups must be pure)
+    and subpixel or staircase otherwise as the options ask (conformal asks for subpixel: the adjoint has no
+    off-diagonal terms); the step count is fixed: the options' ``run_time_fs`` (the driver's ``max_steps``), or
+    ``n_steps``. ``keep_tables`` adds lightsmith's mode tables (not plain data) under ``"tables"``."""
+    from lightsmith.backends._fdtd import device as D
+    from lightsmith.backends._fdtd.engine import DFTMonitor, PMLSpec
+    from lightsmith.backends._fdtd.ports import ModeSource, ModeTable
+    from lightsmith.backends._fdtd.setup import voxelise
+    from lightsmith.problems import wavelength_array
+
+    from . import plan as P
+
+    if not isinstance(problem, DeviceProblem):
+        raise ValueError("the differentiable FDTD solve takes device problems")
+    if problem.dimension != 3:
+        raise NotImplementedError("2D device problems step a periodic axis, which the adjoint does not serve")
+    ok, why = D.supports(problem)
+    if not ok:
+        raise ValueError(why)
+    problem = D._resolved(problem)
+    opts = B200FDTD._options(problem)
+    if D.graded(opts):
+        raise NotImplementedError("graded grids have no CUDA path in lightsmith-b200")
+    single = D.uses_single(opts, device) if device is not None else opts.precision == "single"
+    p = D.plan(problem, opts, single)
+    grid, frames, dt, stride = p["grid"], p["frames"], p["dt"], p["stride"]
+    media = p["media"]
+    wl = wavelength_array(problem.wavelengths)
+    omega = 2 * np.pi / wl
+    _, slots = D._media(problem, wl, [])
+    w1, w2, wc, sigma, wa, wb = p["band"]
+    dx = grid.engine_spacing()
+    slot_fn = D._slot_fn(problem, slots, None)
+    asked = opts.mesh_refinement or ("subpixel" if opts.subpixel else "staircase")
+    mode = "staircase" if asked == "staircase" or any(m.dispersive for m in media) else "subpixel"
+    inv_eps, groups, _, _ = voxelise(slot_fn, media, grid.shape, grid.origin, dx, np.array([1, 1, 1]),
+                                     np.array(grid.shape) - 1, mode=mode, samples=opts.subpixel_samples,
+                                     periodic=grid.periodic, grid=grid.graded)
+    tables = [ModeTable(f, f.ds, dt, wa, wb, D._eps_fn(f, inv_eps, groups, dt), polarization=None) for f in frames]
+    n_bg = float(np.sqrt(max(media[0].eps_inf, 1.0)))
+    cells = tuple((0, 0) if per else (grid.n_pml, grid.n_pml) for per in grid.periodic)
+    pml = PMLSpec(cells=cells, kappa_max=opts.pml_kappa, alpha_max=0.05 * 2 * np.pi * n_bg / float(wl.max()),
+                  eps_ref=media[0].eps_inf)
+    if n_steps is None:
+        if not opts.run_time_fs:
+            raise ValueError("the differentiable FDTD solve runs a fixed step count: set options['fdtd']"
+                             "['run_time_fs'] (or pass n_steps)")
+        n_steps = p["max_steps"]
+    n_steps = int(n_steps) // stride * stride
+    labels = [lab for f in frames for lab in f.labels()]
+    plans = []
+    for f, tab in zip(frames, tables):
+        for m in range(f.num_modes):
+            src = ModeSource(tab, m, inv_eps=inv_eps, dt=dt, omega_c=wc, sigma=sigma,
+                             n_steps=max(p["max_steps"], n_steps) + 4 * stride)
+            mons = [DFTMonitor(omega, g.e_nodes(g.k_m), g.h_nodes(g.k_m), g.h_nodes(g.k_m), energy=True)
+                    for g in frames]
+            pl = P.make_plan(shape=grid.shape, dx=dx, dt=dt, single=single, inv_eps=inv_eps, groups=groups,
+                             pml=pml, sources=[src], monitors=mons, dft_stride=stride, periodic=grid.periodic,
+                             widths=grid.engine_widths())
+            pl.pop("inv_eps")
+            plans.append(pl)
+    e_counts = [len(m["e_idx"]) for m in plans[0]["monitors"]]
+    h_counts = [len(m["h_idx1"]) for m in plans[0]["monitors"]]
+    coords = [np.array([grid.coord(a, i) for i in range(grid.shape[a])], float) for a in range(3)]
+    out = {"shape": tuple(int(v) for v in grid.shape), "inv_eps": np.asarray(inv_eps, float), "plans": plans,
+           "labels": labels, "rows": _port_rows(tables, omega, e_counts, h_counts), "omega": omega,
+           "wavelengths_nm": wl, "n_steps": n_steps, "pml_cells": cells, "coords": coords, "dl": float(grid.dx),
+           "mesh": mode}
+    if keep_tables:
+        out["tables"] = tables
+    return out
+
+
 class B200FDTD(NativeFDTD):
-    """``NativeFDTD`` (backends/fdtd.py:47) whose engine is the B200 one on CUDA devices."""
+    """``NativeFDTD`` (backends/fdtd.py:47) whose engine is the B200 one on CUDA devices, and which serves
+    lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) for 3D device problems on CUDA
+    devices (``lightsmith_b200.differentiable``)."""
 
     name = "lightsmith-fdtd"
     method = "fdtd"
     gpu = True
+    differentiable = True
     citation = NativeFDTD.citation + "; time loop: lightsmith-b200 (sm_100a CUDA kernels)"
+
+    # --- the differentiable-backend protocol -----------------------------------------------------------------
+    @classmethod
+    def prepare(cls, problem) -> dict:
+        """The runs' description and their solver, reused across optimisation iterations."""
+        from .differentiable import DeviceSolver
+
+        desc = device_runs(problem)
+        return {"solver": DeviceSolver(desc)}
+
+    @classmethod
+    def design_grid(cls, problem, solver=None):
+        """The FDTD grid's nodes (``x``, ``y``, ``z`` in nm, ``dl``, ``shape``); node (i, j, k) carries the
+        permittivity of its three E components."""
+        from .differentiable import DesignGrid
+
+        d = solver.desc if solver is not None else device_runs(problem)
+        x, y, z = d["coords"]
+        return DesignGrid(x=x, y=y, z=z, dl=d["dl"], shape=tuple(d["shape"]))
+
+    @classmethod
+    def base_permittivity(cls, problem, solver=None) -> np.ndarray:
+        """(n_wl, Nx, Ny, Nz) complex: per node, 1 over the mean of its three E components' 1/eps."""
+        d = solver.desc if solver is not None else device_runs(problem)
+        nodes = 1.0 / np.asarray(d["inv_eps"], float).mean(axis=0)
+        return np.broadcast_to(nodes, (len(d["wavelengths_nm"]),) + nodes.shape).astype(complex)
+
+    @classmethod
+    def differentiable_solve(cls, problem, eps_grid_override=None, device="gpu", sources=None,
+                             with_fields: bool = False, solver=None):
+        """S-parameters as torch tensors connected to ``eps_grid_override`` ((n_wl, Nx, Ny, Nz) or (Nx, Ny, Nz),
+        real and equal across wavelengths), by the CUDA engine and the discrete adjoint."""
+        import torch
+        from lightsmith.backends.fdfd import DifferentiableSolution
+        from lightsmith.device import resolve_device
+
+        from .differentiable import DeviceSolver, s_parameters
+
+        dev = resolve_device(device) if isinstance(device, str) else device
+        if not dev.is_gpu or dev.framework != "torch":
+            raise ValueError(f"{cls.name} (B200): the differentiable solve runs on PyTorch CUDA devices")
+        if with_fields:
+            raise NotImplementedError("field outputs (field-intensity objectives) have no FDTD path here")
+        if solver is None:
+            solver = DeviceSolver(device_runs(problem, dev))
+        if eps_grid_override is None:
+            eps = torch.as_tensor(solver.base_nodes, dtype=torch.float64)
+        else:
+            e = torch.as_tensor(eps_grid_override)
+            if e.dim() == 3:
+                e = e[None]
+            if torch.is_complex(e):
+                if torch.any(e.imag.detach() != 0):
+                    raise ValueError("FDTD steps a real permittivity: the override must have no imaginary part")
+                e = e.real
+            e = e.to(torch.float64)
+            ref = e[0].detach()
+            if torch.any((e.detach() - ref).abs() > 1e-12 * ref.abs()):
+                raise ValueError("FDTD steps a frequency-independent permittivity: the override must be equal "
+                                 "across wavelengths")
+            eps = e.mean(0)
+        labels = solver.labels if sources is None else list(sources)
+        S = s_parameters(eps, solver, labels)
+        return DifferentiableSolution(s=S, fields=None, outputs=list(solver.labels), inputs=labels,
+                                      wavelengths_nm=np.asarray(solver.desc["wavelengths_nm"]),
+                                      grid=cls.design_grid(problem, solver))
 
     @classmethod
     def supports(cls, sim):

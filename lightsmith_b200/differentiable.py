@@ -1,0 +1,214 @@
+"""S-parameters of a device problem as a torch function of its permittivity grid, with exact gradients by the
+discrete adjoint: the solve behind lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) on
+the FDTD path.
+
+lightsmith's inverse design asks a backend for ``design_grid``, ``base_permittivity`` and
+``differentiable_solve`` (the FDFD backend is its one implementation, backends/fdfd.py:134-160); lightsmith's
+FDTD sets ``differentiable = False``. Here the device driver's runs (backends/_fdtd/device.py:475-561: one run
+per port mode, a mode source and one DFT monitor per port) are handed over as a plain description that
+``lightsmith_b200.backend.device_runs`` builds with lightsmith's own set-up (voxelisation, mode tables, time
+step); this module needs no lightsmith, so the GPU tests replay a recorded description.
+
+The permittivity grid is the FDTD grid's nodes: node (i, j, k) carries one real permittivity for its three E
+components (E_x at i + 1/2, E_y at j + 1/2, E_z at k + 1/2). Where the grid given equals the base (the driver's
+own voxelisation, 1/eps averaged over the three components), a node keeps the driver's per-component values;
+elsewhere its three components take 1/eps of the grid. FDTD steps a real, frequency-independent permittivity:
+an override must be real and equal across wavelengths.
+
+Each S column is one ``AdjointRun`` (``lightsmith_b200.adjoint``) over all port monitors: the forward runs the
+CUDA engine for the description's fixed step count, keeping checkpoints; S[:, out, src] = c_out / a_src from the
+port amplitudes (ports.py:265-280, device.py:553-561), which are linear functionals of the monitors' DFT
+accumulators. The backward gives each run the adjoint source of Re sum conj(dL/dS) S (the same first-order
+change as L) and returns dL/deps = -(1/eps^2) sum_c dL/d(1/eps_c) over the interior box (the nodes outside
+every CPML slab); an override that differs from the base outside that box is rejected. The gradient is exact
+for the fixed step count, with the ports' sources and mode tables built from the base permittivity (the
+protocol requires that the ports do not depend on the override).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .adjoint import AdjointRun
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+@dataclass
+class DesignGrid:
+    """The grid of ``design_grid``: node coordinates (nm) along each axis, the cell size and the shape."""
+
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    dl: float
+    shape: tuple
+
+
+def interior_box(shape, pml_cells):
+    """Node ranges outside every E CPML slab (plan.cpml_terms: the low slab ends at node lo + 1, the high one
+    starts at n - 2 - hi) and off the grid's outer nodes."""
+    box = []
+    for n, (lo, hi) in zip(shape, pml_cells):
+        a = lo + 1 if lo else 1
+        b = n - 2 - hi if hi else n - 1
+        if b <= a:
+            raise ValueError("the grid has no nodes outside its CPML slabs")
+        box.append((int(a), int(b)))
+    return tuple(box)
+
+
+class DeviceSolver:
+    """The runs of one device description (``backend.device_runs``), kept across evaluations: one
+    ``AdjointRun`` per excited port mode, created on first use."""
+
+    def __init__(self, desc: dict, device="cuda:0", precision: str | None = None, checkpoint: int = 256):
+        self.desc = desc
+        self.device, self.precision, self.checkpoint = device, precision, int(checkpoint)
+        self.shape = tuple(int(v) for v in desc["shape"])
+        self.inv_eps = np.asarray(desc["inv_eps"], float).reshape((3,) + self.shape)
+        self.base_nodes = 1.0 / self.inv_eps.mean(axis=0)
+        self.box = interior_box(self.shape, desc["pml_cells"])
+        self.box_sl = tuple(slice(a, b) for a, b in self.box)
+        self.labels = list(desc["labels"])
+        self.n_steps = int(desc["n_steps"])
+        self.omega = np.asarray(desc["omega"], float)
+        self._runs: dict[str, AdjointRun] = {}
+        self._gen: dict[str, int] = {}
+        self._amp = None
+
+    # --- the port amplitudes -------------------------------------------------------------------------------
+    def _coefficients(self, dev):
+        """Per output row: (offset of its monitor's E points, of its H points, in_E, in_H, out_E, out_H) as
+        complex128 tensors (n_w, points)."""
+        if self._amp is None:
+            torch = _torch()
+            rows = []
+            for r in self.desc["rows"]:
+                t = [torch.as_tensor(np.asarray(r[k]), dtype=torch.complex128, device=dev)
+                     for k in ("in_e", "in_h", "out_e", "out_h")]
+                rows.append((int(r["e_off"]), int(r["h_off"]), *t))
+            self._amp = rows
+        return self._amp
+
+    def amplitudes(self, acc_e, acc_h):
+        """(incoming, outgoing) amplitudes of every port mode, (n_w, n_out) each, from the concatenated
+        accumulators of the port monitors."""
+        torch = _torch()
+        a_in, a_out = [], []
+        for e0, h0, ie, ih, oe, oh in self._coefficients(acc_e.device):
+            E = acc_e[:, e0:e0 + ie.shape[1]]
+            H = acc_h[:, h0:h0 + ih.shape[1]]
+            a_in.append((ie * E).sum(1) + (ih * H).sum(1))
+            a_out.append((oe * E).sum(1) + (oh * H).sum(1))
+        return torch.stack(a_in, 1), torch.stack(a_out, 1)
+
+    def s_column(self, label, acc_e, acc_h):
+        a_in, a_out = self.amplitudes(acc_e, acc_h)
+        row = self.labels.index(label)
+        return a_out / a_in[:, row:row + 1]
+
+    # --- runs ----------------------------------------------------------------------------------------------
+    def run(self, label: str) -> AdjointRun:
+        if label not in self._runs:
+            k = self.labels.index(label)
+            plan = dict(self.desc["plans"][k])
+            plan["inv_eps"] = self.inv_eps
+            mons = list(range(len(plan["monitors"])))
+            self._runs[label] = AdjointRun(plan, self.box, monitor=mons, checkpoint=self.checkpoint,
+                                           precision=self.precision, device=self.device,
+                                           objective=lambda e, h: e.real.sum() * 0, sources_in_box=True)
+            self._gen[label] = 0
+        return self._runs[label]
+
+    def inv_eps_box(self, eps_nodes: np.ndarray) -> np.ndarray:
+        """(3, box) 1/eps of each E component over the box for a node permittivity grid."""
+        eps_nodes = np.asarray(eps_nodes, float)
+        if eps_nodes.shape != self.shape:
+            raise ValueError(f"the permittivity grid must have the design grid's shape {self.shape}")
+        changed = ~np.isclose(eps_nodes, self.base_nodes, rtol=1e-12, atol=0)
+        inside = np.zeros(self.shape, bool)
+        inside[self.box_sl] = True
+        if np.any(changed & ~inside):
+            raise ValueError("the permittivity grid differs from the problem's outside the interior box "
+                             f"{self.box} (CPML slabs and outer nodes keep the problem's permittivity)")
+        if np.any(eps_nodes[changed] <= 0):
+            raise ValueError("the permittivity must be positive")
+        inv = self.inv_eps[(slice(None),) + self.box_sl].copy()
+        ch = changed[self.box_sl]
+        inv[:, ch] = 1.0 / eps_nodes[self.box_sl][ch]
+        return inv
+
+    def forward(self, label: str, eps_nodes: np.ndarray):
+        """Runs one column's forward pass; returns its accumulators (acc_e, acc_h), complex128 on the GPU."""
+        run = self.run(label)
+        run.set_inv_eps_box(self.inv_eps_box(eps_nodes))
+        _, acc = run.forward(self.n_steps)
+        self._gen[label] += 1
+        return acc
+
+    def close(self):
+        for r in self._runs.values():
+            r.close()
+        self._runs.clear()
+
+
+def _function():
+    torch = _torch()
+
+    class DeviceSParameters(torch.autograd.Function):
+        """S (n_w, n_out, n_src) of a ``DeviceSolver`` as a function of the node permittivity grid."""
+
+        @staticmethod
+        def forward(ctx, eps_nodes, solver: DeviceSolver, sources):
+            eps_np = eps_nodes.detach().cpu().numpy().astype(float)
+            cols, gens = [], []
+            for lab in sources:
+                acc_e, acc_h = solver.forward(lab, eps_np)
+                cols.append(solver.s_column(lab, acc_e, acc_h))
+                gens.append(solver._gen[lab])
+            ctx.solver, ctx.sources, ctx.gens = solver, list(sources), gens
+            ctx.eps_np = eps_np
+            ctx.save_for_backward(eps_nodes)
+            return torch.stack(cols, 2).to(eps_nodes.device)
+
+        @staticmethod
+        def backward(ctx, gS):
+            (eps_nodes,) = ctx.saved_tensors
+            solver = ctx.solver
+            box_sl = solver.box_sl
+            eps_box = torch.as_tensor(ctx.eps_np[box_sl], dtype=torch.float64)
+            total = torch.zeros(solver.shape, dtype=torch.float64)
+            for j, lab in enumerate(ctx.sources):
+                g = gS[:, :, j].detach().to(torch.complex128)
+                if not torch.any(g != 0):
+                    continue
+                run = solver.run(lab)
+                if solver._gen[lab] != ctx.gens[j]:  # a later forward replaced this one's checkpoints
+                    solver.forward(lab, ctx.eps_np)
+                gd = g.to(run.dev)
+
+                def objective(acc_e, acc_h, lab=lab, gd=gd):
+                    return (gd.conj() * solver.s_column(lab, acc_e, acc_h)).sum().real
+
+                run.objective = objective
+                gc = run.backward(per_component=True).sum(0).cpu()
+                total[box_sl] += -gc / eps_box ** 2
+            return total.to(device=eps_nodes.device, dtype=eps_nodes.dtype), None, None
+
+    return DeviceSParameters
+
+
+def s_parameters(eps_nodes, solver: DeviceSolver, sources=None):
+    """S (n_w, n_out, n_src) complex128, differentiable in ``eps_nodes`` (real, the design grid's shape)."""
+    sources = list(solver.labels if sources is None else sources)
+    for s in sources:
+        if s not in solver.labels:
+            raise ValueError(f"unknown port mode {s!r}; the ports are {solver.labels}")
+    return _function().apply(eps_nodes, solver, sources)

@@ -38,6 +38,7 @@ from lightsmith.backends._fdtd.emission import PointDipole  # noqa: E402
 from lightsmith.backends._fdtd.layered import ObliqueLayeredPlaneWave  # noqa: E402
 from lightsmith.backends._fdtd.media import Medium, Pole  # noqa: E402
 from lightsmith.backends._fdtd.ports import ModeSource  # noqa: E402
+from device_problems import device_problem, diff_device_problem  # noqa: E402
 from lightsmith.backends._fdtd.setup import flux_points, voxelise  # noqa: E402
 from lightsmith.backends._fdtd.tfsf import BlochPlaneSource, TFSFPlaneWave  # noqa: E402
 from lightsmith.device import Device  # noqa: E402
@@ -461,28 +462,16 @@ def emission_problem():
                            options={"fdtd": {"spacing_nm": 4.0, "run_time_fs": 2.0}})
 
 
-def device_problem(dimension: int):
-    """A silicon waveguide width step (500 -> 700 nm) in silica between two x-normal ports: 2D at 25 nm cells
-    (TE), or a 220 nm thick wire in 3D at 40 nm cells."""
-    from lightsmith.problems import Box, DeviceProblem, Port, Prism, Rectangle, Structure
-    si, sio2 = ls.ConstantIndex(n_real=3.48), ls.ConstantIndex(n_real=1.44)
-    if dimension == 2:
-        def rect(cx, sy):
-            return Structure(geometry=Prism(profile=Rectangle(center_nm=(cx, 0), size_nm=(2000, sy)), z_min_nm=-110,
-                                            z_max_nm=110), material=si)
-        return DeviceProblem(
-            dimension=2, background=sio2, structures=[rect(-1000, 500), rect(1000, 700)],
-            domain_size_nm=(2000, 2400, 0), wavelengths=[1500.0, 1600.0],
-            ports=[Port(name="o1", center_nm=(-800, 0, 0), size_nm=(0, 2000, 1), direction="+"),
-                   Port(name="o2", center_nm=(800, 0, 0), size_nm=(0, 2000, 1), direction="-")],
-            options={"fdtd": {"spacing_nm": 25.0, "polarization": "te", "precision": "double", "run_time_fs": 30.0}})
-    return DeviceProblem(
-        structures=[Structure(geometry=Box(center_nm=(-600, 0, 0), size_nm=(1200, 500, 220)), material=si),
-                    Structure(geometry=Box(center_nm=(600, 0, 0), size_nm=(1200, 700, 220)), material=si)],
-        background=sio2, domain_size_nm=(1200, 1600, 1200), wavelengths=[1500.0, 1600.0],
-        ports=[Port(name="o1", center_nm=(-600, 0, 0), size_nm=(0, 1600, 1200), direction="+"),
-               Port(name="o2", center_nm=(600, 0, 0), size_nm=(0, 1600, 1200), direction="-")],
-        options={"fdtd": {"spacing_nm": 40.0, "run_time_fs": 20.0}})
+def diff_device_case():
+    """``backend.device_runs`` of the width step and lightsmith's own S of the same problem."""
+    from lightsmith_b200.backend import device_runs
+    prob = diff_device_problem()
+    desc = device_runs(prob)
+    res = ls.solve(prob, "fdtd", "cpu")
+    assert list(res.ports) == desc["labels"]
+    S = np.asarray(res.s_real) + 1j * np.asarray(res.s_imag)
+    P.save(os.path.join(HERE, "diff_device_3d.npz"), {"desc": desc, "s": S})
+    print("diff_device_3d", desc["shape"], desc["n_steps"], desc["mesh"], np.abs(S[:, 1, 0]))
 
 
 def dielectric_sphere_problem():
@@ -510,7 +499,8 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
                                                         ref_periodic),
          "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission),
          "driver_device_2d": lambda: driver_case("device_2d", device_problem(2), ref_device),
-         "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device)}
+         "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device),
+         "diff_device_3d": diff_device_case}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

@@ -1,0 +1,115 @@
+"""The differentiable FDTD solve on the host: the port-amplitude rows against lightsmith's own
+``ModeTable.amplitudes``, the protocol lightsmith's inverse design checks, and the permittivity mapping of
+``DeviceSolver``. The lightsmith parts run where its sources are available and skip elsewhere."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+from refsrc import add_to_path  # noqa: E402
+
+HAVE_LS = add_to_path()
+needs_ls = pytest.mark.skipif(not HAVE_LS, reason="lightsmith sources not available")
+
+
+def _problem():
+    from device_problems import diff_device_problem
+
+    return diff_device_problem()
+
+
+@pytest.fixture(scope="module")
+def runs():
+    if not HAVE_LS:
+        pytest.skip("lightsmith sources not available")
+    from lightsmith_b200.backend import device_runs
+
+    return device_runs(_problem(), keep_tables=True)
+
+
+@needs_ls
+def test_port_rows_restate_the_mode_amplitudes(runs):
+    """Each row's linear functional gives ModeTable.amplitudes (ports.py:265-280) on random accumulators."""
+    rng = np.random.default_rng(5)
+    nw = len(runs["omega"])
+    mons = runs["plans"][0]["monitors"]
+    ne = [len(m["e_idx"]) for m in mons]
+    nh = [len(m["h_idx1"]) for m in mons]
+    E = [rng.normal(size=(nw, n)) + 1j * rng.normal(size=(nw, n)) for n in ne]
+    H = [rng.normal(size=(nw, n)) + 1j * rng.normal(size=(nw, n)) for n in nh]
+    Ecat, Hcat = np.concatenate(E, 1), np.concatenate(H, 1)
+    r = 0
+    for fi, tab in enumerate(runs["tables"]):
+        for mm in range(tab.frame.num_modes):
+            row = runs["rows"][r]
+            a_ref, c_ref = tab.amplitudes(runs["omega"], E[fi], H[fi], mm)
+            e0, h0 = row["e_off"], row["h_off"]
+            Ef, Hf = Ecat[:, e0:e0 + ne[fi]], Hcat[:, h0:h0 + nh[fi]]
+            a = (row["in_e"] * Ef).sum(1) + (row["in_h"] * Hf).sum(1)
+            c = (row["out_e"] * Ef).sum(1) + (row["out_h"] * Hf).sum(1)
+            np.testing.assert_allclose(a, a_ref, rtol=1e-12, atol=1e-12 * np.abs(a_ref).max())
+            np.testing.assert_allclose(c, c_ref, rtol=1e-12, atol=1e-12 * np.abs(c_ref).max())
+            r += 1
+    assert r == len(runs["labels"]) == 2
+
+
+@needs_ls
+def test_runs_follow_the_device_driver(runs):
+    from lightsmith.backends._fdtd import device as D
+    from lightsmith.backends.fdtd import NativeFDTD
+
+    prob = _problem()
+    p = D.plan(prob, NativeFDTD._options(prob), False)
+    assert tuple(runs["shape"]) == tuple(p["grid"].shape)
+    assert runs["n_steps"] == p["max_steps"]
+    assert runs["mesh"] == "subpixel"
+    for pl in runs["plans"]:
+        assert len(pl["monitors"]) == 2 and type(pl["sources"][0]).__name__ == "ModeSource"
+        assert pl["stride"] == p["stride"]
+
+
+@needs_ls
+def test_backend_serves_lightsmiths_inverse_protocol(runs):
+    from lightsmith.device import Device
+    from lightsmith.inverse.topopt import check_backend
+
+    from lightsmith_b200.backend import B200FDTD
+    from lightsmith_b200.differentiable import DeviceSolver
+
+    check_backend(B200FDTD)
+    solver = DeviceSolver({k: v for k, v in runs.items() if k != "tables"})
+    g = B200FDTD.design_grid(None, solver=solver)
+    assert g.shape == tuple(runs["shape"]) and len(g.x) == g.shape[0] and len(g.z) == g.shape[2]
+    assert np.allclose(np.diff(g.x), g.dl)
+    base = B200FDTD.base_permittivity(None, solver=solver)
+    assert base.shape == (len(runs["wavelengths_nm"]),) + g.shape and np.iscomplexobj(base)
+    assert base.real.min() > 2.0 and base.real.max() < 12.2  # silica 1.44^2 .. silicon 3.48^2
+    with pytest.raises(ValueError, match="CUDA"):
+        B200FDTD.differentiable_solve(_problem(), None, Device("numpy", "cpu"), solver=solver)
+
+
+def test_permittivity_mapping_on_the_box():
+    """Nodes equal to the base keep the per-component 1/eps; changed nodes take 1/eps on all three; changes
+    outside the interior box are rejected."""
+    from lightsmith_b200.differentiable import DeviceSolver, interior_box
+
+    shape = (12, 10, 14)
+    rng = np.random.default_rng(1)
+    inv = rng.uniform(0.1, 1.0, size=(3,) + shape)
+    desc = {"shape": shape, "inv_eps": inv, "pml_cells": ((3, 3), (0, 0), (2, 4)), "labels": ["a"],
+            "n_steps": 10, "omega": [1.0], "plans": [], "rows": []}
+    s = DeviceSolver(desc)
+    assert s.box == interior_box(shape, desc["pml_cells"]) == ((4, 7), (1, 9), (3, 8))
+    eps = s.base_nodes.copy()
+    assert np.array_equal(s.inv_eps_box(eps), inv[:, 4:7, 1:9, 3:8])
+    eps[5, 2, 4] = 4.0
+    got = s.inv_eps_box(eps)
+    assert np.allclose(got[:, 1, 1, 1], 0.25)
+    got[:, 1, 1, 1] = inv[:, 5, 2, 4]
+    assert np.array_equal(got, inv[:, 4:7, 1:9, 3:8])
+    eps[3, 2, 4] = 4.0  # in the x CPML slab
+    with pytest.raises(ValueError, match="interior box"):
+        s.inv_eps_box(eps)
