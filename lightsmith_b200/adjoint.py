@@ -1,8 +1,9 @@
 """Gradients of an FDTD objective by the discrete adjoint, behind ``torch.autograd``.
 
 lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
-the FDTD path: for a run with real fields, no periodic axis and pure (staircase) dispersive groups at most (a
-slab waveguide device, a metal nanoparticle cluster), a real objective J of one DFT monitor's accumulators,
+the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase) and pure (staircase)
+dispersive groups at most (a slab waveguide device, a metal nanoparticle cluster, a 2D device with its
+periodic invariant axis), a real objective J of one DFT monitor's accumulators (or several monitors'),
 and its gradient with respect to 1/eps over a design box of non-dispersive nodes. J is either
 |sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2 at one frequency f, or any torch function of the
 accumulators (a flux spectrum, say): its adjoint source G = 2 dJ/d(acc) comes from torch autograd on J.
@@ -54,8 +55,8 @@ class AdjointRun:
     def __init__(self, plan: dict, box, monitor=0, freq: int = 0, wE=None, wH=None, checkpoint: int = 256,
                  precision: str | None = None, device="cuda:0", objective=None, sources_in_box: bool = False):
         torch = _torch()
-        if plan["complex"] or any(plan["periodic"]):
-            raise ValueError("the adjoint serves real fields without periodic axes")
+        if plan["complex"]:
+            raise ValueError("the adjoint serves real fields (no Bloch phase)")
         if any(g["w"] is not None for g in plan["groups"]):
             raise ValueError("the adjoint serves pure (staircase) dispersive groups, not mixed (subpixel) ones")
         for s in plan["sources"]:

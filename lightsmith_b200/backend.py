@@ -133,8 +133,6 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
 
     if not isinstance(problem, DeviceProblem):
         raise ValueError("the differentiable FDTD solve takes device problems")
-    if problem.dimension != 3:
-        raise NotImplementedError("2D device problems step a periodic axis, which the adjoint does not serve")
     ok, why = D.supports(problem)
     if not ok:
         raise ValueError(why)
@@ -151,13 +149,15 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     _, slots = D._media(problem, wl, [])
     w1, w2, wc, sigma, wa, wb = p["band"]
     dx = grid.engine_spacing()
-    slot_fn = D._slot_fn(problem, slots, None)
+    two_d = bool(grid.two_d)
+    slot_fn = D._slot_fn(problem, slots, problem.domain_center_nm[2] if two_d else None)
     asked = opts.mesh_refinement or ("subpixel" if opts.subpixel else "staircase")
     mode = "staircase" if asked == "staircase" or any(m.dispersive for m in media) else "subpixel"
     inv_eps, groups, _, _ = voxelise(slot_fn, media, grid.shape, grid.origin, dx, np.array([1, 1, 1]),
                                      np.array(grid.shape) - 1, mode=mode, samples=opts.subpixel_samples,
                                      periodic=grid.periodic, grid=grid.graded)
-    tables = [ModeTable(f, f.ds, dt, wa, wb, D._eps_fn(f, inv_eps, groups, dt), polarization=None) for f in frames]
+    pol = {"te": "x", "tm": "y"}[opts.polarization or "te"] if two_d else None
+    tables = [ModeTable(f, f.ds, dt, wa, wb, D._eps_fn(f, inv_eps, groups, dt), polarization=pol) for f in frames]
     n_bg = float(np.sqrt(max(media[0].eps_inf, 1.0)))
     cells = tuple((0, 0) if per else (grid.n_pml, grid.n_pml) for per in grid.periodic)
     pml = PMLSpec(cells=cells, kappa_max=opts.pml_kappa, alpha_max=0.05 * 2 * np.pi * n_bg / float(wl.max()),
@@ -187,7 +187,7 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     out = {"shape": tuple(int(v) for v in grid.shape), "inv_eps": np.asarray(inv_eps, float), "plans": plans,
            "labels": labels, "rows": _port_rows(tables, omega, e_counts, h_counts), "omega": omega,
            "wavelengths_nm": wl, "n_steps": n_steps, "pml_cells": cells, "coords": coords, "dl": float(grid.dx),
-           "mesh": mode}
+           "mesh": mode, "two_d": two_d}
     if keep_tables:
         out["tables"] = tables
     return out
@@ -195,7 +195,7 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
 
 class B200FDTD(NativeFDTD):
     """``NativeFDTD`` (backends/fdtd.py:47) whose engine is the B200 one on CUDA devices, and which serves
-    lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) for 3D device problems on CUDA
+    lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) for device problems on CUDA
     devices (``lightsmith_b200.differentiable``)."""
 
     name = "lightsmith-fdtd"
@@ -216,24 +216,29 @@ class B200FDTD(NativeFDTD):
     @classmethod
     def design_grid(cls, problem, solver=None):
         """The FDTD grid's nodes (``x``, ``y``, ``z`` in nm, ``dl``, ``shape``); node (i, j, k) carries the
-        permittivity of its three E components."""
-        from .differentiable import DesignGrid
+        permittivity of its three E components. A 2D device's grid is (x, y): its stepped plane."""
+        from .differentiable import DesignGrid, DesignGrid2D
 
         d = solver.desc if solver is not None else device_runs(problem)
         x, y, z = d["coords"]
+        if d.get("two_d"):
+            return DesignGrid2D(x=x, y=y, dl=d["dl"], shape=tuple(d["shape"][:2]))
         return DesignGrid(x=x, y=y, z=z, dl=d["dl"], shape=tuple(d["shape"]))
 
     @classmethod
     def base_permittivity(cls, problem, solver=None) -> np.ndarray:
-        """(n_wl, Nx, Ny, Nz) complex: per node, 1 over the mean of its three E components' 1/eps."""
+        """(n_wl, Nx, Ny, Nz), or (n_wl, Nx, Ny) for a 2D device, complex: per node, 1 over the mean of its three
+        E components' 1/eps."""
         d = solver.desc if solver is not None else device_runs(problem)
         nodes = 1.0 / np.asarray(d["inv_eps"], float).mean(axis=0)
+        if d.get("two_d"):
+            nodes = nodes[:, :, 1]
         return np.broadcast_to(nodes, (len(d["wavelengths_nm"]),) + nodes.shape).astype(complex)
 
     @classmethod
     def differentiable_solve(cls, problem, eps_grid_override=None, device="gpu", sources=None,
                              with_fields: bool = False, solver=None):
-        """S-parameters as torch tensors connected to ``eps_grid_override`` ((n_wl, Nx, Ny, Nz) or (Nx, Ny, Nz),
+        """S-parameters as torch tensors connected to ``eps_grid_override`` ((n_wl, Nx, Ny[, Nz]) or (Nx, Ny[, Nz]),
         real and equal across wavelengths), by the CUDA engine and the discrete adjoint."""
         import torch
         from lightsmith.backends.fdfd import DifferentiableSolution
@@ -249,10 +254,10 @@ class B200FDTD(NativeFDTD):
         if solver is None:
             solver = DeviceSolver(device_runs(problem, dev))
         if eps_grid_override is None:
-            eps = torch.as_tensor(solver.base_nodes, dtype=torch.float64)
+            eps = torch.as_tensor(solver.base_design, dtype=torch.float64)
         else:
             e = torch.as_tensor(eps_grid_override)
-            if e.dim() == 3:
+            if e.dim() == len(solver.design_shape):
                 e = e[None]
             if torch.is_complex(e):
                 if torch.any(e.imag.detach() != 0):

@@ -1,4 +1,4 @@
-// The discrete adjoint of the FDTD step (real fields, no periodic axis), for gradients of a DFT objective.
+// The discrete adjoint of the FDTD step (real fields), for gradients of a DFT objective.
 //
 // A forward step is linear in the state (E, H and the CPML psi): H^{n+1/2} from H^{n-1/2} and E^n
 // (update_h_node), then E^{n+1} from E^n and H^{n+1/2} (update_e_node); sources add terms that do not depend
@@ -15,6 +15,10 @@
 // double buffered (each kernel reads the step's old values, also at neighbours, and writes the new ones).
 // A warp whose nodes and neighbours are all interior (stepped, in no slab) takes the plain stencil; any
 // other warp takes the stencil with the stepped-region tests as masks plus the slab terms per axis.
+// A periodic axis steps nodes 1 .. n-2 of both fields between two ghost planes, which the forward step fills
+// by copies (E's high ghost n-1 from plane 1 before the H update, H's low ghost 0 from plane n-2 before the
+// E update); their transposes (k_adj_ghost) move a ghost plane's adjoint onto its source plane and clear it,
+// after the transposed E update for H and after the transposed H update for E.
 //
 // The objective's adjoint source (the DFT samples' weights times e^{i omega t}) is added to Ebar and Hbar at
 // the steps the monitor sampled, before that step's reverse. The gradient with respect to the E curl
@@ -53,17 +57,18 @@ __device__ __forceinline__ int adj_side(const PmlAxis<R>& pm, int c, int u) {
 }
 
 // Transposed E update at H node x for a warp with any node outside the interior: the curl stencil with the
-// stepped-region tests as masks (non-periodic grids), then, per axis d whose slab holds x or x + e_d, the CPML
-// terms of the two components c != d (warp-uniform branches for d = 0, 1), and x's own E psibar.
+// stepped-region tests as masks, then, per axis d whose slab holds x or x + e_d, the CPML terms of the two
+// components c != d (warp-uniform branches for d = 0, 1), and x's own E psibar.
 template <bool UNI, typename R>
 __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
+  // E_c's stepped range along each axis: [1, n - 1), or [0, n - 1) along c itself on a non-periodic axis
   bool okc[3], oko[3], nb[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    okc[a] = x[a] < g.n[a] - 1;  // along the component's own axis
-    oko[a] = x[a] >= 1 && okc[a];
+    oko[a] = x[a] >= 1 && x[a] < g.n[a] - 1;
+    okc[a] = g.periodic[a] ? oko[a] : x[a] < g.n[a] - 1;  // along the component's own axis
     nb[a] = x[a] + 1 < g.n[a] - 1;
   }
   R eb0[3], cb0[3], eb1[3][3], cb1[3][3];
@@ -204,22 +209,25 @@ template <bool UNI, typename R>
 __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
-  bool lt[3], ge1[3];
+  // H_c's stepped range: [0, n - 1), or [0, n) along c itself; [1, n - 1) along a periodic axis. own[a]: x
+  // in range along axis a != c (and along c on a periodic axis), back[a]: x - e_a in range along a
+  bool own[3], back[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    lt[a] = x[a] < g.n[a] - 1;
-    ge1[a] = x[a] >= 1;
+    own[a] = x[a] < g.n[a] - 1 && (!g.periodic[a] || x[a] >= 1);
+    back[a] = g.periodic[a] ? x[a] >= 2 : x[a] >= 1;
   }
   R hb0[3], hb1[3][3];
   bool m0[3], m1[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    m0[c] = lt[(c + 1) % 3] && lt[(c + 2) % 3];
+    const bool alc = !g.periodic[c] || own[c];  // along c itself
+    m0[c] = own[(c + 1) % 3] && own[(c + 2) % 3] && alc;
     hb0[c] = m0[c] ? A.Hb[c][p] : R(0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (d == c) continue;
-      m1[c][d] = ge1[d] && lt[3 - c - d];
+      m1[c][d] = back[d] && own[3 - c - d] && alc;
       hb1[c][d] = m1[c][d] ? A.Hb[c][p - st[d]] : R(0);
     }
   }
@@ -316,6 +324,27 @@ __global__ void __launch_bounds__(256, 5) k_adj_h(const __grid_constant__ AdjArg
   A.Eb[0][p] = eb0 + acc[0];
   A.Eb[1][p] = eb1 + acc[1];
   A.Eb[2][p] = eb2 + acc[2];
+}
+
+// Transpose of one periodic ghost plane's copy (dst <- src, real fields): the adjoint of dst is added to src
+// and dst's cleared, for the three components over the plane normal to `axis` (k_ghost's enumeration).
+template <typename R>
+__global__ void k_adj_ghost(R* f0, R* f1, R* f2, int n0, int n1, int n2, int axis, int dst, int src) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = axis == 0 ? n1 : n0, nb = axis == 2 ? n1 : n2;
+  if (t >= 3 * na * nb) return;
+  const int comp = t / (na * nb);
+  const int r = t % (na * nb);
+  const int u = r / nb, v = r % nb;
+  int xd[3], xs[3];
+  if (axis == 0) { xd[0] = dst; xs[0] = src; xd[1] = xs[1] = u; xd[2] = xs[2] = v; }
+  else if (axis == 1) { xd[1] = dst; xs[1] = src; xd[0] = xs[0] = u; xd[2] = xs[2] = v; }
+  else { xd[2] = dst; xs[2] = src; xd[0] = xs[0] = u; xd[1] = xs[1] = v; }
+  R* f = comp == 0 ? f0 : (comp == 1 ? f1 : f2);
+  const long long pd = ((long long)xd[0] * n1 + xd[1]) * n2 + xd[2];
+  const long long ps = ((long long)xs[0] * n1 + xs[1]) * n2 + xs[2];
+  f[ps] += f[pd];
+  f[pd] = R(0);
 }
 
 constexpr int kAdjMaxFreq = 128;

@@ -541,8 +541,6 @@ struct Engine final : lsfdtd_engine {
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
     if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no conformal off-diagonal terms");
     if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no vertex-tensor mesh");
-    if (desc.periodic[0] || desc.periodic[1] || desc.periodic[2])
-      return fail(LSFDTD_EUNSUPPORTED, "adjoint: no periodic axis");
     for (auto& gr : groups)
       if (gr.mixed) return fail(LSFDTD_EUNSUPPORTED, "adjoint: mixed (subpixel) dispersive groups have no adjoint");
     if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
@@ -1425,7 +1423,7 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
   // inner node ranges per axis: in every component's stepped region and past every slab of the field
   for (int ax = 0; ax < 3; ++ax) {
     const int n = A.y.n[ax];
-    int elo = 1, ehi = n - 1, hlo = 0, hhi = n - 1;
+    int elo = 1, ehi = n - 1, hlo = A.y.periodic[ax] ? 1 : 0, hhi = n - 1;
     const PmlAxis<R>& pm = A.y.pml[ax];
     if (pm.on) {
       const int c = (ax + 1) % 3;  // a component with slabs along ax (both share their extent)
@@ -1457,16 +1455,26 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
     LS_LAUNCHED();
   }
   const dim3 grid(cdiv(A.y.n[2], 32), cdiv(A.y.n[1], 8), A.y.n[0]);
-  if (A.y.uniform) {
-    k_adj_e<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
-    LS_LAUNCHED();
-    k_adj_h<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
-  } else {
-    k_adj_e<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
-    LS_LAUNCHED();
-    k_adj_h<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
-  }
+  // periodic ghost copies of the forward step, transposed in the reverse order (axes 2, 1, 0)
+  auto ghosts_t = [&](R* const* f, bool low) -> int {
+    for (int ax = 2; ax >= 0; --ax) {
+      if (!A.y.periodic[ax]) continue;
+      const int n = A.y.n[ax];
+      const int na = ax == 0 ? A.y.n[1] : A.y.n[0], nb = ax == 2 ? A.y.n[1] : A.y.n[2];
+      k_adj_ghost<R><<<cdiv(3LL * na * nb, 256), 256, 0, s>>>(f[0], f[1], f[2], A.y.n[0], A.y.n[1], A.y.n[2], ax,
+                                                            low ? 0 : n - 1, low ? n - 2 : 1);
+      LS_LAUNCHED();
+    }
+    return LSFDTD_OK;
+  };
+  if (A.y.uniform) k_adj_e<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
+  else k_adj_e<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
   LS_LAUNCHED();
+  LS_TRY(ghosts_t(A.Hb, true));  // H's low ghosts were filled before the E update
+  if (A.y.uniform) k_adj_h<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
+  else k_adj_h<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
+  LS_LAUNCHED();
+  LS_TRY(ghosts_t(A.Eb, false));  // E's high ghosts were filled before the H update
   a->buf = w;
   return LSFDTD_OK;
 }

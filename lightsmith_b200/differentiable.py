@@ -10,9 +10,10 @@ per port mode, a mode source and one DFT monitor per port) are handed over as a 
 step); this module needs no lightsmith, so the GPU tests replay a recorded description.
 
 The permittivity grid is the FDTD grid's nodes: node (i, j, k) carries one real permittivity for its three E
-components (E_x at i + 1/2, E_y at j + 1/2, E_z at k + 1/2). Where the grid given equals the base (the driver's
-own voxelisation, 1/eps averaged over the three components), a node keeps the driver's per-component values;
-elsewhere its three components take 1/eps of the grid. FDTD steps a real, frequency-independent permittivity:
+components (E_x at i + 1/2, E_y at j + 1/2, E_z at k + 1/2); a 2D device's grid is its one stepped z plane
+(node k = 1 between the two ghost planes of the periodic invariant axis). Where the grid given equals the
+base (the driver's own voxelisation, 1/eps averaged over the three components), a node keeps the driver's
+per-component values; elsewhere its three components take 1/eps of the grid. FDTD steps a real, frequency-independent permittivity:
 an override must be real and equal across wavelengths.
 
 Each S column is one ``AdjointRun`` (``lightsmith_b200.adjoint``) over all port monitors: the forward runs the
@@ -42,11 +43,21 @@ def _torch():
 
 @dataclass
 class DesignGrid:
-    """The grid of ``design_grid``: node coordinates (nm) along each axis, the cell size and the shape."""
+    """The grid of ``design_grid`` of a 3D device: node coordinates (nm) along each axis, cell size, shape."""
 
     x: np.ndarray
     y: np.ndarray
     z: np.ndarray
+    dl: float
+    shape: tuple
+
+
+@dataclass
+class DesignGrid2D:
+    """The grid of ``design_grid`` of a 2D device (lightsmith's inverse design tells 2D from 3D by ``z``)."""
+
+    x: np.ndarray
+    y: np.ndarray
     dl: float
     shape: tuple
 
@@ -72,8 +83,11 @@ class DeviceSolver:
         self.desc = desc
         self.device, self.precision, self.checkpoint = device, precision, int(checkpoint)
         self.shape = tuple(int(v) for v in desc["shape"])
+        self.two_d = bool(desc.get("two_d", False))
+        self.design_shape = self.shape[:2] if self.two_d else self.shape
         self.inv_eps = np.asarray(desc["inv_eps"], float).reshape((3,) + self.shape)
         self.base_nodes = 1.0 / self.inv_eps.mean(axis=0)
+        self.base_design = self.base_nodes[:, :, 1] if self.two_d else self.base_nodes
         self.box = interior_box(self.shape, desc["pml_cells"])
         self.box_sl = tuple(slice(a, b) for a, b in self.box)
         self.labels = list(desc["labels"])
@@ -127,11 +141,20 @@ class DeviceSolver:
             self._gen[label] = 0
         return self._runs[label]
 
-    def inv_eps_box(self, eps_nodes: np.ndarray) -> np.ndarray:
-        """(3, box) 1/eps of each E component over the box for a node permittivity grid."""
-        eps_nodes = np.asarray(eps_nodes, float)
-        if eps_nodes.shape != self.shape:
-            raise ValueError(f"the permittivity grid must have the design grid's shape {self.shape}")
+    def nodes(self, eps_design: np.ndarray) -> np.ndarray:
+        """The node permittivity of the whole grid for a design-grid one (a 2D device's plane k = 1)."""
+        eps_design = np.asarray(eps_design, float)
+        if eps_design.shape != self.design_shape:
+            raise ValueError(f"the permittivity grid must have the design grid's shape {self.design_shape}")
+        if not self.two_d:
+            return eps_design
+        out = self.base_nodes.copy()
+        out[:, :, 1] = eps_design
+        return out
+
+    def inv_eps_box(self, eps_design: np.ndarray) -> np.ndarray:
+        """(3, box) 1/eps of each E component over the box for a design-grid permittivity."""
+        eps_nodes = self.nodes(eps_design)
         changed = ~np.isclose(eps_nodes, self.base_nodes, rtol=1e-12, atol=0)
         inside = np.zeros(self.shape, bool)
         inside[self.box_sl] = True
@@ -183,7 +206,7 @@ def _function():
             (eps_nodes,) = ctx.saved_tensors
             solver = ctx.solver
             box_sl = solver.box_sl
-            eps_box = torch.as_tensor(ctx.eps_np[box_sl], dtype=torch.float64)
+            eps_box = torch.as_tensor(solver.nodes(ctx.eps_np)[box_sl], dtype=torch.float64)
             total = torch.zeros(solver.shape, dtype=torch.float64)
             for j, lab in enumerate(ctx.sources):
                 g = gS[:, :, j].detach().to(torch.complex128)
@@ -200,13 +223,16 @@ def _function():
                 run.objective = objective
                 gc = run.backward(per_component=True).sum(0).cpu()
                 total[box_sl] += -gc / eps_box ** 2
+            if solver.two_d:
+                total = total[:, :, 1]
             return total.to(device=eps_nodes.device, dtype=eps_nodes.dtype), None, None
 
     return DeviceSParameters
 
 
 def s_parameters(eps_nodes, solver: DeviceSolver, sources=None):
-    """S (n_w, n_out, n_src) complex128, differentiable in ``eps_nodes`` (real, the design grid's shape)."""
+    """S (n_w, n_out, n_src) complex128, differentiable in ``eps_nodes`` (real, the design grid's shape:
+    ``solver.design_shape``)."""
     sources = list(solver.labels if sources is None else sources)
     for s in sources:
         if s not in solver.labels:

@@ -42,6 +42,39 @@ def small_case(seed: int = 4, n_chunks: int = 4, pml_cells: int = 4):
     return plan, n_steps, wE, wH
 
 
+PERIODIC_BOX = ((1, 21), (1, 17), (5, 8))
+
+
+def periodic_case(seed: int = 11, n_chunks: int = 5, pml_cells: int = 4):
+    """small_case's grid periodic along x and y (ghost planes 0 and n - 1, real fields) with CPML along z, a
+    dipole at z = 9.4 and the monitor on z-plane 12; the design box spans every stepped x and y node (next to
+    both ghost planes of each periodic axis) at z = 5..7. Returns (plan, n_steps, wE, wH)."""
+    dt = 0.99 * DX / math.sqrt(3)
+    rng = np.random.default_rng(seed)
+    inv_eps = 1.0 / rng.uniform(1.0, 4.0, size=SHAPE)
+    omega = 2 * np.pi / 300.0
+    stride = 7
+    n_steps = n_chunks * stride
+
+    def at(flat):
+        rest = np.asarray(flat) % int(np.prod(SHAPE))
+        return inv_eps[np.unravel_index(rest, SHAPE)]
+
+    dip = point_dipole(SHAPE, np.zeros(3), DX, dt, np.array([3.37, 15.37, 9.37]) * DX, (0.3, 1.0, 0.6), at,
+                       omega, 0.4 * omega, n_steps + 400)
+    w = dip.wave
+    first = int(np.nonzero(np.abs(w) > 1e-3 * np.abs(w).max())[0][0])
+    dip.wave = np.concatenate([w[first:], np.zeros(first)])
+    mon = plane_monitor(SHAPE, 12, [omega], energy=1)
+    pml = PMLSpec(cells=((0, 0), (0, 0), (pml_cells, pml_cells)), alpha_max=0.02, eps_ref=1.5)
+    plan = make_plan(shape=SHAPE, dx=DX, dt=dt, single=False, inv_eps=inv_eps, groups=[], pml=pml, sources=[dip],
+                     monitors=[mon], dft_stride=stride, periodic=(True, True, False))
+    m = len(mon.e_idx)
+    wE = rng.normal(size=m) + 1j * rng.normal(size=m)
+    wH = 0.3 * (rng.normal(size=m) + 1j * rng.normal(size=m))
+    return plan, n_steps, wE, wH
+
+
 def flux_objective(acc_e, acc_h):
     """The monitor plane's flux summed over its frequencies: 0.5 Re sum_p s_p acc_e[f, p] conj(acc_h[f, p]),
     s_p = +1 for the E_x / H_y half of the points and -1 for the E_y / H_x half (plane_monitor's layout)."""

@@ -28,9 +28,11 @@ def device_problem(dimension: int):
         options={"fdtd": {"spacing_nm": 40.0, "run_time_fs": 20.0}})
 
 
-def diff_device_problem():
-    """The 3D width step of ``device_problem(3)`` meshed subpixel in float64: the problem of the differentiable
-    solve's fixture, whose runs and S lightsmith's driver makes alike."""
-    p = device_problem(3)
-    return p.model_copy(update={"options": {"fdtd": {**p.options["fdtd"], "mesh_refinement": "subpixel",
-                                                     "precision": "double"}}})
+def diff_device_problem(dimension: int = 3):
+    """The width step of ``device_problem`` meshed subpixel in float64: the problem of the differentiable
+    solve's fixtures, whose runs and S lightsmith's driver makes alike."""
+    p = device_problem(dimension)
+    extra = {"mesh_refinement": "subpixel", "precision": "double"}
+    if dimension == 2:
+        extra["run_time_fs"] = 90.0  # the pulse through the step to the far port
+    return p.model_copy(update={"options": {"fdtd": {**p.options["fdtd"], **extra}}})

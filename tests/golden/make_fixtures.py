@@ -462,16 +462,17 @@ def emission_problem():
                            options={"fdtd": {"spacing_nm": 4.0, "run_time_fs": 2.0}})
 
 
-def diff_device_case():
+def diff_device_case(dimension: int):
     """``backend.device_runs`` of the width step and lightsmith's own S of the same problem."""
     from lightsmith_b200.backend import device_runs
-    prob = diff_device_problem()
+    prob = diff_device_problem(dimension)
     desc = device_runs(prob)
     res = ls.solve(prob, "fdtd", "cpu")
     assert list(res.ports) == desc["labels"]
     S = np.asarray(res.s_real) + 1j * np.asarray(res.s_imag)
-    P.save(os.path.join(HERE, "diff_device_3d.npz"), {"desc": desc, "s": S})
-    print("diff_device_3d", desc["shape"], desc["n_steps"], desc["mesh"], np.abs(S[:, 1, 0]))
+    name = f"diff_device_{dimension}d"
+    P.save(os.path.join(HERE, name + ".npz"), {"desc": desc, "s": S})
+    print(name, desc["shape"], desc["n_steps"], desc["mesh"], np.abs(S[:, 1, 0]))
 
 
 def dielectric_sphere_problem():
@@ -500,7 +501,8 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission),
          "driver_device_2d": lambda: driver_case("device_2d", device_problem(2), ref_device),
          "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device),
-         "diff_device_3d": diff_device_case}
+         "diff_device_3d": lambda: diff_device_case(3),
+         "diff_device_2d": lambda: diff_device_case(2)}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

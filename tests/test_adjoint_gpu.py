@@ -92,6 +92,35 @@ def test_adjoint_gradient_matches_central_differences():
     run.close()
 
 
+def test_periodic_axes_gradient_matches_central_differences():
+    """Periodic x and y: the ghost planes' copies and their transposes; nodes next to both ghost planes of
+    each axis and at a corner of the box, against central differences of the CUDA forward (float64)."""
+    from adjoint_cases import PERIODIC_BOX, periodic_case
+
+    from lightsmith_b200.adjoint import AdjointRun
+
+    plan, n_steps, wE, wH = periodic_case()
+    run = AdjointRun(plan, PERIODIC_BOX, wE=wE, wH=wH, checkpoint=2 * plan["stride"], precision="double")
+    base = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in PERIODIC_BOX)])
+    run.set_inv_eps_box(base)
+    run.forward(n_steps)
+    g = run.backward().cpu().numpy()
+    nx, ny, nz = g.shape
+    picks = [(0, 5, 1), (nx - 1, 5, 1), (4, 0, 2), (4, ny - 1, 2), (0, 0, 0), (nx - 1, ny - 1, nz - 1)]
+    picks += [tuple(int(v) for v in np.unravel_index(f, g.shape)) for f in np.argsort(-np.abs(g).reshape(-1))[:2]]
+    h = 1e-6
+    for idx in picks:
+        vals = []
+        for sgn in (1, -1):
+            x = base.clone()
+            x[idx] += sgn * h
+            run.set_inv_eps_box(x)
+            vals.append(run.forward(n_steps)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-5 * abs(fd) + 1e-7 * np.abs(g).max(), (idx, fd, g[idx])
+    run.close()
+
+
 @pytest.mark.slow
 def test_slab_device_gradient_in_rho_matches_finite_differences_on_32_cells():
     """The inverse-design workload at reduced size (float64): dJ/drho of the extruded design density by the

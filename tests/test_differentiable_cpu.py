@@ -113,3 +113,23 @@ def test_permittivity_mapping_on_the_box():
     eps[3, 2, 4] = 4.0  # in the x CPML slab
     with pytest.raises(ValueError, match="interior box"):
         s.inv_eps_box(eps)
+
+
+@needs_ls
+def test_two_d_device_design_grid_is_its_stepped_plane():
+    """A 2D device: the periodic invariant axis has three nodes; the design grid is (x, y), without ``z``, as
+    lightsmith's region_map tells 2D from 3D (inverse/parametrization.py:159)."""
+    from device_problems import diff_device_problem
+
+    from lightsmith_b200.backend import B200FDTD, device_runs
+    from lightsmith_b200.differentiable import DeviceSolver
+
+    desc = device_runs(diff_device_problem(2))
+    assert desc["two_d"] and desc["shape"][2] == 3 and desc["plans"][0]["periodic"] == (False, False, True)
+    solver = DeviceSolver(desc)
+    g = B200FDTD.design_grid(None, solver=solver)
+    assert not hasattr(g, "z") and g.shape == tuple(desc["shape"][:2]) == solver.design_shape
+    base = B200FDTD.base_permittivity(None, solver=solver)
+    assert base.shape == (2,) + g.shape
+    np.testing.assert_array_equal(solver.nodes(base[0].real), solver.base_nodes)
+    assert solver.box[2] == (1, 2)

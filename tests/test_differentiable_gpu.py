@@ -3,7 +3,8 @@ problem, and gradients against finite differences.
 
 ``diff_device_3d.npz`` holds ``backend.device_runs`` of a silicon wire width step (500 -> 700 nm, 220 nm thick,
 in silica; 73 x 83 x 73 cells at 40 nm, subpixel mesh, two ports, 279 steps) and the S matrix
-``ls.solve(problem, "fdtd", "cpu")`` gave for it in float64.
+``ls.solve(problem, "fdtd", "cpu")`` gave for it in float64; ``diff_device_2d.npz`` the same for the 2D width
+step (TE, 123 x 139 x 3 cells at 25 nm with the invariant z axis periodic, 1640 steps).
 """
 
 import numpy as np
@@ -13,9 +14,9 @@ RTOL_F64 = 1e-9  # float64 on the GPU: the same arithmetic, a different summatio
 RTOL_F32 = 2e-4  # float32 on the GPU against lightsmith's float64 CPU run
 
 
-@pytest.fixture(scope="module")
-def fixture(golden):
-    return golden("diff_device_3d")
+@pytest.fixture(scope="module", params=[3, 2], ids=["3d", "2d"])
+def fixture(golden, request):
+    return golden(f"diff_device_{request.param}d")
 
 
 def _rel(a, b):
@@ -30,7 +31,7 @@ def test_s_parameters_match_lightsmith(fixture, precision):
     from lightsmith_b200.differentiable import DeviceSolver, s_parameters
 
     solver = DeviceSolver(fixture["desc"], precision=precision)
-    S = s_parameters(torch.as_tensor(solver.base_nodes), solver).detach().cpu().numpy()
+    S = s_parameters(torch.as_tensor(solver.base_design), solver).detach().cpu().numpy()
     solver.close()
     assert S.shape == fixture["s"].shape
     err = _rel(S, fixture["s"])
@@ -38,10 +39,11 @@ def test_s_parameters_match_lightsmith(fixture, precision):
 
 
 def _design_block(solver):
-    """A 6 x 6 x 4 node block at the step, set to eps = 6 (between silica and silicon)."""
-    eps = solver.base_nodes.copy()
-    c = [n // 2 for n in solver.shape]
-    sl = (slice(c[0] - 3, c[0] + 3), slice(c[1] - 3, c[1] + 3), slice(c[2] - 2, c[2] + 2))
+    """A 6 x 6 (x 4) node block at the step, set to eps = 6 (between silica and silicon)."""
+    eps = solver.base_design.copy()
+    c = [n // 2 for n in solver.design_shape]
+    half = (3, 3, 2)
+    sl = tuple(slice(ci - h, ci + h) for ci, h in zip(c, half))
     eps[sl] = 6.0
     return eps, sl, c
 
@@ -65,12 +67,13 @@ def test_gradient_matches_finite_differences(fixture):
     L = loss(e)
     L.backward()
     g = e.grad.numpy()
-    assert g.shape == solver.shape
-    outside = np.ones(solver.shape, bool)
-    outside[solver.box_sl] = False
+    assert g.shape == solver.design_shape
+    outside = np.ones(solver.design_shape, bool)
+    outside[solver.box_sl[:len(c)]] = False
     assert np.all(g[outside] == 0) and np.abs(g[sl]).max() > 0
     lo, hi = [s.start for s in sl], [s.stop for s in sl]
-    nodes = [(lo[0], lo[1], lo[2]), (c[0], c[1], c[2]), (hi[0] - 1, c[1], hi[2] - 1), (c[0] + 1, lo[1], c[2] - 1)]
+    nodes = [(lo[0], lo[1], lo[-1]), (c[0], c[1], c[-1]), (hi[0] - 1, c[1], hi[-1] - 1), (c[0] + 1, lo[1], c[-1] - 1)]
+    nodes = [n[:len(c)] for n in nodes]
     h = 1e-3
     with torch.no_grad():
         for n in nodes:
