@@ -45,7 +45,7 @@ def _torch():
 class AdjointRun:
     """One run's forward and adjoint passes. ``box``: ((x0, x1), (y0, y1), (z0, z1)) node ranges of the design
     box; ``monitor``: the objective's monitor, or a list of monitors with the same frequencies, whose points
-    the objective sees concatenated (in list order); ``objective``: J(acc_e, acc_h) -> real torch scalar, with
+    the objective sees concatenated (in list order; the H points of those that record H); ``objective``: J(acc_e, acc_h) -> real torch scalar, with
     acc_e (n_freq, n_e) and acc_h (n_freq, n_h) or None the monitors' accumulators as complex128 tensors; or,
     when it is None, J = |A|^2 at frequency ``freq`` with ``wE``/``wH`` the complex weights of the E and H
     points (None: zero); ``checkpoint``: steps between saved states (a multiple of dft_stride).
@@ -79,15 +79,14 @@ class AdjointRun:
             raise ValueError("the objective's monitors must share their frequencies")
         nf = len(self.omegas)
         cd = torch.complex128
-        self.has_h = mons[0]["h_idx1"] is not None
-        if any((m["h_idx1"] is not None) != self.has_h for m in mons):
-            raise ValueError("the objective's monitors must all record H, or none")
+        h_mons = [m for m in mons if m["h_idx1"] is not None]
+        self.has_h = bool(h_mons)  # the H points: those of the monitors that record H, in list order
 
-        def cat(key):
-            return np.concatenate([np.asarray(m[key], np.int64) for m in mons])
-        mon = {"e_idx": cat("e_idx")}
+        def cat(key, ms):
+            return np.concatenate([np.asarray(m[key], np.int64) for m in ms])
+        mon = {"e_idx": cat("e_idx", mons)}
         if self.has_h:
-            mon["h_idx1"], mon["h_idx2"] = cat("h_idx1"), cat("h_idx2")
+            mon["h_idx1"], mon["h_idx2"] = cat("h_idx1", h_mons), cat("h_idx2", h_mons)
         if objective is None:
             wE_t = torch.as_tensor(np.zeros(len(mon["e_idx"])) if wE is None else np.asarray(wE), dtype=cd,
                                    device=self.dev)
@@ -217,7 +216,8 @@ class AdjointRun:
         ms = [eng.monitors[k] for k in self.monitors]
         torch.cuda.synchronize(self.dev)
         acc_e = torch.cat([m["acc_e"].to(torch.complex128) for m in ms], dim=1)
-        acc_h = torch.cat([m["acc_h"].to(torch.complex128) for m in ms], dim=1) if self.has_h else None
+        acc_h = (torch.cat([m["acc_h"].to(torch.complex128) for m in ms if m["acc_h"] is not None], dim=1)
+                 if self.has_h else None)
         self.acc = (acc_e, acc_h)
         with torch.no_grad():
             J = self.objective(acc_e, acc_h)

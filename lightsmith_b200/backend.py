@@ -187,7 +187,7 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     out = {"shape": tuple(int(v) for v in grid.shape), "inv_eps": np.asarray(inv_eps, float), "plans": plans,
            "labels": labels, "rows": _port_rows(tables, omega, e_counts, h_counts), "omega": omega,
            "wavelengths_nm": wl, "n_steps": n_steps, "pml_cells": cells, "coords": coords, "dl": float(grid.dx),
-           "mesh": mode, "two_d": two_d}
+           "mesh": mode, "two_d": two_d, "polarization": (opts.polarization or "te") if two_d else None}
     if keep_tables:
         out["tables"] = tables
     return out
@@ -237,9 +237,11 @@ class B200FDTD(NativeFDTD):
 
     @classmethod
     def differentiable_solve(cls, problem, eps_grid_override=None, device="gpu", sources=None,
-                             with_fields: bool = False, solver=None):
+                             with_fields: bool = True, solver=None):
         """S-parameters as torch tensors connected to ``eps_grid_override`` ((n_wl, Nx, Ny[, Nz]) or (Nx, Ny[, Nz]),
-        real and equal across wavelengths), by the CUDA engine and the discrete adjoint."""
+        real and equal across wavelengths), by the CUDA engine and the discrete adjoint. ``with_fields``: the
+        DFT field per unit incident mode amplitude, (n_wl, n_src, 3, Nx, Ny, Nz) of E, or (n_wl, n_src, Nx, Ny)
+        of H_z (TE) or E_z (TM) for a 2D device, as lightsmith's field objectives read it."""
         import torch
         from lightsmith.backends.fdfd import DifferentiableSolution
         from lightsmith.device import resolve_device
@@ -249,8 +251,6 @@ class B200FDTD(NativeFDTD):
         dev = resolve_device(device) if isinstance(device, str) else device
         if not dev.is_gpu or dev.framework != "torch":
             raise ValueError(f"{cls.name} (B200): the differentiable solve runs on PyTorch CUDA devices")
-        if with_fields:
-            raise NotImplementedError("field outputs (field-intensity objectives) have no FDTD path here")
         if solver is None:
             solver = DeviceSolver(device_runs(problem, dev))
         if eps_grid_override is None:
@@ -270,8 +270,9 @@ class B200FDTD(NativeFDTD):
                                  "across wavelengths")
             eps = e.mean(0)
         labels = solver.labels if sources is None else list(sources)
-        S = s_parameters(eps, solver, labels)
-        return DifferentiableSolution(s=S, fields=None, outputs=list(solver.labels), inputs=labels,
+        S, F = s_parameters(eps, solver, labels, fields=True) if with_fields else (s_parameters(eps, solver, labels),
+                                                                                  None)
+        return DifferentiableSolution(s=S, fields=F, outputs=list(solver.labels), inputs=labels,
                                       wavelengths_nm=np.asarray(solver.desc["wavelengths_nm"]),
                                       grid=cls.design_grid(problem, solver))
 

@@ -93,8 +93,8 @@ class DeviceSolver:
         self.labels = list(desc["labels"])
         self.n_steps = int(desc["n_steps"])
         self.omega = np.asarray(desc["omega"], float)
-        self._runs: dict[str, AdjointRun] = {}
-        self._gen: dict[str, int] = {}
+        self._runs: dict[tuple, AdjointRun] = {}  # (label, with the field monitor)
+        self._gen: dict[tuple, int] = {}
         self._amp = None
 
     # --- the port amplitudes -------------------------------------------------------------------------------
@@ -128,18 +128,53 @@ class DeviceSolver:
         row = self.labels.index(label)
         return a_out / a_in[:, row:row + 1]
 
+    # --- the field outputs ---------------------------------------------------------------------------------
+    def field_monitor(self) -> dict:
+        """A DFT monitor of the field lightsmith's field objectives read (inverse/objectives.py:53-68): E_x,
+        E_y, E_z at every node of a 3D grid; H_z (TE) or E_z (TM) at every node of a 2D device's plane k = 1
+        (a TE monitor also records that plane's E_z, which is not read)."""
+        n0, n1, n2 = self.shape
+        cells = n0 * n1 * n2
+        if not self.two_d:
+            e = np.arange(3 * cells, dtype=np.int64)
+            h = None
+        else:
+            i, j = np.meshgrid(np.arange(n0), np.arange(n1), indexing="ij")
+            plane = 2 * cells + (i.ravel() * n1 + j.ravel()) * n2 + 1
+            e = plane.astype(np.int64)
+            h = e.copy() if self.desc.get("polarization", "te") == "te" else None
+        return {"omega": self.omega, "e_idx": e, "h_idx1": h, "h_idx2": None if h is None else h.copy(),
+                "energy": 0, "space": ("grid", -1)}
+
+    def field_shape(self):
+        return (3,) + self.shape if not self.two_d else self.design_shape
+
+    def field_column(self, label, acc_e, acc_h):
+        """(n_w, *field_shape) of the run of ``label`` per unit incident amplitude of its port mode."""
+        a_in, _ = self.amplitudes(acc_e, acc_h)
+        row = self.labels.index(label)
+        ne = sum(len(m["e_idx"]) for m in self.desc["plans"][0]["monitors"])
+        nh = sum(len(m["h_idx1"]) for m in self.desc["plans"][0]["monitors"] if m["h_idx1"] is not None)
+        tm = self.desc.get("polarization", "te") == "tm"
+        f = acc_e[:, ne:] if (not self.two_d or tm) else acc_h[:, nh:]
+        f = f.reshape((f.shape[0],) + tuple(self.field_shape()))
+        return f / a_in[:, row].reshape((-1,) + (1,) * (f.dim() - 1))
+
     # --- runs ----------------------------------------------------------------------------------------------
-    def run(self, label: str) -> AdjointRun:
-        if label not in self._runs:
+    def run(self, label: str, fields: bool = False) -> AdjointRun:
+        key = (label, bool(fields))
+        if key not in self._runs:
             k = self.labels.index(label)
             plan = dict(self.desc["plans"][k])
             plan["inv_eps"] = self.inv_eps
+            if fields:
+                plan["monitors"] = list(plan["monitors"]) + [self.field_monitor()]
             mons = list(range(len(plan["monitors"])))
-            self._runs[label] = AdjointRun(plan, self.box, monitor=mons, checkpoint=self.checkpoint,
-                                           precision=self.precision, device=self.device,
-                                           objective=lambda e, h: e.real.sum() * 0, sources_in_box=True)
-            self._gen[label] = 0
-        return self._runs[label]
+            self._runs[key] = AdjointRun(plan, self.box, monitor=mons, checkpoint=self.checkpoint,
+                                         precision=self.precision, device=self.device,
+                                         objective=lambda e, h: e.real.sum() * 0, sources_in_box=True)
+            self._gen[key] = 0
+        return self._runs[key]
 
     def nodes(self, eps_design: np.ndarray) -> np.ndarray:
         """The node permittivity of the whole grid for a design-grid one (a 2D device's plane k = 1)."""
@@ -168,12 +203,12 @@ class DeviceSolver:
         inv[:, ch] = 1.0 / eps_nodes[self.box_sl][ch]
         return inv
 
-    def forward(self, label: str, eps_nodes: np.ndarray):
+    def forward(self, label: str, eps_nodes: np.ndarray, fields: bool = False):
         """Runs one column's forward pass; returns its accumulators (acc_e, acc_h), complex128 on the GPU."""
-        run = self.run(label)
+        run = self.run(label, fields)
         run.set_inv_eps_box(self.inv_eps_box(eps_nodes))
         _, acc = run.forward(self.n_steps)
-        self._gen[label] += 1
+        self._gen[(label, bool(fields))] += 1
         return acc
 
     def close(self):
@@ -186,55 +221,73 @@ def _function():
     torch = _torch()
 
     class DeviceSParameters(torch.autograd.Function):
-        """S (n_w, n_out, n_src) of a ``DeviceSolver`` as a function of the node permittivity grid."""
+        """(S (n_w, n_out, n_src), fields (n_w, n_src, *field_shape) or an empty tensor) of a
+        ``DeviceSolver`` as functions of the design-grid permittivity."""
 
         @staticmethod
-        def forward(ctx, eps_nodes, solver: DeviceSolver, sources):
+        def forward(ctx, eps_nodes, solver: DeviceSolver, sources, fields: bool):
             eps_np = eps_nodes.detach().cpu().numpy().astype(float)
-            cols, gens = [], []
+            cols, fcols, gens = [], [], []
             for lab in sources:
-                acc_e, acc_h = solver.forward(lab, eps_np)
+                acc_e, acc_h = solver.forward(lab, eps_np, fields)
                 cols.append(solver.s_column(lab, acc_e, acc_h))
-                gens.append(solver._gen[lab])
-            ctx.solver, ctx.sources, ctx.gens = solver, list(sources), gens
+                if fields:
+                    fcols.append(solver.field_column(lab, acc_e, acc_h))
+                gens.append(solver._gen[(lab, fields)])
+            ctx.solver, ctx.sources, ctx.gens, ctx.fields = solver, list(sources), gens, fields
             ctx.eps_np = eps_np
             ctx.save_for_backward(eps_nodes)
-            return torch.stack(cols, 2).to(eps_nodes.device)
+            S = torch.stack(cols, 2).to(eps_nodes.device)
+            F = torch.stack(fcols, 1).to(eps_nodes.device) if fields else S.new_zeros(0)
+            if not fields:
+                ctx.mark_non_differentiable(F)
+            return S, F
 
         @staticmethod
-        def backward(ctx, gS):
+        def backward(ctx, gS, gF):
             (eps_nodes,) = ctx.saved_tensors
             solver = ctx.solver
             box_sl = solver.box_sl
             eps_box = torch.as_tensor(solver.nodes(ctx.eps_np)[box_sl], dtype=torch.float64)
             total = torch.zeros(solver.shape, dtype=torch.float64)
+            use_f = ctx.fields and gF is not None and gF.numel() > 0
             for j, lab in enumerate(ctx.sources):
-                g = gS[:, :, j].detach().to(torch.complex128)
-                if not torch.any(g != 0):
+                g = gS[:, :, j].detach().to(torch.complex128) if gS is not None else None
+                gf = gF[:, j].detach().to(torch.complex128) if use_f else None
+                if not ((g is not None and torch.any(g != 0)) or (gf is not None and torch.any(gf != 0))):
                     continue
-                run = solver.run(lab)
-                if solver._gen[lab] != ctx.gens[j]:  # a later forward replaced this one's checkpoints
-                    solver.forward(lab, ctx.eps_np)
-                gd = g.to(run.dev)
+                key = (lab, ctx.fields)
+                run = solver.run(lab, ctx.fields)
+                if solver._gen[key] != ctx.gens[j]:  # a later forward replaced this one's checkpoints
+                    solver.forward(lab, ctx.eps_np, ctx.fields)
+                gd = None if g is None else g.to(run.dev)
+                gfd = None if gf is None else gf.to(run.dev)
 
-                def objective(acc_e, acc_h, lab=lab, gd=gd):
-                    return (gd.conj() * solver.s_column(lab, acc_e, acc_h)).sum().real
+                def objective(acc_e, acc_h, lab=lab, gd=gd, gfd=gfd):
+                    J = acc_e.real.sum() * 0
+                    if gd is not None:
+                        J = J + (gd.conj() * solver.s_column(lab, acc_e, acc_h)).sum().real
+                    if gfd is not None:
+                        J = J + (gfd.conj() * solver.field_column(lab, acc_e, acc_h)).sum().real
+                    return J
 
                 run.objective = objective
                 gc = run.backward(per_component=True).sum(0).cpu()
                 total[box_sl] += -gc / eps_box ** 2
             if solver.two_d:
                 total = total[:, :, 1]
-            return total.to(device=eps_nodes.device, dtype=eps_nodes.dtype), None, None
+            return total.to(device=eps_nodes.device, dtype=eps_nodes.dtype), None, None, None
 
     return DeviceSParameters
 
 
-def s_parameters(eps_nodes, solver: DeviceSolver, sources=None):
+def s_parameters(eps_nodes, solver: DeviceSolver, sources=None, fields: bool = False):
     """S (n_w, n_out, n_src) complex128, differentiable in ``eps_nodes`` (real, the design grid's shape:
-    ``solver.design_shape``)."""
+    ``solver.design_shape``); with ``fields``, (S, F): F (n_w, n_src, *solver.field_shape()) the DFT field per
+    unit incident amplitude of each source's port mode, differentiable too."""
     sources = list(solver.labels if sources is None else sources)
     for s in sources:
         if s not in solver.labels:
             raise ValueError(f"unknown port mode {s!r}; the ports are {solver.labels}")
-    return _function().apply(eps_nodes, solver, sources)
+    S, F = _function().apply(eps_nodes, solver, sources, bool(fields))
+    return (S, F) if fields else S

@@ -117,3 +117,43 @@ def test_gradient_flows_through_a_density(fixture):
     ad = float((rho.grad * d).sum())
     assert abs(ad - fd) <= 1e-5 * abs(fd), (ad, fd)
     solver.close()
+
+
+@pytest.mark.gpu
+def test_field_outputs_and_their_gradient(fixture):
+    """The field outputs (a whole-grid DFT monitor added to each run): S unchanged by it, and the gradient of a
+    mean |field|^2 over a small box (lightsmith's field-intensity term, inverse/objectives.py:53-68) against
+    central differences."""
+    import torch
+
+    from lightsmith_b200.differentiable import DeviceSolver, s_parameters
+
+    solver = DeviceSolver(fixture["desc"], precision="double")
+    eps0, sl, c = _design_block(solver)
+    e = torch.as_tensor(eps0)
+    S_plain = s_parameters(e, solver, sources=["o1"]).detach()
+    S, F = s_parameters(e, solver, sources=["o1"], fields=True)
+    assert torch.equal(S.detach(), S_plain)
+    assert F.shape == (2, 1) + tuple(solver.field_shape())
+    # a box a few nodes past the block towards port o2
+    fb = tuple(slice(ci + 6, ci + 9) for ci in c)
+
+    def loss(x):
+        _, f = s_parameters(x, solver, sources=["o1"], fields=True)
+        f = f[:, 0]
+        if f.dim() == 5:  # 3D: |E|^2 summed over the components
+            return (f[(slice(None), slice(None)) + fb].abs() ** 2).sum(1).mean()
+        return (f[(slice(None),) + fb].abs() ** 2).mean()
+
+    x = e.clone().requires_grad_(True)
+    loss(x).backward()
+    g = x.grad.numpy()
+    h = 1e-3
+    with torch.no_grad():
+        for n in [tuple(ci for ci in c), tuple(s.start for s in sl)]:
+            ep, em = eps0.copy(), eps0.copy()
+            ep[n] += h
+            em[n] -= h
+            fd = (float(loss(torch.as_tensor(ep))) - float(loss(torch.as_tensor(em)))) / (2 * h)
+            assert abs(g[n] - fd) <= 1e-5 * abs(fd) + 1e-9 * np.abs(g).max(), (n, g[n], fd)
+    solver.close()
