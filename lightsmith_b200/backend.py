@@ -112,7 +112,33 @@ def _port_rows(tables, omega, e_counts, h_counts) -> list[dict]:
     return rows
 
 
-def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: bool = False) -> dict:
+def _decay_steps(problem, opts, p, src, kw, device, engine) -> int:
+    """The step count lightsmith's run loop picks for the first port mode's run of the base structure
+    (device.py:547-550 calling setup.py:722-773: until the monitors' energy has decayed, or the time cap), run
+    on ``engine`` (the CUDA engine by default, on ``device``)."""
+    import math
+
+    from lightsmith.backends._fdtd import device as D
+    from lightsmith.backends._fdtd.setup import run_until_decayed
+    from lightsmith.problems import wavelength_array
+
+    if engine is None:
+        if device is None or not device.is_gpu:
+            raise ValueError("the differentiable FDTD solve runs a fixed step count: set options['fdtd']"
+                             "['run_time_fs'], pass n_steps, or give a CUDA device to find it by a decay run")
+        engine = _engine.Engine
+    wl = wavelength_array(problem.wavelengths)
+    w1, dt, stride = p["band"][0], p["dt"], p["stride"]
+    n_max = D._n_max(problem, wl)
+    transit = 1.5 * n_max * float(np.sum(problem.domain_size_nm))
+    eng = engine(device, **kw)
+    steps, _, _ = run_until_decayed(eng, opts, max_steps=p["max_steps"], min_steps=int((src.t_off + transit) / dt),
+                                    window=math.ceil(2 * np.pi * n_max / (w1 * stride * dt)), warnings=[])
+    return int(steps)
+
+
+def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: bool = False,
+                engine=None) -> dict:
     """The runs lightsmith's device driver makes for ``problem`` (backends/_fdtd/device.py:475-561), as the
     plain description ``lightsmith_b200.differentiable.DeviceSolver`` solves: one plan per port mode (its mode
     source and one DFT monitor per port), the driver's 1/eps, the port-amplitude rows, the design grid's node
@@ -121,8 +147,10 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     The set-up is lightsmith's own (plan, voxelisation, mode tables, pulse band, CPML), with two choices the
     adjoint needs: the mesh is staircase where a dispersive medium is present (its D-form groups must be pure)
     and subpixel or staircase otherwise as the options ask (conformal asks for subpixel: the adjoint has no
-    off-diagonal terms); the step count is fixed: the options' ``run_time_fs`` (the driver's ``max_steps``), or
-    ``n_steps``. ``keep_tables`` adds lightsmith's mode tables (not plain data) under ``"tables"``."""
+    off-diagonal terms); the step count is fixed: the options' ``run_time_fs`` (the driver's ``max_steps``),
+    ``n_steps``, or else the count lightsmith's run loop reaches on the base structure's first run (on
+    ``engine``: the CUDA engine on ``device`` by default). ``keep_tables`` adds lightsmith's mode tables (not
+    plain data) under ``"tables"``."""
     from lightsmith.backends._fdtd import device as D
     from lightsmith.backends._fdtd.engine import DFTMonitor, PMLSpec
     from lightsmith.backends._fdtd.ports import ModeSource, ModeTable
@@ -162,25 +190,25 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     cells = tuple((0, 0) if per else (grid.n_pml, grid.n_pml) for per in grid.periodic)
     pml = PMLSpec(cells=cells, kappa_max=opts.pml_kappa, alpha_max=0.05 * 2 * np.pi * n_bg / float(wl.max()),
                   eps_ref=media[0].eps_inf)
-    if n_steps is None:
-        if not opts.run_time_fs:
-            raise ValueError("the differentiable FDTD solve runs a fixed step count: set options['fdtd']"
-                             "['run_time_fs'] (or pass n_steps)")
+    if n_steps is None and opts.run_time_fs:
         n_steps = p["max_steps"]
-    n_steps = int(n_steps) // stride * stride
     labels = [lab for f in frames for lab in f.labels()]
-    plans = []
+    plans, decided = [], None
     for f, tab in zip(frames, tables):
         for m in range(f.num_modes):
             src = ModeSource(tab, m, inv_eps=inv_eps, dt=dt, omega_c=wc, sigma=sigma,
-                             n_steps=max(p["max_steps"], n_steps) + 4 * stride)
+                             n_steps=p["max_steps"] + 4 * stride)
             mons = [DFTMonitor(omega, g.e_nodes(g.k_m), g.h_nodes(g.k_m), g.h_nodes(g.k_m), energy=True)
                     for g in frames]
-            pl = P.make_plan(shape=grid.shape, dx=dx, dt=dt, single=single, inv_eps=inv_eps, groups=groups,
-                             pml=pml, sources=[src], monitors=mons, dft_stride=stride, periodic=grid.periodic,
-                             widths=grid.engine_widths())
+            kw = dict(shape=grid.shape, dx=dx, dt=dt, single=single, inv_eps=inv_eps, groups=groups, pml=pml,
+                      sources=[src], monitors=mons, dft_stride=stride, periodic=grid.periodic,
+                      widths=grid.engine_widths())
+            if n_steps is None and decided is None:
+                decided = _decay_steps(problem, opts, p, src, kw, device, engine)
+            pl = P.make_plan(**kw)
             pl.pop("inv_eps")
             plans.append(pl)
+    n_steps = int(n_steps if n_steps is not None else decided) // stride * stride
     e_counts = [len(m["e_idx"]) for m in plans[0]["monitors"]]
     h_counts = [len(m["h_idx1"]) for m in plans[0]["monitors"]]
     coords = [np.array([grid.coord(a, i) for i in range(grid.shape[a])], float) for a in range(3)]
@@ -208,10 +236,13 @@ class B200FDTD(NativeFDTD):
     @classmethod
     def prepare(cls, problem) -> dict:
         """The runs' description and their solver, reused across optimisation iterations."""
+        import torch
+        from lightsmith.device import resolve_device
+
         from .differentiable import DeviceSolver
 
-        desc = device_runs(problem)
-        return {"solver": DeviceSolver(desc)}
+        dev = resolve_device("gpu") if torch.cuda.is_available() else None
+        return {"solver": DeviceSolver(device_runs(problem, dev))}
 
     @classmethod
     def design_grid(cls, problem, solver=None):
@@ -219,7 +250,7 @@ class B200FDTD(NativeFDTD):
         permittivity of its three E components. A 2D device's grid is (x, y): its stepped plane."""
         from .differentiable import DesignGrid, DesignGrid2D
 
-        d = solver.desc if solver is not None else device_runs(problem)
+        d = solver.desc if solver is not None else device_runs(problem, n_steps=0)
         x, y, z = d["coords"]
         if d.get("two_d"):
             return DesignGrid2D(x=x, y=y, dl=d["dl"], shape=tuple(d["shape"][:2]))
@@ -229,7 +260,7 @@ class B200FDTD(NativeFDTD):
     def base_permittivity(cls, problem, solver=None) -> np.ndarray:
         """(n_wl, Nx, Ny, Nz), or (n_wl, Nx, Ny) for a 2D device, complex: per node, 1 over the mean of its three
         E components' 1/eps."""
-        d = solver.desc if solver is not None else device_runs(problem)
+        d = solver.desc if solver is not None else device_runs(problem, n_steps=0)
         nodes = 1.0 / np.asarray(d["inv_eps"], float).mean(axis=0)
         if d.get("two_d"):
             nodes = nodes[:, :, 1]

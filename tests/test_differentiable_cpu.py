@@ -133,3 +133,25 @@ def test_two_d_device_design_grid_is_its_stepped_plane():
     assert base.shape == (2,) + g.shape
     np.testing.assert_array_equal(solver.nodes(base[0].real), solver.base_nodes)
     assert solver.box[2] == (1, 2)
+
+
+@needs_ls
+def test_step_count_without_a_run_time_follows_lightsmiths_run_loop():
+    """Without run_time_fs the step count is the one lightsmith's run loop reaches on the base structure's
+    first run (here on lightsmith's own CPU engine): the steps its own solve of the problem reports."""
+    import lightsmith as ls
+    from device_problems import diff_device_problem
+    from lightsmith.backends._fdtd.engine import Engine as RefEngine
+    from lightsmith.device import Device
+
+    from lightsmith_b200.backend import device_runs
+
+    p = diff_device_problem(2)
+    fdtd = {k: v for k, v in p.options["fdtd"].items() if k != "run_time_fs"}
+    fdtd.update(max_time_fs=600.0, decay_by=1e-2)  # decays at 6200 steps, before the 10720-step cap
+    p = p.model_copy(update={"options": {"fdtd": fdtd}})
+    with pytest.raises(ValueError, match="run_time_fs"):
+        device_runs(p)
+    desc = device_runs(p, Device("numpy", "cpu"), engine=RefEngine)
+    res = ls.solve(p, "fdtd", "cpu")
+    assert desc["n_steps"] == res.provenance["runs"][0]["steps"] < 10720
