@@ -49,10 +49,13 @@ def _args():
     ap.add_argument("--tile-y", type=int, default=8, help="fused pass: tile rows along y")
     ap.add_argument("--planes", type=int, default=0, help="fused pass: x planes per CTA (0: chosen per grid)")
     ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring")
-    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint", "clusters"],
+    ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint", "clusters",
+                                                                 "sphere"],
                     help="sweep: the batched oblique-incidence sweep (96 Bloch-periodic runs) against the same "
                          "runs one after another; adjoint: the slab device's gradient against its forward run; "
-                         "clusters: forward + gradient over dispersive sphere clusters, with FP64 errors")
+                         "clusters: forward + gradient over dispersive sphere clusters, with FP64 errors; sphere: "
+                         "the whole 129^3 dispersive-sphere solve from lightsmith's own plan, with its cross "
+                         "sections against lightsmith's FP64 CPU solve")
     ap.add_argument("--runs", type=int, default=96, help="sweep: number of runs")
     ap.add_argument("--sweep-steps", type=int, default=3000, help="sweep: FDTD steps per run")
     ap.add_argument("--instances", type=int, default=24, help="clusters: number of instances")
@@ -535,6 +538,85 @@ def run_clusters(args):
     print(json.dumps(out), flush=True)
 
 
+def run_sphere(args):
+    """The whole dispersive-sphere scattering solve at full size: the plan lightsmith's scattering driver built
+    for an r = 40 nm Drude-Lorentz sphere in n = 1.33 (129^3 cells of 2 nm, CPML 12, table-fed TF/SF, two flux
+    boxes and the incident reference view at 81 wavelengths, staircase mesh, dft_stride 100), replayed from
+    ``tests/golden/solve_c0.npz`` for its 4000 steps on the CUDA engine in FP32 and FP64. ``value``: Gcell-updates/s
+    of the FP32 solve on the device clock (40 chunks replayed as CUDA graphs); ``e2e``: the same solve through
+    ``Engine.from_plan`` with the plan's host arrays copied in and the accumulators read back inside the timed
+    region. Cross sections (C_ext, C_sca, C_abs at 9 of the 81 wavelengths) from the accumulators by the
+    restated post-processing, against lightsmith's own FP64 CPU solve, per precision."""
+    import numpy as np
+    import torch
+
+    from lightsmith_b200 import plan as P
+    from lightsmith_b200.engine import Engine
+    from oracle.post import cross_sections
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    d = P.load(os.path.join(HERE, "tests", "golden", "solve_c0.npz"))
+    plan, post, ref = d["plan"], d["post"], d["out"]
+    sel = np.asarray(post["freq_sel"])
+    chunks = post["steps"] // plan["stride"]
+    cells = int(np.prod(plan["shape"]))
+    warm = Engine.from_plan(plan, precision="single")  # untimed: kernels, graphs, allocator
+    run, _ = warm.make_runner(True)
+    for _ in range(2):
+        run()
+    warm.close()
+    clocks = Clocks(_gpu_uuid(torch, dev))
+    # host arrays of the plan (the permittivity, groups, TF/SF tables, monitor and CPML tables), all copied in
+    h2d_solve = sum(int(np.asarray(v).nbytes) for v in P.dumps(plan).values())
+    res = {}
+    for prec in ("single", "double"):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        eng = Engine.from_plan(plan, precision=prec)
+        run, used = eng.make_runner(True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(eng.stream)
+        for _ in range(chunks):
+            run()
+        ev[1].record(eng.stream)
+        es, hs, d2h = [], [], 0
+        for k in range(len(plan["monitors"])):
+            e, h = eng.results(k)  # every frequency row, copied to the host
+            d2h += np.asarray(e).nbytes + (0 if h is None else np.asarray(h).nbytes)
+            es.append(np.asarray(e)[sel])
+            hs.append(None if h is None else np.asarray(h)[sel])
+        t1 = time.perf_counter()
+        cs = cross_sections(es, hs, post)
+        err = {k: float(np.max(np.abs(cs[k] - ref[k]) / np.abs(ref[k]))) for k in ("c_ext", "c_sca", "c_abs")}
+        if prec == "single":
+            d2h_solve = d2h
+            per_wl = {k: (np.abs(cs[k] - ref[k]) / np.abs(ref[k])).tolist() for k in ("c_ext", "c_sca", "c_abs")}
+        res[prec] = {"device_ms": ev[0].elapsed_time(ev[1]), "e2e_ms": (t1 - t0) * 1e3, "err": err,
+                     "graphs": bool(used), "fused_pass": bool(getattr(eng, "fused", False))}
+        eng.close()
+    clk = clocks.stop()
+    s = res["single"]
+    value = cells * post["steps"] / (s["device_ms"] / 1e3) / 1e9
+    out = {"metric": "FDTD Gcell-updates/s, whole dispersive-sphere scattering solve", "value": value,
+           "unit": UNIT, "n_gpus": 1, "steps": int(post["steps"]), "warmup": 2, "ms_per_step": s["device_ms"] / post["steps"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "lightsmith's own plan for the problem (recorded on the host; no randomness)",
+           "config": {"workload": "r = 40 nm Drude-Lorentz sphere (eps_inf 5.9, wp 9 eV, 2 Lorentz poles) in n = 1.33, "
+                                  "129^3 cells of 2 nm, CPML 12, table-fed TF/SF plane wave, 81 wavelengths 400-800 nm, "
+                                  "staircase, 4000 steps, dft_stride 100", "inputs": "larger than L2 (8.6e6 nodes x 6 "
+                                  "fields x 4 B plus CPML and tables)"},
+           "e2e": {"value": cells * post["steps"] / (s["e2e_ms"] / 1e3) / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": h2d_solve // int(post["steps"]),
+                   "d2h_bytes_per_step": d2h_solve // int(post["steps"]),
+                   "note": "one solve: engine construction from the host plan (its arrays copied in), 4000 steps, "
+                           "every accumulator read back; bytes per step are the solve's over its steps"},
+           "cross_section_rel_err_vs_lightsmith_fp64": {"fp32": s["err"], "fp64": res["double"]["err"]},
+           "fp32_rel_err_per_wavelength": per_wl, "wavelengths_nm": (2 * np.pi / np.asarray(post["omega"])).tolist(),
+           "fp64_solve_ms": res["double"]["device_ms"], "clocks": clk}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = _args()
     if args.impl == "reference":
@@ -545,6 +627,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "clusters":
         run_clusters(args)
+    elif args.workload == "sphere":
+        run_sphere(args)
     else:
         run_b200(args)
 

@@ -402,6 +402,86 @@ def solve_case(name: str, sim):
     print(name, rec["plan"]["shape"], "steps", post["steps"], "C_ext", out["c_ext"])
 
 
+def c0_case():
+    """The full-size sphere: the plan and post-processing inputs lightsmith's scattering driver builds, then
+    lightsmith's own engine (float64, on the host) run for exactly 4000 steps and the cross sections from its
+    accumulators by oracle/post.py (which reproduces lightsmith's to 1e-13 on the other solve fixtures).
+    ``ls.solve`` itself is not used for the run: its run loop stops this one at step 3100 with its divergence
+    test (setup.py:749-756), whose reference is the monitor energy of the run's first half, before the pulse
+    has reached the scattered-field box; the energy per chunk is kept in the fixture."""
+    from lightsmith.device import Device
+    from oracle.post import cross_sections
+
+    sim = c0_problem()
+    rec = {}
+
+    class Stop(Exception):
+        pass
+
+    def capture(device, **kw):
+        rec["kw"] = kw
+        raise Stop()
+
+    boxes = []
+    fp_orig = ref_scattering.flux_points
+
+    def flux_points_rec(*a, **k):
+        out = fp_orig(*a, **k)
+        boxes.append(out)
+        return out
+    Base = ref_scattering.Engine
+    ref_scattering.Engine = capture
+    ref_scattering.flux_points = flux_points_rec
+    try:
+        ls.solve(sim, "fdtd", "cpu")
+    except Stop:
+        pass
+    finally:
+        ref_scattering.Engine = Base
+        ref_scattering.flux_points = fp_orig
+    kw = rec["kw"]
+    plan = P.make_plan(**kw)
+    eng = Base(Device("numpy", "cpu"), **kw)
+    run, _ = eng.make_runner(False)
+    steps = 4000
+    energy = []
+    for _ in range(steps // plan["stride"]):
+        run()
+        energy.append(np.asarray(eng.energy, float).copy())
+    src = kw["sources"][0]
+    omega = 2 * np.pi / sim.wavelength_array()
+    sca, tot = boxes
+    post = {"omega": omega, "n_sym": 1.0, "n_inc": float(src.n_inc), "sca_coeff": sca[3], "tot_coeff": tot[3],
+            "unit": src.incident_reference(omega), "bg_e": src.background(omega, tot[0], "E"),
+            "bg_h": 0.5 * (src.background(omega, tot[1], "H") + src.background(omega, tot[2], "H")),
+            "steps": steps}
+    acc_e = [np.asarray(m.acc_e) for m in kw["monitors"]]
+    acc_h = [None if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]
+    cs = cross_sections(acc_e, acc_h, post)
+    sel = np.arange(0, 81, 10)
+    post = {**post, "omega": omega[sel], "unit": post["unit"][sel], "bg_e": post["bg_e"][sel],
+            "bg_h": post["bg_h"][sel], "freq_sel": sel}
+    out = {k: cs[k][sel] for k in ("c_ext", "c_sca", "c_abs")}
+    out.update(n=int(eng.n[0]) if hasattr(eng.n, "__len__") else int(eng.n), energy=np.asarray(energy))
+    P.save(os.path.join(HERE, "solve_c0.npz"), {"plan": plan, "post": post, "out": out})
+    print("c0", plan["shape"], "steps", steps, "C_ext", out["c_ext"], "energy (first, max, last)",
+          np.asarray(energy)[[0, -1]], np.asarray(energy).max(axis=0))
+
+
+def c0_problem():
+    """The dispersive sphere at full size: r = 40 nm Drude-Lorentz (eps_inf 5.9, wp 9.0 eV, gamma 0.07 eV, poles
+    (1.3, 2.6 eV, 0.6 eV) and (1.5, 3.7 eV, 1.0 eV)) in n = 1.33, 81 wavelengths 400-800 nm, 2 nm cells, CPML
+    12, courant 0.99, padding and gap 28 nm (129^3 cells), staircase, exactly 4000 steps, dft_stride 100."""
+    mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
+                          poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
+                                 {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
+    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=40.0), material=mat)], medium_index=1.33,
+                         wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 81},
+                         options={"fdtd": dict(spacing_nm=2.0, pml_cells=12, courant=0.99, symmetry="off",
+                                               mesh_refinement="staircase", padding_nm=28.0, pml_gap_nm=28.0,
+                                               dft_stride=100, run_time_fs=3999.5 * 1.1431535 / 299.792458)})
+
+
 def sphere_problem(mesh: str, symmetry: str = "off"):
     mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
                           poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
@@ -501,6 +581,7 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "driver_emission": lambda: driver_case("emission", emission_problem(), ref_emission),
          "driver_device_2d": lambda: driver_case("device_2d", device_problem(2), ref_device),
          "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device),
+         "solve_c0": c0_case,
          "diff_device_3d": lambda: diff_device_case(3),
          "diff_device_2d": lambda: diff_device_case(2)}
 
