@@ -28,6 +28,7 @@ cdx times the sum of the three components' dJ/dcbE).
 from __future__ import annotations
 
 import ctypes as C
+import functools
 
 import numpy as np
 
@@ -280,6 +281,7 @@ class AdjointRun:
             pass
 
 
+@functools.cache
 def _function():
     torch = _torch()
 

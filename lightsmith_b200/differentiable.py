@@ -28,6 +28,7 @@ protocol requires that the ports do not depend on the override).
 
 from __future__ import annotations
 
+import functools
 from dataclasses import dataclass
 
 import numpy as np
@@ -217,6 +218,7 @@ class DeviceSolver:
         self._runs.clear()
 
 
+@functools.cache
 def _function():
     torch = _torch()
 
