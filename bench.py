@@ -594,10 +594,19 @@ def run_sphere(args):
             per_wl = {k: (np.abs(cs[k] - ref[k]) / np.abs(ref[k])).tolist() for k in ("c_ext", "c_sca", "c_abs")}
         res[prec] = {"device_ms": ev[0].elapsed_time(ev[1]), "e2e_ms": (t1 - t0) * 1e3, "err": err,
                      "graphs": bool(used), "fused_pass": bool(getattr(eng, "fused", False))}
+        if prec == "single":  # after the solve: the bulk Yee kernels alone, eager, over 4 more chunks
+            bulk_ms, bulk_launches = eng.chunk_timed(4)
+            res[prec].update(bulk_ms_per_step=bulk_ms / (4 * plan["stride"]), bulk_launches=bulk_launches,
+                             launches=eng.launches_per_chunk() * chunks)
         eng.close()
     clk = clocks.stop()
     s = res["single"]
     value = cells * post["steps"] / (s["device_ms"] / 1e3) / 1e9
+    from lightsmith_b200.workloads import cells_in_cpml
+
+    alg_bytes = cells * BYTES_PER_CELL + cells_in_cpml(plan) * BYTES_PER_CPML_PAIR
+    achieved = alg_bytes / (s["bulk_ms_per_step"] / 1e3) / 1e9
+    peak, peak_kind = _peak()
     out = {"metric": "FDTD Gcell-updates/s, whole dispersive-sphere scattering solve", "value": value,
            "unit": UNIT, "n_gpus": 1, "steps": int(post["steps"]), "warmup": 2, "ms_per_step": s["device_ms"] / post["steps"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -613,6 +622,13 @@ def run_sphere(args):
                            "every accumulator read back; bytes per step are the solve's over its steps"},
            "cross_section_rel_err_vs_lightsmith_fp64": {"fp32": s["err"], "fp64": res["double"]["err"]},
            "fp32_rel_err_per_wavelength": per_wl, "wavelengths_nm": (2 * np.pi / np.asarray(post["omega"])).tolist(),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "traffic": None,
+                        "kernel": "bulk Yee update (H and E with their CPML terms; the in-place kernels on this "
+                                  "grid), per FDTD step", "alg_bytes_per_step": alg_bytes,
+                        "kernel_ms_per_step": s["bulk_ms_per_step"],
+                        "share_of_step": s["bulk_ms_per_step"] / (s["device_ms"] / post["steps"])},
+           "fused_pass": s["fused_pass"], "gpu_launches": s["launches"],
            "fp64_solve_ms": res["double"]["device_ms"], "clocks": clk}
     print(json.dumps(out), flush=True)
 
