@@ -13,8 +13,8 @@ The permittivity grid is the FDTD grid's nodes: node (i, j, k) carries one real 
 components (E_x at i + 1/2, E_y at j + 1/2, E_z at k + 1/2); a 2D device's grid is its one stepped z plane
 (node k = 1 between the two ghost planes of the periodic invariant axis). Where the grid given equals the
 base (the driver's own voxelisation, 1/eps averaged over the three components), a node keeps the driver's
-per-component values; elsewhere its three components take 1/eps of the grid. FDTD steps a real, frequency-independent permittivity:
-an override must be real and equal across wavelengths.
+per-component values; elsewhere its three components take 1/eps of the grid. FDTD steps a real,
+frequency-independent permittivity: an override must be real and equal across wavelengths.
 
 Each S column is one ``AdjointRun`` (``lightsmith_b200.adjoint``) over all port monitors: the forward runs the
 CUDA engine for the description's fixed step count, keeping checkpoints; S[:, out, src] = c_out / a_src from the
