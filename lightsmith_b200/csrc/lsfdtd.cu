@@ -1037,6 +1037,11 @@ struct Engine final : lsfdtd_engine {
     for (int d = 0; d < 3; ++d)
       for (int c = 0; c < 3; ++c)
         for (int sd = 0; sd < 2; ++sd) a.pml[d].psi[1][c][sd] = psiH[cur][d][c][sd];
+    // the in-place kernels' inner nodes: stepped for every component and outside every slab (on a mirror
+    // axis the stepped range of some components starts at node 2)
+    inner_bounds(a.in_lo, a.in_hi);
+    for (int ax = 0; ax < 3; ++ax)
+      if (desc.mirror[ax]) a.in_lo[ax] = std::min(std::max(a.in_lo[ax], 2), a.in_hi[ax]);
     return a;
   }
 

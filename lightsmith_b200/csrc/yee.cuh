@@ -40,6 +40,9 @@ struct YeeArgs {
   F* H[3];
   const R* cbE[3];  // per component, full grid (the three may alias one array)
   PmlAxis<F> pml[3];
+  // nodes [in_lo, in_hi) per axis stepped for every component of both fields and outside every CPML slab
+  // (empty when unset): there the in-place kernels need no region test and no CPML term
+  int in_lo[3], in_hi[3];
 };
 
 // mir: the mirror planes (null: none); along a mirror axis E_c starts at node 2 when it is tangential to an
@@ -159,23 +162,84 @@ __device__ __forceinline__ void update_e_node(const YeeArgs<F>& g, int i, int j,
   }
 }
 
+template <typename F>
+__device__ __forceinline__ bool in_inner(const YeeArgs<F>& g, int i, int j, int k) {
+  return i >= g.in_lo[0] && i < g.in_hi[0] && j >= g.in_lo[1] && j < g.in_hi[1] && k >= g.in_lo[2] &&
+         k < g.in_hi[2];
+}
+
 // H update: one thread per node (i, j, k), all three components; one instantiation per cell shape (UNI 1:
-// cubic cells)
+// cubic cells). A warp whose nodes are all inner takes the stencil without region tests or CPML terms (the
+// same arithmetic in the same order as update_h_node's for such nodes)
 template <typename F, int UNI>
 __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeArgs<F> g) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.n[2] || j >= g.n[1]) return;
-  update_h_node<F, UNI>(g, blockIdx.z, j, k);
+  const int i = blockIdx.z;
+  if (__all_sync(__activemask(), in_inner(g, i, j, k))) {
+    const bool uni = UNI < 0 ? (bool)g.uniform : UNI == 1;
+    const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+    const long long p = i * s0 + j * s1 + k;
+    const long long step[3] = {s0, s1, 1};
+    F e0[3], e1[3][3];  // E at the node and at its +1 neighbours, every load before the first store
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      e0[c] = g.E[c][p];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d != c) e1[c][d] = g.E[c][p + step[d]];
+    }
+    F h[3] = {g.H[0][p], g.H[1][p], g.H[2][p]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+      const F a = e1[d2][d1] - e0[d2];
+      const F b = e1[d1][d2] - e0[d1];
+      const F curl = uni ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+      g.H[c][p] = h[c] - curl * g.cH;
+    }
+    return;
+  }
+  update_h_node<F, UNI>(g, i, j, k);
 }
 
-// E update: one thread per node, all three components
+// E update: one thread per node, all three components; inner warps as in k_update_h
 template <typename F, int UNI>
 __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeArgs<F> g) {
+  using R = typename real_of<F>::type;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (k >= g.n[2] || j >= g.n[1]) return;
-  update_e_node<F, UNI>(g, blockIdx.z, j, k);
+  const int i = blockIdx.z;
+  if (__all_sync(__activemask(), in_inner(g, i, j, k))) {
+    const bool uni = UNI < 0 ? (bool)g.uniform : UNI == 1;
+    const long long s1 = g.n[2], s0 = (long long)g.n[1] * g.n[2];
+    const long long p = i * s0 + j * s1 + k;
+    const long long step[3] = {s0, s1, 1};
+    F h0[3], h1[3][3];  // H at the node and at its -1 neighbours
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      h0[c] = g.H[c][p];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d != c) h1[c][d] = g.H[c][p - step[d]];
+    }
+    F e[3] = {g.E[0][p], g.E[1][p], g.E[2][p]};
+    R cb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cb[c] = g.cbE[c][p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int d1 = (c + 1) % 3, d2 = (c + 2) % 3;
+      const F a = h0[d2] - h1[d2][d1];
+      const F b = h0[d1] - h1[d1][d2];
+      const F curl = uni ? (a - b) : (a * g.inv_d[d1] - b * g.inv_d[d2]);
+      g.E[c][p] = e[c] + curl * cb[c];
+    }
+    return;
+  }
+  update_e_node<F, UNI>(g, i, j, k);
 }
 
 // Periodic ghost planes of one axis: dst plane <- src plane times a Bloch phase (engine.py:595-611).
