@@ -371,8 +371,9 @@ int32_t lsfdtd_batch_ctas(const lsfdtd_batch* batch);
 
 /* ---- discrete adjoint ----------------------------------------------------------------------------------
  * No counterpart in lightsmith (its FDTD has no gradient): the transpose of one FDTD step of an engine with
- * real fields, no periodic axis and pure (staircase) dispersive groups, for d(objective)/d(E curl
- * coefficient) of a real objective J of one monitor's DFT accumulators. The caller gives J's adjoint source
+ * real fields (periodic axes allowed: their ghost-plane copies are transposed too), no mirror plane and pure
+ * (staircase) dispersive groups, for d(objective)/d(E curl coefficient) of a real objective J of one
+ * monitor's DFT accumulators (several monitors' points may be concatenated into one). The caller gives J's adjoint source
  * as G = 2 dJ/d(acc) (the Wirtinger derivative: the conjugate of the gradient torch reports for a complex
  * tensor) per frequency and point; the E samples then receive sum_f Re(G_e[f, p] e^{i w_f t}) at each
  * sampled step. */
