@@ -221,6 +221,26 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     return out
 
 
+_GRID_DESCS: dict[str, dict] = {}  # the last few problems' run descriptions, for design_grid/base_permittivity
+
+
+def _grid_desc(problem, desc=None) -> dict:
+    """A run description of ``problem`` for its grid and base permittivity (the step count does not matter
+    there): ``desc`` when given (and kept), else one made earlier for the same problem, else a new one.
+    lightsmith's optimiser asks for the grid and the base permittivity without the prepared context
+    (inverse/topopt.py:113-116), so this saves it the driver's set-up twice over."""
+    key = problem.model_dump_json()
+    if desc is None:
+        desc = _GRID_DESCS.get(key)
+        if desc is None:
+            desc = device_runs(problem, n_steps=0)
+    _GRID_DESCS.pop(key, None)
+    _GRID_DESCS[key] = desc
+    while len(_GRID_DESCS) > 4:
+        _GRID_DESCS.pop(next(iter(_GRID_DESCS)))
+    return desc
+
+
 class B200FDTD(NativeFDTD):
     """``NativeFDTD`` (backends/fdtd.py:47) whose engine is the B200 one on CUDA devices, and which serves
     lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) for device problems on CUDA
@@ -242,7 +262,9 @@ class B200FDTD(NativeFDTD):
         from .differentiable import DeviceSolver
 
         dev = resolve_device("gpu") if torch.cuda.is_available() else None
-        return {"solver": DeviceSolver(device_runs(problem, dev))}
+        desc = device_runs(problem, dev)
+        _grid_desc(problem, desc)
+        return {"solver": DeviceSolver(desc)}
 
     @classmethod
     def design_grid(cls, problem, solver=None):
@@ -250,7 +272,7 @@ class B200FDTD(NativeFDTD):
         permittivity of its three E components. A 2D device's grid is (x, y): its stepped plane."""
         from .differentiable import DesignGrid, DesignGrid2D
 
-        d = solver.desc if solver is not None else device_runs(problem, n_steps=0)
+        d = solver.desc if solver is not None else _grid_desc(problem)
         x, y, z = d["coords"]
         if d.get("two_d"):
             return DesignGrid2D(x=x, y=y, dl=d["dl"], shape=tuple(d["shape"][:2]))
@@ -260,7 +282,7 @@ class B200FDTD(NativeFDTD):
     def base_permittivity(cls, problem, solver=None) -> np.ndarray:
         """(n_wl, Nx, Ny, Nz), or (n_wl, Nx, Ny) for a 2D device, complex: per node, 1 over the mean of its three
         E components' 1/eps."""
-        d = solver.desc if solver is not None else device_runs(problem, n_steps=0)
+        d = solver.desc if solver is not None else _grid_desc(problem)
         nodes = 1.0 / np.asarray(d["inv_eps"], float).mean(axis=0)
         if d.get("two_d"):
             nodes = nodes[:, :, 1]

@@ -155,3 +155,40 @@ def test_step_count_without_a_run_time_follows_lightsmiths_run_loop():
     desc = device_runs(p, Device("numpy", "cpu"), engine=RefEngine)
     res = ls.solve(p, "fdtd", "cpu")
     assert desc["n_steps"] == res.provenance["runs"][0]["steps"] < 10720
+
+
+@needs_ls
+def test_lightsmiths_optimiser_takes_the_backend(monkeypatch):
+    """lightsmith's TopologyOptimizer (inverse/topopt.py:96-130) set up on the FDTD backend: it prepares the
+    runs, maps a design region onto the design grid and composes the permittivity; the solve itself needs a
+    CUDA device (raised here, on the host)."""
+    from device_problems import diff_device_problem
+    from lightsmith import inverse
+    from lightsmith.backends import base as ls_base
+    from lightsmith.inverse.topopt import TopologyOptimizer
+
+    from lightsmith_b200.backend import B200FDTD
+
+    monkeypatch.setattr(ls_base, "_REGISTRY", {**ls_base._REGISTRY, "lightsmith-fdtd": B200FDTD})
+    monkeypatch.setattr(ls_base, "_PLUGINS_LOADED", True)
+    import lightsmith as ls
+
+    dev = diff_device_problem(3)
+    spec = inverse.OptimizationProblem(
+        device=dev, backend="lightsmith-fdtd",
+        design_regions=[inverse.DesignRegion(center_nm=(0, 0, 0), size_nm=(400, 600, 220),
+                                             material_low=ls.ConstantIndex(n_real=1.44),
+                                             material_high=ls.ConstantIndex(n_real=3.48))],
+        objective=[inverse.SParameterTerm(out_port="o2", in_port="o1")])
+    opt = TopologyOptimizer(spec, device="cpu")
+    assert opt.grid.shape == tuple(opt.ctx["solver"].design_shape) and opt.sources == ["o1"]
+    (reg,) = opt.regions
+    expect = tuple(int(np.sum(np.abs(c) <= h + 1e-9)) for c, h in ((opt.grid.x, 200), (opt.grid.y, 300)))
+    assert reg.shape == expect and reg.mode == "extruded" and expect[0] >= 10  # nodes of a 400 x 600 nm box
+    import torch
+
+    eps, proj, _ = opt.permittivity(torch.as_tensor(opt.initial_x()), 1.0)
+    assert tuple(eps.shape) == (2,) + opt.grid.shape
+    assert float(eps.real.max()) < 12.2 and float(eps.real.min()) > 2.0
+    with pytest.raises(ValueError, match="CUDA"):
+        opt.solve(eps)
