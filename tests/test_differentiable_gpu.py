@@ -157,3 +157,35 @@ def test_field_outputs_and_their_gradient(fixture):
             fd = (float(loss(torch.as_tensor(ep))) - float(loss(torch.as_tensor(em)))) / (2 * h)
             assert abs(g[n] - fd) <= 1e-5 * abs(fd) + 1e-9 * np.abs(g).max(), (n, g[n], fd)
     solver.close()
+
+
+@pytest.mark.gpu
+def test_gradient_steps_raise_the_transmission(fixture):
+    """Three projected gradient steps on a design density (the step of lightsmith's optimisers, in miniature):
+    the transmission sum_w |S21|^2 rises at each."""
+    import torch
+
+    from lightsmith_b200.differentiable import DeviceSolver, s_parameters
+
+    solver = DeviceSolver(fixture["desc"], precision="single")
+    eps0, sl, _ = _design_block(solver)
+    base = torch.as_tensor(eps0)
+    lo, hi = 1.444 ** 2, 3.476 ** 2
+    rho = torch.full(tuple(s.stop - s.start for s in sl), 0.5, dtype=torch.float64)
+
+    def transmission(r):
+        e = base.clone()
+        e[sl] = lo + r * (hi - lo)
+        return (s_parameters(e, solver, sources=["o1"])[:, 1, 0].abs() ** 2).sum()
+
+    values = []
+    for _ in range(3):
+        r = rho.clone().requires_grad_(True)
+        T = transmission(r)
+        T.backward()
+        values.append(float(T.detach()))
+        rho = (rho + 0.05 * r.grad / r.grad.abs().max()).clamp(0, 1)
+    with torch.no_grad():
+        values.append(float(transmission(rho)))
+    solver.close()
+    assert all(b > a for a, b in zip(values, values[1:])), values
