@@ -8,8 +8,9 @@ plus one DFT sample (lightsmith's unit of work, ``Engine.chunk``), replayed as a
 
     python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference] [--n 640]
 
-``--impl reference`` times the reference algorithm on the host CPU (the NumPy oracle, float64 as lightsmith
-runs on CPUs, all host threads) on a 128^3 sample of the same workload. Under torchrun each rank runs an
+``--impl reference`` times lightsmith's own CPU FDTD (its ``Engine`` from the reference install in
+``baseline/_ref``, float64 as lightsmith runs on CPUs, through PyTorch on all host threads, with its NumPy path
+beside it) on a 128^3 sample of the same workload. Under torchrun each rank runs an
 independent replica (the plain solver does not shard) and rank 0 prints one JSON line.
 """
 
@@ -23,6 +24,8 @@ import statistics
 import subprocess
 import sys
 import time
+
+import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
@@ -141,7 +144,8 @@ def _gpu_uuid(torch, dev):
 
 
 def cpu_sample(n: int, chunks: int, warmup: int, threads: int):
-    """The oracle (float64, as lightsmith runs on CPUs) on an n^3 sample of the workload; Gcell-updates/s."""
+    """The oracle port (float64, as lightsmith runs on CPUs) on an n^3 sample of the workload, used only where
+    lightsmith itself is not installed: (Gcell-updates/s, seconds, stride)."""
     from lightsmith_b200.workloads import throughput_plan
     from oracle.engine import OracleEngine
 
@@ -158,6 +162,81 @@ def cpu_sample(n: int, chunks: int, warmup: int, threads: int):
     return cells * plan["stride"] * chunks / dt / 1e9, dt, plan["stride"]
 
 
+REF_INSTALL = os.path.join(HERE, "baseline", "_ref")
+
+
+def _lightsmith_available() -> bool:
+    """lightsmith itself (the reference install, ``baseline/install_ref.py``) on sys.path."""
+    if not os.path.isdir(os.path.join(REF_INSTALL, "lightsmith")):
+        return False
+    if REF_INSTALL not in sys.path:
+        sys.path.insert(0, REF_INSTALL)
+    try:
+        import lightsmith  # noqa: F401
+    except Exception:  # noqa: BLE001 (a broken install counts as none)
+        return False
+    return True
+
+
+def reference_sample(n: int, chunks: int, warmup: int, threads: int, device: str = "torch-cpu"):
+    """lightsmith's own FDTD engine (``backends/_fdtd/engine.py:Engine``, with its ``PointDipole``,
+    ``DFTMonitor`` and ``PMLSpec``) on an n^3 sample of the throughput workload, float64 as lightsmith runs on
+    CPUs, on ``device`` ("torch-cpu": PyTorch on ``threads`` host threads; "cpu": NumPy, whose ufuncs use one
+    core): (Gcell-updates/s, seconds, stride)."""
+    from lightsmith.backends._fdtd.emission import PointDipole
+    from lightsmith.backends._fdtd.engine import DFTMonitor, Engine, PMLSpec
+    from lightsmith.device import resolve_device
+
+    from lightsmith_b200.workloads import plane_monitor, throughput_band
+
+    if device == "torch-cpu":
+        import torch
+
+        torch.set_num_threads(threads)
+    shape = (n, n, n)
+    dx = 20.0
+    dt, om, omega_c, omega_half, stride = throughput_band(dx)
+    inv = 1.0 / np.random.default_rng(1).uniform(1.0, 12.25, size=shape)
+    inv3 = np.ascontiguousarray(np.broadcast_to(inv, (3,) + shape))
+    steps = stride * (chunks + warmup + 2)
+    dip = PointDipole(shape=shape, origin=np.zeros(3), dx=dx, dt=dt, pos=(np.asarray(shape) // 2) * dx + 0.37 * dx,
+                      pdir=(0.0, 0.0, 1.0), inv_eps=inv3, omega_c=omega_c, omega_half=omega_half, max_steps=steps)
+    m = plane_monitor(shape, n // 2, om, energy=1)
+    mon = DFTMonitor(m.omega, m.e_idx, m.h_idx1, m.h_idx2, energy=1)
+    pml = PMLSpec(cells=((16, 16),) * 3, alpha_max=0.05 * 2 * np.pi / 2000.0, eps_ref=1.0)
+    eng = Engine(resolve_device(device), shape=shape, dx=dx, dt=dt, single=False, inv_eps=inv3, groups=[], pml=pml,
+                 sources=[dip], monitors=[mon], dft_stride=stride)
+    for _ in range(warmup):
+        eng.chunk()
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        eng.chunk()
+    secs = time.perf_counter() - t0
+    return n ** 3 * stride * chunks / secs / 1e9, secs, stride
+
+
+def cpu_baseline_record(n: int, chunks: int, warmup: int, threads: int, numpy_chunks: int = 1) -> dict:
+    """The CPU baseline: lightsmith's own engine on torch-cpu (all threads) with its NumPy path beside it; the
+    oracle port where lightsmith is not installed."""
+    if _lightsmith_available():
+        v, secs, st = reference_sample(n, chunks, warmup, threads, "torch-cpu")
+        rec = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": f"{n}^3 grid of the same workload (CPML 16, random eps, centre dipole, 16-frequency DFT "
+                         f"plane), {chunks} chunks of {st} steps after {warmup}, lightsmith 0.3.0's own Engine on "
+                         f"device 'torch-cpu', float64, {threads} threads ({secs:.1f} s)", "seconds": secs}
+        if numpy_chunks:
+            vn, sn, _ = reference_sample(n, numpy_chunks, 0, threads, "cpu")
+            rec["numpy_fp64"] = {"value": vn, "unit": UNIT, "cores": 1,
+                                 "sample": f"the same engine on device 'cpu' (NumPy float64; its ufuncs run on one "
+                                           f"core of {threads}), {numpy_chunks} chunk(s) ({sn:.1f} s)"}
+        return rec
+    v, secs, st = cpu_sample(n, chunks, warmup, threads)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n}^3 grid of the same workload, {chunks} chunks of {st} steps after {warmup}, NumPy "
+                      f"float64 oracle port on {threads} threads ({secs:.1f} s; lightsmith itself not installed)",
+            "seconds": secs}
+
+
 def _threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -166,20 +245,22 @@ def _threads():
 
 
 def run_reference(args):
+    """lightsmith's own CPU FDTD on the host cores: each bench step is one chunk (stride steps + one DFT sample)
+    of a 128^3 sample of the throughput workload, on lightsmith's engine through PyTorch on all host threads
+    (float64, as lightsmith runs on CPUs); the oracle port stands in only where lightsmith is not installed."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     threads = _threads()
-    # each bench step is one chunk of the 128^3 sample
-    value, secs, stride = cpu_sample(CPU_SAMPLE_N, args.steps, args.warmup, threads)
-    sample = (f"{CPU_SAMPLE_N}^3 grid of the same workload (CPML 16, random eps, centre dipole, 16-frequency DFT "
-              f"plane), {args.steps} chunks of {stride} steps after {args.warmup}, NumPy float64 oracle, "
-              f"{threads} threads")
+    rec = cpu_baseline_record(CPU_SAMPLE_N, args.steps, args.warmup, threads, numpy_chunks=1)
+    value = rec["value"]
+    secs = rec["seconds"]
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(args.steps, 1),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"plain FDTD throughput, {CPU_SAMPLE_N}^3 CPU sample of the 640^3 case",
-                      "grid": [CPU_SAMPLE_N] * 3, "dft_stride": stride},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+           "config": {"workload": f"plain FDTD throughput, {CPU_SAMPLE_N}^3 CPU sample of the 640^3 case (CPML 16, "
+                                  "i.i.d. eps in [1, 12.25], centre dipole pulse, 16-frequency DFT on one plane)",
+                      "grid": [CPU_SAMPLE_N] * 3, "dx_nm": 20.0},
+           "cpu_baseline": rec,
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -293,11 +374,7 @@ def run_b200(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = _threads()
-        v, secs, st = cpu_sample(CPU_SAMPLE_N, 6, 1, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{CPU_SAMPLE_N}^3 grid of the same workload, 6 chunks of {st} steps, NumPy float64 "
-                         f"oracle on {threads} threads ({secs:.1f} s)"}
+        cpu = cpu_baseline_record(CPU_SAMPLE_N, 4, 1, _threads(), numpy_chunks=1)
     eng.close()
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,

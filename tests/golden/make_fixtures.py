@@ -39,6 +39,8 @@ from lightsmith.backends._fdtd.layered import ObliqueLayeredPlaneWave  # noqa: E
 from lightsmith.backends._fdtd.media import Medium, Pole  # noqa: E402
 from lightsmith.backends._fdtd.ports import ModeSource  # noqa: E402
 from device_problems import device_problem, diff_device_problem  # noqa: E402
+from problems import (SOLVE_PROBLEMS, c0_problem, dielectric_sphere_problem, emission_problem,  # noqa: E402
+                      flatten_result, periodic_problem, sphere_problem)
 from lightsmith.backends._fdtd.setup import flux_points, voxelise  # noqa: E402
 from lightsmith.backends._fdtd.tfsf import BlochPlaneSource, TFSFPlaneWave  # noqa: E402
 from lightsmith.device import Device  # noqa: E402
@@ -87,8 +89,10 @@ def run_engine_case(name: str, kw: dict, n_chunks: int, snap: int = 1):
            "n_chunks": n_chunks, "snap": snap, **snaps,
            "acc_e": [np.asarray(m.acc_e) for m in kw["monitors"]],
            "acc_h": [np.zeros(0) if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]}
-    if getattr(eng, "od", None) is not None:  # the reference's off-diagonal gather tables
+    if getattr(eng, "od", None) is not None:  # the reference's off-diagonal gather tables, and the rows
         out["od_e"], out["od_h"], out["od_w"] = (np.asarray(x) for x in eng.od)
+        od = kw["offdiag"]
+        out["od_rows"] = {"idx3": np.asarray(od.idx3), "comp": np.asarray(od.comp), "coef": np.asarray(od.coef)}
     for src in kw["sources"]:
         if hasattr(src, "col"):
             out["col_E"], out["col_H"] = np.asarray(src.col.E), np.asarray(src.col.H)
@@ -468,29 +472,8 @@ def c0_case():
           np.asarray(energy)[[0, -1]], np.asarray(energy).max(axis=0))
 
 
-def c0_problem():
-    """The dispersive sphere at full size: r = 40 nm Drude-Lorentz (eps_inf 5.9, wp 9.0 eV, gamma 0.07 eV, poles
-    (1.3, 2.6 eV, 0.6 eV) and (1.5, 3.7 eV, 1.0 eV)) in n = 1.33, 81 wavelengths 400-800 nm, 2 nm cells, CPML
-    12, courant 0.99, padding and gap 28 nm (129^3 cells), staircase, exactly 4000 steps, dft_stride 100."""
-    mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
-                          poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
-                                 {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
-    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=40.0), material=mat)], medium_index=1.33,
-                         wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 81},
-                         options={"fdtd": dict(spacing_nm=2.0, pml_cells=12, courant=0.99, symmetry="off",
-                                               mesh_refinement="staircase", padding_nm=28.0, pml_gap_nm=28.0,
-                                               dft_stride=100, run_time_fs=3999.5 * 1.1431535 / 299.792458)})
 
 
-def sphere_problem(mesh: str, symmetry: str = "off"):
-    mat = ls.DrudeLorentz(eps_inf=5.9, wp_ev=9.0, gamma_ev=0.07,
-                          poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
-                                 {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
-    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=mat)], medium_index=1.33,
-                         wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
-                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry=symmetry, mesh_refinement=mesh,
-                                               padding_nm=8.0, pml_gap_nm=8.0, dft_stride=10,
-                                               run_time_fs=399.5 * 2.2863 / 299.792458)})
 
 
 # --- every engine a problem driver builds, through ls.solve ----------------------------------------------
@@ -522,24 +505,8 @@ def driver_case(name: str, problem, module):
     print(name, [(r["plan"]["shape"], r["n"], r["plan"]["complex"]) for r in out])
 
 
-def periodic_problem(theta: float, phi: float, pol: str):
-    """A square lattice (300 nm) of TiO2-like pillars (n = 2, radius 80 nm, 120 nm tall) on glass, 15 nm cells."""
-    from lightsmith.problems import Circle, Incidence, PatternedLayer, PeriodicProblem, Structure2D
-    CI = ls.ConstantIndex
-    return PeriodicProblem(
-        lattice_a1_nm=(300, 0), lattice_a2_nm=(0, 300), superstrate=CI(n_real=1.0), substrate=CI(n_real=1.45),
-        layers=[PatternedLayer(thickness_nm=120, background=CI(n_real=1.0),
-                               shapes=[Structure2D(profile=Circle(radius_nm=80), material=CI(n_real=2.0))])],
-        wavelengths=[500.0, 650.0], incidence=Incidence(theta_deg=theta, phi_deg=phi, polarizations=[pol]),
-        options={"fdtd": {"spacing_nm": 15.0, "run_time_fs": 6.0}})
 
 
-def emission_problem():
-    """A dipole 15 nm off an n = 2 sphere (radius 30 nm) in vacuum, 4 nm cells."""
-    from lightsmith.problems import Dipole, EmissionProblem
-    return EmissionProblem(particles=[ls.Particle(shape=ls.Sphere(radius_nm=30), material=ls.ConstantIndex(n_real=2.0))],
-                           wavelengths=[500.0, 700.0], dipole=Dipole(position_nm=(0, 0, 45), orientation=(1, 0, 1)),
-                           options={"fdtd": {"spacing_nm": 4.0, "run_time_fs": 2.0}})
 
 
 def diff_device_case(dimension: int):
@@ -555,13 +522,19 @@ def diff_device_case(dimension: int):
     print(name, desc["shape"], desc["n_steps"], desc["mesh"], np.abs(S[:, 1, 0]))
 
 
-def dielectric_sphere_problem():
-    """A non-dispersive sphere (n = 2, radius 16 nm) in n = 1.33 with conformal interfaces (off-diagonal 1/eps)."""
-    return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
-                         medium_index=1.33, wavelengths={"start_nm": 400.0, "stop_nm": 800.0, "num": 9},
-                         options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, symmetry="off",
-                                               mesh_refinement="conformal", padding_nm=8.0, pml_gap_nm=8.0,
-                                               dft_stride=10, run_time_fs=399.5 * 2.2863 / 299.792458)})
+
+
+
+def results_case():
+    """lightsmith's own ``ls.solve(problem, "fdtd", "cpu")`` (float64) result for every problem of
+    ``problems.SOLVE_PROBLEMS``: the numeric content of each result (``flatten_result``), for the tests that
+    pose the same problems to ``ls.solve(problem, "fdtd", "gpu")`` through the plugin."""
+    out = {}
+    for name, make in SOLVE_PROBLEMS.items():
+        res = ls.solve(make(), "fdtd", "cpu")
+        out[name] = {"result": flatten_result(res), "steps": int(res.provenance.get("steps", -1))}
+        print(name, type(res).__name__, out[name]["steps"], sorted(out[name]["result"]))
+    P.save(os.path.join(HERE, "solve_results.npz"), out)
 
 
 CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_noncubic,
@@ -583,7 +556,8 @@ CASES = {"yee_cpml_dipole": case_yee_cpml_dipole, "kappa_noncubic": case_kappa_n
          "driver_device_3d": lambda: driver_case("device_3d", device_problem(3), ref_device),
          "solve_c0": c0_case,
          "diff_device_3d": lambda: diff_device_case(3),
-         "diff_device_2d": lambda: diff_device_case(2)}
+         "diff_device_2d": lambda: diff_device_case(2),
+         "solve_results": results_case}
 
 if __name__ == "__main__":
     which = sys.argv[2:] or list(CASES)

@@ -1,18 +1,22 @@
-"""Where the lightsmith sources are read from when a fixture is made or a plugin test runs here.
+"""Where the lightsmith sources are imported from when a fixture is made or a test runs lightsmith's own code.
 
-``LIGHTSMITH_SRC`` overrides the default checkout below; ``shim/`` supplies ``array_api_compat``, which the
-sources import and which is not installed here. The GPU host has no lightsmith: the tests that need it skip.
+The default is the reference install under ``baseline/_ref`` (``python baseline/install_ref.py``), which holds
+the unmodified ``lightsmith`` package and the ``array_api_compat`` stand-in and travels with the working tree;
+``LIGHTSMITH_SRC`` names another directory that holds a ``lightsmith`` package. Tests that need lightsmith skip
+where neither is present.
 """
 
 import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("LIGHTSMITH_SRC", "/root/reference/src")
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF_SRC = os.environ.get("LIGHTSMITH_SRC", os.path.join(REPO, "baseline", "_ref"))
 
 
 def add_to_path(src: str = REF_SRC) -> bool:
-    """Put the lightsmith sources (and the shim) on sys.path; False when they are not there."""
+    """Put the lightsmith sources (and the ``array_api_compat`` stand-in) on sys.path; False when they are not
+    there."""
     if not os.path.isdir(os.path.join(src, "lightsmith")):
         return False
     for p in (src, os.path.join(HERE, "shim")):
