@@ -336,8 +336,11 @@ int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng);
  * precision / is_complex describe the sampled arrays as for the grid (m->space 1: real arrays).
  * The energy reduction's scratch is a static device array of 8192 doubles (64 KiB, held by every GPU that
  * loads the library until exit): a monitor may span at most 8192 blocks of 256 points (E points and H points
- * rounded up separately), and larger ones are rejected with LSFDTD_EINVAL. The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * rounded up separately), and larger ones are rejected with LSFDTD_EINVAL. The array's device address belongs
+ * to the CUDA context that is current at the call (the device's primary context for runtime-API callers, or
+ * a caller's own context): the first call in each context looks it up (cudaGetSymbolAddress) and keeps it
+ * under that context's unique id, so a context made after cudaDeviceReset, or another context on the same
+ * device, gets its own lookup. Make the first call in each context before any stream capture in it.
  * All calls share the array: calls whose GPU work overlaps (for example on two streams) race on it; nothing
  * in it needs clearing between calls. */
 int32_t lsfdtd_dft_sample_noalloc(const lsfdtd_monitor_desc* m, int32_t precision, int32_t is_complex,

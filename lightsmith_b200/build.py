@@ -11,7 +11,7 @@ REPO = os.path.dirname(HERE)
 SOURCES = [os.path.join(HERE, "csrc", "lsfdtd.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "yee.cuh", "yee_vec.cuh", "fused.cuh",
                                                    "fused_tma.cuh", "fused_pml.cuh", "shell.cuh", "batch.cuh", "adjoint.cuh", "ade.cuh", "sources.cuh",
-                                                   "monitors.cuh")] + \
+                                                   "monitors.cuh", "tensor.cuh")] + \
     [os.path.join(REPO, "include", "lsfdtd.h")]
 OUT = os.path.join(HERE, "liblsfdtd.so")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",

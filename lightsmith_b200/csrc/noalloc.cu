@@ -9,6 +9,11 @@
 // holds it until the process exits. All calls share it and it keeps whatever the last call left in it; a call
 // writes every partial it reads before reading it, so nothing needs clearing between calls. Two calls whose
 // work overlaps on the GPU (for example on two streams) race on the array and must not be issued.
+//
+// The sample itself is the engine's own kernel pair (k_monitor, k_energy in monitors.cuh) with the partials
+// pointed at the static array, so it is the engine's sample to the last bit.
+#include <cuda.h>  // types of the driver entry points looked up below (nothing links against libcuda)
+
 #include <mutex>
 #include <string>
 
@@ -25,101 +30,91 @@ using namespace lsfdtd;
 
 namespace {
 
-constexpr int kNoAllocPartials = 8192;  // blocks of 256 points: up to 2,097,152 sampled points per call
+constexpr long long kNoAllocPartials = 8192;  // blocks of 256 points: up to 2,097,152 sampled points per call
 
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocPartials];
 
 // errors are reported through lsfdtd_last_error (defined in lsfdtd.cu)
 int noalloc_fail(int code, const std::string& msg) { return lsfdtd::report_error(code, msg); }
 
-// the device address of the array on the current device, looked up once per device (host code must not
-// pass the array's name itself to a kernel: on the host it only stands for the array)
-constexpr int kMaxDevices = 64;
+// The array's device address belongs to a CUDA context (the module's globals are loaded per context), not to
+// a device index: after cudaDeviceReset the device's primary context is a new one, and a caller may run on a
+// context of its own. So the address is looked up once per context, keyed by the driver's id of the current
+// context (cuCtxGetId: unique for the life of the process, never reused), with that context current. Host code
+// must not pass the array's name itself to a kernel: on the host it only stands for the array.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+struct CtxAddr {
+  unsigned long long id;
+  double* addr;
+};
+constexpr int kMaxContexts = 64;
 std::mutex g_addr_mutex;
-double* g_addr[kMaxDevices] = {};
+CtxAddr g_cache[kMaxContexts] = {};
+int g_cache_n = 0, g_cache_next = 0;
+CtxGetCurrentFn g_get_current = nullptr;
+CtxGetIdFn g_get_id = nullptr;
+bool g_entry_looked_up = false;
+
+// the current context's id, or 0 when the driver cannot say (then the address is looked up on every call)
+unsigned long long current_context_id() {
+  if (!g_entry_looked_up) {
+    g_entry_looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();  // a failed lookup leaves no error behind
+  }
+  if (!g_get_current || !g_get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 int partials_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return noalloc_fail(LSFDTD_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(LSFDTD_EUNSUPPORTED, "device index out of range");
   std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (e != cudaSuccess || !p)
-      return noalloc_fail(LSFDTD_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_addr[dev];
-  return LSFDTD_OK;
-}
-
-// the sample of k_monitor (monitors.cuh), with its partials in the static array
-template <typename S>
-__global__ void __launch_bounds__(kMonBlock) k_monitor_noalloc(MonArgs<S> a) {
-  __shared__ double ph_re[kMonFreqTile], ph_im[kMonFreqTile];
-  __shared__ double red[kMonBlock / 32];
-  const bool is_h = blockIdx.x >= a.blocks_e;
-  const long long p = (long long)(is_h ? blockIdx.x - a.blocks_e : blockIdx.x) * kMonBlock + threadIdx.x;
-  const long long np = is_h ? a.nh : a.ne;
-  const bool live = p < np;
-  cplx<double> s = {0.0, 0.0};
-  double e2 = 0.0;
-  if (live) {
-    if (!is_h) {
-      const S v = a.Esrc[a.e_idx[p]];
-      s = to_c64(v);
-      e2 = norm2(v);
-    } else {
-      const S v = (a.Hsrc[a.h1[p]] + a.Hsrc[a.h2[p]]) * (typename real_of<S>::type)0.5;
-      s = to_c64(v);
-      e2 = norm2(v);
-    }
-  }
-  const double t = (double)(*a.nstep) * a.dt - (is_h ? 0.5 * a.dt : 0.0);
-  cplx<double>* acc = is_h ? a.acc_h : a.acc_e;
-  for (int f0 = 0; f0 < a.nf; f0 += kMonFreqTile) {
-    const int nt = min(kMonFreqTile, a.nf - f0);
-    __syncthreads();
-    for (int f = threadIdx.x; f < nt; f += kMonBlock) {
-      double sn, cs;
-      sincos(a.omega[f0 + f] * t, &sn, &cs);
-      ph_re[f] = cs;
-      ph_im[f] = sn;
-    }
-    __syncthreads();
-    if (live) {
-      for (int f = 0; f < nt; ++f) {
-        cplx<double>* q = acc + (long long)(f0 + f) * np + p;
-        const cplx<double> ph = {ph_re[f], ph_im[f]};
-        *q = *q + ph * s;
+  unsigned long long id = current_context_id();
+  if (id)
+    for (int i = 0; i < g_cache_n; ++i)
+      if (g_cache[i].id == id) {
+        *out = g_cache[i].addr;
+        return LSFDTD_OK;
       }
-    }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);  // makes the device's context current if needed
+  if (e != cudaSuccess || !p)
+    return noalloc_fail(LSFDTD_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
+  if (!id) id = current_context_id();  // the first runtime call of the process has just created the context
+  if (id) {
+    const int slot = g_cache_n < kMaxContexts ? g_cache_n++ : (g_cache_next++ % kMaxContexts);
+    g_cache[slot] = {id, *out};
   }
-  if (a.want_energy) {
-    double v = warp_sum(e2);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      double w = threadIdx.x < kMonBlock / 32 ? red[threadIdx.x] : 0.0;
-      w = warp_sum(w);
-      if (threadIdx.x == 0) a.partial[blockIdx.x] = w;
-    }
-  }
-}
-
-// energy = the sum of the first `count` partials (a fixed-order warp sum)
-__global__ void k_energy_noalloc(const double* partial, long long count, double* energy) {
-  const int lane = threadIdx.x;
-  double v = 0.0;
-  for (long long i = lane; i < count; i += 32) v += partial[i];
-  v = warp_sum(v);
-  if (lane == 0) *energy = v;
+  return LSFDTD_OK;
 }
 
 template <typename S>
 int sample(const lsfdtd_monitor_desc* m, const int64_t* step, double dt, double* energy, cudaStream_t s) {
+  // block counts in 64-bit arithmetic, checked against the array before any narrowing
+  const long long blocks_e = ((long long)m->n_e + kMonBlock - 1) / kMonBlock;
+  const long long blocks_h = m->n_h > 0 ? ((long long)m->n_h + kMonBlock - 1) / kMonBlock : 0;
+  const long long blocks = blocks_e + blocks_h;
+  if (blocks > kNoAllocPartials)
+    return noalloc_fail(LSFDTD_EINVAL, "lsfdtd_dft_sample_noalloc: " + std::to_string(blocks) +
+                                           " blocks of 256 points exceed the static scratch of " +
+                                           std::to_string(kNoAllocPartials) + " (split the monitor)");
+  double* partials = nullptr;
+  int r = partials_address(&partials);
+  if (r != LSFDTD_OK) return r;
   MonArgs<S> a{};
   a.nf = m->n_freq;
   a.omega = m->omega;
@@ -135,21 +130,13 @@ int sample(const lsfdtd_monitor_desc* m, const int64_t* step, double dt, double*
   a.dt = dt;
   a.nstep = reinterpret_cast<const long long*>(step);
   a.want_energy = (m->energy && m->n_h > 0 && energy) ? 1 : 0;
-  a.blocks_e = cdiv(m->n_e, kMonBlock);
-  const long long blocks = (long long)a.blocks_e + (m->n_h > 0 ? cdiv(m->n_h, kMonBlock) : 0);
-  if (blocks > kNoAllocPartials)
-    return noalloc_fail(LSFDTD_EINVAL, "lsfdtd_dft_sample_noalloc: " + std::to_string(blocks) +
-                                           " blocks of 256 points exceed the static scratch of " +
-                                           std::to_string(kNoAllocPartials) + " (split the monitor)");
-  double* partials = nullptr;
-  int r = partials_address(&partials);
-  if (r != LSFDTD_OK) return r;
+  a.blocks_e = blocks_e;
   a.partial = partials;
-  k_monitor_noalloc<S><<<(unsigned)blocks, kMonBlock, 0, s>>>(a);
+  k_monitor<S><<<(unsigned)blocks, kMonBlock, 0, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(LSFDTD_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   if (a.want_energy) {
-    k_energy_noalloc<<<1, 32, 0, s>>>(partials, blocks, energy);
+    k_energy<<<1, 32, 0, s>>>(partials, 0, blocks, 0, 0, energy);
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(LSFDTD_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   }

@@ -63,6 +63,17 @@ def test_noalloc_sample_matches_engine_sample_twice(golden):
         np.testing.assert_allclose(acc_e.cpu().numpy(), ref_e, rtol=RTOL, atol=0)
         np.testing.assert_allclose(acc_h.cpu().numpy(), ref_h, rtol=RTOL, atol=0)
         np.testing.assert_allclose(energy.cpu().numpy()[0], eng.energy.cpu().numpy()[0], rtol=RTOL, atol=0)
+
+    # after those calls, more calls change neither the device's free memory nor torch's reserved pool
+    torch.cuda.synchronize(dev)
+    free0, reserved0 = torch.cuda.mem_get_info(dev)[0], torch.cuda.memory_reserved(dev)
+    for _ in range(4):
+        rc = L.lsfdtd_dft_sample_noalloc(C.byref(d), _abi.F32, 0, eng.n.data_ptr(), eng.dt, energy.data_ptr(),
+                                         eng.stream.cuda_stream)
+        _abi.check(rc, "lsfdtd_dft_sample_noalloc")
+    torch.cuda.synchronize(dev)
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    assert torch.cuda.memory_reserved(dev) == reserved0
     eng.close()
 
 
