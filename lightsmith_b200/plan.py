@@ -95,10 +95,25 @@ class DFTMonitor:
 # --- region helpers ----------------------------------------------------------------------------------
 
 
-def _mirror_start(c: int, a: int, m: int, kind: str) -> int:
-    """First stepped index along a mirror axis (``engine.py:41-44``): 1, or 2 for the fields that vanish on an
-    antisymmetric plane (tangential E, normal H)."""
-    return 2 if m < 0 and (c != a) == (kind == "E") else 1
+def _parity(kind: str, c: int, a: int, m: int) -> int:
+    """Sign a field component takes under reflection in a mirror plane normal to axis a (m = +1 symmetric, -1
+    antisymmetric in E): an E component parallel to the plane keeps the plane's sign m, the normal one takes the
+    opposite; H, a pseudovector, takes the opposite of E's."""
+    e = m if c != a else -m
+    return e if kind == "E" else -e
+
+
+def _on_node_planes(kind: str, c: int, a: int) -> bool:
+    """Whether component c of E or H sits on the node planes along axis a (Yee staggering: E_c is half a cell
+    off along c, H_c half a cell off along both other axes)."""
+    return (c != a) if kind == "E" else (c == a)
+
+
+def _first_stepped(kind: str, c: int, a: int, m: int) -> int:
+    """First stepped index along a mirror axis (the plane at node 1, a ghost plane at 0): a component that is odd
+    under the reflection and sits on the plane vanishes there and is stepped from index 2; every other one is
+    stepped from index 1."""
+    return 2 if _parity(kind, c, a, m) < 0 and _on_node_planes(kind, c, a) else 1
 
 
 def e_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[int, int]:
@@ -106,7 +121,7 @@ def e_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[in
     outer (PEC) planes; periodic axes step the real cells 1..n-2 between two ghost planes; on a mirror axis
     (mirror = +1 or -1, the plane at node 1, a ghost plane at 0) the range starts at 1 or 2."""
     if mirror:
-        return _mirror_start(c, a, mirror, "E"), n - 1
+        return _first_stepped("E", c, a, mirror), n - 1
     if periodic or a != c:
         return 1, n - 1
     return 0, n - 1
@@ -115,7 +130,7 @@ def e_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[in
 def h_range(c: int, a: int, n: int, periodic: bool, mirror: int = 0) -> tuple[int, int]:
     """Stepped index range of H_c along axis a (``engine.py:63-66``)."""
     if mirror:
-        return _mirror_start(c, a, mirror, "H"), (n if a == c else n - 1)
+        return _first_stepped("H", c, a, mirror), (n if a == c else n - 1)
     if periodic:
         return 1, n - 1
     return (0, n) if a == c else (0, n - 1)
@@ -137,34 +152,48 @@ def pole_coefficients(pole, dt: float) -> tuple[float, float, float]:
 # --- CPML terms --------------------------------------------------------------------------------------
 
 
+def _depth_fraction(x, n_cells: int):
+    """How far into an n-cell layer a position lies, as a fraction clipped to [0, 1] (x: cells inward from the
+    layer's inner face); zero everywhere when the side has no layer."""
+    return np.clip(x / n_cells, 0, 1) if n_cells else np.zeros_like(x)
+
+
+def _grading(rho, sigma_max, pml, dt):
+    """CPML coefficients at depth fraction rho in [0, 1] (the grading of ``engine.py:361-371``: polynomial sigma
+    and kappa of order m, alpha falling linearly to zero at the outer face and zero outside the layer), as
+    (b, c, kappa) with b = exp(-(sigma/kappa + alpha) dt) and c = sigma (b - 1) / (sigma kappa + kappa^2
+    alpha), c = 0 where sigma = 0."""
+    poly = rho ** pml.m
+    sigma = sigma_max * poly
+    kappa = 1 + (pml.kappa_max - 1) * poly
+    alpha = pml.alpha_max * (1 - rho) * (rho > 0)
+    b = np.exp(-(sigma / kappa + alpha) * dt)
+    c = np.zeros_like(rho)
+    live = sigma > 0
+    c[live] = sigma[live] * (b[live] - 1) / (sigma[live] * kappa[live] + kappa[live] ** 2 * alpha[live])
+    return b, c, kappa
+
+
 def cpml_profiles(pml, shape, spacing, dt):
-    """Per axis d with a CPML: (lo_n, hi_n, {"E": (b, c, kappa), "H": (b, c, kappa)}) with 1D profiles over the
-    axis' node positions u (E) and half-integer positions u + 1/2 (H), as graded in ``engine.py:355-371``:
-    sigma = sigma_max rho^m, sigma_max = 0.8 (m + 1) / (sqrt(eps_ref) dx) (the high side may use its own eps),
-    kappa = 1 + (kappa_max - 1) rho^m, alpha = alpha_max (1 - rho) inside the layer, b = exp(-(sigma/kappa +
-    alpha) dt), c = sigma (b - 1) / (sigma kappa + kappa^2 alpha)."""
+    """Per axis d with a CPML: (lo_n, hi_n, {"E": (b, c, kappa), "H": (b, c, kappa)}), 1D profiles over the
+    axis' node positions (E) and half-integer positions (H). A position's depth fraction is taken in whichever
+    layer it lies deeper in; sigma_max = 0.8 (m + 1) / (sqrt(eps_ref) dx), with the high side's own eps_ref
+    where one is given."""
     out = {}
     for d in range(3):
         lo_n, hi_n = (int(v) for v in pml.cells[d])
         if not (lo_n or hi_n):
             continue
-        N = shape[d]
-        dx = spacing[d]
-        s_lo = 0.8 * (pml.m + 1) / (np.sqrt(pml.eps_ref) * dx)
-        s_hi = 0.8 * (pml.m + 1) / (np.sqrt(pml.eps_ref_high or pml.eps_ref) * dx)
+        n, dx = shape[d], spacing[d]
+        smax_lo, smax_hi = (0.8 * (pml.m + 1) / (np.sqrt(eps) * dx)
+                            for eps in (pml.eps_ref, pml.eps_ref_high or pml.eps_ref))
+        nodes = np.arange(n, dtype=float)
         prof = {}
-        for kind, half in (("E", 0.0), ("H", 0.5)):
-            u = np.arange(N, dtype=float) + half
-            r_lo = np.clip((lo_n - u) / lo_n, 0, 1) if lo_n else np.zeros_like(u)
-            r_hi = np.clip((u - (N - 1 - hi_n)) / hi_n, 0, 1) if hi_n else np.zeros_like(u)
-            rho = np.maximum(r_lo, r_hi)
-            sig = np.where(r_lo >= r_hi, s_lo, s_hi) * rho ** pml.m
-            kap = 1 + (pml.kappa_max - 1) * rho ** pml.m
-            alp = pml.alpha_max * (1 - rho) * (rho > 0)
-            b = np.exp(-(sig / kap + alp) * dt)
-            den = sig * kap + kap ** 2 * alp
-            c = np.where(sig > 0, sig * (b - 1) / np.where(den > 0, den, 1), 0.0)
-            prof[kind] = (b, c, kap)
+        for kind, u in (("E", nodes), ("H", nodes + 0.5)):
+            into_lo = _depth_fraction(lo_n - u, lo_n)
+            into_hi = _depth_fraction(u - (n - 1 - hi_n), hi_n)
+            sigma_max = np.where(into_lo >= into_hi, smax_lo, smax_hi)
+            prof[kind] = _grading(np.maximum(into_lo, into_hi), sigma_max, pml, dt)
         out[d] = (lo_n, hi_n, prof)
     return out
 
@@ -402,123 +431,155 @@ def _inv_eps(inv_eps, shape):
     return np.asarray(a, dtype=float).reshape((3,) + tuple(shape))
 
 
-def _mirror_fold(comp, idx3, mirror):
-    """Nodes on the ghost side of mirror planes mapped to their stepped images (``engine.py:75-90``): (idx3,
-    sign), sign the image's parity, 0 for a node that vanishes on an antisymmetric plane."""
+# --- mirror-plane geometry ----------------------------------------------------------------------------
+# A mirror plane normal to axis a lies on node plane 1; index 0 is its ghost plane. Reflection maps a node
+# position j to 2 - j and the half-integer position of the normal E component (j + 1/2) to (1 - j) + 1/2; it
+# multiplies E_c by the component's reflection sign (_parity) and a (1/eps) tensor entry (c, d) by s_c s_d,
+# with s_x = -1 for x = a.
+
+
+def _reflected_index(comp, j, a):
+    """Index along axis a of the mirror image of E_comp's position j."""
+    return np.where(comp == a, 1 - j, 2 - j)
+
+
+def fold_to_stepped(comp, idx3, mirror):
+    """E nodes (comp (n,), idx3 (n, 3)) on the ghost side of the mirror planes (index <= 0 along a mirror axis)
+    replaced by their images on the stepped side: (idx3, sign), sign the product of the reflection signs taken,
+    and 0 for a node whose image is an odd component lying on a plane (it vanishes there)."""
     idx3 = np.array(idx3, dtype=np.int64)
     comp = np.broadcast_to(np.asarray(comp), (len(idx3),))
     sign = np.ones(len(idx3), dtype=np.int64)
     for a, m in enumerate(mirror):
         if not m:
             continue
-        normal = comp == a
-        j = idx3[:, a]
-        ghost = j <= 0
-        idx3[:, a] = np.where(ghost, np.where(normal, 1 - j, 2 - j), j)
-        sign = np.where(ghost, sign * np.where(normal, -m, m), sign)
-        sign = np.where((m < 0) & ~normal & (idx3[:, a] == 1), 0, sign)
+        refl = np.where(comp == a, -m, m)  # the reflection sign of E_comp, vectorised _parity("E", ...)
+        ghost = idx3[:, a] <= 0
+        idx3[:, a] = np.where(ghost, _reflected_index(comp, idx3[:, a], a), idx3[:, a])
+        sign = sign * np.where(ghost, refl, 1)
+        sign[(refl < 0) & (comp != a) & (idx3[:, a] == 1)] = 0
     return idx3, sign
 
 
-def _mirror_rows(idx3, comp, coef, mirror):
-    """Off-diagonal rows plus their images across every mirror plane (``engine.py:540-553``): rows on a plane
-    (tangential components at node 1) are their own images; an image's (1/eps)_cd changes sign when exactly one
-    of c, d is the mirror axis."""
+def _with_mirror_twins(idx3, comp, coef, mirror):
+    """The off-diagonal rows of the whole symmetric grid that the stepped part couples to: for each mirror axis
+    in turn, every row not lying on the plane gains its reflected twin, whose tensor row is reflected too."""
     for a, m in enumerate(mirror):
         if not m:
             continue
-        normal = comp == a
-        new = normal | (idx3[:, a] != 1)
-        im = idx3[new].copy()
-        im[:, a] = np.where(normal[new], 1 - im[:, a], 2 - im[:, a])
-        flip = np.where((np.arange(3)[None, :] == a) != normal[new][:, None], -1.0, 1.0)
-        idx3 = np.concatenate([idx3, im])
-        comp = np.concatenate([comp, comp[new]])
-        coef = np.concatenate([coef, coef[new] * flip])
+        img = _reflected_index(comp, idx3[:, a], a)
+        off = img != idx3[:, a]
+        twin = idx3[off].copy()
+        twin[:, a] = img[off]
+        s_ax = np.where(np.arange(3) == a, -1.0, 1.0)
+        idx3 = np.concatenate([idx3, twin])
+        coef = np.concatenate([coef, coef[off] * (s_ax[comp[off]][:, None] * s_ax[None, :])])
+        comp = np.concatenate([comp, comp[off]])
     return idx3, comp, coef
 
 
-def offdiag_tables(od, shape, spacing, dt, periodic, bloch, mirror, group_idx, complex_fields):
-    """Gather tables of the conformal off-diagonal 1/eps terms (``engine.py:421-518``, cubic or rectangular
-    cells, no graded axes): (targets (n,), h (n, 4 W), w (n, 4 W)); row r adds sum_k w[r, k] H_flat[h[r, k]] to
-    E_flat[targets[r]] after the E curl update.
+# --- conformal off-diagonal terms ---------------------------------------------------------------------
 
-    E_c at node p couples to curl_d H at the four E_d nodes q around it (p + e_c (0 or 1) - e_d (0 or 1)); the
-    coupling is symmetrised, (1/eps)_cd(p) / 8 from q to p and its conjugate / 8 from p to q; periodic axes
-    wrap q onto the real cells with the Bloch phase of the period crossed; along other axes q must lie in
-    E_d's stepped range (mirror axes: any index, folded below). With mirror planes the rows' images are added,
-    couplings into ghost-side targets dropped, and ghost-side sources act through their images with the parity
-    sign. Pairs touching a dispersive node are dropped, equal pairs merged, and each pair's source D_d (the time
-    integral of curl_d H) expanded into its four H differences with dt / dx along each difference's axis."""
+
+def _period_phase(shift, bloch, shape, spacing):
+    """exp(i k . L n) for a position shifted by ``shift`` periods (..., 3) along the periodic axes, L the period
+    (n - 2 real cells) per axis."""
+    period = np.array([(n - 2) * h for n, h in zip(shape, spacing)], float)
+    return np.exp(1j * (np.asarray(shift, float) * (np.asarray(bloch, float) * period)).sum(-1))
+
+
+def _curl_taps(d, q, shape, spacing, dt):
+    """The four H taps of dt (curl H)_d at E_d nodes q (Yee backward differences, as the E update takes them):
+    (flat H index (4, n), weight (4, n))."""
+    d1, d2 = (d + 1) % 3, (d + 2) % 3
+    n = len(d)
+    eye = np.eye(3, dtype=np.int64)
+    inv = 1.0 / np.asarray(spacing, float)
+    taps, wts = np.empty((4, n), np.int64), np.empty((4, n))
+    for k, (cmp, back, sgn, ax) in enumerate(((d2, None, 1.0, d1), (d2, d1, -1.0, d1),
+                                               (d1, None, -1.0, d2), (d1, d2, 1.0, d2))):
+        at = q if back is None else q - eye[back]
+        taps[k] = flat_index(cmp, at[:, 0], at[:, 1], at[:, 2], shape)
+        wts[k] = dt * sgn * inv[ax]
+    return taps, wts
+
+
+def offdiag_tables(od, shape, spacing, dt, periodic, bloch, mirror, group_idx, complex_fields):
+    """Gather tables of the conformal off-diagonal 1/eps terms of tensor subpixel smoothing (``OffDiagonal``,
+    applied in ``engine.py:421-518, 653-655``; cubic or rectangular cells, no graded axes): (targets (n,),
+    h (n, W), w (n, W)); row r adds sum_k w[r, k] H_flat[h[r, k]] to E_flat[targets[r]] after the E curl
+    update, one row per target node.
+
+    The tables are one merged sparse operator, built in two products. First the E-to-E coupling K: the row of
+    E_c at node p couples to D_d (the time integral of curl_d H) at the four E_d nodes q on the cell edges
+    around p, entered in both directions, (1/eps)_cd(p) / 8 from q to p and its conjugate from p to q, so that
+    K is Hermitian (periodic axes wrap q onto the real cells with the Bloch phase of the period crossed; along
+    other axes q must be an E_d node inside the grid). Mirror planes extend the rows by their reflected twins;
+    targets on the ghost side are dropped and ghost-side sources act through their stepped images with their
+    reflection signs. Couplings touching a dispersive node are dropped. Then K times the curl: every source
+    D_d(q) is replaced by its four H taps with dt / dx along each difference's axis, and entries with the same
+    (target, H node) are summed, so each H value is read once per target."""
     shape = tuple(int(n) for n in shape)
-    ncell = int(np.prod(shape))
-    nflat = 3 * ncell
+    nflat = 3 * int(np.prod(shape))
     idx3 = np.asarray(od.idx3, np.int64)
     comp = np.asarray(od.comp, np.int64)
     coef = np.asarray(od.coef, float)
     if any(mirror):
-        idx3, comp, coef = _mirror_rows(idx3, comp, coef, mirror)
+        idx3, comp, coef = _with_mirror_twins(idx3, comp, coef, mirror)
     eye = np.eye(3, dtype=np.int64)
-    tc, ti, sc, si, fwd, bwd = [], [], [], [], [], []
+    pairs = []  # (target comp, target idx3, source comp, source idx3, value)
     for d in range(3):
-        for corner in range(4):
-            q = idx3 + eye[comp] * (corner & 1)
-            q[:, d] -= corner >> 1
-            phase = np.ones(len(q), complex)
-            ok = (comp != d) & (coef[:, d] != 0)
-            for a in range(3):
-                n = shape[a]
-                if periodic[a]:
-                    kl = bloch[a] * (n - 2) * spacing[a]
-                    lo, hi = q[:, a] == 0, q[:, a] == n - 1
-                    q[lo, a], q[hi, a] = n - 2, 1
-                    phase[lo] *= np.exp(-1j * kl)
-                    phase[hi] *= np.exp(1j * kl)
-                else:
-                    start, stop = e_range(d, a, n, False)
-                    ok &= (q[:, a] < stop) & ((q[:, a] >= start) | bool(mirror[a]))
-            tc.append(comp[ok])
-            ti.append(idx3[ok])
-            sc.append(np.full(int(ok.sum()), d))
-            si.append(q[ok])
-            fwd.append(coef[ok, d] * phase[ok] / 8)
-            bwd.append(np.conj(coef[ok, d] * phase[ok]) / 8)
-    tc, ti, sc, si, f = (np.concatenate(x) for x in (tc, ti, sc, si, fwd))
-    tc, sc = np.concatenate([tc, sc]), np.concatenate([sc, tc])
-    ti, si = np.concatenate([ti, si]), np.concatenate([si, ti])
-    v = np.concatenate([f, np.concatenate(bwd)])
+        rows = np.nonzero((comp != d) & (coef[:, d] != 0))[0]
+        p, c, o = idx3[rows], comp[rows], coef[rows, d]
+        for along_c in (0, 1):
+            for back_d in (0, 1):
+                q = p + eye[c] * along_c
+                q[:, d] -= back_d
+                shift = np.zeros(q.shape, np.int64)
+                inside = np.ones(len(q), bool)
+                for a in range(3):
+                    n = shape[a]
+                    if periodic[a]:  # ghost planes 0 and n-1 stand for the real planes n-2 and 1
+                        shift[:, a] = (q[:, a] == n - 1).astype(np.int64) - (q[:, a] == 0)
+                        q[:, a] -= shift[:, a] * (n - 2)
+                    else:
+                        lo, hi = e_range(d, a, n, False)
+                        inside &= (q[:, a] < hi) & ((q[:, a] >= lo) | bool(mirror[a]))
+                kq = o[inside] * _period_phase(shift[inside], bloch, shape, spacing)
+                dd = np.full(int(inside.sum()), d)
+                pairs.append((c[inside], p[inside], dd, q[inside], kq / 8))
+                pairs.append((dd, q[inside], c[inside], p[inside], np.conj(kq) / 8))
+    tc, ti, sc, si, v = (np.concatenate([x[k] for x in pairs]) for k in range(5))
     if any(mirror):
-        ti_f, t_sign = _mirror_fold(tc, ti, mirror)
-        si, s_sign = _mirror_fold(sc, si, mirror)
-        keep = (np.all(ti_f == ti, axis=1) & (t_sign != 0) & (s_sign != 0) &
+        tf, t_sign = fold_to_stepped(tc, ti, mirror)
+        si, s_sign = fold_to_stepped(sc, si, mirror)
+        keep = (np.all(tf == ti, axis=1) & (t_sign != 0) & (s_sign != 0) &
                 np.all(si < np.asarray(shape) - 1, axis=1))
         tc, ti, sc, si, v = tc[keep], ti[keep], sc[keep], si[keep], v[keep] * s_sign[keep]
     t = flat_index(tc, ti[:, 0], ti[:, 1], ti[:, 2], shape)
     src = flat_index(sc, si[:, 0], si[:, 1], si[:, 2], shape)
     if len(group_idx):
         keep = ~(np.isin(t, group_idx) | np.isin(src, group_idx))
-        t, src, v = t[keep], src[keep], v[keep]
+        t, sc, si, v = t[keep], sc[keep], si[keep], v[keep]
     if not len(t):
         return None
-    key, inv = np.unique(t * nflat + src, return_inverse=True)
-    v = np.bincount(inv, v.real, len(key)) + 1j * np.bincount(inv, v.imag, len(key))
-    t, src = key // nflat, key % nflat
-    targets, first, count = np.unique(t, return_index=True, return_counts=True)
-    slot = np.arange(len(t)) - np.repeat(first, count)
-    row = np.repeat(np.arange(len(targets)), count)
+    taps, wts = _curl_taps(sc, si, shape, spacing, dt)
+    key = (np.repeat(t[None], 4, 0) * nflat + taps).ravel()
+    val = (wts * v[None]).ravel()
+    key, inv = np.unique(key, return_inverse=True)
+    merged = np.bincount(inv, val.real, len(key)) + 1j * np.bincount(inv, val.imag, len(key))
+    nz = merged != 0
+    key, merged = key[nz], merged[nz]
+    if not len(key):
+        return None
+    tgt, hh = key // nflat, key % nflat
+    targets, first, count = np.unique(tgt, return_index=True, return_counts=True)
     width = int(count.max())
-    h = np.ones((len(targets), 4 * width), np.int64)  # padding: any valid index, weight 0
-    w = np.zeros((len(targets), 4 * width), complex)
-    d, rest = np.divmod(src, ncell)
-    q = np.stack(np.unravel_index(rest, shape), axis=1)
-    d1, d2 = (d + 1) % 3, (d + 2) % 3
-    inv_d = 1.0 / np.asarray(spacing, float)
-    # curl_d H at q = (H_d2[q] - H_d2[q - e_d1]) / dx_d1 - (H_d1[q] - H_d1[q - e_d2]) / dx_d2
-    for k, (cmp, back, sgn, ax) in enumerate(((d2, None, 1.0, d1), (d2, d1, -1.0, d1),
-                                               (d1, None, -1.0, d2), (d1, d2, 1.0, d2))):
-        pp = q if back is None else q - eye[back]
-        h[row, 4 * slot + k] = flat_index(cmp, pp[:, 0], pp[:, 1], pp[:, 2], shape)
-        w[row, 4 * slot + k] = dt * sgn * inv_d[ax] * v
+    slot = np.arange(len(tgt)) - np.repeat(first, count)
+    row = np.repeat(np.arange(len(targets)), count)
+    h = np.zeros((len(targets), width), np.int64)  # padding: index 0 with weight 0
+    w = np.zeros((len(targets), width), complex)
+    h[row, slot], w[row, slot] = hh, merged
     return targets.astype(np.int64), h, (w if complex_fields else w.real)
 
 
@@ -532,13 +593,11 @@ def tensor_plan(tm, shape, spacing, bloch, complex_fields) -> dict:
     phase under a Bloch wavevector), a (``_Harmonic``) and b (``_Arithmetic``) with their own pole states and
     the vertex's medium fractions; per plain slot out = (1/2) medium[D] of its one medium; a node's E is the sum
     of its two slots."""
-    nN, nV = len(tm.node_comp), len(tm.normal)
+    n_nodes = len(tm.node_comp)
     idx = np.asarray(tm.idx, np.int64)
-    L = np.array([(n - 2) * d for n, d in zip(shape, spacing)])
-    ph = np.exp(1j * (np.asarray(tm.shift) * (np.asarray(bloch, float) * L)).sum(-1))  # (nV, 3, 2)
-    scale = ph if complex_fields else np.ones(ph.shape)
-    if tm.sign is not None:
-        scale = scale * np.asarray(tm.sign, float)
+    ph = _period_phase(tm.shift, bloch, shape, spacing)  # per vertex, d and side: (nV, 3, 2)
+    parity = np.ones(ph.shape) if tm.sign is None else np.asarray(tm.sign, float)
+    scale = ph * parity if complex_fields else parity
     sv = np.asarray(tm.slot_vert)
     tk, tnode = np.nonzero((sv >= 0).T)  # slots ordered (k, node)
     tv = sv[tnode, tk]
@@ -546,11 +605,11 @@ def tensor_plan(tm, shape, spacing, bloch, complex_fields) -> dict:
     side = 1 - tk
     nrm = np.asarray(tm.normal, float)
     pk, pnode = np.nonzero((sv < 0).T)
-    out = {"idx": idx, "n_nodes": nN, "vn": np.asarray(tm.vert_nodes, np.int64).reshape(-1),
-           "normal": nrm.reshape(-1), "t_pos": (tk * nN + tnode).astype(np.int64), "t_v": tv.astype(np.int64),
+    out = {"idx": idx, "n_nodes": n_nodes, "vn": np.asarray(tm.vert_nodes, np.int64).reshape(-1),
+           "normal": nrm.reshape(-1), "t_pos": (tk * n_nodes + tnode).astype(np.int64), "t_v": tv.astype(np.int64),
            "t_vc": (tv * 3 + tc).astype(np.int64), "t_g": ((tv * 3 + tc) * 2 + side).astype(np.int64),
            "t_nc": nrm[tv, tc], "frac": np.asarray(tm.frac, float)[:, tv],
-           "p_pos": (pk * nN + pnode).astype(np.int64), "p_node": pnode.astype(np.int64),
+           "p_pos": (pk * n_nodes + pnode).astype(np.int64), "p_node": pnode.astype(np.int64),
            "p_medium": np.asarray(tm.slot_medium, np.int64)[pnode, pk], "media": _media_plan(tm.media)}
     scaled = complex_fields or tm.sign is not None
     out["scale"] = (scale.reshape(-1) if complex_fields else scale.real.reshape(-1)) if scaled else None

@@ -62,13 +62,40 @@ def test_oracle_detects_a_planted_mistake(golden):
     assert _rel(eng.H, d["out"]["H"]) > 1e-6
 
 
+def sparse_operator(e, h, w):
+    """The gather tables (targets, H indices, weights) as a merged sparse operator: keys target * 2^32 + H node
+    and their summed weights, padding and other zero entries dropped."""
+    e, h, w = np.asarray(e), np.asarray(h), np.asarray(w)
+    key = np.repeat(e.astype(np.int64), h.shape[1]) * (1 << 32) + h.ravel()
+    key, inv = np.unique(key, return_inverse=True)
+    val = np.bincount(inv, w.ravel().real, len(key)) + 1j * np.bincount(inv, w.ravel().imag, len(key))
+    nz = val != 0
+    return key[nz], val[nz]
+
+
 @pytest.mark.parametrize("case", ["offdiag", "offdiag_mirror"])
-def test_offdiag_gather_tables_equal_the_reference(case, golden):
-    """The plan builder's conformal off-diagonal gather tables (targets, H indices, weights) against the ones
+def test_offdiag_gather_tables_equal_the_reference_operator(case, golden):
+    """The plan builder's conformal off-diagonal tables, rebuilt here from the fixture's rows, against the ones
     lightsmith's engine built from the same rows (engine.py:421-518), mirror planes and a dispersive group
-    included."""
+    included: the same operator (every (target, H node) weight, to rounding), in a merged layout of its own."""
+    from lightsmith_b200.plan import offdiag_tables
+
     d = golden("engine_" + case)
-    od, out = d["plan"]["offdiag"], d["out"]
-    assert np.array_equal(od["e"], out["od_e"])
-    assert np.array_equal(od["h"], out["od_h"])
-    assert np.array_equal(od["w"], out["od_w"])
+    plan, out = d["plan"], d["out"]
+    rows = out["od_rows"]
+
+    class Rows:
+        idx3, comp, coef = rows["idx3"], rows["comp"], rows["coef"]
+    gidx = np.concatenate([np.asarray(g["idx"]) for g in plan["groups"]]) if plan["groups"] else np.zeros(0, int)
+    e, h, w = offdiag_tables(Rows, plan["shape"], plan["spacing"], plan["dt"], plan["periodic"], plan["bloch"],
+                             plan.get("mirror", (0, 0, 0)), gidx, plan["complex"])
+    for x, y in zip((e, h, w), (plan["offdiag"]["e"], plan["offdiag"]["h"], plan["offdiag"]["w"])):
+        assert np.array_equal(x, y)  # the fixture's plan holds this builder's tables
+    ka, va = sparse_operator(e, h, w)
+    kb, vb = sparse_operator(out["od_e"], out["od_h"], out["od_w"])
+    keys = np.union1d(ka, kb)  # an entry one side sums to exactly zero may be a rounding residue on the other
+    dense_a, dense_b = np.zeros(len(keys), complex), np.zeros(len(keys), complex)
+    dense_a[np.searchsorted(keys, ka)], dense_b[np.searchsorted(keys, kb)] = va, vb
+    np.testing.assert_allclose(dense_a, dense_b, rtol=0, atol=1e-14 * np.abs(vb).max())
+    assert len(np.setdiff1d(ka, kb)) < 0.01 * len(kb)
+    assert h.shape[1] < np.asarray(out["od_h"]).shape[1]  # merged: fewer taps per target than lightsmith's
