@@ -310,7 +310,7 @@ int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
  * pass over an interior box that needs no region or CPML tests, and shell kernels over the CPML slabs and
  * walls. variant 4: variant 1 with region tests as bit masks and each axis's CPML terms under warp-uniform
  * branches. Variants 3 and 4 compute the values of variant 1 up to the contraction of multiplies and adds
- * into fused multiply-adds. planes 0 chooses per grid: 32, or fewer where 32 would leave fewer than about
+ * into fused multiply-adds. planes 0 chooses per grid: 48, or fewer where 48 would leave fewer than about
  * three waves of CTAs. Default: variant 4, tile_y 8, planes 0, ring 4 (the in-place kernels where the fused
  * pass does not apply). */
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
@@ -318,6 +318,13 @@ int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t ti
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting
  * for its copies, else LSFDTD_OK */
 int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status);
+/* clear the status word on `stream` (after a reported timeout, before the engine's arrays are rebuilt) */
+int32_t lsfdtd_engine_clear_status(lsfdtd_engine* eng, void* stream);
+/* clock cycles a CTA of the fused pass waits for one plane's copies before it gives up (records the status
+ * word, waits a bounded time for its own copies still in flight and returns): the default, about 2 s, when
+ * cycles <= 0. Set before the first graph capture. A budget shorter than a copy's latency makes the pass give
+ * up at once, which exercises the timeout path with every copy still completing normally. */
+int32_t lsfdtd_engine_set_wait_budget(lsfdtd_engine* eng, int64_t cycles);
 /* whether the fused pass may copy planes with the Tensor Memory Accelerator (default 1); before the first
  * step. With 0, or where the layout rules it out (rows not a multiple of 16 bytes), it uses cp.async. */
 int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma);

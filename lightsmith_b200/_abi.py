@@ -127,6 +127,8 @@ SIGNATURES = {
     "lsfdtd_engine_chunk_timed": (i32, [vp, i32, vp, C.POINTER(f64), C.POINTER(i64)]),
     "lsfdtd_engine_buffer": (i32, [vp]),
     "lsfdtd_engine_status": (i32, [vp, vp, C.POINTER(i32)]),
+    "lsfdtd_engine_clear_status": (i32, [vp, vp]),
+    "lsfdtd_engine_set_wait_budget": (i32, [vp, C.c_int64]),
     "lsfdtd_engine_set_copy_engine": (i32, [vp, i32]),
     "lsfdtd_engine_uses_tma": (i32, [vp]),
     "lsfdtd_engine_fused": (i32, [vp]),

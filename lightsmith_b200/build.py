@@ -14,7 +14,7 @@ HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "yee.cuh", "yee
                                                    "monitors.cuh", "tensor.cuh")] + \
     [os.path.join(REPO, "include", "lsfdtd.h")]
 OUT = os.path.join(HERE, "liblsfdtd.so")
-FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "--threads", "0", "-Xcompiler", "-fPIC",
          "-shared", "-I" + os.path.join(REPO, "include")]
 
 

@@ -32,6 +32,7 @@ struct TmaArgs {
   CUtensorMap mH[3];   // H^n components, box 40 x (TY + 1) x 1
   CUtensorMap mC;      // cbE (component 0), box 32 x TY x 1
   int* status;         // set to 1 when a copy wait exceeded its budget
+  long long wait_budget;  // clock cycles a CTA waits for one plane's copies before it gives up
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -65,8 +66,28 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 __device__ __forceinline__ float shfl_up(unsigned m, float v) { return __shfl_up_sync(m, v, 1); }
 __device__ __forceinline__ double shfl_up(unsigned m, double v) { return __shfl_up_sync(m, v, 1); }
 
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// budgets below this many cycles are polled with the non-blocking test (try_wait may suspend the thread for
+// longer than such a budget, until the phase completes)
+constexpr long long kPollBelow = 1LL << 20;
+
 // bounded wait: false when the budget ran out
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long budget) {
+  if (budget < kPollBelow) {
+    const long long t0 = clock64();
+    while (!mbar_test_wait(bar, parity))
+      if (clock64() - t0 > budget) return false;
+    return true;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
@@ -75,7 +96,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
   return true;
 }
 
-constexpr long long kWaitBudget = 4000000000LL;  // cycles (about 2 s): copies of a few KB take microseconds
+// the default wait budget: about 2 s, where copies of a few KB take microseconds
+constexpr long long kWaitBudget = 4000000000LL;
 constexpr long long kDrainBudget = 200000000LL;
 
 template <typename F, int TY>
@@ -156,7 +178,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
   };
   auto ready = [&](int p) -> bool {
-    return mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, kWaitBudget);
+    return mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, t.wait_budget);
   };
   int issued = xb - 1;  // last plane whose copies were issued
   if (tid == 0) {

@@ -119,6 +119,7 @@ struct lsfdtd_engine {
   int sm_count = 0;
   int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
   bool tuned = false;   // a kernel choice was set explicitly (lsfdtd_engine_set_tuning)
+  long long wait_budget = lsfdtd::kWaitBudget;  // cycles the fused pass waits for a plane's copies
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
@@ -300,27 +301,24 @@ struct Engine final : lsfdtd_engine {
     }
     return LSFDTD_OK;
   }
-  template <int TY, int S>
-  int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+  template <int TY, int S, bool UNI>
+  int launch_pml_one(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
       constexpr size_t sm = fused_pml_smem_bytes<F, TY, S>();
-      static bool attr[2] = {false, false};  // per instantiation (cubic cells or not)
-      const int u = y.uniform ? 1 : 0;
-      if (!attr[u]) {
-        if (u)
-          LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm));
-        else
-          LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm));
-        attr[u] = true;
+      static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
+      if (!attr) {
+        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+        attr = true;
       }
-      if (u)
-        k_fused_pml<F, TY, S, true><<<grid, dim3(32, TY), sm, s>>>(ta);
-      else
-        k_fused_pml<F, TY, S, false><<<grid, dim3(32, TY), sm, s>>>(ta);
+      k_fused_pml<F, TY, S, UNI><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
+  }
+  // the lean-CPML pass, one instantiation per cell shape (cubic or not)
+  template <int TY, int S>
+  int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+    return y.uniform ? launch_pml_one<TY, S, true>(grid, ta, s) : launch_pml_one<TY, S, false>(grid, ta, s);
   }
   // kind 0: the fused pass over the grid, 1: over the interior box of the split step, 2: with lean CPML terms
   template <int TY, int S>
@@ -425,7 +423,7 @@ struct Engine final : lsfdtd_engine {
     }
     const long long per_sm = sizeof(R) == 4 ? (rows == 8 ? 4 : 2) : 1;
     const long long p = (long long)nx * columns / (3 * per_sm * std::max(sm_count, 1));
-    *seg = (int)std::max(4LL, std::min(32LL, p));
+    *seg = (int)std::max(4LL, std::min(48LL, p));
     return LSFDTD_OK;
   }
 
@@ -477,6 +475,7 @@ struct Engine final : lsfdtd_engine {
         }
         ta.mC = mapC;
         ta.status = static_cast<int*>(scratch);
+        ta.wait_budget = wait_budget;
         // the deepest ring, up to the requested depth, that fits the device's shared memory per CTA
         int smax = 0, dev = 0;
         LS_CUDA(cudaGetDevice(&dev));
@@ -1703,6 +1702,21 @@ int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status) 
   LS_CUDA(cudaStreamSynchronize(s));
   *status = v;
   if (v) return fail(LSFDTD_ETIMEOUT, "a kernel gave up waiting for its copies (status word set)");
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_clear_status(lsfdtd_engine* eng, void* stream) {
+  LS_NEED(eng);
+  if (!eng->scratch || eng->scratch_bytes < sizeof(int32_t)) return LSFDTD_OK;
+  LS_CUDA(cudaMemsetAsync(eng->scratch, 0, sizeof(int32_t), static_cast<cudaStream_t>(stream)));
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_set_wait_budget(lsfdtd_engine* eng, int64_t cycles) {
+  LS_NEED(eng);
+  if (eng->exec[0] || eng->exec[1])
+    return fail(LSFDTD_EINVAL, "the wait budget must be set before the first graph capture");
+  eng->wait_budget = cycles > 0 ? (long long)cycles : lsfdtd::kWaitBudget;
   return LSFDTD_OK;
 }
 

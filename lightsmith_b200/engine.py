@@ -566,12 +566,22 @@ class Engine:
         _abi.check(_abi.lib().lsfdtd_engine_status(self._h, self.stream.cuda_stream, C.byref(st)),
                    "lsfdtd_engine_status")
 
+    def clear_status(self) -> None:
+        """Clear the status word a timed-out copy wait set (on the engine's stream)."""
+        _abi.check(_abi.lib().lsfdtd_engine_clear_status(self._h, self.stream.cuda_stream),
+                   "lsfdtd_engine_clear_status")
+
+    def set_wait_budget(self, cycles: int) -> None:
+        """Clock cycles the fused pass waits for one plane's copies before it gives up (default about 2 s when
+        ``cycles`` <= 0); before the first graph capture."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_wait_budget(self._h, int(cycles)), "lsfdtd_engine_set_wait_budget")
+
     def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:
         """Kernel choice and launch shape (before the first graph capture): variant 0 the in-place H and E
         kernels, 2 their four-node vector form, 1 the fused pass (CTA tile rows 8 or 16, x planes per tile,
         copy ring 4/6/8), 3 the fused pass split into an interior box and CPML/wall shell kernels, 4 the fused
         pass with lean CPML terms (the default, with tile rows 8, planes per grid and ring 4; runs the fused pass
-        does not serve take the in-place kernels). ``planes=0`` chooses per grid: 32, or fewer on grids too
+        does not serve take the in-place kernels). ``planes=0`` chooses per grid: 48, or fewer on grids too
         small for about three waves of CTAs."""
         _abi.check(_abi.lib().lsfdtd_engine_set_tuning(self._h, int(variant), int(tile_y), int(planes),
                                                        int(stages)), "lsfdtd_engine_set_tuning")

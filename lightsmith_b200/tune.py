@@ -17,7 +17,7 @@ import os
 
 # (variant, tile rows, x planes per tile, ring depth): variant 0 the in-place kernels, 2 their four-node
 # vector form, 1 the fused pass, 3 the fused pass split into an interior box and the CPML/wall shell, 4 the
-# fused pass with lean CPML terms; planes 0 lets the engine choose per grid (32, fewer on small grids)
+# fused pass with lean CPML terms; planes 0 lets the engine choose per grid (48, fewer on small grids)
 CANDIDATES = [(0, 8, 32, 4), (2, 8, 32, 4), (1, 8, 0, 4), (1, 16, 0, 4), (3, 8, 0, 4), (3, 16, 0, 4),
               (4, 8, 0, 4), (4, 16, 0, 4), (4, 8, 8, 4), (4, 8, 24, 4), (4, 8, 48, 4), (4, 8, 64, 4)]
 
