@@ -24,17 +24,23 @@ def cross_sections(acc_e, acc_h, post: dict) -> dict:
     total-field box, incident reference view; scattering.py:344-363). ``post`` holds what the driver computes
     from its source object on the host: ``n_inc`` and ``n_sym``, the flux weights of the two boxes
     (``sca_coeff``, ``tot_coeff``), the incident reference polarisation ``unit`` (f, 3) and the unit-amplitude
-    background fields on the total-field box, ``bg_e`` and the H average ``bg_h`` (scattering.py:438-441).
+    background fields on the total-field box, ``bg_e`` and the H average ``bg_h`` (scattering.py:438-441), or
+    instead their flux through that box per frequency, ``bg_flux``.
     """
     e_ref = np.asarray(acc_e[2], complex)
     e0sq = np.sum(np.abs(e_ref) ** 2, axis=1)
     intensity = 0.5 * post["n_inc"] * e0sq  # scattering.py:433-435
     unit = np.asarray(post["unit"], complex)
     amp = np.sum(e_ref * np.conj(unit), axis=1) / np.sum(np.abs(unit) ** 2, axis=1)
-    e_bg = amp[:, None] * post["bg_e"]
-    h_bg = amp[:, None] * post["bg_h"]
     n_sym = post.get("n_sym", 1.0)
-    bg_out = n_sym * flux(e_bg, h_bg, post["tot_coeff"])  # scattering.py:442
+    if "bg_flux" in post:
+        # the flux is bilinear in (E, H) and both background fields carry the same amplitude: the unit-amplitude
+        # background's flux per frequency, times |amp|^2
+        bg_out = n_sym * np.abs(amp) ** 2 * np.asarray(post["bg_flux"], float)
+    else:
+        e_bg = amp[:, None] * post["bg_e"]
+        h_bg = amp[:, None] * post["bg_h"]
+        bg_out = n_sym * flux(e_bg, h_bg, post["tot_coeff"])  # scattering.py:442
     c_sca = n_sym * flux(acc_e[0], acc_h[0], post["sca_coeff"]) / intensity  # scattering.py:457-459
     c_abs = -(n_sym * flux(acc_e[1], acc_h[1], post["tot_coeff"]) - bg_out) / intensity
     return {"c_sca": c_sca, "c_abs": c_abs, "c_ext": c_sca + c_abs}

@@ -408,75 +408,81 @@ def solve_case(name: str, sim):
 
 def c0_case():
     """The full-size sphere: the plan and post-processing inputs lightsmith's scattering driver builds, then
-    lightsmith's own engine (float64, on the host) run for exactly 4000 steps and the cross sections from its
-    accumulators by oracle/post.py (which reproduces lightsmith's to 1e-13 on the other solve fixtures).
-    ``ls.solve`` itself is not used for the run: its run loop stops this one at step 3100 with its divergence
-    test (setup.py:749-756), whose reference is the monitor energy of the run's first half, before the pulse
-    has reached the scattered-field box; the energy per chunk is kept in the fixture."""
-    from lightsmith.device import Device
-    from oracle.post import cross_sections
+    lightsmith's own engine run on the host for exactly 4000 steps twice, in float64 and in float32 (its GPU
+    precision; here through PyTorch on the CPU), and the cross sections at all 81 wavelengths from each run's
+    accumulators by oracle/post.py (which reproduces lightsmith's post-processing to 1e-13 on the other solve
+    fixtures). The background's flux through the total-field box is kept per wavelength (``bg_flux``, the
+    unit-amplitude flux; the post-processing scales it by the measured incident amplitude), which keeps the
+    fixture small. ``ls.solve`` itself is not used for the run: its run loop stops this one at step 3100 with
+    its divergence test (setup.py:749-756), whose reference is the monitor energy of the run's first half,
+    before the pulse has reached the scattered-field box; the energy per chunk is kept in the fixture."""
+    import torch
+    from lightsmith.device import resolve_device
+
+    from oracle.post import cross_sections, flux
 
     sim = c0_problem()
-    rec = {}
 
     class Stop(Exception):
         pass
 
-    def capture(device, **kw):
-        rec["kw"] = kw
-        raise Stop()
+    def setup():
+        rec, boxes = {}, []
 
-    boxes = []
-    fp_orig = ref_scattering.flux_points
+        def capture(device, **kw):
+            rec["kw"] = kw
+            raise Stop()
 
-    def flux_points_rec(*a, **k):
-        out = fp_orig(*a, **k)
-        boxes.append(out)
-        return out
-    Base = ref_scattering.Engine
-    ref_scattering.Engine = capture
-    ref_scattering.flux_points = flux_points_rec
-    try:
-        ls.solve(sim, "fdtd", "cpu")
-    except Stop:
-        pass
-    finally:
-        ref_scattering.Engine = Base
-        ref_scattering.flux_points = fp_orig
-    kw = rec["kw"]
-    plan = P.make_plan(**kw)
-    eng = Base(Device("numpy", "cpu"), **kw)
-    run, _ = eng.make_runner(False)
+        def flux_points_rec(*a, **k):
+            out = fp_orig(*a, **k)
+            boxes.append(out)
+            return out
+        fp_orig, Base = ref_scattering.flux_points, ref_scattering.Engine
+        ref_scattering.Engine, ref_scattering.flux_points = capture, flux_points_rec
+        try:
+            ls.solve(sim, "fdtd", "cpu")
+        except Stop:
+            pass
+        finally:
+            ref_scattering.Engine, ref_scattering.flux_points = Base, fp_orig
+        return rec["kw"], boxes
+
+    torch.set_num_threads(os.cpu_count() or 1)
     steps = 4000
-    energy = []
-    for _ in range(steps // plan["stride"]):
-        run()
-        energy.append(np.asarray(eng.energy, float).copy())
+    runs = {}
+    for prec in ("double", "single"):
+        kw, boxes = setup()
+        if prec == "double":
+            plan = P.make_plan(**kw)
+        kw = {**kw, "single": prec == "single"}
+        eng = ref_scattering.Engine(resolve_device("torch-cpu"), **kw)
+        energy = []
+        for _ in range(steps // plan["stride"]):
+            eng.chunk()
+            energy.append(Device.to_numpy(eng.energy).astype(float).copy())
+        runs[prec] = (kw, eng, boxes, np.asarray(energy))
+    kw, eng, boxes, energy = runs["double"]
     src = kw["sources"][0]
     omega = 2 * np.pi / sim.wavelength_array()
     sca, tot = boxes
+    bg_e = src.background(omega, tot[0], "E")
+    bg_h = 0.5 * (src.background(omega, tot[1], "H") + src.background(omega, tot[2], "H"))
     post = {"omega": omega, "n_sym": 1.0, "n_inc": float(src.n_inc), "sca_coeff": sca[3], "tot_coeff": tot[3],
-            "unit": src.incident_reference(omega), "bg_e": src.background(omega, tot[0], "E"),
-            "bg_h": 0.5 * (src.background(omega, tot[1], "H") + src.background(omega, tot[2], "H")),
-            "steps": steps}
-    acc_e = [np.asarray(m.acc_e) for m in kw["monitors"]]
-    acc_h = [None if m.acc_h is None else np.asarray(m.acc_h) for m in kw["monitors"]]
-    cs = cross_sections(acc_e, acc_h, post)
-    sel = np.arange(0, 81, 10)
-    post = {**post, "omega": omega[sel], "unit": post["unit"][sel], "bg_e": post["bg_e"][sel],
-            "bg_h": post["bg_h"][sel], "freq_sel": sel}
-    out = {k: cs[k][sel] for k in ("c_ext", "c_sca", "c_abs")}
-    out.update(n=int(eng.n[0]) if hasattr(eng.n, "__len__") else int(eng.n), energy=np.asarray(energy))
+            "unit": src.incident_reference(omega), "bg_flux": flux(bg_e, bg_h, tot[3]), "steps": steps}
+    out = {"n": int(Device.to_numpy(eng.n)[0]), "energy": energy}
+    for prec, tag in (("double", "fp64"), ("single", "fp32")):
+        kw_p, eng_p = runs[prec][:2]
+        acc_e = [Device.to_numpy(m.acc_e).astype(complex) for m in kw_p["monitors"]]
+        acc_h = [None if m.acc_h is None else Device.to_numpy(m.acc_h).astype(complex) for m in kw_p["monitors"]]
+        cs = cross_sections(acc_e, acc_h, post)
+        if prec == "double":
+            out.update({k: cs[k] for k in ("c_ext", "c_sca", "c_abs")})
+        else:
+            out["lightsmith_fp32"] = {k: cs[k] for k in ("c_ext", "c_sca", "c_abs")}
     P.save(os.path.join(HERE, "solve_c0.npz"), {"plan": plan, "post": post, "out": out})
-    print("c0", plan["shape"], "steps", steps, "C_ext", out["c_ext"], "energy (first, max, last)",
-          np.asarray(energy)[[0, -1]], np.asarray(energy).max(axis=0))
-
-
-
-
-
-
-# --- every engine a problem driver builds, through ls.solve ----------------------------------------------
+    err = {k: float(np.max(np.abs(out["lightsmith_fp32"][k] - out[k]) / np.abs(out[k]))) for k in ("c_ext", "c_sca",
+                                                                                                  "c_abs")}
+    print("c0", plan["shape"], "steps", steps, "lightsmith fp32 vs fp64 (max rel over 81 wavelengths)", err)
 
 
 def driver_case(name: str, problem, module):

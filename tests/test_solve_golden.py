@@ -79,20 +79,27 @@ def test_cuda_engine_replays_the_solve(case, precision, golden):
         np.testing.assert_allclose(cs[k], out[k], rtol=rtol, atol=0, err_msg=f"{case} {precision} {k}")
 
 
+# the full-size sphere's FP32 bar: a cross section's error against lightsmith's FP64 engine may be this many
+# times the error of lightsmith's own FP32 engine at that wavelength (measured per wavelength and cross
+# section on the same plan), and is always allowed lightsmith's GPU-against-CPU tolerance (tests/test_fdtd.py:131)
+F32_MULTIPLE = 3.0
+F32_FLOOR = 1e-4
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["double", "single"])
 def test_cuda_engine_replays_the_full_size_sphere(precision, golden):
     """The full-size dispersive sphere (``solve_c0.npz``: r = 40 nm, 129^3 cells of 2 nm, CPML 12, 81
-    wavelengths, staircase, 4000 steps): lightsmith's plan replayed on the CUDA engine, cross sections at 9 of
-    the 81 wavelengths (the fixture keeps the post-processing inputs of those rows) against lightsmith's own
-    engine run in FP64 on the host, per wavelength. FP64: 1e-9 relative. FP32: every cross section within
-    1e-3 of that wavelength's C_ext (the scale of the fluxes they are differences of; measured at most 8e-4,
-    at 800 nm where C_abs is 7 % of C_ext and its own relative error 1e-2)."""
+    wavelengths, staircase, 4000 steps): lightsmith's plan replayed on the CUDA engine, cross sections at all 81
+    wavelengths against lightsmith's own engine run on the same plan in FP64, per wavelength and per cross
+    section. FP64: 1e-9 relative. FP32: within max(1e-4, 3 x lightsmith's own FP32 error) of the FP64 value,
+    per wavelength and cross section; lightsmith's own FP32 run (the same plan, 4000 steps in float32) is off
+    its FP64 run by up to 8.1e-4 (C_ext), 2.6e-4 (C_sca) and 1.1e-2 (C_abs at 800 nm, where C_abs is 7 % of
+    C_ext), so FP32 arithmetic itself, not the kernels, sets those errors."""
     from lightsmith_b200.engine import Engine
 
     d = golden("solve_c0")
     plan, out, post = d["plan"], d["out"], d["post"]
-    sel = np.asarray(post["freq_sel"])
     eng = Engine.from_plan(plan, precision=precision)
     run, used = eng.make_runner(True)
     assert used
@@ -101,10 +108,14 @@ def test_cuda_engine_replays_the_full_size_sphere(precision, golden):
     assert eng.n_host == out["n"] == 4000
     es, hs = _accumulators(eng, len(plan["monitors"]))
     eng.close()
-    cs = cross_sections([e[sel] for e in es], [None if h is None else h[sel] for h in hs], post)
+    cs = cross_sections(es, hs, post)
     for k in ("c_ext", "c_sca", "c_abs"):
+        assert cs[k].shape == (81,)
+        err = np.abs(cs[k] - out[k]) / np.abs(out[k])
         if precision == "double":
-            np.testing.assert_allclose(cs[k], out[k], rtol=RTOL_F64, atol=0, err_msg=f"c0 {precision} {k}")
+            assert err.max() < RTOL_F64, (k, err.max())
         else:
-            err = np.abs(cs[k] - out[k]) / np.abs(out["c_ext"])
-            assert err.max() <= 1e-3, (k, err)
+            err_ls = np.abs(out["lightsmith_fp32"][k] - out[k]) / np.abs(out[k])
+            bar = np.maximum(F32_FLOOR, F32_MULTIPLE * err_ls)
+            worst = int(np.argmax(err / bar))
+            assert np.all(err <= bar), (k, worst, err[worst], err_ls[worst])
