@@ -31,7 +31,8 @@ enum {
   LSFDTD_ECUDA = 2,       /* a CUDA call failed (the message names it) */
   LSFDTD_EUNSUPPORTED = 3,
   LSFDTD_ERANGE = 4,      /* the run would read a source waveform past its end */
-  LSFDTD_ETIMEOUT = 5     /* a kernel gave up waiting for its own copies (bounded wait, status word set) */
+  LSFDTD_ETIMEOUT = 5,    /* a kernel gave up waiting for its own copies (bounded wait, status word set) */
+  LSFDTD_ENONFINITE = 6   /* a batched run's fields turned non-finite; the run retired (status word 2) */
 };
 #define LSFDTD_MAX_MEDIA 4
 #define LSFDTD_MAX_POLES 6
@@ -274,6 +275,18 @@ int64_t lsfdtd_tensor_state_len(int64_t n_nodes, int64_t n_vert, int64_t n_tslot
 int32_t lsfdtd_engine_add_tensor(lsfdtd_engine* eng, const lsfdtd_tensor_desc* d);
 /* sources act in the order they are added (Engine.step, engine.py:665-678) */
 int32_t lsfdtd_engine_add_table_source(lsfdtd_engine* eng, const lsfdtd_table_source_desc* s);
+/* The slab boxes of a table-fed source's H corrections (source `table`, counted among the engine's table
+ * sources), for the fused single pass to add them as it steps. lightsmith adds them after the whole H update
+ * (ObliqueLayeredPlaneWave.correct_H through apply_fused, backends/_fdtd/layered.py:231-242, 469-476); the
+ * fused pass computes H and E plane by plane, so the step's values are computed first (one per correction
+ * entry, in the source's slab order) and each H value of a tile gets the values of the boxes that hold it
+ * before the E half reads it. boxes: host int32 [n_boxes][8] = component, lo[3], hi[3] (node ranges), offset of
+ * the box's first entry; a box's entries are its nodes in row-major order. perm: device int64 [n_entries], the
+ * position of each slab-order entry among the entries as given in the source's descriptor (grouped by node);
+ * vals: device scratch of n_entries values of the field precision. Before the first step. Without boxes a
+ * source with H corrections keeps the in-place kernels. */
+int32_t lsfdtd_engine_set_table_boxes(lsfdtd_engine* eng, int32_t table, int32_t n_boxes, const int32_t* boxes,
+                                      const int64_t* perm, int64_t n_entries, void* vals);
 int32_t lsfdtd_engine_add_dipole(lsfdtd_engine* eng, const lsfdtd_dipole_desc* s);
 int32_t lsfdtd_engine_add_line_source(lsfdtd_engine* eng, const lsfdtd_line_source_desc* s);
 int32_t lsfdtd_engine_add_column_source(lsfdtd_engine* eng, const lsfdtd_column_source_desc* s);
@@ -316,14 +329,16 @@ int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
                                  int32_t stages);
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting
- * for its copies, else LSFDTD_OK */
+ * for its copies, LSFDTD_ENONFINITE with *status = 2 if the run's fields turned non-finite in a batched launch
+ * (the run retired then), else LSFDTD_OK */
 int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status);
 /* clear the status word on `stream` (after a reported timeout, before the engine's arrays are rebuilt) */
 int32_t lsfdtd_engine_clear_status(lsfdtd_engine* eng, void* stream);
 /* clock cycles a CTA of the fused pass waits for one plane's copies before it gives up (records the status
  * word, waits a bounded time for its own copies still in flight and returns): the default, about 2 s, when
- * cycles <= 0. Set before the first graph capture. A budget shorter than a copy's latency makes the pass give
- * up at once, which exercises the timeout path with every copy still completing normally. */
+ * cycles == 0. Negative: a test of that path, in which every wait is on a barrier that nothing completes and
+ * gives up after -cycles cycles, while the copies the pass issued still complete and are drained. Set before
+ * the first graph capture. */
 int32_t lsfdtd_engine_set_wait_budget(lsfdtd_engine* eng, int64_t cycles);
 /* whether the fused pass may copy planes with the Tensor Memory Accelerator (default 1); before the first
  * step. With 0, or where the layout rules it out (rows not a multiple of 16 bytes), it uses cp.async. */
@@ -367,6 +382,12 @@ typedef struct lsfdtd_batch lsfdtd_batch;
 /* a batch of n engines of one precision; last[i]: the step count run i stops at (at most what its source
  * waveform covers). The runs are spread over the kernel's CTAs longest first. */
 int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out);
+/* the same with the launch's shape: cluster_ctas CTAs of 512 threads per run (1 to 16; above 8 the GPU must
+ * allow non-portable clusters) and at most max_clusters clusters in flight (0: as many as fit). Fewer clusters
+ * step fewer runs at a time, whose state then stays in L2 through the steps of a launch; the default shape is
+ * 8 CTAs and as many clusters as fit */
+int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, const int64_t* last,
+                                   int32_t cluster_ctas, int32_t max_clusters, lsfdtd_batch** out);
 int32_t lsfdtd_batch_destroy(lsfdtd_batch* batch);
 /* device scratch the batch needs (run descriptors and the CTAs' run lists), set once; set_scratch copies
  * the descriptors in (synchronously) */

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblsfdtd.so")
 
 F32, F64 = 0, 1
-OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE, ETIMEOUT = 0, 1, 2, 3, 4, 5
+OK, EINVAL, ECUDA, EUNSUPPORTED, ERANGE, ETIMEOUT, ENONFINITE = 0, 1, 2, 3, 4, 5, 6
 MAX_MEDIA, MAX_POLES = 4, 6
 ABI_VERSION = 2
 
@@ -128,6 +128,8 @@ SIGNATURES = {
     "lsfdtd_engine_buffer": (i32, [vp]),
     "lsfdtd_engine_status": (i32, [vp, vp, C.POINTER(i32)]),
     "lsfdtd_engine_clear_status": (i32, [vp, vp]),
+    "lsfdtd_batch_create_shaped": (i32, [vp, i32, vp, i32, i32, vp]),
+    "lsfdtd_engine_set_table_boxes": (i32, [vp, i32, i32, vp, vp, i64, vp]),
     "lsfdtd_engine_set_wait_budget": (i32, [vp, C.c_int64]),
     "lsfdtd_engine_set_copy_engine": (i32, [vp, i32]),
     "lsfdtd_engine_uses_tma": (i32, [vp]),

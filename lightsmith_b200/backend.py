@@ -241,6 +241,134 @@ def _grid_desc(problem, desc=None) -> dict:
     return desc
 
 
+class _Deferred(Exception):
+    """Raised in place of lightsmith's run loop while the runs of a batch are collected."""
+
+
+class _BatchedRun:
+    """One oblique run of a periodic solve: lightsmith's own set-up of it (``_run_oblique``, periodic.py:426-459)
+    built its CUDA engine; the batch advances it; the driver's post-processing then reads it."""
+
+    def __init__(self, key, eng, max_steps):
+        self.key, self.eng, self.max_steps = key, eng, int(max_steps)
+
+
+def _oblique_key(pol, kpar, wavelength):
+    return (str(pol), round(float(kpar[0]), 15), round(float(kpar[1]), 15), round(float(wavelength), 12))
+
+
+@contextmanager
+def _patched(module, **attrs):
+    saved = {k: getattr(module, k) for k in attrs}
+    try:
+        for k, v in attrs.items():
+            setattr(module, k, v)
+        yield
+    finally:
+        for k, v in saved.items():
+            setattr(module, k, v)
+
+
+def _solve_periodic_batched(cls, sim, device, steps_per_launch: int = 512):
+    """A periodic solve whose oblique runs (one per angle, wavelength and polarisation; lightsmith runs them one
+    after another, periodic.py:503-518) advance together in one persistent kernel (``BlochBatch``).
+
+    Pass 1 runs lightsmith's driver with each oblique run recorded instead of made (and the normal-incidence
+    runs skipped); each recorded run is then set up by lightsmith's own ``_run_oblique`` up to its run loop,
+    which is where its CUDA engine is taken; the batch advances every engine to the run's fixed step count
+    (``run_time_fs``); pass 2 runs the driver again, and each oblique run's set-up gets its advanced engine back
+    (its new monitors bound to that engine's accumulators) and a run loop that only reports the steps, so the
+    driver's own post-processing (orders, R and T) reads the batched results. Returns None where the runs cannot
+    be batched (no fixed step count, fewer than two oblique runs, or a feature the batch does not serve: then
+    the caller solves as usual)."""
+    import math
+
+    import torch
+
+    from .batch import BlochBatch
+
+    P = _periodic_driver
+    opts = cls._options(sim)
+    if not opts.run_time_fs or not isinstance(sim, PeriodicProblem):
+        return None, "no fixed run time (run_time_fs): each run stops when its own fields have decayed"
+    from lightsmith.problems import wavelength_array
+
+    if sum(abs(a) > 1e-12 for a in P._angles(sim)) * len(wavelength_array(sim.wavelengths)) < 2:
+        return None, "fewer than two oblique runs"  # a normal-incidence run is one broadband run
+    calls = []
+    placeholder = {"steps": 0, "decay_level": 0.0}  # what the driver's provenance reads of each run
+
+    def record(c, pol, kpar, wavelength):
+        calls.append((c, pol, kpar, wavelength))
+        nx, ny = c.cell.n_cells
+        return np.zeros((1, nx, ny)), np.zeros((1, nx, ny)), dict(placeholder)
+
+    def skip_normal(c, pol, p, omega):
+        nx, ny = c.cell.n_cells
+        z = np.zeros((len(omega), nx, ny))
+        return z, z.copy(), (None, None), dict(placeholder)
+
+    with _patched(P, _run_oblique=record, _run_normal=skip_normal):
+        NativeFDTD.solve.__func__(cls, sim, device)
+    if len(calls) < 2:
+        return None, "fewer than two oblique runs"
+
+    runs, taken = [], {}
+
+    def take(eng, opts_, *, max_steps, **_):
+        taken["eng"], taken["max_steps"] = eng, max_steps
+        raise _Deferred
+
+    original = P._run_oblique
+    with _patched(P, run_until_decayed=take):
+        for c, pol, kpar, wavelength in calls:
+            try:
+                original(c, pol, kpar, wavelength)
+            except _Deferred:
+                pass
+            runs.append(_BatchedRun(_oblique_key(pol, kpar, wavelength), taken.pop("eng"), taken.pop("max_steps")))
+    try:
+        batch = BlochBatch([r.eng for r in runs], [r.max_steps for r in runs])
+    except Exception as e:  # noqa: BLE001 (a run the batch does not serve: the caller solves run by run)
+        return None, str(e)
+    try:
+        batch.run_to_end(steps_per_launch)
+        bad = batch.diverged()
+    finally:
+        batch.close()
+    if bad:  # lightsmith's run loop raises the same error for a run it steps itself (setup.py:749-756)
+        r = runs[bad[0]]
+        raise FloatingPointError(
+            f"FDTD diverged after {int(r.eng.n.item())} steps (non-finite fields in the batched oblique run "
+            f"{r.key}); the results would be meaningless. Use a finer mesh (smaller spacing_nm or larger "
+            "cells_per_wavelength), lower courant, or give lossy/dispersive materials as Drude/DrudeLorentz")
+    by_key = {r.key: r for r in runs}
+    current = {}
+
+    def engine_back(device_, **kw):
+        r = current["run"]
+        for obj, m in zip(kw["monitors"], r.eng.monitors):
+            obj.acc_e, obj.acc_h = m["acc_e"], m["acc_h"]
+        return r.eng
+
+    def loop_done(eng, opts_, *, max_steps, **_):
+        return int(eng.n_host), float("nan"), True
+
+    def replay(c, pol, kpar, wavelength):
+        current["run"] = by_key[_oblique_key(pol, kpar, wavelength)]
+        with _patched(P, Engine=engine_back, run_until_decayed=loop_done):
+            r, t, prov = original(c, pol, kpar, wavelength)
+        return r, t, {**prov, "batched": True}
+
+    with _engine_swapped(), _patched(P, _run_oblique=replay):
+        res = NativeFDTD.solve.__func__(cls, sim, device)
+    for r in runs:
+        r.eng.close()
+    res.provenance["batched_oblique_runs"] = len(runs)
+    res.provenance["batch_steps_per_launch"] = int(steps_per_launch)
+    return res, ""
+
+
 class B200FDTD(NativeFDTD):
     """``NativeFDTD`` (backends/fdtd.py:47) whose engine is the B200 one on CUDA devices, and which serves
     lightsmith's differentiable-backend protocol (inverse/__init__.py:14-43) for device problems on CUDA
@@ -251,6 +379,8 @@ class B200FDTD(NativeFDTD):
     gpu = True
     differentiable = True
     citation = NativeFDTD.citation + "; time loop: lightsmith-b200 (sm_100a CUDA kernels)"
+    # a periodic solve with a fixed run time advances its oblique runs together in one persistent kernel
+    batch_oblique = True
 
     # --- the differentiable-backend protocol -----------------------------------------------------------------
     @classmethod
@@ -351,4 +481,12 @@ class B200FDTD(NativeFDTD):
         if device.framework != "torch":
             raise ValueError(f"{cls.name} (B200) runs on PyTorch CUDA devices, not {device.framework!r}")
         with _engine_swapped():
-            return NativeFDTD.solve.__func__(cls, sim, device)
+            why = ""
+            if isinstance(sim, PeriodicProblem) and cls.batch_oblique:
+                res, why = _solve_periodic_batched(cls, sim, device)
+                if res is not None:
+                    return res
+            res = NativeFDTD.solve.__func__(cls, sim, device)
+            if why:
+                res.provenance["oblique_runs_one_by_one"] = why
+            return res

@@ -18,9 +18,10 @@ from . import _abi
 
 class BlochBatch:
     """The runs of ``engines`` (complex fields, periodic x and y, CPML along z, one Bloch column source),
-    each to run until its step count reaches ``last`` (an int for all, or one per engine)."""
+    each to run until its step count reaches ``last`` (an int for all, or one per engine). ``cluster_ctas``:
+    CTAs per run (a thread-block cluster, 1 to 16); ``max_clusters``: clusters in flight (0: as many as fit)."""
 
-    def __init__(self, engines, last):
+    def __init__(self, engines, last, cluster_ctas: int = 8, max_clusters: int = 0):
         import torch
 
         self.engines = list(engines)
@@ -37,7 +38,8 @@ class BlochBatch:
         torch.cuda.synchronize(self.dev)  # the engines' set-up (zeroed fields, copied tables) is complete
         h = C.c_void_p()
         arr = (C.c_void_p * n)(*[e._h.value for e in self.engines])
-        _abi.check(L.lsfdtd_batch_create(arr, n, (C.c_int64 * n)(*last), C.byref(h)), "lsfdtd_batch_create")
+        _abi.check(L.lsfdtd_batch_create_shaped(arr, n, (C.c_int64 * n)(*last), int(cluster_ctas), int(max_clusters),
+                                                C.byref(h)), "lsfdtd_batch_create_shaped")
         self._h = h
         nbytes = C.c_size_t()
         _abi.check(L.lsfdtd_batch_scratch_bytes(h, C.byref(nbytes)), "lsfdtd_batch_scratch_bytes")
@@ -68,6 +70,20 @@ class BlochBatch:
         if launches:
             self.run(steps_per_launch, launches, use_graph)
         return launches
+
+    def diverged(self) -> list[int]:
+        """Indices of the runs whose fields turned non-finite (each retired after that step; its device step
+        counter ``Engine.n`` holds the steps it ran). Synchronises."""
+        import torch
+
+        torch.cuda.synchronize(self.dev)
+        out = []
+        for i, e in enumerate(self.engines):
+            st = C.c_int32()
+            _abi.lib().lsfdtd_engine_status(e._h, e.stream.cuda_stream, C.byref(st))
+            if st.value == 2:
+                out.append(i)
+        return out
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

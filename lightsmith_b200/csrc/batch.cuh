@@ -16,7 +16,13 @@
 //            start of the next H update instead, so after a launch's last step they are left as they were
 //            and refreshed when the run enters its next launch: between launches an engine's arrays are,
 //            ghosts included, what its own steps would have left;
+//   gather:  the conformal off-diagonal terms of E (k_offdiag's rows, one thread per target), the targets'
+//            high ghosts written through;
 //   sample:  every dft_stride steps, the running DFT of each monitor point (k_monitor's arithmetic).
+//
+// A run whose E turns non-finite in a step (a diverging run, as lightsmith's run loop would report it,
+// setup.py:749-756) sets its engine's status word and retires after that step: its step counter records the
+// steps it ran and later launches skip it, so it no longer holds its cluster.
 //
 // The cluster's hardware barrier (barrier.cluster, release / acquire) separates the phases; nothing else is
 // shared between threads. Every CTA of a cluster walks the same run list and step counts, so each reaches
@@ -31,8 +37,9 @@
 namespace lsfdtd {
 
 constexpr int kBatchMaxMon = 4;
+constexpr int kBatchNonFinite = 2;  // status word value of a run whose fields turned non-finite (it retires)
 constexpr int kBatchThreads = 512;
-constexpr int kBatchCluster = 8;  // CTAs per run (the portable cluster size)
+constexpr int kBatchCluster = 8;  // CTAs per run by default (the portable cluster size); 2 to 16 at launch
 
 // every thread of every CTA of the cluster arrives; global writes before it are visible after it
 __device__ __forceinline__ void cluster_barrier() {
@@ -74,6 +81,14 @@ struct BlochRun {
   int stride;
   long long last;  // the run's final step count
   long long* nstep;  // the engine's step counter (steps completed)
+  int* status;       // the engine's status word: set to kBatchNonFinite when the run's E turns non-finite
+  // conformal off-diagonal 1/eps terms (k_offdiag's tables): row q adds sum_k od_w[q, k] H_flat[od_h[q, k]] to
+  // E_flat[od_e[q]] after the E update
+  const long long* od_e;
+  const long long* od_h;
+  const F* od_w;
+  long long od_n;
+  int od_width;
   int n_mon;
   MonArgs<F> mon[kBatchMaxMon];
   UDiv div_n2, div_ny;  // by the nodes along z and the real cells along y
@@ -120,14 +135,18 @@ __device__ __forceinline__ void batch_sample_point(const MonArgs<F>& m, long lon
 }
 
 // complex64: two CTAs per SM (64 registers per thread), for twice the nodes in flight
+// launched with a cluster dimension (CTAs per run) set at launch: the CTA's rank in its cluster, the
+// cluster's index in the grid and its size come from the special registers
 template <typename F>
-__global__ void __cluster_dims__(kBatchCluster, 1, 1)
-    __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
+__global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     k_bloch_batch(const BlochRun<F>* runs, const int* order, const int* first, int steps) {
   using R = typename real_of<F>::type;
   __shared__ BlochRun<F> r;
-  const unsigned cl = blockIdx.x / kBatchCluster, rank = blockIdx.x % kBatchCluster;
-  const unsigned t0 = rank * blockDim.x + threadIdx.x, tstride = kBatchCluster * blockDim.x;
+  unsigned cl, rank, ncta;
+  asm("mov.u32 %0, %%clusterid.x;" : "=r"(cl));
+  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+  asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+  const unsigned t0 = rank * blockDim.x + threadIdx.x, tstride = ncta * blockDim.x;
   for (int q = first[cl]; q < first[cl + 1]; ++q) {
     // the run's descriptor into each CTA's shared memory (read by every thread at every node)
     {
@@ -145,7 +164,9 @@ __global__ void __cluster_dims__(kBatchCluster, 1, 1)
     const long long cs1 = n2, cs0 = 3LL * n2;
     const long long ccol = 4LL * n2;  // flat index of the column node (1, 1, 0)
     long long n = *r.nstep;
-    const long long n_end = min(n + (long long)steps, r.last);
+    // a run that turned non-finite in an earlier launch is skipped (the word was written before this launch)
+    long long n_end = *reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite ? n : min(n + (long long)steps, r.last);
+    bool bad = false;  // this thread's E values of the run: any non-finite
     cluster_barrier();  // every thread has read the counter
     if (n < n_end) {
       // E's high ghosts as lightsmith refreshes them before each H update (x = n0 - 1 from x = 1, then
@@ -325,6 +346,7 @@ __global__ void __cluster_dims__(kBatchCluster, 1, 1)
               e += psi;
             }
             if (plane && c < 2) e = c == 0 ? e + r.cE * inc[0] : e - r.cE * inc[1];  // correct_E
+            bad |= !(isfinite(e.re) && isfinite(e.im));
             g.E[c][p] = e;
             // high ghosts (x = n0 - 1 from x = 1, then y = n1 - 1 from y = 1, and the corner)
             if (!through) continue;
@@ -354,7 +376,36 @@ __global__ void __cluster_dims__(kBatchCluster, 1, 1)
           }
         }
       }
+      if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(r.status, kBatchNonFinite);
       cluster_barrier();
+      if (*reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite) {  // every CTA reads it after the barrier
+        n_end = n + 1;
+        break;
+      }
+      // ---- the conformal off-diagonal gather (after the whole E update, as lightsmith adds it) ----
+      if (r.od_n > 0) {
+        const long long cells = (long long)n0 * s0;
+        for (long long q = t0; q < r.od_n; q += tstride) {
+          const long long tt = r.od_e[q];
+          F acc = zero<F>();
+          for (int kk = 0; kk < r.od_width; ++kk)
+            acc = acc + r.od_w[q * r.od_width + kk] * g.H[0][r.od_h[q * r.od_width + kk]];
+          const F e = g.E[0][tt] + acc;
+          g.E[0][tt] = e;
+          if (!through) continue;
+          const int c = (int)(tt / cells);
+          const long long rem = tt - c * cells;
+          const int x = (int)(rem / s0), y = (int)((rem / s1) % n1);
+          const long long z = rem % s1;
+          if (x == 1) {
+            const F gx = e * r.gph[0][1];
+            g.E[c][(long long)(n0 - 1) * s0 + y * s1 + z] = gx;
+            if (y == 1) g.E[c][(long long)(n0 - 1) * s0 + (long long)(n1 - 1) * s1 + z] = gx * r.gph[1][1];
+          }
+          if (y == 1) g.E[c][x * s0 + (long long)(n1 - 1) * s1 + z] = e * r.gph[1][1];
+        }
+        cluster_barrier();
+      }
       // ---- DFT sample after every dft_stride steps ----
       if ((n + 1) % r.stride == 0) {
         for (int m = 0; m < r.n_mon; ++m) {

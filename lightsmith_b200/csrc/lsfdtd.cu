@@ -133,6 +133,8 @@ struct lsfdtd_engine {
   virtual int add_offdiag(const lsfdtd_offdiag_desc* d) = 0;
   virtual int add_tensor(const lsfdtd_tensor_desc* d) = 0;
   virtual int add_table(const lsfdtd_table_source_desc* s) = 0;
+  virtual int set_table_boxes(int table, int n, const int32_t* boxes, const int64_t* perm, int64_t n_entries,
+                              void* vals) = 0;
   virtual int add_dipole(const lsfdtd_dipole_desc* s) = 0;
   virtual int add_line(const lsfdtd_line_source_desc* s) = 0;
   virtual int add_column(const lsfdtd_column_source_desc* s) = 0;
@@ -174,6 +176,12 @@ struct Engine final : lsfdtd_engine {
   struct Table {
     TableArgs<R> corr[2];
     bool has[2];
+    long long n_entries[2];
+    // the H corrections' slab boxes for the fused pass (hc.n = 0: not given), the CSR position of each
+    // slab-order entry and the step's values in slab order
+    HCorr hc;
+    const long long* hperm;
+    R* hvals;
     const R* Tinc;
     const long long *inc_base, *inc_i0;
     const R* inc_u0;
@@ -259,15 +267,24 @@ struct Engine final : lsfdtd_engine {
   F* Eflat() const { return Ebuf[cur]; }
   F* Hflat() const { return Hbuf[cur]; }
 
-  // the fused single pass needs the second buffers, no periodic axis and sources that only correct E
+  // the fused single pass needs the second buffers, no periodic axis and sources that only correct E, or
+  // table-fed TF/SF sources whose H corrections the lean pass applies as it steps (one at most, boxes given)
   int decide() override {
     if (fused >= 0) return fused;
     fused = 0;
     if (kComplex || !Ebuf[1] || !Hbuf[1]) return 0;  // Bloch fields come with periodic axes
     for (int a = 0; a < 3; ++a)
       if (desc.periodic[a] || desc.mirror[a]) return 0;  // the fused pass's region tests know neither
-    for (auto& o : order)
+    int h_tables = 0;
+    for (auto& o : order) {
+      if (o.first == kTable) {
+        const Table& t = tables[o.second];
+        if (!t.has[1]) continue;
+        if (t.hc.n == 0 || variant != 4 || ++h_tables > 1) return 0;
+        continue;
+      }
       if (o.first != kDipole) return 0;
+    }
     for (int d = 0; d < 3; ++d) {
       if (!y.pml[d].on) continue;
       for (int c = 0; c < 3; ++c)
@@ -275,10 +292,11 @@ struct Engine final : lsfdtd_engine {
           if (y.pml[d].len[1][c][sd] > 0 && !psiH[1][d][c][sd]) return 0;
     }
     tma_ok = use_tma && make_maps() == LSFDTD_OK;
-    // rows the copies cannot take (not a multiple of 16 bytes): the cp.async ring of the fused pass runs
-    // slower than the in-place kernels (measured on B200, CPML 12: 607 against 296 us per step at 214^3, 226
-    // against 74 us at 129^3), so the default steps in place there; an explicit kernel choice or copy engine
-    // keeps the fused pass
+    // rows the tensor copies cannot take (not a multiple of 16 bytes): both fused passes then fill their rings
+    // with cp.async copies, which run slower than the in-place kernels (measured on B200, CPML 12: the generic
+    // pass 607 against 296 us per step at 214^3, 226 against 74 us at 129^3; the lean pass 224 against 73 us
+    // on the 129^3 sphere, issue-bound on its copies), so the default steps in place there; an explicit kernel
+    // choice keeps the fused pass
     if (use_tma && !tma_ok && !tuned) return 0;
     fused = 1;
     return 1;
@@ -301,24 +319,37 @@ struct Engine final : lsfdtd_engine {
     }
     return LSFDTD_OK;
   }
-  template <int TY, int S, bool UNI>
+  template <int TY, int S, bool UNI, bool ASYNC, bool HC>
   int launch_pml_one(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
       constexpr size_t sm = fused_pml_smem_bytes<F, TY, S>();
       static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
       if (!attr) {
-        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sm));
+        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI, ASYNC, HC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         attr = true;
       }
-      k_fused_pml<F, TY, S, UNI><<<grid, dim3(32, TY), sm, s>>>(ta);
+      k_fused_pml<F, TY, S, UNI, ASYNC, HC><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
   }
-  // the lean-CPML pass, one instantiation per cell shape (cubic or not)
+  // the lean-CPML pass, one instantiation per cell shape (cubic or not), copy engine (cp.async: rows the
+  // tensor copies cannot stride) and whether a table-fed source's H corrections are added as it steps (those
+  // two with a ring of 4 only)
+  template <int TY, int S, bool ASYNC, bool HC>
+  int launch_pml_kind(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+    return y.uniform ? launch_pml_one<TY, S, true, ASYNC, HC>(grid, ta, s)
+                     : launch_pml_one<TY, S, false, ASYNC, HC>(grid, ta, s);
+  }
   template <int TY, int S>
   int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
-    return y.uniform ? launch_pml_one<TY, S, true>(grid, ta, s) : launch_pml_one<TY, S, false>(grid, ta, s);
+    if (ta.f.hc.n > 0) return launch_pml_kind<TY, 4, false, true>(grid, ta, s);
+    return launch_pml_kind<TY, S, false, false>(grid, ta, s);
+  }
+  template <int TY>
+  int launch_pml_async(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
+    return ta.f.hc.n > 0 ? launch_pml_kind<TY, 4, true, true>(grid, ta, s)
+                         : launch_pml_kind<TY, 4, true, false>(grid, ta, s);
   }
   // kind 0: the fused pass over the grid, 1: over the interior box of the split step, 2: with lean CPML terms
   template <int TY, int S>
@@ -334,7 +365,7 @@ struct Engine final : lsfdtd_engine {
   // the lean-CPML pass needs its copies by the Tensor Memory Accelerator and, per axis, CPML slabs that do
   // not overlap
   bool lean_ok() const {
-    if (variant != 4 || !tma_ok) return false;
+    if (variant != 4 || kComplex) return false;
     for (int d = 0; d < 3; ++d) {
       if (!y.pml[d].on) continue;
       for (int f = 0; f < 2; ++f) {
@@ -431,6 +462,14 @@ struct Engine final : lsfdtd_engine {
     const long long cells = (long long)desc.shape[0] * desc.shape[1] * desc.shape[2];
     FusedArgs<F> fa;
     fa.y = y;
+    fa.hc.n = 0;
+    fa.hc.vals = nullptr;
+    for (auto& tb : tables) {  // a table-fed source's H corrections for this step, added by the lean pass
+      if (!tb.has[1] || tb.hc.n == 0) continue;
+      k_table_values<R><<<cdiv(tb.n_entries[1], 256), 256, 0, s>>>(tb.corr[1], tb.hperm, tb.n_entries[1], tb.hvals);
+      LS_LAUNCHED();
+      fa.hc = tb.hc;
+    }
     const int o = cur ^ 1;
     for (int a = 0; a < 3; ++a) {
       fa.y.E[a] = Ebuf[cur] + a * cells;
@@ -466,7 +505,14 @@ struct Engine final : lsfdtd_engine {
     grid.z = (unsigned)cdiv(nx, fa.seg);
     LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
-      if (tma_ok) {
+      if (!tma_ok && kind == 2) {  // the lean pass with cp.async copies
+        TmaArgs<F> ta;
+        ta.f = fa;
+        ta.status = static_cast<int*>(scratch);
+        ta.wait_budget = wait_budget;
+        const int r = tile_y == 16 ? launch_pml_async<16>(grid, ta, s) : launch_pml_async<8>(grid, ta, s);
+        if (r != LSFDTD_OK) return r;
+      } else if (tma_ok) {
         TmaArgs<F> ta;
         ta.f = fa;
         for (int c = 0; c < 3; ++c) {
@@ -560,7 +606,6 @@ struct Engine final : lsfdtd_engine {
       if (!desc.periodic[0] || !desc.periodic[1] || desc.periodic[2])
         return fail(LSFDTD_EUNSUPPORTED, "batch: a run must be periodic along x and y, not z");
       if (desc.mirror[2]) return fail(LSFDTD_EUNSUPPORTED, "batch: no mirror plane");
-      if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "batch: no conformal off-diagonal terms");
       if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "batch: no vertex-tensor mesh");
       if (y.pml[0].on || y.pml[1].on) return fail(LSFDTD_EUNSUPPORTED, "batch: CPML along z only");
       if (!groups.empty()) return fail(LSFDTD_EUNSUPPORTED, "batch: dispersive groups have no batched path");
@@ -597,6 +642,13 @@ struct Engine final : lsfdtd_engine {
       r.stride = desc.dft_stride;
       r.last = last;
       r.nstep = reinterpret_cast<long long*>(desc.step);
+      r.status = static_cast<int*>(scratch);
+      r.od_e = od_e;
+      r.od_h = od_h;
+      r.od_w = od_w;
+      r.od_n = od_n;
+      r.od_width = od_width;
+      if (!r.status) return fail(LSFDTD_EINVAL, "batch: the engine's scratch (its status word) is not set");
       r.div_n2 = udiv_make((unsigned)desc.shape[2]);
       r.div_ny = udiv_make((unsigned)(desc.shape[1] - 2));
       r.n_mon = (int)monitors.size();
@@ -855,7 +907,12 @@ struct Engine final : lsfdtd_engine {
       a.coef = static_cast<const R*>(s->coef[k]);
       a.target = nullptr;  // the current E (k = 0) or H buffer, set at launch
       a.nstep = reinterpret_cast<const long long*>(desc.step);
+      t.n_entries[k] = t.has[k] ? s->pts[k].n_entries : 0;
     }
+    t.hc.n = 0;
+    t.hc.vals = nullptr;
+    t.hperm = nullptr;
+    t.hvals = nullptr;
     t.Tinc = static_cast<const R*>(s->inc_table);
     t.inc_base = reinterpret_cast<const long long*>(s->inc_base);
     t.inc_i0 = reinterpret_cast<const long long*>(s->inc_i0);
@@ -863,6 +920,48 @@ struct Engine final : lsfdtd_engine {
     t.view = static_cast<R*>(s->view);
     order.push_back({kTable, tables.size()});
     tables.push_back(t);
+    return LSFDTD_OK;
+  }
+
+  int set_table_boxes(int table, int n, const int32_t* boxes, const int64_t* perm, int64_t n_entries,
+                      void* vals) override {
+    if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "table-fed sources need real fields");
+    if (table < 0 || table >= (int)tables.size()) return fail(LSFDTD_EINVAL, "table boxes: no such table source");
+    Table& t = tables[table];
+    if (!t.has[1] || n_entries != t.n_entries[1])
+      return fail(LSFDTD_EINVAL, "table boxes: the entry count differs from the source's H corrections");
+    if (n < 1 || n > kMaxHBoxes || !boxes || !perm || !vals)
+      return fail(LSFDTD_EINVAL, "table boxes: 1 to 24 boxes, a permutation and a value array");
+    HCorr hc{};
+    hc.n = n;
+    long long total = 0;
+    for (int b = 0; b < n; ++b) {
+      const int32_t* q = boxes + 8 * b;
+      HCorrBox& x = hc.box[b];
+      x.c = q[0];
+      long long vol = 1;
+      for (int a = 0; a < 3; ++a) {
+        x.lo[a] = q[1 + a];
+        x.hi[a] = q[4 + a];
+        if (x.lo[a] < 0 || x.hi[a] > desc.shape[a] || x.hi[a] <= x.lo[a])
+          return fail(LSFDTD_ERANGE, "table boxes: a box outside the grid or empty");
+        vol *= x.hi[a] - x.lo[a];
+      }
+      x.off = q[7];
+      if (x.c < 0 || x.c > 2 || x.off < 0 || x.off + vol > n_entries)
+        return fail(LSFDTD_ERANGE, "table boxes: a component or an entry offset out of range");
+      total += vol;
+    }
+    if (total != n_entries) return fail(LSFDTD_EINVAL, "table boxes: the boxes do not cover the entries once");
+    // the permutation indexes the CSR entries: checked once here, on the host
+    std::vector<long long> h(n_entries);
+    LS_CUDA(cudaMemcpy(h.data(), perm, n_entries * sizeof(long long), cudaMemcpyDeviceToHost));
+    for (long long v : h)
+      if (v < 0 || v >= n_entries) return fail(LSFDTD_ERANGE, "table boxes: a permutation entry out of range");
+    hc.vals = vals;
+    t.hc = hc;
+    t.hperm = reinterpret_cast<const long long*>(perm);
+    t.hvals = static_cast<R*>(vals);
     return LSFDTD_OK;
   }
 
@@ -1292,6 +1391,7 @@ struct Engine final : lsfdtd_engine {
     for (auto& g : groups) per_step += g.n > 0;
     for (auto& o : order) {
       switch (o.first) {
+        // (on the fused pass the H corrections are k_table_values before it, in place of k_table_correct)
         case kTable: per_step += tables[o.second].has[0] + tables[o.second].has[1] + (tables[o.second].view ? 1 : 0); break;
         case kDipole: per_step += 1; break;
         case kLine: per_step += lines[o.second].has[0] + lines[o.second].has[1] + 2; break;
@@ -1314,6 +1414,7 @@ struct BatchImpl {
   std::vector<unsigned char> descs;  // n * run_bytes
   std::vector<int> order, first;     // runs of CTA b: order[first[b] .. first[b + 1])
   int ctas = 0;
+  int cluster = kBatchCluster;  // CTAs per run (cluster size)
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
   size_t off_order = 0, off_first = 0, need = 0;
@@ -1322,15 +1423,17 @@ struct BatchImpl {
   int graph_steps = -1;
 };
 
-// clusters of the persistent kernel that fit on the device at once
+// clusters of `cl` CTAs of the persistent kernel that fit on the device at once (clusters above the
+// portable 8 CTAs are allowed on the kernel first)
 template <typename F>
-int batch_max_clusters(int* out) {
+int batch_max_clusters(int cl, int* out) {
+  if (cl > 8) LS_CUDA(cudaFuncSetAttribute(k_bloch_batch<F>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kBatchCluster, 1, 1);
+  cfg.gridDim = dim3(cl, 1, 1);
   cfg.blockDim = dim3(kBatchThreads, 1, 1);
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kBatchCluster;
+  attr[0].val.clusterDim.x = cl;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
@@ -1346,7 +1449,18 @@ int batch_launch(const BatchImpl& b, int steps, cudaStream_t s) {
   const auto* runs = static_cast<const BlochRun<F>*>(b.scratch);
   const int* order = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_order);
   const int* first = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_first);
-  k_bloch_batch<F><<<b.ctas, kBatchThreads, 0, s>>>(runs, order, first, steps);  // whole clusters
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(b.ctas, 1, 1);  // whole clusters
+  cfg.blockDim = dim3(kBatchThreads, 1, 1);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = b.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LS_CUDA(cudaLaunchKernelEx(&cfg, k_bloch_batch<F>, runs, order, first, steps));
   LS_LAUNCHED();
   return LSFDTD_OK;
 }
@@ -1701,6 +1815,7 @@ int32_t lsfdtd_engine_status(lsfdtd_engine* eng, void* stream, int32_t* status) 
   LS_CUDA(cudaMemcpyAsync(&v, eng->scratch, sizeof(v), cudaMemcpyDeviceToHost, s));
   LS_CUDA(cudaStreamSynchronize(s));
   *status = v;
+  if (v == lsfdtd::kBatchNonFinite) return fail(LSFDTD_ENONFINITE, "the run's fields turned non-finite in a batched launch");
   if (v) return fail(LSFDTD_ETIMEOUT, "a kernel gave up waiting for its copies (status word set)");
   return LSFDTD_OK;
 }
@@ -1716,8 +1831,15 @@ int32_t lsfdtd_engine_set_wait_budget(lsfdtd_engine* eng, int64_t cycles) {
   LS_NEED(eng);
   if (eng->exec[0] || eng->exec[1])
     return fail(LSFDTD_EINVAL, "the wait budget must be set before the first graph capture");
-  eng->wait_budget = cycles > 0 ? (long long)cycles : lsfdtd::kWaitBudget;
+  eng->wait_budget = cycles != 0 ? (long long)cycles : lsfdtd::kWaitBudget;
   return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_set_table_boxes(lsfdtd_engine* eng, int32_t table, int32_t n_boxes, const int32_t* boxes,
+                                      const int64_t* perm, int64_t n_entries, void* vals) {
+  LS_NEED(eng);
+  if (eng->fused >= 0) return fail(LSFDTD_EINVAL, "table boxes must be given before the first step");
+  return eng->set_table_boxes(table, n_boxes, boxes, perm, n_entries, vals);
 }
 
 int32_t lsfdtd_engine_set_copy_engine(lsfdtd_engine* eng, int32_t use_tma) {
@@ -1757,7 +1879,14 @@ int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng) { return eng ? eng->n_host
 int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng) { return eng ? eng->launches_per_chunk() : -1; }
 
 int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out) {
+  return lsfdtd_batch_create_shaped(engines, n, last, kBatchCluster, 0, out);
+}
+
+int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, const int64_t* last,
+                                   int32_t cluster_ctas, int32_t max_clusters, lsfdtd_batch** out) {
   LS_NEED(engines && last && out && n > 0);
+  if (cluster_ctas < 1 || cluster_ctas > 16 || max_clusters < 0)
+    return fail(LSFDTD_EINVAL, "batch: 1 to 16 CTAs per cluster, a non-negative cluster limit");
   *out = nullptr;
   auto b = std::make_unique<lsfdtd_batch>();
   b->precision = engines[0] ? engines[0]->desc.precision : LSFDTD_F32;
@@ -1776,10 +1905,12 @@ int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int6
   }
   // one wave of clusters; the runs longest first, each to the cluster with the least work so far
   int clusters = 0;
-  LS_TRY(b->precision == LSFDTD_F32 ? batch_max_clusters<cplx<float>>(&clusters)
-                                    : batch_max_clusters<cplx<double>>(&clusters));
+  LS_TRY(b->precision == LSFDTD_F32 ? batch_max_clusters<cplx<float>>(cluster_ctas, &clusters)
+                                    : batch_max_clusters<cplx<double>>(cluster_ctas, &clusters));
   clusters = std::max(1, std::min<int>(n, clusters));
-  b->ctas = clusters * kBatchCluster;
+  if (max_clusters > 0) clusters = std::min(clusters, (int)max_clusters);
+  b->cluster = cluster_ctas;
+  b->ctas = clusters * cluster_ctas;
   for (int32_t i = 0; i < n; ++i) {
     const auto& d = b->engines[i]->desc;
     if ((double)(d.shape[0] - 2) * (d.shape[1] - 2) * d.shape[2] + d.shape[2] >= 4294967296.0)

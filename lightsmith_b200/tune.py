@@ -7,6 +7,7 @@ the engine on the fastest. ``best_shape`` caches the choice per GPU model and gr
 
     python -m lightsmith_b200.tune --n 640                  # sweep the throughput case, print the best
     python -m lightsmith_b200.tune --n 384 --shape 3,8,32,4   # one shape (e.g. under ncu)
+    python -m lightsmith_b200.tune --plan run.npz --shape 4,8,0,4  # a recorded plan (lightsmith_b200.plan.save)
 """
 
 from __future__ import annotations
@@ -77,6 +78,38 @@ def best_shape(eng, candidates=CANDIDATES, path: str | None = None):
     return best
 
 
+BATCH_SHAPES = [(8, 0), (4, 0), (16, 0)]  # (CTAs per run, clusters in flight; 0: as many as fit)
+
+
+def tune_batch(engines, last, shapes=BATCH_SHAPES, steps: int = 30, launches: int = 2):
+    """Time the batched kernel's launch shapes on ``engines`` (which advance: tune on runs made for it) and
+    return (best shape, {shape: Gcell-updates/s})."""
+    import numpy as np
+    import torch
+
+    from .batch import BlochBatch
+
+    cells = [int(np.prod(e.shape)) for e in engines]
+    res = {}
+    for cl, mx in shapes:
+        try:
+            b = BlochBatch(engines, last, cluster_ctas=cl, max_clusters=mx)
+        except Exception:  # noqa: BLE001 (a shape the device cannot launch)
+            continue
+        b.run(steps, 1)  # capture
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        before = [e.n_host for e in engines]
+        t0.record(b.stream)
+        b.run(steps, launches)
+        t1.record(b.stream)
+        torch.cuda.synchronize()
+        moved = sum(c * (e.n_host - n) for c, e, n in zip(cells, engines, before))
+        res[(cl, mx)] = moved / max(t0.elapsed_time(t1), 1e-9) / 1e6
+        b.close()
+    best = max(res, key=res.get) if res else (8, 0)
+    return best, res
+
+
 def _main():
     import torch
 
@@ -89,20 +122,29 @@ def _main():
     ap.add_argument("--chunks", type=int, default=2)
     ap.add_argument("--cp-async", action="store_true", help="copy planes with cp.async instead of TMA")
     ap.add_argument("--pml", type=int, default=16, help="CPML cells on every face")
+    ap.add_argument("--plan", default=None, help="a plan saved with lightsmith_b200.plan.save, run in FP32")
     args = ap.parse_args()
-    n = args.n
-    inv = 1.0 / (torch.rand((n, n, n), device="cuda", dtype=torch.float32) * 11.25 + 1.0)
-    plan = throughput_plan(n, inv_eps=inv, max_steps=31 * 200, pml=args.pml)
-    del inv
-    eng = Engine.from_plan(plan)
+    if args.plan:
+        from .plan import load
+
+        d = load(args.plan)
+        plan = d.get("plan", d)
+        eng = Engine.from_plan(plan, precision="single")
+    else:
+        n = args.n
+        inv = 1.0 / (torch.rand((n, n, n), device="cuda", dtype=torch.float32) * 11.25 + 1.0)
+        plan = throughput_plan(n, inv_eps=inv, max_steps=31 * 200, pml=args.pml)
+        del inv
+        eng = Engine.from_plan(plan)
     if args.cp_async:
         eng.set_copy_engine(False)
-    alg = n ** 3 * 52 + cells_in_cpml(eng.plan) * 32
+    cells = eng.cells
+    alg = cells * 52 + cells_in_cpml(eng.plan) * 32
     shapes = [tuple(int(v) for v in args.shape.split(","))] if args.shape else CANDIDATES
     for sh in shapes:
         ms = time_shape(eng, sh, args.chunks)
-        print(json.dumps({"shape": sh, "tma": eng.uses_tma, "ms_per_step": ms, "Gcell_s": n ** 3 / ms / 1e6,
-                          "alg_GBps": alg / ms / 1e6}), flush=True)
+        print(json.dumps({"shape": sh, "fused": eng.fused, "tma": eng.uses_tma, "ms_per_step": ms,
+                          "Gcell_s": cells / ms / 1e6, "alg_GBps": alg / ms / 1e6}), flush=True)
     eng.close()
 
 

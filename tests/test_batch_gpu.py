@@ -122,3 +122,40 @@ def test_batch_rejects_runs_it_cannot_batch(golden):
         BlochBatch([col], 10 ** 7)
     eng.close()
     col.close()
+
+
+def test_a_run_turning_non_finite_retires_alone():
+    """A NaN written from the host into one run's E between launches: that run's status word reports it and it
+    stops stepping, while the other runs of the batch finish with the values of a batch without the NaN."""
+    import torch
+
+    from lightsmith_b200 import _abi
+    from lightsmith_b200.batch import BlochBatch
+    from lightsmith_b200.engine import Engine
+
+    plans = _small_runs("double", n=3, steps=240)
+    last = [p["stride"] * (240 // p["stride"]) for p in plans]
+    ref = [Engine.from_plan(p) for p in plans]
+    b_ref = BlochBatch(ref, last)
+    b_ref.run_to_end(steps_per_launch=30)
+    engs = [Engine.from_plan(p) for p in plans]
+    batch = BlochBatch(engs, last)
+    batch.run(30, 2)
+    torch.cuda.synchronize()
+    n0, n1, n2 = engs[1].shape
+    node = ((1 * n0 + n0 // 2) * n1 + n1 // 2) * n2 + n2 // 2  # E_y at the middle node (ghost planes are never read)
+    engs[1].E_flat[node] = float("nan")
+    batch.run_to_end(steps_per_launch=30)
+    assert batch.diverged() == [1] and b_ref.diverged() == []
+    n1 = int(engs[1].n.item())
+    assert 60 < n1 < last[1], (n1, last[1])
+    with pytest.raises(_abi.LsfdtdError, match="non-finite"):
+        engs[1].check_status()
+    for i in (0, 2):
+        assert int(engs[i].n.item()) == last[i]
+        for k in range(len(engs[i].monitors)):
+            assert np.array_equal(engs[i].results(k)[0], ref[i].results(k)[0])
+    for x in (batch, b_ref):
+        x.close()
+    for e in engs + ref:
+        e.close()

@@ -196,3 +196,27 @@ def test_cancelled_progress_stops_the_solve_and_the_next_solve_runs(plugin, expe
     res = ls.solve(problem, "fdtd", "gpu")
     want = expected["sphere_staircase"]["result"]
     assert _rel(np.asarray(res.c_ext_nm2), want["c_ext_nm2"]) < 1e-9
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_periodic_oblique_runs_are_batched_and_match_runs_one_by_one(plugin, expected, precision):
+    """With a fixed run time, the periodic driver's oblique runs (one per wavelength here) advance together in
+    one persistent kernel; R, T and the orders equal those of the same solve with the runs made one after
+    another on the CUDA engine, and lightsmith's own CPU solve."""
+    B = plugin
+    problem = with_options(SOLVE_PROBLEMS["periodic_oblique"](), precision=precision)
+    res_b = ls.solve(problem, "fdtd", "gpu")
+    assert res_b.provenance.get("batched_oblique_runs") == 2
+    assert all(r.get("batched") for r in res_b.provenance["runs"])
+    with pytest.MonkeyPatch.context() as mp:
+        mp.setattr(B.B200FDTD, "batch_oblique", False)
+        res_s = ls.solve(problem, "fdtd", "gpu")
+    assert "batched_oblique_runs" not in res_s.provenance
+    got, seq, want = flatten_result(res_b), flatten_result(res_s), expected["periodic_oblique"]["result"]
+    assert sorted(got) == sorted(seq) == sorted(want)
+    for key in want:
+        assert _rel(got[key], seq[key]) < (1e-12 if precision == "double" else 1e-5), key
+        if precision == "double":
+            assert _rel(got[key], want[key]) < 1e-9, key
+        else:
+            _f32_check("periodic_oblique", key, got[key], want[key])
