@@ -22,6 +22,21 @@
 
 namespace lsfdtd {
 
+// TF/SF corrections of H applied inside the fused pass (a table-fed source's correct_H, layered.py:231-242):
+// box b adds vals[off + ((x - lo0) (hi1 - lo1) + (y - lo1)) (hi2 - lo2) + (z - lo2)] to H_c at the nodes
+// [lo, hi) of the box, boxes in the source's slab order; vals holds the step's values, one per entry
+constexpr int kMaxHBoxes = 24;
+struct HCorrBox {
+  int c;
+  int lo[3], hi[3];
+  int off;
+};
+struct HCorr {
+  int n;  // boxes (0: none)
+  HCorrBox box[kMaxHBoxes];
+  const void* vals;
+};
+
 template <typename F>
 struct FusedArgs {
   YeeArgs<F> y;        // in buffers (E, H, psi) and coefficients
@@ -35,6 +50,7 @@ struct FusedArgs {
   int pml_hi[3];
   int box_lo[3];       // the interior box of the split step: nodes [box_lo, box_hi) per axis, each of them and
   int box_hi[3];       // its low-side neighbours inside [inner_lo, inner_hi); box_lo[2] a multiple of four
+  HCorr hc;            // TF/SF corrections of H (the lean pass only)
 };
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {

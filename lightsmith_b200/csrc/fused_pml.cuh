@@ -102,8 +102,13 @@ __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabIn
 
 // FP32: four CTAs of 8 rows (two of 16) per SM, at most 64 registers per thread, which their shared memory
 // allows; FP64 tiles need twice the shared memory and are not constrained. UNI: cubic cells, so the curl
-// differences and CPML coefficients carry no per-axis spacing (one instantiation each way)
-template <typename F, int TY, int S, bool UNI>
+// differences and CPML coefficients carry no per-axis spacing (one instantiation each way).
+// ASYNC: the ring is filled by every thread with cp.async copies of whole rows (zero-filled outside the
+// grid), completing on the same mbarriers, for grids whose rows the tensor copies cannot stride (not a
+// multiple of 16 bytes). A table-fed TF/SF source's corrections of H (FusedArgs::hc) are added to every H
+// value the tile computes (its own nodes and its halo) before the E half uses them (HC: compiled in only for
+// runs that have such corrections).
+template <typename F, int TY, int S, bool UNI, bool ASYNC = false, bool HC = false>
 __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 1)
     k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
   using R = typename real_of<F>::type;
@@ -146,25 +151,71 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       tab.z[f][r - Tab::NY] = f ? slab_info<1>(g.pml[2], 2, z0 - 1 + r - Tab::NY)
                                 : slab_info<0>(g.pml[2], 2, z0 - 1 + r - Tab::NY);
   }
+  __shared__ unsigned long long never;  // a barrier nothing completes: the wait of a timeout test
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+    mbar_init(&never, 1);
+    for (int s = 0; s < S; ++s) mbar_init(&bar[s], ASYNC ? NT : 1);  // cp.async: every thread arrives
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
 
   auto produce = [&](int p) {
     const int s = (int)((unsigned)(p - xb) % S);  // p >= xb: unsigned, so the ring slot is a mask or a multiply
-    mbar_expect_tx(&bar[s], St::kTx);
-    for (int c = 0; c < 3; ++c) tma_load_3d(stE(s, c), &t.mE[c], z0 - 4, y0 - 1, p, &bar[s]);
-    for (int c = 0; c < 3; ++c) tma_load_3d(stH(s, c), &t.mH[c], z0 - 4, y0 - 1, p, &bar[s]);
-    tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
+    if constexpr (ASYNC) {
+      static_assert(sizeof(F) == sizeof(R), "the fused pass steps real fields");
+      // warp ty copies rows ty, ty + TY, ...: E (3 x (TY + 2) rows) and H (3 x (TY + 1) rows) of BZ values
+      // from z0 - 4, then the coefficient's TY rows of TZ values from z0; the tensor copies' layout
+      constexpr int kRE = TY + 2, kRH = TY + 1, kRows = 3 * kRE + 3 * kRH + TY;
+      const bool px = p < n0;
+#pragma unroll 1
+      for (int rr = ty; rr < kRows; rr += TY) {
+        const F* src;
+        F* dst;
+        int y, z, w;
+        if (rr < 3 * kRE) {
+          src = g.E[rr / kRE];
+          dst = stE(s, rr / kRE)[rr % kRE];
+          y = y0 - 1 + rr % kRE;
+          z = z0 - 4;
+          w = BZ;
+        } else if (rr < 3 * kRE + 3 * kRH) {
+          const int q = rr - 3 * kRE;
+          src = g.H[q / kRH];
+          dst = stH(s, q / kRH)[q % kRH];
+          y = y0 - 1 + q % kRH;
+          z = z0 - 4;
+          w = BZ;
+        } else {
+          const int row = rr - 3 * kRE - 3 * kRH;
+          src = reinterpret_cast<const F*>(g.cbE[0]);
+          dst = reinterpret_cast<F*>(stC(s)[row]);
+          y = y0 + row;
+          z = z0;
+          w = TZ;
+        }
+        const bool yin = px && y >= 0 && y < n1;
+        const long long base = ((long long)p * n1 + y) * n2;
+        for (int col = tx; col < w; col += 32) {
+          const int zz = z + col;
+          const bool v = yin && zz >= 0 && zz < n2;
+          cp_async(dst + col, v ? src + base + zz : src, v);
+        }
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&bar[s])) : "memory");
+    } else {
+      mbar_expect_tx(&bar[s], St::kTx);
+      for (int c = 0; c < 3; ++c) tma_load_3d(stE(s, c), &t.mE[c], z0 - 4, y0 - 1, p, &bar[s]);
+      for (int c = 0; c < 3; ++c) tma_load_3d(stH(s, c), &t.mH[c], z0 - 4, y0 - 1, p, &bar[s]);
+      tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
+    }
   };
   auto ready = [&](int p) -> bool {
     const unsigned r = (unsigned)(p - xb);
-    return mbar_wait_bounded(&bar[r % S], (r / S) & 1, kWaitBudget);
+    if (t.wait_budget < 0) return mbar_wait_bounded(&never, 0, -t.wait_budget);  // a timeout test: see TmaArgs
+    return mbar_wait_bounded(&bar[r % S], (r / S) & 1, t.wait_budget);
   };
   int issued = xb - 1;
-  if (tid == 0) {
+  if (ASYNC || tid == 0) {
     for (int p = xb; p < xb + S - 1; ++p) produce(p);
   }
   issued = xb + S - 2;
@@ -256,6 +307,23 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     yz_em |= (ey_ok && ez_ok ? 1u : 0u) << c;
   }
 
+  // the TF/SF correction boxes of H that meet the tile (rows y0 - 1 .. y0 + TY - 1, columns z0 - 1 .. z0 + 31)
+  unsigned tile_hc = 0;
+  for (int b = 0; HC && b < a.hc.n; ++b) {
+    const HCorrBox& q = a.hc.box[b];
+    if (q.lo[1] < y0 + TY && q.hi[1] > y0 - 1 && q.lo[2] < z0 + TZ && q.hi[2] > z0 - 1) tile_hc |= 1u << b;
+  }
+  // H_c at (x, y, z) plus the corrections of the boxes in pm that hold it, in box order
+  auto hcorr = [&](F h, int c, int x, int y, int z, unsigned pm) -> F {
+    for (; pm; pm &= pm - 1) {
+      const HCorrBox& q = a.hc.box[__ffs(pm) - 1];
+      if (q.c == c && y >= q.lo[1] && y < q.hi[1] && z >= q.lo[2] && z < q.hi[2])
+        h = h + static_cast<const F*>(a.hc.vals)[q.off + ((long long)(x - q.lo[0]) * (q.hi[1] - q.lo[1]) +
+                                                          (y - q.lo[1])) * (q.hi[2] - q.lo[2]) + (z - q.lo[2])];
+    }
+    return h;
+  };
+
   F prev_hy = zero<F>(), prev_hz = zero<F>();
   bool failed = false;
   int cons = xb - 1;
@@ -308,15 +376,25 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       break;
     }
     cons = i + 1;
-    if (tid == 0) produce(i + S - 1);
+    if (ASYNC || tid == 0) produce(i + S - 1);
     issued = i + S - 1;
     const int si = (int)((unsigned)(i - xb) % S), sn = (int)((unsigned)(i + 1 - xb) % S);
     const long long p = i * s0 + off_jk;
+    unsigned pm = 0;  // the correction boxes of H that hold nodes of this plane and tile
+    for (unsigned m = tile_hc; HC && m; m &= m - 1) {
+      const HCorrBox& q = a.hc.box[__ffs(m) - 1];
+      if (i >= q.lo[0] && i < q.hi[0]) pm |= m & (0u - m);
+    }
     F hx = zero<F>(), hy = zero<F>(), hz = zero<F>();
     if (fast) {
       hx = hx_fast(si, oo);
       hy = hy_fast(si, sn, oo);
       hz = hz_fast(si, sn, oo);
+      if (HC && pm) {
+        hx = hcorr(hx, 0, i, j, k, pm);
+        hy = hcorr(hy, 1, i, j, k, pm);
+        hz = hcorr(hz, 2, i, j, k, pm);
+      }
       if (i >= xs) {
         st_global(a.Ho[0] + p, hx);
         st_global(a.Ho[1] + p, hy);
@@ -352,6 +430,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
             pml_term<1, UNI>(h, g, zh, 2, c, qh[2], d1 == 2 ? av[c] : bv[c], g.cH, pre_h[c][2],
                         st ? a.psiHo[2][c][zh.side] : nullptr);
         }
+        if (HC && pm) h = hcorr(h, c, i, j, k, pm);
         if (st) st_global(a.Ho[c] + p, h);
         hv[c] = h;
       }
@@ -368,25 +447,39 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     hs[0][ty + 1][tx] = hx;
     hs[1][ty + 1][tx] = hz;
     if (ty == 0 && y0 > 0 && k < n2) {  // the halo row y0 - 1
+      F hxr, hzr;
       if (fast) {
-        hs[0][0][tx] = hx_fast(si, tx + 4);
-        hs[1][0][tx] = hz_fast(si, sn, tx + 4);
+        hxr = hx_fast(si, tx + 4);
+        hzr = hz_fast(si, sn, tx + 4);
       } else {
-        hs[0][0][tx] = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
-        hs[1][0][tx] = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
+        hxr = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
+        hzr = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
       }
+      if (HC && pm) {
+        hxr = hcorr(hxr, 0, i, y0 - 1, k, pm);
+        hzr = hcorr(hzr, 2, i, y0 - 1, k, pm);
+      }
+      hs[0][0][tx] = hxr;
+      hs[1][0][tx] = hzr;
     }
     // the halo column z0 - 1 (H_x, H_y of every row, for lane 0 of each warp): one warp, lane r for row r
     if (ty == kColWarp && tx < TY && z0 > 0 && y0 + tx < n1) {
+      F hxc, hyc;
       if (col_clean && i >= a.inner_lo[0] && i < a.inner_hi[0]) {
         const int o = (tx + 1) * BZ + 3;
-        zc[i & 1][0][tx] = hx_fast(si, o);
-        zc[i & 1][1][tx] = hy_fast(si, sn, o);
+        hxc = hx_fast(si, o);
+        hyc = hy_fast(si, sn, o);
       } else {
         SlabInfo<R> xc_h = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;  // this warp may be fast itself
-        zc[i & 1][0][tx] = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
-        zc[i & 1][1][tx] = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
+        hxc = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
+        hyc = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
       }
+      if (HC && pm) {
+        hxc = hcorr(hxc, 0, i, y0 + tx, z0 - 1, pm);
+        hyc = hcorr(hyc, 1, i, y0 + tx, z0 - 1, pm);
+      }
+      zc[i & 1][0][tx] = hxc;
+      zc[i & 1][1][tx] = hyc;
     }
     F hx_zm = shfl_up(full, hx), hy_zm = shfl_up(full, hy);
     __syncthreads();
@@ -446,6 +539,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       mbar_wait_bounded(&bar[(unsigned)(p - xb) % S], ((unsigned)(p - xb) / S) & 1, kDrainBudget);
     if (failed && t.status) atomicExch(t.status, 1);
   }
+  if constexpr (ASYNC) asm volatile("cp.async.wait_all;\n" ::: "memory");  // every thread's own copies landed
   __syncthreads();
 }
 

@@ -32,7 +32,10 @@ struct TmaArgs {
   CUtensorMap mH[3];   // H^n components, box 40 x (TY + 1) x 1
   CUtensorMap mC;      // cbE (component 0), box 32 x TY x 1
   int* status;         // set to 1 when a copy wait exceeded its budget
-  long long wait_budget;  // clock cycles a CTA waits for one plane's copies before it gives up
+  // clock cycles a CTA waits for one plane's copies before it gives up; negative: a timeout test, in which
+  // every wait is on a barrier that nothing completes and gives up after -wait_budget cycles (the copies the
+  // pass issued still complete, and it drains them before it returns)
+  long long wait_budget;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -163,7 +166,9 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
   };
   auto stC = [&](int s) { return reinterpret_cast<R(*)[TZ]>(smem + s * St::kBytes + 3 * St::kE + 3 * St::kH); };
 
+  __shared__ unsigned long long never;  // a barrier nothing completes: the wait of a timeout test
   if (tid == 0) {
+    mbar_init(&never, 1);
     for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -178,6 +183,7 @@ __global__ void __launch_bounds__(32 * TY) k_fused_tma(const __grid_constant__ T
     tma_load_3d(stC(s), &t.mC, z0, y0, p, &bar[s]);
   };
   auto ready = [&](int p) -> bool {
+    if (t.wait_budget < 0) return mbar_wait_bounded(&never, 0, -t.wait_budget);  // a timeout test: see TmaArgs
     return mbar_wait_bounded(&bar[(p - xb) % S], ((p - xb) / S) & 1, t.wait_budget);
   };
   int issued = xb - 1;  // last plane whose copies were issued

@@ -69,6 +69,16 @@ __global__ void k_table_correct(TableArgs<R> a) {
   a.target[node] = v;
 }
 
+// the step's correction values of one kind in the source's slab order, for the fused pass to add as it steps
+// (k_table_correct adds them node by node instead): vals[e] = coef * T(n) of the entry at CSR position perm[e]
+template <typename R>
+__global__ void k_table_values(TableArgs<R> a, const long long* perm, long long n_entries, R* vals) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_entries) return;
+  const long long q = perm[e];
+  vals[e] = a.coef[q] * table_read(a.T, *a.nstep, a.i0[q], a.u0[q], a.base[q], a.m, a.cmax);
+}
+
 // the incident-reference view: E_inc (3 components) at the end of the step
 template <typename R>
 __global__ void k_table_view(const R* Tinc, int m, long long cmax, const long long* base, const long long* i0,

@@ -97,9 +97,11 @@ class Engine:
             # the fused single-pass step alternates between two field buffers; it serves runs without periodic
             # axes whose sources only correct E (point dipoles)
             self.mirror = tuple(int(m) for m in plan.get("mirror", (0, 0, 0)))
+            # (table-fed TF/SF sources too: the lean pass adds their H corrections as it steps)
             self.double_buffered = (fused is not False and not any(self.periodic) and not self.complex and
                                     not any(self.mirror) and
-                                    all(isinstance(s, DipoleSource) for s in plan["sources"]))
+                                    all(isinstance(s, (DipoleSource, TableSource)) for s in plan["sources"]) and
+                                    sum(isinstance(s, TableSource) for s in plan["sources"]) <= 1)
             if self.double_buffered:
                 self._E.append(torch.zeros_like(self._E[0]))
                 self._H.append(torch.zeros_like(self._H[0]))
@@ -309,7 +311,7 @@ class Engine:
         torch = _torch()
         nodes, offsets, order = _csr(pts.node)
         out = {"nodes": self._dev(nodes, torch.int64), "offsets": self._dev(offsets, torch.int64),
-               "n_nodes": len(nodes), "n_entries": len(order)}
+               "n_nodes": len(nodes), "n_entries": len(order), "order": order}
         for name, dt in fields:
             out[name] = self._dev(np.asarray(getattr(pts, name))[order], dt)
         return out
@@ -330,6 +332,8 @@ class Engine:
                 if np.max(pts.base) + s.cmax + 5 >= T.numel() or np.min(pts.base) < 0 or np.min(pts.i0) < 0:
                     raise ValueError("table source reads outside its tables")
                 q = self._points(pts, [("base", i64), ("i0", i64), ("u0", self.rdt), ("coef", self.rdt)])
+                if k == 1:
+                    q_h = q
                 d.pts[k].n_nodes, d.pts[k].nodes, d.pts[k].offsets = q["n_nodes"], _ptr(q["nodes"]), _ptr(q["offsets"])
                 d.pts[k].n_entries = q["n_entries"]
                 d.base[k], d.i0[k], d.u0[k], d.coef[k] = (_ptr(q[x]) for x in ("base", "i0", "u0", "coef"))
@@ -341,6 +345,8 @@ class Engine:
             view = self._zeros((3,), self.rdt)
             d.view = _ptr(view)
             _abi.check(L.lsfdtd_engine_add_table_source(self._h, C.byref(d)), "lsfdtd_engine_add_table_source")
+            if self.double_buffered and s.H is not None:
+                self._table_boxes(s.H, q_h, L)
             return {"kind": "table", "view": view}
         if isinstance(s, DipoleSource):
             idx = np.asarray(s.idx, np.int64)
@@ -411,6 +417,29 @@ class Engine:
             _abi.check(L.lsfdtd_engine_add_mode_source(self._h, C.byref(d)), "lsfdtd_engine_add_mode_source")
             return {"kind": "mode"}
         raise NotImplementedError(f"no CUDA path for the source {type(s).__name__}")
+
+    def _table_boxes(self, pts, q, L):
+        """Give the fused pass the H corrections of the (only) table-fed source as slab boxes (plan.slab_boxes),
+        with the position of each slab-order entry among the source's CSR entries and a value array. Sources
+        whose points do not form at most 24 boxes keep the in-place kernels."""
+        from .plan import slab_boxes
+
+        torch = _torch()
+        try:
+            boxes = slab_boxes(pts.node, self.shape)
+        except ValueError:
+            return
+        if not 1 <= len(boxes) <= 24:
+            return
+        rows = np.array([[bc, *lo, *hi, off] for bc, lo, hi, off in boxes], dtype=np.int32)
+        perm = np.empty(len(q["order"]), np.int64)
+        perm[q["order"]] = np.arange(len(q["order"]))  # slab-order entry e sits at CSR position perm[e]
+        perm_d = self._dev(perm, torch.int64)
+        vals = self._zeros((len(perm),), self.rdt)
+        _abi.check(L.lsfdtd_engine_set_table_boxes(self._h, 0, len(boxes), rows.ctypes.data_as(C.c_void_p),
+                                                   _ptr(perm_d), len(perm), _ptr(vals)),
+                   "lsfdtd_engine_set_table_boxes")
+        self._keep.append(rows)
 
     def _build_monitor(self, m, obj, L):
         torch = _torch()
@@ -573,7 +602,8 @@ class Engine:
 
     def set_wait_budget(self, cycles: int) -> None:
         """Clock cycles the fused pass waits for one plane's copies before it gives up (default about 2 s when
-        ``cycles`` <= 0); before the first graph capture."""
+        ``cycles`` is 0; negative: a test of the timeout path, every wait on a barrier nothing completes for
+        -cycles cycles); before the first graph capture."""
         _abi.check(_abi.lib().lsfdtd_engine_set_wait_budget(self._h, int(cycles)), "lsfdtd_engine_set_wait_budget")
 
     def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:

@@ -344,6 +344,48 @@ def _points_by_slab(slabs, shape, kind, make):
     return rows
 
 
+def slab_boxes(node, shape) -> list[tuple]:
+    """The boxes a list of flat field nodes enumerates: [(component, lo (3,), hi (3,), offset)], each box's
+    nodes in row-major order starting at its offset, the boxes one after another (a table-fed source's
+    correction points come slab by slab this way, ``layered.py:190-228``). Each box is grown as far as the
+    list continues its pattern: along z, then rows along y, then planes along x. Raises ValueError if the
+    boxes do not reproduce the list."""
+    node = np.asarray(node, np.int64)
+    n0, n1, n2 = (int(v) for v in shape)
+    c, r = np.divmod(node, n0 * n1 * n2)
+    i, r = np.divmod(r, n1 * n2)
+    j, k = np.divmod(r, n2)
+    boxes, e, total = [], 0, len(node)
+
+    def same(s, length, di, dj, dk):
+        """Entries s .. s + length: component c[e], at (i[e] + di, j[e] + dj, k[e] + dk + t)."""
+        if s + length > total:
+            return False
+        sl = slice(s, s + length)
+        return bool(np.all(c[sl] == c[e]) and np.all(i[sl] == i[e] + di) and np.all(j[sl] == j[e] + dj) and
+                    np.array_equal(k[sl], k[e] + dk + np.arange(length)))
+
+    while e < total:
+        lz = 1
+        while same(e + lz, 1, 0, 0, lz):
+            lz += 1
+        ly = 1
+        while same(e + ly * lz, lz, 0, ly, 0):
+            ly += 1
+        lx = 1
+        while all(same(e + (lx * ly + row) * lz, lz, lx, row, 0) for row in range(ly)):
+            lx += 1
+        lo = (int(i[e]), int(j[e]), int(k[e]))
+        boxes.append((int(c[e]), lo, (lo[0] + lx, lo[1] + ly, lo[2] + lz), e))
+        e += lx * ly * lz
+    rebuilt = np.concatenate([
+        flat_index(bc, *np.meshgrid(np.arange(lo[0], hi[0]), np.arange(lo[1], hi[1]), np.arange(lo[2], hi[2]),
+                                    indexing="ij"), shape).reshape(-1) for bc, lo, hi, _ in boxes]) if boxes else node
+    if not np.array_equal(rebuilt, node):
+        raise ValueError("the nodes are not a sequence of row-major boxes")
+    return boxes
+
+
 def table_source_from(src, shape) -> TableSource:
     """TableSource from a constructed ``ObliqueLayeredPlaneWave`` (before ``bind``, which drops its tables).
 

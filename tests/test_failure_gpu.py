@@ -2,9 +2,10 @@
 
 The fused pass bounds every wait on its copy ring by a clock budget; a CTA that runs out records the engine's
 status word, waits (bounded) for its own copies still in flight and returns, and ``Engine.check_status``
-raises. Here the budget is set below a copy's latency, so the pass gives up on its first plane while every
-copy it issued still completes: the status must be reported, stay set until cleared, and the GPU must go on
-answering (a fresh engine on the same plan matches the oracle afterwards).
+raises. Here a negative budget makes every wait one on a barrier that nothing completes (a flag nothing sets),
+for 10^5 cycles, while every copy the pass issued still completes and is drained: the status must be
+reported, stay set until cleared, and the GPU must go on answering (a fresh engine on the same plan matches the
+oracle afterwards).
 """
 
 import numpy as np
@@ -22,7 +23,7 @@ def test_copy_wait_timeout_is_reported_and_the_gpu_still_answers(golden):
     eng = Engine.from_plan(plan, precision="single")
     assert eng.fused and eng.uses_tma
     eng.check_status()
-    eng.set_wait_budget(1)  # one clock cycle: shorter than any copy
+    eng.set_wait_budget(-100000)  # every wait runs out after 1e5 cycles (about 50 us)
     eng.chunk(1)
     with pytest.raises(_abi.LsfdtdError, match="gave up waiting"):
         eng.check_status()

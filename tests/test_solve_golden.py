@@ -119,3 +119,30 @@ def test_cuda_engine_replays_the_full_size_sphere(precision, golden):
             bar = np.maximum(F32_FLOOR, F32_MULTIPLE * err_ls)
             worst = int(np.argmax(err / bar))
             assert np.all(err <= bar), (k, worst, err[worst], err_ls[worst])
+
+
+@pytest.mark.gpu
+def test_full_size_sphere_on_the_fused_pass_gives_the_in_place_kernels_values(golden):
+    """The 129^3 sphere (rows of 129 nodes, which the tensor copies cannot stride; a table-fed TF/SF box; a
+    dispersive group) steps in place by default (faster on this grid); asked for the lean fused pass, it runs
+    it with cp.async copies and the TF/SF corrections of H added as it steps, and gives the in-place kernels'
+    fields and accumulators after 3 chunks, in FP64."""
+    from lightsmith_b200.engine import Engine
+
+    plan = golden("solve_c0")["plan"]
+    out = {}
+    for fused in (None, False):
+        eng = Engine.from_plan(plan, precision="double", fused=fused)
+        if fused is None:
+            eng.set_tuning(4, 8, 0, 4)
+        eng.chunk(3, use_graph=True)
+        out[fused] = (eng.fused, eng.uses_tma, eng.E.cpu().numpy(), eng.H.cpu().numpy(),
+                      [eng.results(k) for k in range(len(plan["monitors"]))])
+        eng.close()
+    assert out[None][:2] == (True, False) and out[False][0] is False
+    for a, b in ((out[None][2], out[False][2]), (out[None][3], out[False][3])):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    for (ea, ha), (eb, hb) in zip(out[None][4], out[False][4]):
+        assert np.abs(ea - eb).max() <= 1e-12 * np.abs(eb).max()
+        if hb is not None:
+            assert np.abs(ha - hb).max() <= 1e-12 * np.abs(hb).max()
