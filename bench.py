@@ -19,7 +19,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -63,6 +62,10 @@ def _args():
     ap.add_argument("--sweep-steps", type=int, default=3000, help="sweep: FDTD steps per run")
     ap.add_argument("--instances", type=int, default=24, help="clusters: number of instances")
     ap.add_argument("--cluster-steps", type=int, default=2000, help="clusters: FDTD steps per instance")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="the default line without its records of the other forms (sphere solve, batched sweep, "
+                         "adjoint, clusters)")
+    ap.add_argument("--form-instances", type=int, default=4, help="cluster instances in the default line's record")
     return ap.parse_args()
 
 
@@ -74,19 +77,21 @@ def _peak():
         return 6650.0, "fallback"
 
 
-def _ncu_traffic_per_cell(variant: int):
-    """DRAM bytes per cell update of the bulk kernels of one variant, from the committed ncu summaries (lines
-    ``dram_bytes_per_cell_update[variant V]: X``), if any."""
-    pattern = re.compile(r"dram_bytes_per_cell_update\[variant (\d)\]:\s*([0-9.]+)")
-    for name in sorted(os.listdir(os.path.join(HERE, "profiles"))):
-        try:
-            text = open(os.path.join(HERE, "profiles", name)).read()
-        except OSError:
-            continue
-        for v, x in pattern.findall(text):
-            if int(v) == variant:
-                return float(x)
-    return None
+def _ncu_traffic(kernel: str, grid, shape_tuple):
+    """DRAM bytes (read + write) of one launch of ``kernel`` on ``grid`` in kernel variant ``shape_tuple[0]``,
+    as one ncu capture of the same kernel on the same grid recorded them (``profiles/ncu_traffic.json``, each
+    record with the command that made it): (bytes, source) or (None, None) without a matching record."""
+    try:
+        with open(os.path.join(HERE, "profiles", "ncu_traffic.json")) as f:
+            records = json.load(f)
+    except (OSError, ValueError):
+        return None, None
+    for r in records:  # the same kernel, grid and kernel variant (planes per CTA change the halo re-reads only)
+        if (r.get("kernel") == kernel and list(r.get("grid", [])) == list(grid) and
+                int(r.get("variant", -1)) == int(shape_tuple[0])):
+            return float(r["dram_bytes_read"]) + float(r["dram_bytes_write"]), \
+                f"ncu capture of one launch of the same kernel and grid: {r['command']}"
+    return None, None
 
 
 class Clocks:
@@ -342,7 +347,7 @@ def run_b200(args):
     alg_bytes = cells * BYTES_PER_CELL + cells_in_cpml(eng.plan) * BYTES_PER_CPML_PAIR
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     peak, peak_kind = _peak()
-    tpc = _ncu_traffic_per_cell(variant)
+    traffic, traffic_source = _ncu_traffic("k_fused_pml", shape, tuned)
 
     # end to end through the C ABI with host buffers: permittivity from pinned host memory, K chunks, the DFT
     # accumulators and the energy back to pinned host memory
@@ -376,6 +381,9 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_record(CPU_SAMPLE_N, 4, 1, _threads(), numpy_chunks=1)
     eng.close()
+    del eng
+    torch.cuda.empty_cache()
+    other = forms(args) if (rank == 0 and world == 1 and not args.no_forms) else None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -395,7 +403,7 @@ def run_b200(args):
                           "copy_engine": ("TMA" if eng_tma else "cp.async") if variant in (1, 3, 4) else None},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_source": peak_kind,
-                            "traffic": None if tpc is None else tpc * cells,
+                            "traffic": traffic, "traffic_source": traffic_source,
                             "kernel": "bulk Yee update (H and E with their CPML terms), per FDTD step",
                             "alg_bytes_per_step": alg_bytes, "kernel_ms_per_step": step_ms,
                             "bulk_launches_timed": bulk_launches},
@@ -403,6 +411,8 @@ def run_b200(args):
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                        "fields_finite": finite},
                "gpu_launches": launches, "clocks": clk}
+        if other is not None:
+            out["forms"] = other
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -486,7 +496,7 @@ def run_sweep(args):
            "speedup_vs_sequential": value / seq_value,
            "equal_spectra": {"max_rel_diff_dft": worst, "tolerance": 1e-4},
            "clocks": clk}
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_adjoint(args):
@@ -542,7 +552,7 @@ def run_adjoint(args):
            "fused_pass": bool(run.eng.fused),
            "forward_gcells": cells * info["n_steps"] / (t_plain / 1e3) / 1e9,
            "objective": J, "grad_rho_absmax": float(g_rho.abs().max()), "clocks": clk}
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_clusters(args):
@@ -612,7 +622,7 @@ def run_clusters(args):
            "max_spectrum_err_vs_fp64": max(r["spectrum_err_vs_fp64"] for r in rows),
            "max_gradient_err_vs_fp64": max(r["gradient_err_vs_fp64"] for r in rows),
            "instances": rows, "clocks": clk}
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_sphere(args):
@@ -710,7 +720,29 @@ def run_sphere(args):
                         "share_of_step": s["bulk_ms_per_step"] / (s["device_ms"] / post["steps"])},
            "fused_pass": s["fused_pass"], "gpu_launches": s["launches"],
            "fp64_solve_ms": res["double"]["device_ms"], "clocks": clk}
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def forms(args) -> dict:
+    """The method's other forms on this GPU, each a record with its own clock samples, for the default line:
+    the whole 129^3 dispersive-sphere solve (Gcell/s, roofline of its bulk kernel, FP32 and FP64 errors), the
+    batched oblique sweep against the same runs one after another, the adjoint gradient's cost over a forward
+    run, and forward + gradient over dispersive clusters with FP64 errors (a few instances)."""
+    import torch
+
+    out = {}
+    for name, fn, kw in (("sphere", run_sphere, {}), ("sweep", run_sweep, {}), ("adjoint", run_adjoint, {}),
+                         ("clusters", run_clusters, {"instances": args.form_instances})):
+        sub = argparse.Namespace(**{**vars(args), **kw})
+        t0 = time.perf_counter()
+        try:
+            rec = fn(sub)
+        except Exception as e:  # noqa: BLE001 (one form failing must not lose the headline line)
+            rec = {"error": f"{type(e).__name__}: {e}"}
+        rec["wall_s"] = round(time.perf_counter() - t0, 2)
+        out[name] = rec
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -718,13 +750,13 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "sweep":
-        run_sweep(args)
+        print(json.dumps(run_sweep(args)), flush=True)
     elif args.workload == "adjoint":
-        run_adjoint(args)
+        print(json.dumps(run_adjoint(args)), flush=True)
     elif args.workload == "clusters":
-        run_clusters(args)
+        print(json.dumps(run_clusters(args)), flush=True)
     elif args.workload == "sphere":
-        run_sphere(args)
+        print(json.dumps(run_sphere(args)), flush=True)
     else:
         run_b200(args)
 

@@ -160,6 +160,52 @@ def test_slab_device_gradient_in_rho_matches_finite_differences_on_32_cells():
     assert max(errs) < 1e-5, max(errs)
 
 
+@pytest.mark.slow
+def test_full_size_slab_device_gradient_in_rho_matches_finite_differences_on_32_cells():
+    """The inverse-design workload at its full size (200 x 200 x 120 cells of 20 nm, CPML 12, 100 x 100 x 11
+    design nodes, 8000 steps, checkpoints every 256 steps), float64: dJ/drho by the adjoint against central
+    differences of the CUDA forward on 32 random design cells, each within 1e-3 of its difference (the
+    north star's bar) and all within 1e-6 of the largest entry."""
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import slab_device_plan
+
+    plan, box, wE, info = slab_device_plan(n_steps=8000, single=False)
+    assert plan["shape"] == (200, 200, 120)
+    run = AdjointRun(plan, box, wE=wE, checkpoint=256, precision="double")
+    nz = box[2][1] - box[2][0]
+    a, b = info["eps_clad"], info["eps_core"]
+
+    def set_rho(rho):
+        eps = a + rho[:, :, None] * (b - a)
+        run.set_inv_eps_box(torch.as_tensor(np.broadcast_to(1.0 / eps, rho.shape + (nz,)).copy()))
+
+    rho = info["rho"]
+    set_rho(rho)
+    J0 = run.forward(info["n_steps"])[0]
+    g_inv = run.backward().cpu().numpy()
+    eps = a + rho[:, :, None] * (b - a)
+    g = (g_inv * (-(b - a) / eps ** 2)).sum(axis=2)
+    assert J0 > 0 and np.abs(g).max() > 0
+    rng = np.random.default_rng(3)
+    cells = rng.choice(rho.size, 32, replace=False)
+    h = 1e-5
+    worst_rel, worst_abs = 0.0, 0.0
+    for c in cells:
+        i, j = np.unravel_index(c, rho.shape)
+        vals = []
+        for sgn in (1, -1):
+            r = rho.copy()
+            r[i, j] += sgn * h
+            set_rho(r)
+            vals.append(run.forward(info["n_steps"], keep=False)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[i, j]) <= 1e-3 * abs(fd) + 1e-6 * np.abs(g).max(), (i, j, fd, g[i, j])
+        worst_rel = max(worst_rel, abs(fd - g[i, j]) / max(abs(fd), 1e-300))
+        worst_abs = max(worst_abs, abs(fd - g[i, j]) / np.abs(g).max())
+    run.close()
+    print(f"full-size slab device: worst relative error {worst_rel:.2e}, worst against max|g| {worst_abs:.2e}")
+
+
 def test_dispersive_group_and_flux_objective():
     """A Drude-Lorentz block (pure D-form group) between the dipole and the design box, and the monitor's
     three-frequency flux as the objective: the float64 gradient against torch autograd through the
