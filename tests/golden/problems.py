@@ -36,6 +36,18 @@ def sphere_problem(mesh: str, symmetry: str = "off"):
                                                run_time_fs=399.5 * 2.2863 / 299.792458)})
 
 
+def sphere_fields_problem():
+    """The 16 nm sphere (staircase) with lightsmith's field outputs: the total E on an xz plane through it and
+    the differential scattering cross section at three polar angles in two azimuthal planes."""
+    from lightsmith.spec import FarFieldRequest, NearFieldRequest, Outputs
+    p = sphere_problem("staircase")
+    outputs = Outputs(near_field=NearFieldRequest(plane="xz", half_width_nm=24.0, points=9,
+                                                  wavelengths_nm=[500.0, 700.0]),
+                      far_field=FarFieldRequest(theta_deg=[0.0, 60.0, 120.0], phi_deg=[0.0, 90.0],
+                                                wavelengths_nm=[500.0, 700.0]))
+    return p.model_copy(update={"outputs": outputs})
+
+
 def dielectric_sphere_problem():
     """A non-dispersive sphere (n = 2, radius 16 nm) in n = 1.33 with conformal interfaces (off-diagonal 1/eps)."""
     return ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=16.0), material=ls.ConstantIndex(n_real=2.0))],
@@ -73,6 +85,7 @@ SOLVE_PROBLEMS = {
     "sphere_conformal": lambda: sphere_problem("conformal"),
     "sphere_symmetric": lambda: sphere_problem("staircase", "auto"),
     "sphere_defaults": lambda: sphere_problem("conformal", "auto"),
+    "sphere_fields": sphere_fields_problem,
     "dielectric_conformal": dielectric_sphere_problem,
     "periodic_normal": lambda: periodic_problem(0.0, 0.0, "s"),
     "periodic_oblique": lambda: periodic_problem(30.0, 10.0, "p"),

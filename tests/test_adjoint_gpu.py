@@ -165,7 +165,7 @@ def test_full_size_slab_device_gradient_in_rho_matches_finite_differences_on_32_
     """The inverse-design workload at its full size (200 x 200 x 120 cells of 20 nm, CPML 12, 100 x 100 x 11
     design nodes, 8000 steps, checkpoints every 256 steps), float64: dJ/drho by the adjoint against central
     differences of the CUDA forward on 32 random design cells, each within 1e-3 of its difference (the
-    north star's bar) and all within 1e-6 of the largest entry."""
+    agreement the gradient is required to reach) and all within 1e-6 of the largest entry."""
     from lightsmith_b200.adjoint import AdjointRun
     from lightsmith_b200.workloads import slab_device_plan
 

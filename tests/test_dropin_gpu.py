@@ -89,8 +89,14 @@ def _rel(got, want):
 
 # float32 tolerances: lightsmith's own GPU-against-CPU bounds for the same kind of result
 def _f32_check(name, key, got, want):
-    if key in ("wavelengths_nm", "angles_deg", "equivalent_radius_nm") or key.endswith("/order"):
+    exact = ("wavelengths_nm", "angles_deg", "equivalent_radius_nm", "wavelength_nm", "offset_nm", "axis1_nm",
+             "axis2_nm", "theta_deg", "phi_deg")
+    if key.split("/")[-1] in exact or key.endswith("/order"):
         np.testing.assert_allclose(got, want, rtol=1e-12, err_msg=key)
+    elif key.startswith(("near_field", "far_field")):
+        # fields on a plane and dC_sca/dOmega at a few angles: relative to the largest value of the array (a
+        # pointwise bound would fail at the near-zeros of a field pattern)
+        assert _rel(got, want) < 1e-3, (key, _rel(got, want))
     elif name.startswith(("sphere", "dielectric")):
         np.testing.assert_allclose(got, want, rtol=1e-4, err_msg=key)  # tests/test_fdtd.py:131-132
     elif name.startswith("periodic"):

@@ -37,6 +37,33 @@ def test_throughput_case_matches_oracle_at_128():
     np.testing.assert_allclose(gpu32.energy.cpu().numpy()[0], ref.energy[0], rtol=1e-3)
 
 
+@pytest.mark.parametrize("precision,tol", [("double", 1e-9), ("single", 3e-4)])
+def test_bench_kernel_matches_oracle_at_128(precision, tol):
+    """The bench's own kernel and launch shape (the lean fused pass, variant 4, x planes chosen per grid, TMA
+    copies) in both precisions against the float64 oracle on the throughput case at 128^3 (CPML 16), over six
+    chunks (186 steps): fields, both DFT accumulators and the decay-energy proxy."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+    from oracle.engine import OracleEngine
+
+    plan = throughput_plan(128, max_steps=4000, seed=5, single=False)
+    ref = OracleEngine(plan, threads=8)
+    eng = Engine.from_plan(plan, precision=precision)
+    eng.set_tuning(4, 8, 0, 4)
+    assert eng.fused and eng.uses_tma
+    for _ in range(6):
+        ref.chunk()
+        eng.chunk(1, use_graph=True)
+    ref.close()
+    assert np.abs(ref.E).max() > 0
+    assert _rel(eng.E.cpu().numpy(), ref.E) < tol
+    assert _rel(eng.H.cpu().numpy(), ref.H) < tol
+    assert _rel(eng.results(0)[0], ref.monitors[0]["acc_e"]) < tol
+    assert _rel(eng.results(0)[1], ref.monitors[0]["acc_h"]) < tol
+    np.testing.assert_allclose(eng.energy.cpu().numpy()[0], ref.energy[0], rtol=10 * tol)
+    eng.close()
+
+
 @pytest.mark.parametrize("variant", [3, 4])
 @pytest.mark.parametrize("n,pml", [(128, 16), (100, 10), (72, 12)])
 def test_split_and_lean_passes_equal_fused_pass_on_the_throughput_case(n, pml, variant):
