@@ -328,6 +328,12 @@ int32_t lsfdtd_engine_fused(lsfdtd_engine* eng);
  * pass does not apply). */
 int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t tile_y, int32_t planes,
                                  int32_t stages);
+/* variant 4 with tensor copies: on (the default) steps the clean interior of the grid (the tiles and x planes
+ * whose nodes and halo nodes all lie outside every CPML slab and inside every component's stepped region)
+ * with a kernel compiled without region or CPML code, on a second stream beside the lean kernel that steps
+ * the CTAs around it, where the grid has such an interior and no source corrects H; off steps every CTA with
+ * the lean kernel. The values are the same either way. Set before the first graph capture. */
+int32_t lsfdtd_engine_set_clean_split(lsfdtd_engine* eng, int32_t on);
 /* reads the status word (synchronises `stream`): LSFDTD_ETIMEOUT with *status = 1 if a kernel gave up waiting
  * for its copies, LSFDTD_ENONFINITE with *status = 2 if the run's fields turned non-finite in a batched launch
  * (the run retired then), else LSFDTD_OK */

@@ -131,6 +131,7 @@ SIGNATURES = {
     "lsfdtd_batch_create_shaped": (i32, [vp, i32, vp, i32, i32, vp]),
     "lsfdtd_engine_set_table_boxes": (i32, [vp, i32, i32, vp, vp, i64, vp]),
     "lsfdtd_engine_set_wait_budget": (i32, [vp, C.c_int64]),
+    "lsfdtd_engine_set_clean_split": (i32, [vp, i32]),
     "lsfdtd_engine_set_copy_engine": (i32, [vp, i32]),
     "lsfdtd_engine_uses_tma": (i32, [vp]),
     "lsfdtd_engine_fused": (i32, [vp]),

@@ -64,6 +64,9 @@ struct PmlTables {
   static constexpr int NY = TY + 1, NZ = 33;
   SlabInfo<R> y[2][NY];  // [E, H][row]: y = y0 - 1 + row
   SlabInfo<R> z[2][NZ];  // [E, H][col]: z = z0 - 1 + col
+  // the psi of the halo nodes' H CPML terms, per axis, copied ahead of the plane's wait: [plane parity][H_x and
+  // H_z of the halo row, H_x and H_y of the halo column][lane][axis]
+  F hpsi[2][4][32][3];
 };
 
 template <typename F, int TY, int S>
@@ -108,9 +111,14 @@ __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabIn
 // multiple of 16 bytes). A table-fed TF/SF source's corrections of H (FusedArgs::hc) are added to every H
 // value the tile computes (its own nodes and its halo) before the E half uses them (HC: compiled in only for
 // runs that have such corrections).
-template <typename F, int TY, int S, bool UNI, bool ASYNC = false, bool HC = false>
+// CLEAN: every CTA of the launch lies in the clean interior (each of its nodes, halo nodes and x planes,
+// the plane before its segment included, inside [inner_lo, inner_hi) on every axis): the region tests and
+// CPML terms are compiled out, and with them the registers they hold (the lean path's code, though never
+// taken there, costs the interior warps a quarter of their speed)
+template <typename F, int TY, int S, bool UNI, bool ASYNC = false, bool HC = false, bool CLEAN = false>
 __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 1)
     k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
+  static_assert(!CLEAN || (!ASYNC && !HC), "the clean interior pass copies by tensor maps and has no sources");
   using R = typename real_of<F>::type;
   using St = TmaStage<F, TY>;
   using Tab = PmlTables<F, TY>;
@@ -127,11 +135,19 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   const YeeArgs<F>& g = a.y;
   const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
-  const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY;
+  int z0, y0, xs, xe;  // the CTA's tile and x segment, from the launch's box list
+  {
+    int b = 0;
+    while (b + 1 < t.map.n && (int)blockIdx.x >= t.map.box[b + 1].first) ++b;
+    const CtaBox& q = t.map.box[b];
+    const int l = (int)blockIdx.x - q.first, nz = q.t1[0] - q.t0[0], ny = q.t1[1] - q.t0[1];
+    z0 = (q.t0[0] + l % nz) * TZ;
+    y0 = (q.t0[1] + (l / nz) % ny) * TY;
+    xs = q.x0 + (l / nz / ny) * q.seg;
+    xe = min(min(q.x1, n0), xs + q.seg);
+  }
+  if (xs >= xe) return;
   const int k = z0 + tx, j = y0 + ty;
-  const int xs = blockIdx.z * a.seg;
-  if (xs >= n0) return;
-  const int xe = min(n0, xs + a.seg);
   const int xb = xs > 0 ? xs - 1 : 0;
   const bool own = k < n2 && j < n1;
   const long long s1 = n2, s0 = (long long)n1 * n2;
@@ -143,7 +159,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   auto stC = [&](int s) { return reinterpret_cast<R(*)[TZ]>(smem + s * St::kBytes + 3 * St::kE + 3 * St::kH); };
 
   // the slab tables of the tile's rows and columns (halo included)
-  for (int e = tid; e < 2 * (Tab::NY + Tab::NZ); e += NT) {
+  for (int e = tid; !CLEAN && e < 2 * (Tab::NY + Tab::NZ); e += NT) {
     const int f = e / (Tab::NY + Tab::NZ), r = e % (Tab::NY + Tab::NZ);
     if (r < Tab::NY)
       tab.y[f][r] = f ? slab_info<1>(g.pml[1], 1, y0 - 1 + r) : slab_info<0>(g.pml[1], 1, y0 - 1 + r);
@@ -214,11 +230,13 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     if (t.wait_budget < 0) return mbar_wait_bounded(&never, 0, -t.wait_budget);  // a timeout test: see TmaArgs
     return mbar_wait_bounded(&bar[r % S], (r / S) & 1, t.wait_budget);
   };
-  int issued = xb - 1;
+  // the planes a segment reads are xb .. xe (plane xe as the next plane of the last one), and no others are
+  // copied
+  const int first_fill = min(xb + S - 2, xe);
   if (ASYNC || tid == 0) {
-    for (int p = xb; p < xb + S - 1; ++p) produce(p);
+    for (int p = xb; p <= first_fill; ++p) produce(p);
   }
-  issued = xb + S - 2;
+  int issued = first_fill;
 
   auto curl = [&](F av, F bv, int d1, int d2) -> F {
     if constexpr (UNI) return av - bv;
@@ -329,7 +347,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   int cons = xb - 1;
 #pragma unroll 1
   for (int i = xb; i < xe; ++i) {
-    const bool fast = warp_clean && i >= a.inner_lo[0] && i < a.inner_hi[0];
+    const bool fast = CLEAN || (warp_clean && i >= a.inner_lo[0] && i < a.inner_hi[0]);
     SlabInfo<R> xs_h, xs_e;
     // a lean warp issues the psi loads of its own nodes for this plane before it waits for the plane's
     // copies, so that their latency overlaps the wait and each other: [component][axis], with the psi index
@@ -370,14 +388,41 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         }
       }
     }
+    // the psi of the halo nodes that take the lean path (warp 0: the halo row, warp kColWarp: the halo column),
+    // copied into shared memory ahead of the plane's wait like the own nodes' loads above (tensor-copy ring
+    // only: the cp.async ring's copies share the wait that these need)
+    const bool x_in = i >= a.inner_lo[0] && i < a.inner_hi[0];
+    const bool row_lean = !CLEAN && ty == 0 && !fast && y0 > 0 && k < n2 && i >= xs;
+    const bool col_lean = !CLEAN && ty == kColWarp && tx < TY && z0 > 0 && y0 + tx < n1 && i >= xs &&
+                          !(col_clean && x_in);
+    if constexpr (!ASYNC && !CLEAN) {
+      if (row_lean || col_lean) {
+        const SlabInfo<R> xh = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;
+        const int yy = row_lean ? 0 : tx + 1, zz = row_lean ? tx + 1 : 0;
+        const int x[3] = {i, y0 - 1 + yy, z0 - 1 + zz};
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+          const int c = row_lean ? 2 * w : w;  // the row's H_x and H_z, the column's H_x and H_y
+          F* dst = tab.hpsi[i & 1][row_lean ? w : 2 + w][tx];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            if (d == c) continue;
+            const SlabInfo<R>& sl = d == 0 ? xh : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
+            if (sl.side >= 0) cp_async(dst + d, g.pml[d].psi[1][c][sl.side] + pml_index(g, sl, d, x), true);
+          }
+        }
+      }
+    }
     const bool ok = (i > xb || ready(i)) && ready(i + 1);  // plane i was waited for as plane i + 1 before
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
     }
     cons = i + 1;
-    if (ASYNC || tid == 0) produce(i + S - 1);
-    issued = i + S - 1;
+    if (i + S - 1 <= xe) {
+      if (ASYNC || tid == 0) produce(i + S - 1);
+      issued = i + S - 1;
+    }
     const int si = (int)((unsigned)(i - xb) % S), sn = (int)((unsigned)(i + 1 - xb) % S);
     const long long p = i * s0 + off_jk;
     unsigned pm = 0;  // the correction boxes of H that hold nodes of this plane and tile
@@ -452,8 +497,9 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         hxr = hx_fast(si, tx + 4);
         hzr = hz_fast(si, sn, tx + 4);
       } else {
-        hxr = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
-        hzr = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false, nullptr);
+        if constexpr (!ASYNC) asm volatile("cp.async.wait_all;\n" ::: "memory");  // this lane's halo psi
+        hxr = h_lean(0, si, sn, i, 0, tx + 1, xs_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][0][tx]);
+        hzr = h_lean(2, si, sn, i, 0, tx + 1, xs_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][1][tx]);
       }
       if (HC && pm) {
         hxr = hcorr(hxr, 0, i, y0 - 1, k, pm);
@@ -465,14 +511,15 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     // the halo column z0 - 1 (H_x, H_y of every row, for lane 0 of each warp): one warp, lane r for row r
     if (ty == kColWarp && tx < TY && z0 > 0 && y0 + tx < n1) {
       F hxc, hyc;
-      if (col_clean && i >= a.inner_lo[0] && i < a.inner_hi[0]) {
+      if (CLEAN || (col_clean && i >= a.inner_lo[0] && i < a.inner_hi[0])) {
         const int o = (tx + 1) * BZ + 3;
         hxc = hx_fast(si, o);
         hyc = hy_fast(si, sn, o);
       } else {
         SlabInfo<R> xc_h = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;  // this warp may be fast itself
-        hxc = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
-        hyc = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, nullptr);
+        if constexpr (!ASYNC) asm volatile("cp.async.wait_all;\n" ::: "memory");
+        hxc = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][2][tx]);
+        hyc = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][3][tx]);
       }
       if (HC && pm) {
         hxc = hcorr(hxc, 0, i, y0 + tx, z0 - 1, pm);
@@ -539,7 +586,8 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       mbar_wait_bounded(&bar[(unsigned)(p - xb) % S], ((unsigned)(p - xb) / S) & 1, kDrainBudget);
     if (failed && t.status) atomicExch(t.status, 1);
   }
-  if constexpr (ASYNC) asm volatile("cp.async.wait_all;\n" ::: "memory");  // every thread's own copies landed
+  // every thread's own copies landed (the ring's with cp.async, or the halo psi)
+  if constexpr (!CLEAN) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 }
 

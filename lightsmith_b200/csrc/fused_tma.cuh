@@ -25,9 +25,24 @@
 
 namespace lsfdtd {
 
+// CTAs of the lean pass over boxes of tiles and x planes: box b holds CTAs first .. first + count - 1, z tiles
+// [t0[0], t1[0]) (of 32 nodes), y tiles [t0[1], t1[1]) (of the launch's tile rows) and x planes [x0, x1) in
+// segments of seg planes, z tile fastest, then y tile, then segment
+struct CtaBox {
+  int t0[2], t1[2];
+  int x0, x1, seg;
+  int first;
+};
+constexpr int kMaxCtaBoxes = 6;
+struct CtaMap {
+  int n;
+  CtaBox box[kMaxCtaBoxes];
+};
+
 template <typename F>
 struct TmaArgs {
   FusedArgs<F> f;
+  CtaMap map;          // the CTAs of this launch (k_fused_pml)
   CUtensorMap mE[3];   // E^n components, box 40 x (TY + 2) x 1
   CUtensorMap mH[3];   // H^n components, box 40 x (TY + 1) x 1
   CUtensorMap mC;      // cbE (component 0), box 32 x TY x 1

@@ -120,6 +120,10 @@ struct lsfdtd_engine {
   int use_tma = 1;      // fused pass copies planes with the Tensor Memory Accelerator where the layout allows
   bool tuned = false;   // a kernel choice was set explicitly (lsfdtd_engine_set_tuning)
   long long wait_budget = lsfdtd::kWaitBudget;  // cycles the fused pass waits for a plane's copies
+  // the lean pass steps the clean interior of the grid with a kernel that has no region or CPML code, beside
+  // the lean kernel on the CTAs around it (where the grid has such an interior and no source corrects H)
+  int split_clean = 1;
+  virtual int init_side() = 0;  // the second stream of that split and its fork and join events
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
@@ -263,6 +267,23 @@ struct Engine final : lsfdtd_engine {
   int maps_tile_y = 0;  // tile rows the tensor-map boxes were made for
   CUtensorMap mapE[2][3], mapH[2][3], mapC;  // per buffer and component; the coefficient of component 0
   static constexpr int kStages = 4;  // x planes in the fused pass's copy ring
+  // the lean pass's boundary CTAs run on this second stream, beside the clean interior's (fork and join
+  // events on the caller's stream; made when the engine settles on the lean pass)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int init_side() override {
+    if constexpr (!kComplex) {
+      LS_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      LS_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+      LS_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    }
+    return LSFDTD_OK;
+  }
+  ~Engine() override {
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+  }
 
   F* Eflat() const { return Ebuf[cur]; }
   F* Hflat() const { return Hbuf[cur]; }
@@ -319,27 +340,28 @@ struct Engine final : lsfdtd_engine {
     }
     return LSFDTD_OK;
   }
-  template <int TY, int S, bool UNI, bool ASYNC, bool HC>
+  template <int TY, int S, bool UNI, bool ASYNC, bool HC, bool CLEAN = false>
   int launch_pml_one(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
-      constexpr size_t sm = fused_pml_smem_bytes<F, TY, S>();
+      // the clean interior pass reads no slab tables
+      constexpr size_t sm = CLEAN ? fused_tma_smem_bytes<F, TY, S>() : fused_pml_smem_bytes<F, TY, S>();
       static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
       if (!attr) {
-        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI, ASYNC, HC>,
+        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         attr = true;
       }
-      k_fused_pml<F, TY, S, UNI, ASYNC, HC><<<grid, dim3(32, TY), sm, s>>>(ta);
+      k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
   }
   // the lean-CPML pass, one instantiation per cell shape (cubic or not), copy engine (cp.async: rows the
   // tensor copies cannot stride) and whether a table-fed source's H corrections are added as it steps (those
   // two with a ring of 4 only)
-  template <int TY, int S, bool ASYNC, bool HC>
+  template <int TY, int S, bool ASYNC, bool HC, bool CLEAN = false>
   int launch_pml_kind(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
-    return y.uniform ? launch_pml_one<TY, S, true, ASYNC, HC>(grid, ta, s)
-                     : launch_pml_one<TY, S, false, ASYNC, HC>(grid, ta, s);
+    return y.uniform ? launch_pml_one<TY, S, true, ASYNC, HC, CLEAN>(grid, ta, s)
+                     : launch_pml_one<TY, S, false, ASYNC, HC, CLEAN>(grid, ta, s);
   }
   template <int TY, int S>
   int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
@@ -352,9 +374,10 @@ struct Engine final : lsfdtd_engine {
                          : launch_pml_kind<TY, 4, true, false>(grid, ta, s);
   }
   // kind 0: the fused pass over the grid, 1: over the interior box of the split step, 2: with lean CPML terms
+  // (clean: its clean interior CTAs)
   template <int TY, int S>
-  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s, int kind) {
-    if (kind == 2) return launch_pml<TY, S>(grid, ta, s);
+  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s, int kind, bool clean) {
+    if (kind == 2) return clean ? launch_pml_kind<TY, S, false, false, true>(grid, ta, s) : launch_pml<TY, S>(grid, ta, s);
     return kind == 1 ? launch_tma_box<TY, S, true>(grid, ta, s) : launch_tma_box<TY, S, false>(grid, ta, s);
   }
   template <int TY, int S>
@@ -374,6 +397,70 @@ struct Engine final : lsfdtd_engine {
         if (y.pml[d].len[f][c][0] > 0 && y.pml[d].len[f][c][1] > 0 && lo_end > y.pml[d].start[f][c][1]) return false;
       }
     }
+    return true;
+  }
+
+  // the clean interior of the lean pass: z tiles [zc0, zc1), y tiles [yc0, yc1) (of `rows`), x planes [xc0, xc1)
+  void clean_box(int rows, int* zc0, int* zc1, int* yc0, int* yc1, int* xc0, int* xc1) const {
+    int lo[3], hi[3];
+    inner_bounds(lo, hi);
+    *zc0 = (lo[2] + 1 + 31) / 32;
+    *zc1 = hi[2] >= 32 ? (hi[2] - 32) / 32 + 1 : 0;
+    *yc0 = (lo[1] + 1 + rows - 1) / rows;
+    *yc1 = hi[1] >= rows ? (hi[1] - rows) / rows + 1 : 0;
+    *xc0 = lo[0] + 1;
+    *xc1 = hi[0];
+  }
+  // whether the lean pass runs as two kernels (clean interior and the rest)
+  bool lean_split() const {
+    if (kComplex || !tma_ok || !split_clean || !side || !lean_ok()) return false;
+    for (auto& tb : tables)
+      if (tb.has[1] && tb.hc.n > 0) return false;
+    int zc0, zc1, yc0, yc1, xc0, xc1;
+    clean_box(tile_y == 16 ? 16 : 8, &zc0, &zc1, &yc0, &yc1, &xc0, &xc1);
+    return zc1 > zc0 && yc1 > yc0 && xc1 > xc0;
+  }
+
+  // a box of z tiles [tz0, tz1), y tiles [ty0, ty1) and x planes [x0, x1) in segments of at most seg planes
+  // (evened out), appended to m with its CTAs counted in total; nothing for an empty box
+  static void add_cta_box(CtaMap& m, long long& total, int tz0, int tz1, int ty0, int ty1, int x0, int x1,
+                          int seg) {
+    if (tz1 <= tz0 || ty1 <= ty0 || x1 <= x0) return;
+    const int len = x1 - x0, nseg = (len + seg - 1) / seg, sg = (len + nseg - 1) / nseg;
+    CtaBox& b = m.box[m.n++];
+    b.t0[0] = tz0;
+    b.t1[0] = tz1;
+    b.t0[1] = ty0;
+    b.t1[1] = ty1;
+    b.x0 = x0;
+    b.x1 = x1;
+    b.seg = sg;
+    b.first = (int)total;
+    total += (long long)(tz1 - tz0) * (ty1 - ty0) * ((len + sg - 1) / sg);
+  }
+
+  // the lean pass's CTAs (tiles of 32 z nodes by `rows` y nodes, segments of seg x planes): with may_split
+  // and a clean interior of whole tiles, that interior in `clean` and the six boxes around it in `rest`
+  // (true); else all of them in `rest`. A clean CTA's nodes and halo nodes (row y0 - 1, column z0 - 1) and
+  // its x planes, the plane before its segment included, are inner on every axis
+  bool lean_maps(int rows, int seg, bool may_split, CtaMap* clean, long long* n_clean, CtaMap* rest,
+                 long long* n_rest) const {
+    const int n0 = desc.shape[0], nz = (desc.shape[2] + 31) / 32, ny = (desc.shape[1] + rows - 1) / rows;
+    clean->n = rest->n = 0;
+    *n_clean = *n_rest = 0;
+    int zc0, zc1, yc0, yc1, xc0, xc1;
+    clean_box(rows, &zc0, &zc1, &yc0, &yc1, &xc0, &xc1);
+    if (!may_split || zc1 <= zc0 || yc1 <= yc0 || xc1 <= xc0) {
+      add_cta_box(*rest, *n_rest, 0, nz, 0, ny, 0, n0, seg);
+      return false;
+    }
+    add_cta_box(*clean, *n_clean, zc0, zc1, yc0, yc1, xc0, xc1, seg);
+    add_cta_box(*rest, *n_rest, 0, nz, 0, ny, 0, xc0, seg);
+    add_cta_box(*rest, *n_rest, 0, nz, 0, ny, xc1, n0, seg);
+    add_cta_box(*rest, *n_rest, 0, nz, 0, yc0, xc0, xc1, seg);
+    add_cta_box(*rest, *n_rest, 0, nz, yc1, ny, xc0, xc1, seg);
+    add_cta_box(*rest, *n_rest, 0, zc0, yc0, yc1, xc0, xc1, seg);
+    add_cta_box(*rest, *n_rest, zc1, nz, yc0, yc1, xc0, xc1, seg);
     return true;
   }
 
@@ -442,11 +529,11 @@ struct Engine final : lsfdtd_engine {
     return LSFDTD_OK;
   }
 
-  // x planes per CTA of the fused pass when none is requested: 32, or fewer where 32 would give fewer than
-  // about three waves of CTAs (resident CTAs per SM as the kernels' launch bounds ask). A small grid steps
-  // faster in more, shorter CTAs: measured on B200, a 200 x 200 x 120 grid with 12-cell CPML took 157 us per
-  // step at 12 planes and 199 us at 34, while 640^3 keeps 32.
-  int auto_planes(int nx, long long columns, int rows, int* seg) {
+  // x planes per CTA of the fused pass when none is requested: `most`, or fewer where that would give fewer
+  // than about three waves of CTAs (resident CTAs per SM as the kernels' launch bounds ask). A small grid
+  // steps faster in more, shorter CTAs: measured on B200, a 200 x 200 x 120 grid with 12-cell CPML took 157 us
+  // per step at 12 planes and 199 us at 34.
+  int auto_planes(int nx, long long columns, int rows, int* seg, int most = 48) {
     if (sm_count <= 0) {
       int dev = 0;
       LS_CUDA(cudaGetDevice(&dev));
@@ -454,7 +541,7 @@ struct Engine final : lsfdtd_engine {
     }
     const long long per_sm = sizeof(R) == 4 ? (rows == 8 ? 4 : 2) : 1;
     const long long p = (long long)nx * columns / (3 * per_sm * std::max(sm_count, 1));
-    *seg = (int)std::max(4LL, std::min(48LL, p));
+    *seg = (int)std::max(4LL, std::min((long long)most, p));
     return LSFDTD_OK;
   }
 
@@ -501,43 +588,65 @@ struct Engine final : lsfdtd_engine {
                       : dim3(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], rows), 1);
     const int nx = split ? fa.box_hi[0] - fa.box_lo[0] : desc.shape[0];
     fa.seg = planes;
-    if (fa.seg <= 0) LS_TRY(auto_planes(nx, (long long)grid.x * grid.y, rows, &fa.seg));
+    // the lean pass split in two kernels balances its two halves better in shorter segments (measured on B200
+    // at 640^3: 3.32 ms per step at 32 planes, 3.52 at 48; the lean kernel alone is fastest at 48)
+    if (fa.seg <= 0) LS_TRY(auto_planes(nx, (long long)grid.x * grid.y, rows, &fa.seg, lean_split() ? 32 : 48));
     grid.z = (unsigned)cdiv(nx, fa.seg);
     LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
-      if (!tma_ok && kind == 2) {  // the lean pass with cp.async copies
-        TmaArgs<F> ta;
-        ta.f = fa;
-        ta.status = static_cast<int*>(scratch);
-        ta.wait_budget = wait_budget;
-        const int r = tile_y == 16 ? launch_pml_async<16>(grid, ta, s) : launch_pml_async<8>(grid, ta, s);
-        if (r != LSFDTD_OK) return r;
-      } else if (tma_ok) {
-        TmaArgs<F> ta;
-        ta.f = fa;
+      // the fused passes by tensor copies, with the deepest ring up to the requested depth that fits the
+      // device's shared memory per CTA
+      auto launch_ring = [&](const TmaArgs<F>& ta, dim3 g, cudaStream_t st, bool clean) -> int {
+        int smax = 0, dev = 0;
+        LS_CUDA(cudaGetDevice(&dev));
+        LS_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        auto fits = [&](size_t b) { return b <= (size_t)smax; };
+        if (tile_y == 16) {
+          if (stages >= 8 && fits(tma_smem<16, 8>(kind))) return launch_tma<16, 8>(g, ta, st, kind, clean);
+          if (stages >= 6 && fits(tma_smem<16, 6>(kind))) return launch_tma<16, 6>(g, ta, st, kind, clean);
+          return launch_tma<16, 4>(g, ta, st, kind, clean);
+        }
+        if (stages >= 8 && fits(tma_smem<8, 8>(kind))) return launch_tma<8, 8>(g, ta, st, kind, clean);
+        if (stages >= 6 && fits(tma_smem<8, 6>(kind))) return launch_tma<8, 6>(g, ta, st, kind, clean);
+        return launch_tma<8, 4>(g, ta, st, kind, clean);
+      };
+      TmaArgs<F> ta;
+      ta.f = fa;
+      ta.status = static_cast<int*>(scratch);
+      ta.wait_budget = wait_budget;
+      if (tma_ok) {
         for (int c = 0; c < 3; ++c) {
           ta.mE[c] = mapE[cur][c];
           ta.mH[c] = mapH[cur][c];
         }
         ta.mC = mapC;
-        ta.status = static_cast<int*>(scratch);
-        ta.wait_budget = wait_budget;
-        // the deepest ring, up to the requested depth, that fits the device's shared memory per CTA
-        int smax = 0, dev = 0;
-        LS_CUDA(cudaGetDevice(&dev));
-        LS_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        auto fits = [&](size_t b) { return b <= (size_t)smax; };
-        int r = LSFDTD_OK;
-        if (tile_y == 16) {
-          if (stages >= 8 && fits(tma_smem<16, 8>(kind))) r = launch_tma<16, 8>(grid, ta, s, kind);
-          else if (stages >= 6 && fits(tma_smem<16, 6>(kind))) r = launch_tma<16, 6>(grid, ta, s, kind);
-          else r = launch_tma<16, 4>(grid, ta, s, kind);
-        } else {
-          if (stages >= 8 && fits(tma_smem<8, 8>(kind))) r = launch_tma<8, 8>(grid, ta, s, kind);
-          else if (stages >= 6 && fits(tma_smem<8, 6>(kind))) r = launch_tma<8, 6>(grid, ta, s, kind);
-          else r = launch_tma<8, 4>(grid, ta, s, kind);
+      }
+      if (kind == 2) {
+        // the lean pass: the clean interior's CTAs by the clean kernel and the others by the lean one, on
+        // two streams, where the grid has such an interior; else every CTA by the lean kernel
+        CtaMap clean{}, rest{};
+        long long n_clean = 0, n_rest = 0;
+        const bool two = lean_maps(rows, fa.seg, lean_split(), &clean, &n_clean, &rest, &n_rest);
+        if (two) {
+          LS_CUDA(cudaEventRecord(ev_fork, s));
+          LS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
         }
+        ta.map = rest;
+        const dim3 g_rest((unsigned)n_rest);
+        int r = LSFDTD_OK;
+        if (tma_ok) r = launch_ring(ta, g_rest, two ? side : s, false);
+        else r = tile_y == 16 ? launch_pml_async<16>(g_rest, ta, s) : launch_pml_async<8>(g_rest, ta, s);
         if (r != LSFDTD_OK) return r;
+        if (two) {
+          LS_LAUNCHED();
+          ta.map = clean;
+          LS_TRY(launch_ring(ta, dim3((unsigned)n_clean), s, true));
+          LS_LAUNCHED();
+          LS_CUDA(cudaEventRecord(ev_join, side));
+          LS_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
+        }
+      } else if (tma_ok) {
+        LS_TRY(launch_ring(ta, grid, s, false));
         if (split) {
           LS_LAUNCHED();
           const unsigned blocks = (unsigned)cdiv((long long)sb.total, 256);
@@ -1381,7 +1490,8 @@ struct Engine final : lsfdtd_engine {
     if (fused == 1 && fused_variant()) {
       int lo[3], hi[3];
       ShellBoxes sb{};
-      per_step = (split_box(lo, hi, &sb) ? 3 : 1) + 1;  // fused pass (interior box, shell H and E), counter
+      // fused pass (interior box, shell H and E; or the lean pass's clean interior and the rest), counter
+      per_step = (split_box(lo, hi, &sb) ? 3 : (lean_split() ? 2 : 1)) + 1;
     }
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;
@@ -1640,7 +1750,13 @@ int32_t lsfdtd_engine_create(const lsfdtd_grid_desc* grid, lsfdtd_engine** out) 
     return fail(LSFDTD_EINVAL, "grid arrays missing");
   const double cells = (double)grid->shape[0] * grid->shape[1] * grid->shape[2];
   if (cells * 3 > 9.0e18) return fail(LSFDTD_EINVAL, "grid too large");
-  *out = make_engine(*grid);
+  lsfdtd_engine* e = make_engine(*grid);
+  const int r = e->init_side();
+  if (r != LSFDTD_OK) {
+    delete e;
+    return r;
+  }
+  *out = e;
   return LSFDTD_OK;
 }
 
@@ -1871,6 +1987,13 @@ int32_t lsfdtd_engine_set_tuning(lsfdtd_engine* eng, int32_t variant, int32_t ti
   eng->tile_y = tile_y;
   eng->planes = planes;
   eng->stages = stages;
+  return LSFDTD_OK;
+}
+
+int32_t lsfdtd_engine_set_clean_split(lsfdtd_engine* eng, int32_t on) {
+  LS_NEED(eng);
+  if (eng->exec[0] || eng->exec[1]) return fail(LSFDTD_EINVAL, "the split must be set before the first graph capture");
+  eng->split_clean = on ? 1 : 0;
   return LSFDTD_OK;
 }
 

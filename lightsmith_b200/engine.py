@@ -606,6 +606,12 @@ class Engine:
         -cycles cycles); before the first graph capture."""
         _abi.check(_abi.lib().lsfdtd_engine_set_wait_budget(self._h, int(cycles)), "lsfdtd_engine_set_wait_budget")
 
+    def set_clean_split(self, on: bool) -> None:
+        """Variant 4: step the grid's clean interior (no CPML, no walls) with its own kernel beside the lean
+        kernel on the rest (on, the default), or every tile with the lean kernel; the same values either way.
+        Before the first graph capture."""
+        _abi.check(_abi.lib().lsfdtd_engine_set_clean_split(self._h, 1 if on else 0), "lsfdtd_engine_set_clean_split")
+
     def set_tuning(self, variant: int, tile_y: int, planes: int, stages: int = 4) -> None:
         """Kernel choice and launch shape (before the first graph capture): variant 0 the in-place H and E
         kernels, 2 their four-node vector form, 1 the fused pass (CTA tile rows 8 or 16, x planes per tile,

@@ -123,6 +123,8 @@ def _main():
     ap.add_argument("--cp-async", action="store_true", help="copy planes with cp.async instead of TMA")
     ap.add_argument("--pml", type=int, default=16, help="CPML cells on every face")
     ap.add_argument("--plan", default=None, help="a plan saved with lightsmith_b200.plan.save, run in FP32")
+    ap.add_argument("--whole", action="store_true",
+                    help="variant 4: step every tile with the lean kernel (no clean-interior kernel)")
     args = ap.parse_args()
     if args.plan:
         from .plan import load
@@ -138,12 +140,14 @@ def _main():
         eng = Engine.from_plan(plan)
     if args.cp_async:
         eng.set_copy_engine(False)
+    if args.whole:
+        eng.set_clean_split(False)
     cells = eng.cells
     alg = cells * 52 + cells_in_cpml(eng.plan) * 32
     shapes = [tuple(int(v) for v in args.shape.split(","))] if args.shape else CANDIDATES
     for sh in shapes:
         ms = time_shape(eng, sh, args.chunks)
-        print(json.dumps({"shape": sh, "fused": eng.fused, "tma": eng.uses_tma, "ms_per_step": ms,
+        print(json.dumps({"shape": sh, "fused": eng.fused, "tma": eng.uses_tma, "whole": args.whole, "ms_per_step": ms,
                           "Gcell_s": cells / ms / 1e6, "alg_GBps": alg / ms / 1e6}), flush=True)
     eng.close()
 

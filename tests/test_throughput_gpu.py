@@ -37,6 +37,36 @@ def test_throughput_case_matches_oracle_at_128():
     np.testing.assert_allclose(gpu32.energy.cpu().numpy()[0], ref.energy[0], rtol=1e-3)
 
 
+# (72, 200, 64) with CPML 8 has no clean interior of whole 32-node z tiles: both engines take the lean kernel
+@pytest.mark.parametrize("shape,pml,interior", [((128, 128, 128), 16, True), ((100, 90, 136), 12, True),
+                                                ((72, 200, 64), 8, False), ((64, 64, 96), 0, True)])
+@pytest.mark.parametrize("precision", ["single", "double"])
+def test_clean_interior_split_gives_the_lean_kernels_values(shape, pml, interior, precision):
+    """Variant 4 with the grid's clean interior stepped by the kernel compiled without region or CPML code (on
+    a second stream, beside the lean kernel on the tiles around it) against the lean kernel on every tile:
+    the same fields and DFT accumulators bit for bit, on grids whose sides are and are not whole tiles,
+    with CPML slabs of several widths and with walls only."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.workloads import throughput_plan
+
+    plan = throughput_plan(shape, pml=pml, max_steps=4000, seed=11, single=precision == "single")
+    split, whole = Engine.from_plan(plan, precision=precision), Engine.from_plan(plan, precision=precision)
+    for e in (split, whole):
+        e.set_tuning(4, 8, 0, 4)
+    whole.set_clean_split(False)
+    assert split.fused and split.uses_tma and whole.fused
+    # one more launch per step where the clean interior has its own kernel
+    assert split.launches_per_chunk() == whole.launches_per_chunk() + (split.stride if interior else 0)
+    for _ in range(4):
+        split.chunk(1, use_graph=True)
+        whole.chunk(1, use_graph=True)
+    assert np.abs(whole.E.cpu().numpy()).max() > 0
+    assert np.array_equal(split.E.cpu().numpy(), whole.E.cpu().numpy())
+    assert np.array_equal(split.H.cpu().numpy(), whole.H.cpu().numpy())
+    for a, b in zip(split.results(0), whole.results(0)):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision,tol", [("double", 1e-9), ("single", 3e-4)])
 def test_bench_kernel_matches_oracle_at_128(precision, tol):
     """The bench's own kernel and launch shape (the lean fused pass, variant 4, x planes chosen per grid, TMA
