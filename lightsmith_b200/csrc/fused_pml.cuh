@@ -111,11 +111,15 @@ __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabIn
 // multiple of 16 bytes). A table-fed TF/SF source's corrections of H (FusedArgs::hc) are added to every H
 // value the tile computes (its own nodes and its halo) before the E half uses them (HC: compiled in only for
 // runs that have such corrections).
+// AX: the axes (bit d for axis d) along which the launch's CTAs may meet CPML slabs or walls; a CTA of a
+// launch without bit d has its nodes, halo nodes and planes inner along axis d, so that axis's slab lookups
+// and terms are compiled out (7: any CTA).
 // CLEAN: every CTA of the launch lies in the clean interior (each of its nodes, halo nodes and x planes,
 // the plane before its segment included, inside [inner_lo, inner_hi) on every axis): the region tests and
 // CPML terms are compiled out, and with them the registers they hold (the lean path's code, though never
 // taken there, costs the interior warps a quarter of their speed)
-template <typename F, int TY, int S, bool UNI, bool ASYNC = false, bool HC = false, bool CLEAN = false>
+template <typename F, int TY, int S, bool UNI, bool ASYNC = false, bool HC = false, bool CLEAN = false,
+          int AX = 7>
 __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 1)
     k_fused_pml(const __grid_constant__ TmaArgs<F> t) {
   static_assert(!CLEAN || (!ASYNC && !HC), "the clean interior pass copies by tensor maps and has no sources");
@@ -161,6 +165,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
   // the slab tables of the tile's rows and columns (halo included)
   for (int e = tid; !CLEAN && e < 2 * (Tab::NY + Tab::NZ); e += NT) {
     const int f = e / (Tab::NY + Tab::NZ), r = e % (Tab::NY + Tab::NZ);
+    if (r < Tab::NY ? !(AX & 2) : !(AX & 4)) continue;  // an axis this launch's CTAs are inner along
     if (r < Tab::NY)
       tab.y[f][r] = f ? slab_info<1>(g.pml[1], 1, y0 - 1 + r) : slab_info<0>(g.pml[1], 1, y0 - 1 + r);
     else
@@ -292,6 +297,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (d == c) continue;
+      if (!(AX >> d & 1)) continue;
       const SlabInfo<R>& sl = d == 0 ? xs_h : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
       if (sl.side < 0) continue;
       const long long q = pml_index(g, sl, d, x);
@@ -359,7 +365,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
 #pragma unroll
       for (int d = 0; d < 3; ++d) pre_h[c][d] = pre_e[c][d] = zero<F>();
     if (!fast) {
-      if (i >= a.inner_lo[0] && i < a.inner_hi[0]) {  // a plane outside the x slabs (most lean planes)
+      if (!(AX & 1) || (i >= a.inner_lo[0] && i < a.inner_hi[0])) {  // a plane outside the x slabs
         xs_h.side = xs_e.side = -1;
         xs_h.st = xs_e.st = 0;
         xs_h.len = xs_e.len = 1;
@@ -372,6 +378,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         const int x[3] = {i, j, k};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
+          if (!(AX >> d & 1)) continue;
           const SlabInfo<R>& sh = d == 0 ? xs_h : (d == 1 ? tab.y[1][ty + 1] : tab.z[1][tx + 1]);
           const SlabInfo<R>& se = d == 0 ? xs_e : (d == 1 ? tab.y[0][ty + 1] : tab.z[0][tx + 1]);
           const int c1 = (d + 1) % 3, c2 = (d + 2) % 3;  // the components with a psi along d
@@ -397,7 +404,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
                           !(col_clean && x_in);
     if constexpr (!ASYNC && !CLEAN) {
       if (row_lean || col_lean) {
-        const SlabInfo<R> xh = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;
+        const SlabInfo<R> xh = fast && (AX & 1) ? slab_info<1>(g.pml[0], 0, i) : xs_h;
         const int yy = row_lean ? 0 : tx + 1, zz = row_lean ? tx + 1 : 0;
         const int x[3] = {i, y0 - 1 + yy, z0 - 1 + zz};
 #pragma unroll
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
           F* dst = tab.hpsi[i & 1][row_lean ? w : 2 + w][tx];
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            if (d == c) continue;
+            if (d == c || !(AX >> d & 1)) continue;
             const SlabInfo<R>& sl = d == 0 ? xh : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
             if (sl.side >= 0) cp_async(dst + d, g.pml[d].psi[1][c][sl.side] + pml_index(g, sl, d, x), true);
           }
@@ -465,13 +472,13 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         F h = h0;
         if (hm >> c & 1u) {
           h = h0 - curl(av[c], bv[c], d1, d2) * g.cH;
-          if (c != 0 && xs_h.side >= 0)
+          if ((AX & 1) && c != 0 && xs_h.side >= 0)
             pml_term<1, UNI>(h, g, xs_h, 0, c, qh[0], d1 == 0 ? av[c] : bv[c], g.cH, pre_h[c][0],
                         st ? a.psiHo[0][c][xs_h.side] : nullptr);
-          if (c != 1 && yh.side >= 0)
+          if ((AX & 2) && c != 1 && yh.side >= 0)
             pml_term<1, UNI>(h, g, yh, 1, c, qh[1], d1 == 1 ? av[c] : bv[c], g.cH, pre_h[c][1],
                         st ? a.psiHo[1][c][yh.side] : nullptr);
-          if (c != 2 && zh.side >= 0)
+          if ((AX & 4) && c != 2 && zh.side >= 0)
             pml_term<1, UNI>(h, g, zh, 2, c, qh[2], d1 == 2 ? av[c] : bv[c], g.cH, pre_h[c][2],
                         st ? a.psiHo[2][c][zh.side] : nullptr);
         }
@@ -516,7 +523,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
         hxc = hx_fast(si, o);
         hyc = hy_fast(si, sn, o);
       } else {
-        SlabInfo<R> xc_h = fast ? slab_info<1>(g.pml[0], 0, i) : xs_h;  // this warp may be fast itself
+        SlabInfo<R> xc_h = fast && (AX & 1) ? slab_info<1>(g.pml[0], 0, i) : xs_h;  // this warp may be fast itself
         if constexpr (!ASYNC) asm volatile("cp.async.wait_all;\n" ::: "memory");
         hxc = h_lean(0, si, sn, i, tx + 1, 0, xc_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][2][tx]);
         hyc = h_lean(1, si, sn, i, tx + 1, 0, xc_h, false, ASYNC ? nullptr : tab.hpsi[i & 1][3][tx]);
@@ -564,13 +571,13 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
           const R cbc = (c == 0 || !multi_cb) ? cb : ro(g.cbE[c] + p);
           F ev = e0 + curl(av[c], bv[c], d1, d2) * cbc;
           if (!fast) {
-            if (c != 0 && xs_e.side >= 0)
+            if ((AX & 1) && c != 0 && xs_e.side >= 0)
               pml_term<0, UNI>(ev, g, xs_e, 0, c, qe[0], d1 == 0 ? av[c] : bv[c], cbc, pre_e[c][0],
                           g.pml[0].psi[0][c][xs_e.side]);
-            if (c != 1 && ye.side >= 0)
+            if ((AX & 2) && c != 1 && ye.side >= 0)
               pml_term<0, UNI>(ev, g, ye, 1, c, qe[1], d1 == 1 ? av[c] : bv[c], cbc, pre_e[c][1],
                           g.pml[1].psi[0][c][ye.side]);
-            if (c != 2 && ze.side >= 0)
+            if ((AX & 4) && c != 2 && ze.side >= 0)
               pml_term<0, UNI>(ev, g, ze, 2, c, qe[2], d1 == 2 ? av[c] : bv[c], cbc, pre_e[c][2],
                           g.pml[2].psi[0][c][ze.side]);
           }

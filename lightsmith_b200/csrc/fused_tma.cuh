@@ -33,7 +33,7 @@ struct CtaBox {
   int x0, x1, seg;
   int first;
 };
-constexpr int kMaxCtaBoxes = 6;
+constexpr int kMaxCtaBoxes = 12;
 struct CtaMap {
   int n;
   CtaBox box[kMaxCtaBoxes];

@@ -340,28 +340,40 @@ struct Engine final : lsfdtd_engine {
     }
     return LSFDTD_OK;
   }
-  template <int TY, int S, bool UNI, bool ASYNC, bool HC, bool CLEAN = false>
+  template <int TY, int S, bool UNI, bool ASYNC, bool HC, bool CLEAN = false, int AX = 7>
   int launch_pml_one(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
     if constexpr (!kComplex) {
       // the clean interior pass reads no slab tables
       constexpr size_t sm = CLEAN ? fused_tma_smem_bytes<F, TY, S>() : fused_pml_smem_bytes<F, TY, S>();
       static bool attr = false;  // per instantiation: the attribute belongs to the kernel, not the engine
       if (!attr) {
-        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN>,
+        LS_CUDA(cudaFuncSetAttribute(k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN, AX>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         attr = true;
       }
-      k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN><<<grid, dim3(32, TY), sm, s>>>(ta);
+      k_fused_pml<F, TY, S, UNI, ASYNC, HC, CLEAN, AX><<<grid, dim3(32, TY), sm, s>>>(ta);
     }
     return LSFDTD_OK;
   }
   // the lean-CPML pass, one instantiation per cell shape (cubic or not), copy engine (cp.async: rows the
   // tensor copies cannot stride) and whether a table-fed source's H corrections are added as it steps (those
   // two with a ring of 4 only)
-  template <int TY, int S, bool ASYNC, bool HC, bool CLEAN = false>
+  template <int TY, int S, bool ASYNC, bool HC, bool CLEAN = false, int AX = 7>
   int launch_pml_kind(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
-    return y.uniform ? launch_pml_one<TY, S, true, ASYNC, HC, CLEAN>(grid, ta, s)
-                     : launch_pml_one<TY, S, false, ASYNC, HC, CLEAN>(grid, ta, s);
+    return y.uniform ? launch_pml_one<TY, S, true, ASYNC, HC, CLEAN, AX>(grid, ta, s)
+                     : launch_pml_one<TY, S, false, ASYNC, HC, CLEAN, AX>(grid, ta, s);
+  }
+  // the kernels of the split lean pass (tile rows 8, ring of 4), per class of CTA box: 0 the clean interior,
+  // 1, 2, 3 the boxes that meet slabs or walls along x, y, z only, 4 the edges and corners (any axis)
+  static constexpr int kClasses = 5;
+  int launch_class(int cls, dim3 g, const TmaArgs<F>& ta, cudaStream_t st) {
+    switch (cls) {
+      case 0: return launch_pml_kind<8, 4, false, false, true, 0>(g, ta, st);
+      case 1: return launch_pml_kind<8, 4, false, false, false, 1>(g, ta, st);
+      case 2: return launch_pml_kind<8, 4, false, false, false, 2>(g, ta, st);
+      case 3: return launch_pml_kind<8, 4, false, false, false, 4>(g, ta, st);
+      default: return launch_pml_kind<8, 4, false, false, false, 7>(g, ta, st);
+    }
   }
   template <int TY, int S>
   int launch_pml(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s) {
@@ -374,10 +386,9 @@ struct Engine final : lsfdtd_engine {
                          : launch_pml_kind<TY, 4, true, false>(grid, ta, s);
   }
   // kind 0: the fused pass over the grid, 1: over the interior box of the split step, 2: with lean CPML terms
-  // (clean: its clean interior CTAs)
   template <int TY, int S>
-  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s, int kind, bool clean) {
-    if (kind == 2) return clean ? launch_pml_kind<TY, S, false, false, true>(grid, ta, s) : launch_pml<TY, S>(grid, ta, s);
+  int launch_tma(dim3 grid, const TmaArgs<F>& ta, cudaStream_t s, int kind) {
+    if (kind == 2) return launch_pml<TY, S>(grid, ta, s);
     return kind == 1 ? launch_tma_box<TY, S, true>(grid, ta, s) : launch_tma_box<TY, S, false>(grid, ta, s);
   }
   template <int TY, int S>
@@ -413,7 +424,7 @@ struct Engine final : lsfdtd_engine {
   }
   // whether the lean pass runs as two kernels (clean interior and the rest)
   bool lean_split() const {
-    if (kComplex || !tma_ok || !split_clean || !side || !lean_ok()) return false;
+    if (kComplex || !tma_ok || !split_clean || !side || !lean_ok() || tile_y != 8 || stages != 4) return false;
     for (auto& tb : tables)
       if (tb.has[1] && tb.hc.n > 0) return false;
     int zc0, zc1, yc0, yc1, xc0, xc1;
@@ -439,29 +450,46 @@ struct Engine final : lsfdtd_engine {
     total += (long long)(tz1 - tz0) * (ty1 - ty0) * ((len + sg - 1) / sg);
   }
 
-  // the lean pass's CTAs (tiles of 32 z nodes by `rows` y nodes, segments of seg x planes): with may_split
-  // and a clean interior of whole tiles, that interior in `clean` and the six boxes around it in `rest`
-  // (true); else all of them in `rest`. A clean CTA's nodes and halo nodes (row y0 - 1, column z0 - 1) and
-  // its x planes, the plane before its segment included, are inner on every axis
-  bool lean_maps(int rows, int seg, bool may_split, CtaMap* clean, long long* n_clean, CtaMap* rest,
-                 long long* n_rest) const {
+  // the lean pass's CTAs (tiles of 32 z nodes by `rows` y nodes, segments of seg x planes) per class (see
+  // launch_class): with may_split and a clean interior of whole tiles, that interior in maps[0], the boxes
+  // beside it that are inner along all axes but x, y or z in maps[1], [2], [3], and the edges and corners in
+  // maps[4] (true); else every CTA in maps[4]. A clean CTA's nodes and halo nodes (row y0 - 1, column z0 - 1)
+  // and its x planes, the plane before its segment included, are inner on every axis
+  bool lean_plan(int rows, int seg, bool may_split, CtaMap* maps, long long* n) const {
     const int n0 = desc.shape[0], nz = (desc.shape[2] + 31) / 32, ny = (desc.shape[1] + rows - 1) / rows;
-    clean->n = rest->n = 0;
-    *n_clean = *n_rest = 0;
+    for (int c = 0; c < kClasses; ++c) {
+      maps[c].n = 0;
+      n[c] = 0;
+    }
     int zc0, zc1, yc0, yc1, xc0, xc1;
     clean_box(rows, &zc0, &zc1, &yc0, &yc1, &xc0, &xc1);
     if (!may_split || zc1 <= zc0 || yc1 <= yc0 || xc1 <= xc0) {
-      add_cta_box(*rest, *n_rest, 0, nz, 0, ny, 0, n0, seg);
+      add_cta_box(maps[4], n[4], 0, nz, 0, ny, 0, n0, seg);
       return false;
     }
-    add_cta_box(*clean, *n_clean, zc0, zc1, yc0, yc1, xc0, xc1, seg);
-    add_cta_box(*rest, *n_rest, 0, nz, 0, ny, 0, xc0, seg);
-    add_cta_box(*rest, *n_rest, 0, nz, 0, ny, xc1, n0, seg);
-    add_cta_box(*rest, *n_rest, 0, nz, 0, yc0, xc0, xc1, seg);
-    add_cta_box(*rest, *n_rest, 0, nz, yc1, ny, xc0, xc1, seg);
-    add_cta_box(*rest, *n_rest, 0, zc0, yc0, yc1, xc0, xc1, seg);
-    add_cta_box(*rest, *n_rest, zc1, nz, yc0, yc1, xc0, xc1, seg);
+    const int xr[2][2] = {{0, xc0}, {xc1, n0}}, yr[2][2] = {{0, yc0}, {yc1, ny}}, zr[2][2] = {{0, zc0}, {zc1, nz}};
+    add_cta_box(maps[0], n[0], zc0, zc1, yc0, yc1, xc0, xc1, seg);
+    for (int s = 0; s < 2; ++s) {
+      add_cta_box(maps[1], n[1], zc0, zc1, yc0, yc1, xr[s][0], xr[s][1], seg);
+      add_cta_box(maps[2], n[2], zc0, zc1, yr[s][0], yr[s][1], xc0, xc1, seg);
+      add_cta_box(maps[3], n[3], zr[s][0], zr[s][1], yc0, yc1, xc0, xc1, seg);
+    }
+    for (int s = 0; s < 2; ++s)
+      for (int t = 0; t < 2; ++t) {
+        add_cta_box(maps[4], n[4], 0, nz, yr[t][0], yr[t][1], xr[s][0], xr[s][1], seg);
+        add_cta_box(maps[4], n[4], zr[t][0], zr[t][1], yc0, yc1, xr[s][0], xr[s][1], seg);
+        add_cta_box(maps[4], n[4], zr[t][0], zr[t][1], yr[s][0], yr[s][1], xc0, xc1, seg);
+      }
     return true;
+  }
+  // launches of the lean pass per step
+  int lean_launches() const {
+    CtaMap maps[kClasses];
+    long long n[kClasses];
+    if (!lean_plan(8, 32, lean_split(), maps, n)) return 1;
+    int k = 0;
+    for (int c = 0; c < kClasses; ++c) k += n[c] > 0;
+    return k;
   }
 
   // nodes [lo, hi) per axis stepped for every component and outside every CPML slab
@@ -596,19 +624,19 @@ struct Engine final : lsfdtd_engine {
     if constexpr (!kComplex) {
       // the fused passes by tensor copies, with the deepest ring up to the requested depth that fits the
       // device's shared memory per CTA
-      auto launch_ring = [&](const TmaArgs<F>& ta, dim3 g, cudaStream_t st, bool clean) -> int {
+      auto launch_ring = [&](const TmaArgs<F>& ta, dim3 g, cudaStream_t st) -> int {
         int smax = 0, dev = 0;
         LS_CUDA(cudaGetDevice(&dev));
         LS_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         auto fits = [&](size_t b) { return b <= (size_t)smax; };
         if (tile_y == 16) {
-          if (stages >= 8 && fits(tma_smem<16, 8>(kind))) return launch_tma<16, 8>(g, ta, st, kind, clean);
-          if (stages >= 6 && fits(tma_smem<16, 6>(kind))) return launch_tma<16, 6>(g, ta, st, kind, clean);
-          return launch_tma<16, 4>(g, ta, st, kind, clean);
+          if (stages >= 8 && fits(tma_smem<16, 8>(kind))) return launch_tma<16, 8>(g, ta, st, kind);
+          if (stages >= 6 && fits(tma_smem<16, 6>(kind))) return launch_tma<16, 6>(g, ta, st, kind);
+          return launch_tma<16, 4>(g, ta, st, kind);
         }
-        if (stages >= 8 && fits(tma_smem<8, 8>(kind))) return launch_tma<8, 8>(g, ta, st, kind, clean);
-        if (stages >= 6 && fits(tma_smem<8, 6>(kind))) return launch_tma<8, 6>(g, ta, st, kind, clean);
-        return launch_tma<8, 4>(g, ta, st, kind, clean);
+        if (stages >= 8 && fits(tma_smem<8, 8>(kind))) return launch_tma<8, 8>(g, ta, st, kind);
+        if (stages >= 6 && fits(tma_smem<8, 6>(kind))) return launch_tma<8, 6>(g, ta, st, kind);
+        return launch_tma<8, 4>(g, ta, st, kind);
       };
       TmaArgs<F> ta;
       ta.f = fa;
@@ -622,31 +650,35 @@ struct Engine final : lsfdtd_engine {
         ta.mC = mapC;
       }
       if (kind == 2) {
-        // the lean pass: the clean interior's CTAs by the clean kernel and the others by the lean one, on
-        // two streams, where the grid has such an interior; else every CTA by the lean kernel
-        CtaMap clean{}, rest{};
-        long long n_clean = 0, n_rest = 0;
-        const bool two = lean_maps(rows, fa.seg, lean_split(), &clean, &n_clean, &rest, &n_rest);
-        if (two) {
+        // the lean pass: where the grid has a clean interior, one kernel per class of CTA box (launch_class),
+        // the interior's on the caller's stream and the others one after another on the second stream; else
+        // every CTA by the lean kernel
+        CtaMap maps[kClasses];
+        long long n[kClasses];
+        const bool two = lean_plan(rows, fa.seg, lean_split(), maps, n);
+        if (!two) {
+          ta.map = maps[4];
+          const dim3 g((unsigned)n[4]);
+          const int r = tma_ok ? launch_ring(ta, g, s)
+                               : (tile_y == 16 ? launch_pml_async<16>(g, ta, s) : launch_pml_async<8>(g, ta, s));
+          if (r != LSFDTD_OK) return r;
+        } else {
           LS_CUDA(cudaEventRecord(ev_fork, s));
           LS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
-        }
-        ta.map = rest;
-        const dim3 g_rest((unsigned)n_rest);
-        int r = LSFDTD_OK;
-        if (tma_ok) r = launch_ring(ta, g_rest, two ? side : s, false);
-        else r = tile_y == 16 ? launch_pml_async<16>(g_rest, ta, s) : launch_pml_async<8>(g_rest, ta, s);
-        if (r != LSFDTD_OK) return r;
-        if (two) {
-          LS_LAUNCHED();
-          ta.map = clean;
-          LS_TRY(launch_ring(ta, dim3((unsigned)n_clean), s, true));
+          for (int c = kClasses - 1; c >= 1; --c) {
+            if (n[c] == 0) continue;
+            ta.map = maps[c];
+            LS_TRY(launch_class(c, dim3((unsigned)n[c]), ta, side));
+            LS_LAUNCHED();
+          }
+          ta.map = maps[0];
+          LS_TRY(launch_class(0, dim3((unsigned)n[0]), ta, s));
           LS_LAUNCHED();
           LS_CUDA(cudaEventRecord(ev_join, side));
           LS_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
         }
       } else if (tma_ok) {
-        LS_TRY(launch_ring(ta, grid, s, false));
+        LS_TRY(launch_ring(ta, grid, s));
         if (split) {
           LS_LAUNCHED();
           const unsigned blocks = (unsigned)cdiv((long long)sb.total, 256);
@@ -1491,7 +1523,7 @@ struct Engine final : lsfdtd_engine {
       int lo[3], hi[3];
       ShellBoxes sb{};
       // fused pass (interior box, shell H and E; or the lean pass's clean interior and the rest), counter
-      per_step = (split_box(lo, hi, &sb) ? 3 : (lean_split() ? 2 : 1)) + 1;
+      per_step = (split_box(lo, hi, &sb) ? 3 : (lean_ok() ? lean_launches() : 1)) + 1;
     }
     int nper = desc.periodic[0] + desc.periodic[1] + desc.periodic[2];
     per_step += 2 * nper;

@@ -42,8 +42,9 @@ def test_throughput_case_matches_oracle_at_128():
                                                 ((72, 200, 64), 8, False), ((64, 64, 96), 0, True)])
 @pytest.mark.parametrize("precision", ["single", "double"])
 def test_clean_interior_split_gives_the_lean_kernels_values(shape, pml, interior, precision):
-    """Variant 4 with the grid's clean interior stepped by the kernel compiled without region or CPML code (on
-    a second stream, beside the lean kernel on the tiles around it) against the lean kernel on every tile:
+    """Variant 4 with one kernel per class of CTA box (the clean interior compiled without region or CPML
+    code, the boxes beside it with one axis's slab code each, the edges and corners with all of it; all but
+    the interior's on a second stream) against the lean kernel on every tile:
     the same fields and DFT accumulators bit for bit, on grids whose sides are and are not whole tiles,
     with CPML slabs of several widths and with walls only."""
     from lightsmith_b200.engine import Engine
@@ -55,8 +56,9 @@ def test_clean_interior_split_gives_the_lean_kernels_values(shape, pml, interior
         e.set_tuning(4, 8, 0, 4)
     whole.set_clean_split(False)
     assert split.fused and split.uses_tma and whole.fused
-    # one more launch per step where the clean interior has its own kernel
-    assert split.launches_per_chunk() == whole.launches_per_chunk() + (split.stride if interior else 0)
+    # where the grid has a clean interior the step takes five launches, one per class of CTA box (the clean
+    # interior, the boxes beside it along x, y and z, the edges and corners), in place of one
+    assert split.launches_per_chunk() == whole.launches_per_chunk() + (4 * split.stride if interior else 0)
     for _ in range(4):
         split.chunk(1, use_graph=True)
         whole.chunk(1, use_graph=True)
