@@ -74,13 +74,14 @@ constexpr size_t fused_pml_smem_bytes() {
   return fused_tma_smem_bytes<F, TY, S>() + (sizeof(PmlTables<F, TY>) + 15) / 16 * 16;  // tables after kUsed
 }
 
-// index of node x in the psi slab of axis d described by si
+// index of node x in the psi slab of axis d described by si, in 32-bit arithmetic: the engine takes the lean
+// pass only where every slab has fewer than 2^31 nodes
 template <typename F>
-__device__ __forceinline__ long long pml_index(const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
-                                               int d, const int* x) {
-  if (d == 0) return ((long long)(x[0] - si.st) * g.n[1] + x[1]) * g.n[2] + x[2];
-  if (d == 1) return ((long long)x[0] * si.len + (x[1] - si.st)) * g.n[2] + x[2];
-  return ((long long)x[0] * g.n[1] + x[1]) * si.len + (x[2] - si.st);
+__device__ __forceinline__ int pml_index(const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si, int d,
+                                         const int* x) {
+  if (d == 0) return ((x[0] - si.st) * g.n[1] + x[1]) * g.n[2] + x[2];
+  if (d == 1) return (x[0] * si.len + (x[1] - si.st)) * g.n[2] + x[2];
+  return (x[0] * g.n[1] + x[1]) * si.len + (x[2] - si.st);
 }
 
 // the CPML term along axis d of a value v of field FLD, component c, at psi index q, from psi_prev (the node's
@@ -88,7 +89,7 @@ __device__ __forceinline__ long long pml_index(const YeeArgs<F>& g, const SlabIn
 // grid's uniform flag, known when the kernel is compiled)
 template <int FLD, bool UNI, typename F>
 __device__ __forceinline__ void pml_term(F& v, const YeeArgs<F>& g, const SlabInfo<typename real_of<F>::type>& si,
-                                         int d, int c, long long q, F der, typename real_of<F>::type scale,
+                                         int d, int c, int q, F der, typename real_of<F>::type scale,
                                          F psi_prev, F* psi_out) {
   using R = typename real_of<F>::type;
   const int d1 = (c + 1) % 3;
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
       if (!(AX >> d & 1)) continue;
       const SlabInfo<R>& sl = d == 0 ? xs_h : (d == 1 ? tab.y[1][yy] : tab.z[1][zz]);
       if (sl.side < 0) continue;
-      const long long q = pml_index(g, sl, d, x);
+      const int q = pml_index(g, sl, d, x);
       const F prev = pre ? pre[d] : ro(g.pml[d].psi[1][c][sl.side] + q);
       F* pout = store ? a.psiHo[d][c][sl.side] : nullptr;
       pml_term<1, UNI>(h, g, sl, d, c, q, d == d1 ? av : bv, g.cH, prev, pout);
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(32 * TY, sizeof(F) == 4 ? (TY == 8 ? 4 : 2) : 
     // copies, so that their latency overlaps the wait and each other: [component][axis], with the psi index
     // per axis (H, E)
     F pre_h[3][3], pre_e[3][3];
-    long long qh[3] = {0, 0, 0}, qe[3] = {0, 0, 0};
+    int qh[3] = {0, 0, 0}, qe[3] = {0, 0, 0};
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll

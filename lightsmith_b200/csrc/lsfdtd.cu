@@ -402,6 +402,12 @@ struct Engine final : lsfdtd_engine {
     if (variant != 4 || kComplex) return false;
     for (int d = 0; d < 3; ++d) {
       if (!y.pml[d].on) continue;
+      // its psi slabs indexed in 32-bit arithmetic: fewer than 2^31 nodes each
+      const long long face = (long long)desc.shape[(d + 1) % 3] * desc.shape[(d + 2) % 3];
+      for (int f = 0; f < 2; ++f)
+        for (int c = 0; c < 3; ++c)
+          for (int sd = 0; sd < 2; ++sd)
+            if ((long long)y.pml[d].len[f][c][sd] * face >= (1LL << 31)) return false;
       for (int f = 0; f < 2; ++f) {
         const int c = (d + 1) % 3;
         const int lo_end = y.pml[d].start[f][c][0] + y.pml[d].len[f][c][0];
