@@ -388,10 +388,13 @@ typedef struct lsfdtd_batch lsfdtd_batch;
 /* a batch of n engines of one precision; last[i]: the step count run i stops at (at most what its source
  * waveform covers). The runs are spread over the kernel's CTAs longest first. */
 int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out);
-/* the same with the launch's shape: cluster_ctas CTAs of 512 threads per run (1 to 16; above 8 the GPU must
- * allow non-portable clusters) and at most max_clusters clusters in flight (0: as many as fit). Fewer clusters
- * step fewer runs at a time, whose state then stays in L2 through the steps of a launch; the default shape is
- * 8 CTAs and as many clusters as fit */
+/* the same with the launch's shape: cluster_ctas CTAs of 512 threads per run and at most max_clusters runs in
+ * flight (0: as many as fit). 1 to 16 CTAs: a thread-block cluster per run (above 8 the GPU must allow
+ * non-portable clusters). 17 to 4096: a group of CTAs per run that meet at barriers in global memory, in a
+ * cooperative launch (every CTA resident at once); a barrier wait is bounded, and a CTA that gives up sets
+ * its run's status word to 1 (lsfdtd_engine_status: LSFDTD_ETIMEOUT) and the launch ends. Fewer, larger
+ * groups step fewer runs at a time, whose state then stays in L2 through the steps of a launch. 0: the
+ * default, groups of half the CTAs resident at once (two runs in flight), which lsfdtd_batch_create takes */
 int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, const int64_t* last,
                                    int32_t cluster_ctas, int32_t max_clusters, lsfdtd_batch** out);
 int32_t lsfdtd_batch_destroy(lsfdtd_batch* batch);

@@ -19,9 +19,11 @@ from . import _abi
 class BlochBatch:
     """The runs of ``engines`` (complex fields, periodic x and y, CPML along z, one Bloch column source),
     each to run until its step count reaches ``last`` (an int for all, or one per engine). ``cluster_ctas``:
-    CTAs per run (a thread-block cluster, 1 to 16); ``max_clusters``: clusters in flight (0: as many as fit)."""
+    CTAs per run (1 to 16: a thread-block cluster; more: a group meeting at barriers in global memory, in a
+    cooperative launch; 0: groups of half the CTAs resident at once); ``max_clusters``: runs in flight (0: as
+    many as fit)."""
 
-    def __init__(self, engines, last, cluster_ctas: int = 8, max_clusters: int = 0):
+    def __init__(self, engines, last, cluster_ctas: int = 0, max_clusters: int = 0):
         import torch
 
         self.engines = list(engines)

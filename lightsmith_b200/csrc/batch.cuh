@@ -28,6 +28,12 @@
 // shared between threads. Every CTA of a cluster walks the same run list and step counts, so each reaches
 // every barrier. The run's step counter is the engine's own, so an engine that took part in a batch is in the
 // state its own steps would have left.
+//
+// GROUP: the CTAs of a run are a group of any size (a cooperative launch keeps every CTA resident) that meet
+// at a barrier in global memory (group_barrier) instead of the cluster's. Few runs then advance at once, each
+// on many SMs, and the runs in flight stay in L2 from one step to the next. A barrier wait is bounded: a CTA
+// that gives up sets the run's status word to 1 and returns, and the group's other CTAs give up at their next
+// barrier.
 #pragma once
 
 #include "common.cuh"
@@ -45,6 +51,37 @@ constexpr int kBatchCluster = 8;  // CTAs per run by default (the portable clust
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// polls of a group barrier's counter before a CTA gives up (each after a 256 ns sleep: a few seconds, where a
+// barrier of the batched sweep takes microseconds)
+constexpr long long kGroupSpinLimit = 8LL << 20;
+
+// every thread of the ncta CTAs counting on `count` arrives (one 64-bit counter per group, zero at the launch's
+// start, bumped once per CTA and barrier: the barrier's generation is ticket / ncta); global writes before it
+// are visible after it. False when this CTA gave up waiting (then on every thread of the CTA).
+__device__ __forceinline__ bool group_barrier(unsigned long long* count, unsigned ncta) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // release: the CTA's writes (ordered before thread 0's by the CTA barrier) at GPU scope
+    const unsigned long long ticket = atomicAdd(count, 1ull);
+    const unsigned long long target = (ticket / ncta + 1) * ncta;
+    bool good = false;
+    for (long long spin = 0; spin < kGroupSpinLimit; ++spin) {
+      unsigned long long v;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(count) : "memory");
+      if (v >= target) {
+        good = true;
+        break;
+      }
+      __nanosleep(256);
+    }
+    __threadfence();
+    ok = good ? 1 : 0;
+  }
+  __syncthreads();
+  return ok != 0;
 }
 
 // unsigned division by a run constant with one multiply-high (Granlund and Montgomery, "Division by
@@ -137,15 +174,35 @@ __device__ __forceinline__ void batch_sample_point(const MonArgs<F>& m, long lon
 // complex64: two CTAs per SM (64 registers per thread), for twice the nodes in flight
 // launched with a cluster dimension (CTAs per run) set at launch: the CTA's rank in its cluster, the
 // cluster's index in the grid and its size come from the special registers
-template <typename F>
+// (GROUP: CTAs blockIdx.x / gsize share a run list; gbar holds each group's barrier counter)
+template <typename F, bool GROUP>
 __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
-    k_bloch_batch(const BlochRun<F>* runs, const int* order, const int* first, int steps) {
+    k_bloch_batch(const BlochRun<F>* runs, const int* order, const int* first, int steps, int gsize,
+                  unsigned long long* gbar) {
   using R = typename real_of<F>::type;
   __shared__ BlochRun<F> r;
   unsigned cl, rank, ncta;
-  asm("mov.u32 %0, %%clusterid.x;" : "=r"(cl));
-  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+  if constexpr (GROUP) {
+    cl = blockIdx.x / (unsigned)gsize;
+    rank = blockIdx.x % (unsigned)gsize;
+    ncta = (unsigned)gsize;
+  } else {
+    asm("mov.u32 %0, %%clusterid.x;" : "=r"(cl));
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+  }
+  // the barrier between phases; false: this CTA gave up waiting (a group barrier), the run's status word is
+  // set and the CTA returns
+  auto sync = [&]() -> bool {
+    if constexpr (GROUP) {
+      if (group_barrier(gbar + 16 * cl, ncta)) return true;
+      if (threadIdx.x == 0) atomicExch(r.status, 1);
+      return false;
+    } else {
+      cluster_barrier();
+      return true;
+    }
+  };
   const unsigned t0 = rank * blockDim.x + threadIdx.x, tstride = ncta * blockDim.x;
   for (int q = first[cl]; q < first[cl + 1]; ++q) {
     // the run's descriptor into each CTA's shared memory (read by every thread at every node)
@@ -167,7 +224,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     // a run that turned non-finite in an earlier launch is skipped (the word was written before this launch)
     long long n_end = *reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite ? n : min(n + (long long)steps, r.last);
     bool bad = false;  // this thread's E values of the run: any non-finite
-    cluster_barrier();  // every thread has read the counter
+    if (!sync()) return;  // every thread has read the counter
     if (n < n_end) {
       // E's high ghosts as lightsmith refreshes them before each H update (x = n0 - 1 from x = 1, then
       // y = n1 - 1 from y = 1, and the corner), for the cell and the column: the E phase of a launch's last
@@ -198,7 +255,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           }
         }
       }
-      cluster_barrier();
+      if (!sync()) return;
     }
 #pragma unroll 1
     for (; n < n_end; ++n) {
@@ -285,7 +342,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           }
         }
       }
-      cluster_barrier();
+      if (!sync()) return;
       // ---- E phase ----
       const R w_src = r.wave[n];
       for (unsigned w = t0; w < n_work; w += tstride) {
@@ -377,7 +434,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
         }
       }
       if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(r.status, kBatchNonFinite);
-      cluster_barrier();
+      if (!sync()) return;
       if (*reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite) {  // every CTA reads it after the barrier
         n_end = n + 1;
         break;
@@ -404,7 +461,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           }
           if (y == 1) g.E[c][x * s0 + (long long)(n1 - 1) * s1 + z] = e * r.gph[1][1];
         }
-        cluster_barrier();
+        if (!sync()) return;
       }
       // ---- DFT sample after every dft_stride steps ----
       if ((n + 1) % r.stride == 0) {
@@ -412,11 +469,11 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           const MonArgs<F>& mon = r.mon[m];
           for (long long i = t0; i < mon.ne + mon.nh; i += tstride) batch_sample_point(mon, i, n + 1);
         }
-        cluster_barrier();
+        if (!sync()) return;
       }
     }
     if (rank == 0 && threadIdx.x == 0) *r.nstep = n_end;
-    cluster_barrier();  // the counter is written and every CTA is done with the descriptor
+    if (!sync()) return;  // the counter is written and every CTA is done with the descriptor
   }
 }
 

@@ -1562,20 +1562,31 @@ struct BatchImpl {
   std::vector<unsigned char> descs;  // n * run_bytes
   std::vector<int> order, first;     // runs of CTA b: order[first[b] .. first[b + 1])
   int ctas = 0;
-  int cluster = kBatchCluster;  // CTAs per run (cluster size)
+  int cluster = kBatchCluster;  // CTAs per run (cluster size, or group size)
+  bool group = false;           // more than 16 CTAs per run: a group with barriers in global memory
+  int groups = 0;
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
-  size_t off_order = 0, off_first = 0, need = 0;
+  size_t off_order = 0, off_first = 0, off_bar = 0, need = 0;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   int graph_steps = -1;
 };
 
 // clusters of `cl` CTAs of the persistent kernel that fit on the device at once (clusters above the
-// portable 8 CTAs are allowed on the kernel first)
+// portable 8 CTAs are allowed on the kernel first); above 16 CTAs, groups of `cl` CTAs of the cooperative form
 template <typename F>
 int batch_max_clusters(int cl, int* out) {
-  if (cl > 8) LS_CUDA(cudaFuncSetAttribute(k_bloch_batch<F>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  if (cl > 16) {
+    int per_sm = 0, dev = 0, sms = 0;
+    LS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bloch_batch<F, true>, kBatchThreads, 0));
+    LS_CUDA(cudaGetDevice(&dev));
+    LS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *out = per_sm * sms / cl;
+    if (*out < 1) return fail(LSFDTD_EUNSUPPORTED, "batch: a group of that many CTAs does not fit the device at once");
+    return LSFDTD_OK;
+  }
+  if (cl > 8) LS_CUDA(cudaFuncSetAttribute(k_bloch_batch<F, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cl, 1, 1);
   cfg.blockDim = dim3(kBatchThreads, 1, 1);
@@ -1586,7 +1597,7 @@ int batch_max_clusters(int cl, int* out) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaOccupancyMaxActiveClusters(out, k_bloch_batch<F>, &cfg);
+  const cudaError_t e = cudaOccupancyMaxActiveClusters(out, k_bloch_batch<F, false>, &cfg);
   if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("batch: cluster occupancy: ") + cudaGetErrorString(e));
   if (*out < 1) return fail(LSFDTD_EUNSUPPORTED, "batch: no cluster of the persistent kernel fits the device");
   return LSFDTD_OK;
@@ -1598,17 +1609,27 @@ int batch_launch(const BatchImpl& b, int steps, cudaStream_t s) {
   const int* order = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_order);
   const int* first = reinterpret_cast<const int*>(static_cast<const char*>(b.scratch) + b.off_first);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(b.ctas, 1, 1);  // whole clusters
+  cfg.gridDim = dim3(b.ctas, 1, 1);  // whole clusters or groups
   cfg.blockDim = dim3(kBatchThreads, 1, 1);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = b.cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  LS_CUDA(cudaLaunchKernelEx(&cfg, k_bloch_batch<F>, runs, order, first, steps));
+  if (b.group) {
+    // the groups' barrier counters start at zero in every launch; every CTA resident at once
+    auto* bar = reinterpret_cast<unsigned long long*>(static_cast<char*>(b.scratch) + b.off_bar);
+    LS_CUDA(cudaMemsetAsync(bar, 0, (size_t)b.groups * 128, s));
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    LS_CUDA(cudaLaunchKernelEx(&cfg, k_bloch_batch<F, true>, runs, order, first, steps, b.cluster, bar));
+  } else {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = b.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    LS_CUDA(cudaLaunchKernelEx(&cfg, k_bloch_batch<F, false>, runs, order, first, steps, b.cluster,
+                               (unsigned long long*)nullptr));
+  }
   LS_LAUNCHED();
   return LSFDTD_OK;
 }
@@ -2040,14 +2061,15 @@ int64_t lsfdtd_engine_steps(const lsfdtd_engine* eng) { return eng ? eng->n_host
 int64_t lsfdtd_engine_launches_per_chunk(const lsfdtd_engine* eng) { return eng ? eng->launches_per_chunk() : -1; }
 
 int32_t lsfdtd_batch_create(lsfdtd_engine* const* engines, int32_t n, const int64_t* last, lsfdtd_batch** out) {
-  return lsfdtd_batch_create_shaped(engines, n, last, kBatchCluster, 0, out);
+  return lsfdtd_batch_create_shaped(engines, n, last, 0, 0, out);
 }
 
 int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, const int64_t* last,
                                    int32_t cluster_ctas, int32_t max_clusters, lsfdtd_batch** out) {
   LS_NEED(engines && last && out && n > 0);
-  if (cluster_ctas < 1 || cluster_ctas > 16 || max_clusters < 0)
-    return fail(LSFDTD_EINVAL, "batch: 1 to 16 CTAs per cluster, a non-negative cluster limit");
+  if (cluster_ctas < 0 || cluster_ctas > 4096 || max_clusters < 0)
+    return fail(LSFDTD_EINVAL, "batch: 1 to 16 CTAs per cluster (or up to 4096 per group, 0: the default), a "
+                               "non-negative limit");
   *out = nullptr;
   auto b = std::make_unique<lsfdtd_batch>();
   b->precision = engines[0] ? engines[0]->desc.precision : LSFDTD_F32;
@@ -2064,6 +2086,21 @@ int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, con
     b->engines.push_back(e);
     b->last.push_back(last[i]);
   }
+  // the default: groups of half the CTAs resident at once, two runs in flight (measured on B200 over 96
+  // metasurface runs of 30-60 x 30-60 x 200 cells: 30.7 Gcell-updates/s, against 29.4 with four groups and
+  // 26.9 with clusters of 8 CTAs; the two runs in flight stay in L2, 90 % of sectors hit)
+  if (cluster_ctas == 0) {
+    int per_sm = 0, dev = 0, sms = 0;
+    const cudaError_t e = b->precision == LSFDTD_F32
+                              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bloch_batch<cplx<float>, true>,
+                                                                              kBatchThreads, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bloch_batch<cplx<double>, true>,
+                                                                              kBatchThreads, 0);
+    if (e != cudaSuccess) return fail(LSFDTD_ECUDA, std::string("batch: occupancy: ") + cudaGetErrorString(e));
+    LS_CUDA(cudaGetDevice(&dev));
+    LS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cluster_ctas = std::max(17, per_sm * sms / 2);
+  }
   // one wave of clusters; the runs longest first, each to the cluster with the least work so far
   int clusters = 0;
   LS_TRY(b->precision == LSFDTD_F32 ? batch_max_clusters<cplx<float>>(cluster_ctas, &clusters)
@@ -2071,6 +2108,8 @@ int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, con
   clusters = std::max(1, std::min<int>(n, clusters));
   if (max_clusters > 0) clusters = std::min(clusters, (int)max_clusters);
   b->cluster = cluster_ctas;
+  b->group = cluster_ctas > 16;
+  b->groups = clusters;
   b->ctas = clusters * cluster_ctas;
   for (int32_t i = 0; i < n; ++i) {
     const auto& d = b->engines[i]->desc;
@@ -2100,7 +2139,8 @@ int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, con
   auto up = [](size_t x) { return (x + 255) / 256 * 256; };
   b->off_order = up(b->descs.size());
   b->off_first = b->off_order + up(b->order.size() * sizeof(int));
-  b->need = b->off_first + up(b->first.size() * sizeof(int));
+  b->off_bar = b->off_first + up(b->first.size() * sizeof(int));
+  b->need = b->off_bar + up((size_t)clusters * 128);  // a 128-byte line per group's barrier counter
   *out = b.release();
   return LSFDTD_OK;
 }

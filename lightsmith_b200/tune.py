@@ -78,7 +78,9 @@ def best_shape(eng, candidates=CANDIDATES, path: str | None = None):
     return best
 
 
-BATCH_SHAPES = [(8, 0), (4, 0), (16, 0)]  # (CTAs per run, clusters in flight; 0: as many as fit)
+# (CTAs per run, runs in flight; 0: as many as fit): clusters of 4, 8 or 16 CTAs, groups of 37 or 74 CTAs, and
+# the default (0: groups of half the resident CTAs)
+BATCH_SHAPES = [(0, 0), (8, 0), (4, 0), (16, 0), (37, 0), (74, 0)]
 
 
 def tune_batch(engines, last, shapes=BATCH_SHAPES, steps: int = 30, launches: int = 2):
@@ -106,7 +108,7 @@ def tune_batch(engines, last, shapes=BATCH_SHAPES, steps: int = 30, launches: in
         moved = sum(c * (e.n_host - n) for c, e, n in zip(cells, engines, before))
         res[(cl, mx)] = moved / max(t0.elapsed_time(t1), 1e-9) / 1e6
         b.close()
-    best = max(res, key=res.get) if res else (8, 0)
+    best = max(res, key=res.get) if res else (0, 0)
     return best, res
 
 

@@ -56,15 +56,18 @@ def _small_runs(precision, n=5, steps=240):
     return plans
 
 
+# launch shapes: the default (groups of half the resident CTAs), clusters of 8 CTAs per run (as many as fit),
+# and groups of 24 CTAs per run (two in flight) that meet at barriers in global memory
+@pytest.mark.parametrize("shape", [(0, 0), (8, 0), (24, 2)])
 @pytest.mark.parametrize("precision", ["double", "single"])
-def test_batch_equals_sequential_runs(precision):
+def test_batch_equals_sequential_runs(precision, shape):
     from lightsmith_b200.batch import BlochBatch
     from lightsmith_b200.engine import Engine
 
     plans = _small_runs(precision)
     lasts = [(200 // p["stride"]) * p["stride"] for p in plans]  # whole chunks, uneven per run
     batched = [Engine.from_plan(p, precision=precision) for p in plans]
-    batch = BlochBatch(batched, lasts)
+    batch = BlochBatch(batched, lasts, cluster_ctas=shape[0], max_clusters=shape[1])
     batch.run_to_end(steps_per_launch=64)
     tol = SAME[precision]
     for p, eb, last in zip(plans, batched, lasts):
