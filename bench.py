@@ -52,12 +52,13 @@ def _args():
     ap.add_argument("--planes", type=int, default=0, help="fused pass: x planes per CTA (0: chosen per grid)")
     ap.add_argument("--stages", type=int, default=4, help="fused pass: x planes in the copy ring")
     ap.add_argument("--workload", default="throughput", choices=["throughput", "sweep", "adjoint", "clusters",
-                                                                 "sphere"],
+                                                                 "sphere", "setup"],
                     help="sweep: the batched oblique-incidence sweep (96 Bloch-periodic runs) against the same "
                          "runs one after another; adjoint: the slab device's gradient against its forward run; "
                          "clusters: forward + gradient over dispersive sphere clusters, with FP64 errors; sphere: "
                          "the whole 129^3 dispersive-sphere solve from lightsmith's own plan, with its cross "
-                         "sections against lightsmith's FP64 CPU solve")
+                         "sections against lightsmith's FP64 CPU solve; setup: that sphere's meshing by lightsmith "
+                         "on the host and on the GPU")
     ap.add_argument("--runs", type=int, default=96, help="sweep: number of runs")
     ap.add_argument("--sweep-steps", type=int, default=3000, help="sweep: FDTD steps per run")
     ap.add_argument("--instances", type=int, default=24, help="clusters: number of instances")
@@ -723,16 +724,77 @@ def run_sphere(args):
     return out
 
 
+def run_setup(args):
+    """Host set-up on the GPU: the meshing of the 129^3 dispersive sphere (the call of lightsmith's ``voxelise``
+    that its scattering driver makes, captured from lightsmith's own solve of the problem) by lightsmith on the
+    host and by ``lightsmith_b200.voxel`` on the GPU, with the problem's staircase mesh and with subpixel
+    smoothing; wall-clock milliseconds (the GPU figure includes its copies and the host assembly, after one
+    untimed call), and whether every output is the same bit for bit."""
+    import numpy as np
+    import torch
+
+    if not _lightsmith_available():
+        return {"unavailable": "lightsmith (baseline/_ref) is not installed"}
+    sys.path.insert(0, os.path.join(HERE, "tests", "golden"))
+    import lightsmith as ls
+    from lightsmith.backends._fdtd import scattering as S
+    from problems import c0_problem, with_options
+
+    from lightsmith_b200 import voxel
+
+    class Stop(Exception):
+        pass
+
+    def captured(prob):
+        got = {}
+        saved = S._slot_fn, S.voxelise
+
+        def slots(sim, slot_of, n):
+            return voxel.ShapeSlots(saved[0](sim, slot_of, n), sim.particles, slot_of)
+
+        def rec(*a, **k):
+            got.update(a=a, k=k)
+            raise Stop
+        S._slot_fn, S.voxelise = slots, rec
+        try:
+            ls.solve(prob, method="fdtd", device="cpu")
+        except Stop:
+            pass
+        finally:
+            S._slot_fn, S.voxelise = saved
+        return got["a"], got["k"], saved[1]
+
+    out = {}
+    for mode in ("staircase", "subpixel"):
+        a, k, host_vox = captured(with_options(c0_problem(), mesh_refinement=mode))
+        k = {n: v for n, v in k.items() if n in ("mode", "samples", "base", "background")}
+        t0 = time.perf_counter()
+        host = host_vox(*a, **k)
+        t1 = time.perf_counter()
+        voxel.voxelise_gpu(*a, **k, device="cuda:0")  # untimed: library, context and allocator
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        gpu = voxel.voxelise_gpu(*a, **k, device="cuda:0")
+        t3 = time.perf_counter()
+        same = bool(np.array_equal(host[0], gpu[0]) and host[2] == gpu[2] and len(host[1]) == len(gpu[1]) and all(
+            np.array_equal(g.idx, h.idx) and np.array_equal(g.frac, h.frac) for g, h in zip(gpu[1], host[1])))
+        out[mode] = {"host_ms": (t1 - t0) * 1e3, "gpu_ms": (t3 - t2) * 1e3, "speedup": (t1 - t0) / max(t3 - t2, 1e-9),
+                     "interface_cells": int(host[2]["interface_cells"]), "identical": same}
+    return {"workload": "meshing of the 129^3 Drude-Lorentz sphere (r = 40 nm, 2 nm cells) as lightsmith's "
+                        "scattering driver calls voxelise", **out}
+
+
 def forms(args) -> dict:
     """The method's other forms on this GPU, each a record with its own clock samples, for the default line:
     the whole 129^3 dispersive-sphere solve (Gcell/s, roofline of its bulk kernel, FP32 and FP64 errors), the
     batched oblique sweep against the same runs one after another, the adjoint gradient's cost over a forward
-    run, and forward + gradient over dispersive clusters with FP64 errors (a few instances)."""
+    run, forward + gradient over dispersive clusters with FP64 errors (a few instances), and the sphere's host
+    set-up (meshing) on the host and on the GPU."""
     import torch
 
     out = {}
     for name, fn, kw in (("sphere", run_sphere, {}), ("sweep", run_sweep, {}), ("adjoint", run_adjoint, {}),
-                         ("clusters", run_clusters, {"instances": args.form_instances})):
+                         ("clusters", run_clusters, {"instances": args.form_instances}), ("setup", run_setup, {})):
         sub = argparse.Namespace(**{**vars(args), **kw})
         t0 = time.perf_counter()
         try:
@@ -757,6 +819,8 @@ def main():
         print(json.dumps(run_clusters(args)), flush=True)
     elif args.workload == "sphere":
         print(json.dumps(run_sphere(args)), flush=True)
+    elif args.workload == "setup":
+        print(json.dumps(run_setup(args)), flush=True)
     else:
         run_b200(args)
 

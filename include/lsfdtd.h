@@ -455,6 +455,69 @@ int32_t lsfdtd_adjoint_record(lsfdtd_adjoint* adj, int32_t slot, void* stream);
  * transposes of the E and H updates, and accumulates the gradient */
 int32_t lsfdtd_adjoint_step(lsfdtd_adjoint* adj, int64_t n, int32_t slot, void* stream);
 
+/* ---- host set-up on the GPU: material on the Yee E grid from particle shapes ----------------------------------
+ * Replaces the per-point work of lightsmith's voxelise (backends/_fdtd/setup.py:110-289) for the scenes of its
+ * scattering driver: particles (spec.py:28-122: sphere, spheroid, cylinder, layered sphere, each at a position,
+ * the first listed winning overlaps, setup.py:707-716) over a host medium, optionally above a substrate
+ * (scattering.py:81-90). The caller assembles inv_eps, the dispersive groups and the off-diagonal terms from
+ * the three results as voxelise does (lightsmith_b200/voxel.py). Every array is device memory. */
+#define LSFDTD_VOX_MAX_REGIONS 8
+#define LSFDTD_VOX_MAX_MEDIA 16
+enum { LSFDTD_VOX_SPHERE = 0, LSFDTD_VOX_SPHEROID = 1, LSFDTD_VOX_CYLINDER = 2, LSFDTD_VOX_LAYERED_SPHERE = 3 };
+enum { LSFDTD_VOX_STAIRCASE = 0, LSFDTD_VOX_VOLUME_AVERAGE = 1, LSFDTD_VOX_SUBPIXEL = 2, LSFDTD_VOX_CONFORMAL = 3 };
+
+typedef struct {
+  int32_t kind;       /* LSFDTD_VOX_* shape */
+  int32_t n_regions;  /* 1, or the core and shells of a layered sphere */
+  double pos[3];      /* centre, nm */
+  double a, b;        /* sphere: radius; spheroid: semi-axes xy and z; cylinder: radius and length (along z) */
+  double radii[LSFDTD_VOX_MAX_REGIONS];  /* layered sphere: outer radius of each region, ascending */
+  int32_t slot[LSFDTD_VOX_MAX_REGIONS];  /* medium slot of each region */
+} lsfdtd_vox_particle;
+
+typedef struct {
+  int32_t n_particles;
+  const lsfdtd_vox_particle* particles;  /* device array */
+  int32_t has_substrate;                 /* points below z_int that no particle holds take sub_slot */
+  double z_int;
+  int32_t sub_slot;
+  double origin[3], dx[3];               /* node (0, 0, 0) and the cell size, nm */
+  int32_t shape[3];
+  int32_t roi_lo[3], roi_hi[3];          /* the nodes examined */
+} lsfdtd_vox_scene;
+
+typedef struct {
+  int32_t n;        /* media: slots 0 .. n - 1 (0 the host medium) */
+  int32_t samples;  /* supersamples per axis of an interface cell */
+  int32_t mode;     /* LSFDTD_VOX_* mesh refinement */
+  double eps_inf[LSFDTD_VOX_MAX_MEDIA];
+  int8_t dispersive[LSFDTD_VOX_MAX_MEDIA];
+  int8_t background[LSFDTD_VOX_MAX_MEDIA];  /* media of a layered background filled beforehand */
+} lsfdtd_vox_media;
+
+typedef struct {  /* per interface cell q of n */
+  double* frac;     /* [s * n + q] fraction of medium s */
+  double* nhat;     /* [3 q + d] unit normal (first moment of the dominant medium), zero when undefined */
+  double* w;        /* [q] n_c^2, 1/3 without a normal, 0 for volume averaging */
+  int8_t* part;     /* [q] holds a medium outside the background set */
+  int8_t* has_disp; /* [q] holds a dispersive medium */
+  double* inv;      /* [q] smoothed 1/eps_cc (w <1/eps> + (1 - w) / <eps>) */
+  double* od;       /* [3 q + d] off-diagonal terms n_d n_c (<1/eps> - 1/<eps>), column c zero */
+} lsfdtd_vox_cells;
+
+/* the medium slot at every point of the half-cell lattice origin + (m / 2) dx, m from 2 roi_lo - 1 to 2 roi_hi
+ * per axis: (2 n0 + 2) x (2 n1 + 2) x (2 n2 + 2) int16 values (n_a = roi_hi - roi_lo), row-major
+ * (setup.py:276-289, _half_lattice) */
+int32_t lsfdtd_vox_lattice(const lsfdtd_vox_scene* scene, int16_t* lattice, void* stream);
+/* per node of the region (row-major from roi_lo) for E component c: the slot of its E_c position, or -1 where
+ * subpixel != 0 and a corner or edge midpoint of its cell holds another slot (setup.py:153-177) */
+int32_t lsfdtd_vox_classify(const lsfdtd_vox_scene* scene, const int16_t* lattice, int32_t c, int32_t subpixel,
+                            int16_t* cls, void* stream);
+/* per interface cell (cells[q]: row-major node index of the region, component c): the supersampled fractions,
+ * normal, weight and smoothed 1/eps (setup.py:190-234) */
+int32_t lsfdtd_vox_supersample(const lsfdtd_vox_scene* scene, const lsfdtd_vox_media* media, int32_t c,
+                               const int64_t* cells, int64_t n, lsfdtd_vox_cells out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,31 @@ class AdjointDesc(C.Structure):
                 ("n_groups", i32), ("group_bar", vp * 8)]
 
 
+# the GPU voxeliser's descriptors (lsfdtd_vox_* in include/lsfdtd.h)
+VOX_MAX_REGIONS = 8
+VOX_MAX_MEDIA = 16
+
+
+class VoxParticle(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_regions", C.c_int32), ("pos", C.c_double * 3), ("a", C.c_double),
+                ("b", C.c_double), ("radii", C.c_double * VOX_MAX_REGIONS), ("slot", C.c_int32 * VOX_MAX_REGIONS)]
+
+
+class VoxScene(C.Structure):
+    _fields_ = [("n_particles", C.c_int32), ("particles", C.c_void_p), ("has_substrate", C.c_int32),
+                ("z_int", C.c_double), ("sub_slot", C.c_int32), ("origin", C.c_double * 3), ("dx", C.c_double * 3),
+                ("shape", C.c_int32 * 3), ("roi_lo", C.c_int32 * 3), ("roi_hi", C.c_int32 * 3)]
+
+
+class VoxMedia(C.Structure):
+    _fields_ = [("n", C.c_int32), ("samples", C.c_int32), ("mode", C.c_int32), ("eps_inf", C.c_double * VOX_MAX_MEDIA),
+                ("dispersive", C.c_int8 * VOX_MAX_MEDIA), ("background", C.c_int8 * VOX_MAX_MEDIA)]
+
+
+class VoxCells(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("frac", "nhat", "w", "part", "has_disp", "inv", "od")]
+
+
 SIGNATURES = {
     "lsfdtd_abi_version": (i32, []),
     "lsfdtd_last_error": (C.c_char_p, []),
@@ -150,6 +175,9 @@ SIGNATURES = {
     "lsfdtd_adjoint_destroy": (i32, [vp]),
     "lsfdtd_adjoint_record": (i32, [vp, i32, vp]),
     "lsfdtd_adjoint_step": (i32, [vp, i64, i32, vp]),
+    "lsfdtd_vox_lattice": (i32, [vp, vp, vp]),
+    "lsfdtd_vox_classify": (i32, [vp, vp, i32, i32, vp, vp]),
+    "lsfdtd_vox_supersample": (i32, [vp, vp, i32, vp, i64, VoxCells, vp]),
 }
 
 _lib = None

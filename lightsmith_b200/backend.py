@@ -33,6 +33,7 @@ from lightsmith.problems import DeviceProblem, EmissionProblem, LayerStackProble
 from lightsmith.spec import Simulation
 
 from . import engine as _engine
+from . import voxel as _voxel
 
 __all__ = ["B200FDTD"]
 
@@ -61,6 +62,47 @@ def _engine_swapped():
         finally:
             for m, e in zip(_DRIVERS, saved):
                 m.Engine = e
+
+
+@contextmanager
+def _nothing():
+    yield
+
+
+@contextmanager
+def _voxeliser_swapped(device, used: list):
+    """For the duration of one solve, the particle meshing of the scattering and emission drivers
+    (``voxelise`` of their particle slot functions, setup.py:110-289) by the GPU voxeliser
+    (``lightsmith_b200.voxel``) where it serves the scene; every call it serves is appended to ``used``."""
+    S, E = _scattering_driver, _emission_driver
+    saved = (S._slot_fn, S.voxelise, E.particle_slot_fn, E.voxelise)
+    dev = _engine._device_name(device)
+
+    def scattering_slots(sim, slot_of, n_media):
+        sub = None if sim.substrate is None else (sim.substrate.interface_z_nm, n_media - 1)
+        return _voxel.ShapeSlots(saved[0](sim, slot_of, n_media), sim.particles, slot_of, sub)
+
+    def emission_slots(prob, slot_of):
+        return _voxel.ShapeSlots(saved[2](prob, slot_of), prob.particles, slot_of)
+
+    def dispatch(host_voxelise):
+        def voxelise(slot_fn, media, shape, origin, dx, roi_lo, roi_hi, *, mode="subpixel", samples=8, base=None,
+                     background=(), grid=None, **kw):
+            if _voxel.supports(slot_fn, media, mode, samples, grid):
+                used.append(mode)
+                return _voxel.voxelise_gpu(slot_fn, media, shape, origin, dx, roi_lo, roi_hi, mode=mode,
+                                           samples=samples, base=base, background=background, device=dev)
+            return host_voxelise(slot_fn, media, shape, origin, dx, roi_lo, roi_hi, mode=mode, samples=samples,
+                                 base=base, background=background, grid=grid, **kw)
+        return voxelise
+
+    with _SWAP_LOCK:
+        try:
+            S._slot_fn, S.voxelise = scattering_slots, dispatch(saved[1])
+            E.particle_slot_fn, E.voxelise = emission_slots, dispatch(saved[3])
+            yield
+        finally:
+            S._slot_fn, S.voxelise, E.particle_slot_fn, E.voxelise = saved
 
 
 def _static_rejection(sim, opts) -> str:
@@ -381,6 +423,8 @@ class B200FDTD(NativeFDTD):
     citation = NativeFDTD.citation + "; time loop: lightsmith-b200 (sm_100a CUDA kernels)"
     # a periodic solve with a fixed run time advances its oblique runs together in one persistent kernel
     batch_oblique = True
+    # the scattering and emission drivers' particle meshing runs on the GPU where the scene allows it
+    gpu_voxelise = True
 
     # --- the differentiable-backend protocol -----------------------------------------------------------------
     @classmethod
@@ -480,7 +524,8 @@ class B200FDTD(NativeFDTD):
             return NativeFDTD.solve.__func__(cls, sim, device)
         if device.framework != "torch":
             raise ValueError(f"{cls.name} (B200) runs on PyTorch CUDA devices, not {device.framework!r}")
-        with _engine_swapped():
+        used: list = []
+        with _engine_swapped(), (_voxeliser_swapped(device, used) if cls.gpu_voxelise else _nothing()):
             why = ""
             if isinstance(sim, PeriodicProblem) and cls.batch_oblique:
                 res, why = _solve_periodic_batched(cls, sim, device)
@@ -489,4 +534,6 @@ class B200FDTD(NativeFDTD):
             res = NativeFDTD.solve.__func__(cls, sim, device)
             if why:
                 res.provenance["oblique_runs_one_by_one"] = why
+            if used:
+                res.provenance["voxelise_on_gpu"] = used[-1]
             return res

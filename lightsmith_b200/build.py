@@ -8,7 +8,7 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-SOURCES = [os.path.join(HERE, "csrc", "lsfdtd.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("lsfdtd.cu", "noalloc.cu", "voxel.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "yee.cuh", "yee_vec.cuh", "fused.cuh",
                                                    "fused_tma.cuh", "fused_pml.cuh", "shell.cuh", "batch.cuh", "adjoint.cuh", "ade.cuh", "sources.cuh",
                                                    "monitors.cuh", "tensor.cuh")] + \

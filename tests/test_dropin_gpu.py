@@ -28,37 +28,12 @@ if not add_to_path():
     pytest.skip("lightsmith (the reference install, baseline/_ref) not available", allow_module_level=True)
 
 import lightsmith as ls  # noqa: E402
-from lightsmith.backends import base as ls_base  # noqa: E402
 from problems import SOLVE_PROBLEMS, flatten_result, with_options  # noqa: E402
 
 from lightsmith_b200 import plan as P  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-
-
-@pytest.fixture(scope="module")
-def plugin(tmp_path_factory):
-    """lightsmith with this package installed as a plugin: a distribution declaring the entry point (as
-    pyproject.toml does) on sys.path, and lightsmith's registry reloaded from the entry points."""
-    import torch
-
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
-    d = tmp_path_factory.mktemp("site")
-    info = d / "lightsmith_b200-0.1.0.dist-info"
-    info.mkdir()
-    (info / "METADATA").write_text("Metadata-Version: 2.1\nName: lightsmith-b200\nVersion: 0.1.0\n")
-    (info / "entry_points.txt").write_text(
-        "[lightsmith.backends]\nlightsmith-fdtd-b200 = lightsmith_b200.backend:B200FDTD\n")
-    with pytest.MonkeyPatch.context() as mp:
-        mp.syspath_prepend(str(d))
-        mp.setattr(ls_base, "_REGISTRY", dict(ls_base._REGISTRY))
-        mp.setattr(ls_base, "_PLUGINS_LOADED", False)
-        from lightsmith_b200 import backend as B
-
-        assert ls_base.get_backend("fdtd", kind="scattering") is B.B200FDTD
-        yield B
 
 
 @pytest.fixture(scope="module")
