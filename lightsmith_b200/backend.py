@@ -85,10 +85,14 @@ def _voxeliser_swapped(device, used: list):
     def emission_slots(prob, slot_of):
         return _voxel.ShapeSlots(saved[2](prob, slot_of), prob.particles, slot_of)
 
+    import torch
+
+    on_gpu = torch.cuda.is_available()  # (the drivers' set-up runs without a GPU in the host-only tests)
+
     def dispatch(host_voxelise):
         def voxelise(slot_fn, media, shape, origin, dx, roi_lo, roi_hi, *, mode="subpixel", samples=8, base=None,
                      background=(), grid=None, **kw):
-            if _voxel.supports(slot_fn, media, mode, samples, grid):
+            if on_gpu and _voxel.supports(slot_fn, media, mode, samples, grid):
                 used.append(mode)
                 return _voxel.voxelise_gpu(slot_fn, media, shape, origin, dx, roi_lo, roi_hi, mode=mode,
                                            samples=samples, base=base, background=background, device=dev)
