@@ -79,9 +79,12 @@ def _peak():
 
 
 def _ncu_traffic(kernel: str, grid, shape_tuple):
-    """DRAM bytes (read + write) of one launch of ``kernel`` on ``grid`` in kernel variant ``shape_tuple[0]``,
-    as one ncu capture of the same kernel on the same grid recorded them (``profiles/ncu_traffic.json``, each
-    record with the command that made it): (bytes, source) or (None, None) without a matching record."""
+    """DRAM bytes (read + write) of one step of ``kernel`` on ``grid`` in kernel variant ``shape_tuple[0]``
+    (the launches of one step summed: the lean pass split by class of CTA box, which tile rows 8 and a ring of
+    4 select, takes five), as one ncu capture of the same kernel on the same grid recorded them
+    (``profiles/ncu_traffic.json``, each record with the command that made it): (bytes, source) or
+    (None, None) without a matching record."""
+    split = int(shape_tuple[0]) == 4 and int(shape_tuple[1]) == 8 and int(shape_tuple[3]) == 4
     try:
         with open(os.path.join(HERE, "profiles", "ncu_traffic.json")) as f:
             records = json.load(f)
@@ -89,9 +92,9 @@ def _ncu_traffic(kernel: str, grid, shape_tuple):
         return None, None
     for r in records:  # the same kernel, grid and kernel variant (planes per CTA change the halo re-reads only)
         if (r.get("kernel") == kernel and list(r.get("grid", [])) == list(grid) and
-                int(r.get("variant", -1)) == int(shape_tuple[0])):
+                int(r.get("variant", -1)) == int(shape_tuple[0]) and bool(r.get("split", False)) == split):
             return float(r["dram_bytes_read"]) + float(r["dram_bytes_write"]), \
-                f"ncu capture of one launch of the same kernel and grid: {r['command']}"
+                f"ncu capture of one step of the same kernel and grid: {r['command']}"
     return None, None
 
 
