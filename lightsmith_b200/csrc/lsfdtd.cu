@@ -567,14 +567,14 @@ struct Engine final : lsfdtd_engine {
   // than about three waves of CTAs (resident CTAs per SM as the kernels' launch bounds ask). A small grid
   // steps faster in more, shorter CTAs: measured on B200, a 200 x 200 x 120 grid with 12-cell CPML took 157 us
   // per step at 12 planes and 199 us at 34.
-  int auto_planes(int nx, long long columns, int rows, int* seg, int most = 48) {
+  int auto_planes(int nx, long long columns, int rows, int* seg, int most = 48, int waves = 3) {
     if (sm_count <= 0) {
       int dev = 0;
       LS_CUDA(cudaGetDevice(&dev));
       LS_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
     }
     const long long per_sm = sizeof(R) == 4 ? (rows == 8 ? 4 : 2) : 1;
-    const long long p = (long long)nx * columns / (3 * per_sm * std::max(sm_count, 1));
+    const long long p = (long long)nx * columns / (waves * per_sm * std::max(sm_count, 1));
     *seg = (int)std::max(4LL, std::min((long long)most, p));
     return LSFDTD_OK;
   }
@@ -622,9 +622,13 @@ struct Engine final : lsfdtd_engine {
                       : dim3(cdiv(desc.shape[2], 32), cdiv(desc.shape[1], rows), 1);
     const int nx = split ? fa.box_hi[0] - fa.box_lo[0] : desc.shape[0];
     fa.seg = planes;
-    // the lean pass split in two kernels balances its two halves better in shorter segments (measured on B200
-    // at 640^3: 3.32 ms per step at 32 planes, 3.52 at 48; the lean kernel alone is fastest at 48)
-    if (fa.seg <= 0) LS_TRY(auto_planes(nx, (long long)grid.x * grid.y, rows, &fa.seg, lean_split() ? 32 : 48));
+    // the lean pass split by class of box balances its classes better in shorter segments, at least about
+    // twelve waves of CTAs (measured on B200: 640^3 at 32 planes 3.32 ms per step, at 48 3.52; 256^3 at 8
+    // planes 0.317 ms, at 32 0.421); the lean kernel alone is fastest at 48 planes and three waves
+    if (fa.seg <= 0) {
+      const bool two = lean_split();
+      LS_TRY(auto_planes(nx, (long long)grid.x * grid.y, rows, &fa.seg, two ? 32 : 48, two ? 12 : 3));
+    }
     grid.z = (unsigned)cdiv(nx, fa.seg);
     LS_TRY(mark(s, true));
     if constexpr (!kComplex) {
