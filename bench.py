@@ -561,9 +561,13 @@ def run_adjoint(args):
 
 def run_clusters(args):
     """Forward + adjoint over dispersive clusters: ``--instances`` seeded instances of 3-12 silver spheres
-    (Drude + 2 Lorentz poles, radii U(10, 40) nm, 2 nm grid, 96^3-256^3 cells sized to the cluster), each
-    excited by a point dipole just outside a 60 nm shell, objective the power out of a closed box at 24
-    wavelengths in 350-700 nm, gradient with respect to the background index of the shell's cells. Each
+    (Drude + 2 Lorentz poles, radii U(10, 40) nm, 2 nm grid). With lightsmith installed each instance is a
+    lightsmith ``Simulation`` set up by its own scattering driver (``workloads.cluster_scattering``: its
+    table-fed TF/SF plane wave and flux boxes; grids of about 100^3-260^3 cells) and the objective is the sum
+    over 24 wavelengths in 350-700 nm of C_sca; without it, a point dipole just outside the shell excites a
+    cubic grid sized to the cluster and the objective is the power out of a closed box
+    (``workloads.cluster_instance``). The gradient is with respect to the background index of the cells of a
+    60 nm shell around the spheres. Each
     instance runs forward (checkpoints every 256 steps) and backward in FP32 on the device clock; the same
     in FP64 gives the errors of each spectrum and each gradient. The instances run one after another (each
     is a whole-GPU grid)."""
@@ -571,17 +575,29 @@ def run_clusters(args):
     import torch
 
     from lightsmith_b200.adjoint import AdjointRun
-    from lightsmith_b200.workloads import cluster_instance
+    from lightsmith_b200.workloads import cluster_instance, cluster_scattering
+    from lightsmith_b200.scattering import cross_section_objective
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
+    # with lightsmith installed, each instance is posed to it and set up by its own scattering driver (TF/SF
+    # plane wave, flux boxes; objective sum_f C_sca); without it, a point dipole and the power out of a box
+    posed = _lightsmith_available()
     clocks = Clocks(_gpu_uuid(torch, dev))
     rows, t_f_tot, t_g_tot, cell_steps = [], 0.0, 0.0, 0
     for seed in range(args.instances):
         out = {}
+        if posed:  # lightsmith's set-up once per instance; each precision its own objective
+            plan, info = cluster_scattering(seed, n_steps=args.cluster_steps)
         for prec in ("single", "double"):
-            plan, info = cluster_instance(seed, n_steps=args.cluster_steps, single=prec == "single")
+            if posed:
+                ref = {}
+                info = {**info, "ref": ref, "objective": cross_section_objective(info["post"], ref)}
+            else:
+                plan, info = cluster_instance(seed, n_steps=args.cluster_steps, single=prec == "single")
             run = AdjointRun(plan, info["box"], objective=info["objective"], checkpoint=256, precision=prec)
+            if posed:
+                ref["acc_ref"] = run.eng.monitors[2]["acc_e"]
             if prec == "single":  # untimed warm-up of this instance's kernels and graphs
                 run.forward(2 * plan["stride"])
                 run.backward()
@@ -593,8 +609,11 @@ def run_clusters(args):
             g = run.backward()
             ev[2].record()
             torch.cuda.synchronize(dev)
-            s = torch.as_tensor(info["sign"], device=acc_e.device)
-            spectrum = (0.5 * (acc_e * acc_h.conj() * s).real.sum(dim=1)).cpu().numpy()
+            if posed:
+                spectrum = np.asarray(info["ref"]["spectrum"])
+            else:
+                s = torch.as_tensor(info["sign"], device=acc_e.device)
+                spectrum = (0.5 * (acc_e * acc_h.conj() * s).real.sum(dim=1)).cpu().numpy()
             n_bg = info["n_bg"]
             shell = torch.as_tensor(info["shell"], device=g.device)
             g_n = (g * (-2.0 / n_bg ** 3))[shell].cpu().numpy()  # dJ/dn per shell cell (1/eps = 1/n^2)
@@ -608,7 +627,7 @@ def run_clusters(args):
         t_f_tot += tf
         t_g_tot += tg
         cell_steps += cells * info["n_steps"]
-        rows.append({"seed": seed, "grid": plan["shape"][0], "spheres": len(info["spheres"]),
+        rows.append({"seed": seed, "grid": [int(v) for v in plan["shape"]], "spheres": len(info["spheres"]),
                      "shell_cells": int(info["shell"].sum()), "forward_ms": round(tf, 2), "gradient_ms": round(tg, 2),
                      "spectrum_err_vs_fp64": float(np.abs(s32 - s64).max() / max(np.abs(s64).max(), 1e-300)),
                      "gradient_err_vs_fp64": float(np.abs(g32 - g64).max() / max(np.abs(g64).max(), 1e-300))})
@@ -619,9 +638,13 @@ def run_clusters(args):
            "steps": args.cluster_steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"{args.instances} seeded clusters of 3-12 silver spheres (Drude + 2 Lorentz, "
-                                  "radii U(10, 40) nm) in n = 1.33, 2 nm grid, CPML 12, dipole outside a 60 nm "
-                                  "shell, power out of a closed box at 24 wavelengths in 350-700 nm, gradient in "
-                                  "the shell's background index", "checkpoint_steps": 256},
+                                  "radii U(10, 40) nm) in n = 1.33, 2 nm grid, CPML 12, " + (
+                                      "posed to lightsmith and set up by its scattering driver (table-fed TF/SF "
+                                      "plane wave, flux boxes), objective sum_f C_sca at 24 wavelengths in "
+                                      "350-700 nm" if posed else "dipole outside the shell, power out of a closed "
+                                      "box at 24 wavelengths in 350-700 nm") +
+                                  ", gradient in the background index of a 60 nm shell", "checkpoint_steps": 256,
+                      "excitation": "TF/SF plane wave (lightsmith's set-up)" if posed else "point dipole"},
            "forward_ms_total": t_f_tot, "gradient_ms_total": t_g_tot, "gradient_over_forward": t_g_tot / t_f_tot,
            "max_spectrum_err_vs_fp64": max(r["spectrum_err_vs_fp64"] for r in rows),
            "max_gradient_err_vs_fp64": max(r["gradient_err_vs_fp64"] for r in rows),

@@ -346,18 +346,9 @@ def box_flux_monitor(shape, lo, hi, omega):
     return mon, np.concatenate(sg)
 
 
-def cluster_instance(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int = 24, lam=(350.0, 700.0),
-                     n_steps: int = 2000, shell_nm: float = 60.0, pml: int = 12, single: bool = True,
-                     stride: int = 16, n_min: int = 96, n_max: int = 256):
-    """One instance of the dispersive-cluster workload: 3-12 silver spheres (radii U(10, 40) nm) at random
-    non-overlapping positions in a background of index n_bg on a cubic grid of dx, sized to the cluster
-    (n_min^3 .. n_max^3 cells); node-centred staircase spheres (every E component of a node whose centre lies
-    in a sphere belongs to one pure D-form group, with 1/eps = 1 there); a point dipole just outside the
-    60 nm shell around the spheres; the power out of a closed box around the shell at n_freq wavelengths in
-    lam as the objective. Returns (plan, info) with info: box (the shell's bounding box of nodes, the
-    gradient's design box), shell (a bool mask over that box: background nodes within shell_nm of a sphere),
-    objective (J of the accumulators), the spheres and the step count."""
-    rng = np.random.default_rng(seed)
+def cluster_spheres(rng, dx: float):
+    """3-12 spheres (radii U(10, 40) nm) at random non-overlapping positions (at least 2 dx apart), drawn from
+    ``rng``: a list of (centre (3,), radius) in nm around the origin."""
     n_sph = int(rng.integers(3, 13))
     radii = rng.uniform(10.0, 40.0, n_sph)
     side = 2.2 * float(np.sum(radii ** 3)) ** (1 / 3) + 2 * radii.max()
@@ -375,6 +366,22 @@ def cluster_instance(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int
         if len(centres) == n_sph:
             break
         side *= 1.1
+    return centres
+
+
+def cluster_instance(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int = 24, lam=(350.0, 700.0),
+                     n_steps: int = 2000, shell_nm: float = 60.0, pml: int = 12, single: bool = True,
+                     stride: int = 16, n_min: int = 96, n_max: int = 256):
+    """One instance of the dispersive-cluster workload: 3-12 silver spheres (radii U(10, 40) nm) at random
+    non-overlapping positions in a background of index n_bg on a cubic grid of dx, sized to the cluster
+    (n_min^3 .. n_max^3 cells); node-centred staircase spheres (every E component of a node whose centre lies
+    in a sphere belongs to one pure D-form group, with 1/eps = 1 there); a point dipole just outside the
+    60 nm shell around the spheres; the power out of a closed box around the shell at n_freq wavelengths in
+    lam as the objective. Returns (plan, info) with info: box (the shell's bounding box of nodes, the
+    gradient's design box), shell (a bool mask over that box: background nodes within shell_nm of a sphere),
+    objective (J of the accumulators), the spheres and the step count."""
+    rng = np.random.default_rng(seed)
+    centres = cluster_spheres(rng, dx)
     lo_nm = np.min([c - r for c, r in centres], axis=0) - shell_nm
     hi_nm = np.max([c + r for c, r in centres], axis=0) + shell_nm
     margin = 14  # cells: dipole and flux box outside the shell, then the CPML
@@ -432,3 +439,60 @@ def cluster_instance(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int
     info = {"box": box, "shell": shell, "objective": objective, "sign": sgn, "spheres": centres,
             "n_steps": int(n_steps), "n_bg": n_bg, "wavelengths": wl, "cells": cells}
     return plan, info
+
+
+SILVER_DRUDE_LORENTZ = dict(eps_inf=3.7, wp_ev=9.2, gamma_ev=0.02,
+                            poles=[{"delta_eps": 1.3, "omega0_ev": 2.6, "gamma_ev": 0.6},
+                                   {"delta_eps": 1.5, "omega0_ev": 3.7, "gamma_ev": 1.0}])
+
+
+def cluster_scattering(seed: int, dx: float = 2.0, n_bg: float = 1.33, n_freq: int = 24, lam=(350.0, 700.0),
+                       n_steps: int = 2000, shell_nm: float = 60.0, pml: int = 12, stride: int = 16,
+                       precision: str = "single"):
+    """One instance of the dispersive-cluster workload posed to lightsmith: the spheres of ``cluster_spheres``
+    (silver: the sphere benchmark's Drude + two Lorentz form with eps_inf 3.7, wp 9.2 eV, gamma 0.02 eV) as a
+    lightsmith ``Simulation`` in a background of index n_bg (dx cells, CPML pml, staircase meshing, n_freq
+    wavelengths in lam, the TF/SF box shell_nm + 4 dx beyond the spheres' bounding box), set up by lightsmith's
+    own scattering driver (``scattering.scattering_setup``: its table-fed TF/SF plane wave and flux boxes) for
+    n_steps steps. Returns (plan, info): info has box (the design box: the node ranges of the shell, background
+    nodes within shell_nm of a sphere), shell (a bool mask over it), objective (sum_f C_sca(f) of the
+    scattered-field box, ``scattering.cross_section_objective``) with ``ref`` (its reference-view input,
+    ``ref["acc_ref"]`` to be set to the run's third monitor's accumulators, and ``ref["spectrum"]``), post,
+    spheres, n_steps, n_bg, cells."""
+    import lightsmith as ls
+
+    from .scattering import cross_section_objective, scattering_setup
+
+    rng = np.random.default_rng(seed)
+    centres = cluster_spheres(rng, dx)
+    metal = ls.DrudeLorentz(**SILVER_DRUDE_LORENTZ)
+    dt = 0.99 * dx / math.sqrt(3)
+    sim = ls.Simulation(
+        particles=[ls.Particle(shape=ls.Sphere(radius_nm=float(r)), material=metal,
+                               position_nm=tuple(float(v) for v in c)) for c, r in centres],
+        medium_index=n_bg, wavelengths={"start_nm": float(lam[0]), "stop_nm": float(lam[1]), "num": int(n_freq)},
+        options={"fdtd": dict(spacing_nm=dx, pml_cells=pml, courant=0.99, symmetry="off",
+                              mesh_refinement="staircase", padding_nm=shell_nm + 4 * dx, dft_stride=stride,
+                              run_time_fs=(n_steps - 0.5) * dt / 299.792458, precision=precision)})
+    plan, post, lay = scattering_setup(sim)
+    shape = tuple(int(v) for v in plan["shape"])
+    pos = [np.asarray(lay.origin, dtype=float)[a] + dx * np.arange(shape[a]) for a in range(3)]
+    lo = np.min([c - r for c, r in centres], axis=0) - shell_nm
+    hi = np.max([c + r for c, r in centres], axis=0) + shell_nm
+    blo = [int(np.searchsorted(pos[a], lo[a])) for a in range(3)]
+    bhi = [int(np.searchsorted(pos[a], hi[a], side="right")) for a in range(3)]
+    box = tuple((a, b) for a, b in zip(blo, bhi))
+    X, Y, Z = np.meshgrid(*[pos[a][blo[a]:bhi[a]] for a in range(3)], indexing="ij")
+    dist = np.full(X.shape, np.inf)
+    for c, r in centres:
+        dist = np.minimum(dist, np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r)
+    inv = np.asarray(plan["inv_eps"])
+    inv = inv.reshape((-1,) + shape)
+    bsl = (slice(None),) + tuple(slice(a, b) for a, b in box)
+    background = np.all(np.abs(inv[bsl] - 1.0 / n_bg ** 2) < 1e-12 / n_bg ** 2, axis=0)
+    shell = background & (dist > 0) & (dist <= shell_nm)
+    ref: dict = {}
+    info = {"box": box, "shell": shell, "objective": cross_section_objective(post, ref), "ref": ref, "post": post,
+            "spheres": centres, "n_steps": int(n_steps), "n_bg": n_bg, "cells": int(np.prod(shape))}
+    return plan, info
+

@@ -274,3 +274,52 @@ def test_cluster_instance_gradient_matches_finite_differences():
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
     run.close()
+
+
+def test_cluster_scattering_gradient_matches_finite_differences():
+    """The cluster workload as lightsmith poses it (its own set-up: the table-fed TF/SF plane wave, the flux
+    boxes and the incident reference view of its scattering driver), reduced: 4 nm grid, 12 nm shell, 640
+    steps, float64. J = sum_f C_sca(f) of the scattered-field box; dJ/d(1/eps) on the shell's largest entries
+    (the three E components of a node together) against central differences of the CUDA forward."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from refsrc import add_to_path
+
+    if not add_to_path():
+        pytest.skip("lightsmith (the reference install, baseline/_ref) not available")
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.workloads import cluster_scattering
+
+    n_steps = 640
+    plan, info = cluster_scattering(1, dx=4.0, shell_nm=12.0, n_steps=n_steps, precision="double")
+    box, shape = info["box"], tuple(int(v) for v in plan["shape"])
+    run = AdjointRun(plan, box, objective=info["objective"], checkpoint=128, precision="double")
+    info["ref"]["acc_ref"] = run.eng.monitors[2]["acc_e"]
+    inv = np.asarray(plan["inv_eps"]).reshape((-1,) + shape)
+    base = torch.as_tensor(inv[(slice(None),) + tuple(slice(a, b) for a, b in box)]).clone()
+    if base.shape[0] == 1:
+        base = base[0]
+    run.set_inv_eps_box(base)
+    J0, _ = run.forward(n_steps)
+    g = run.backward().cpu().numpy()
+    shell = info["shell"]
+    assert J0 > 0 and np.abs(g[shell]).max() > 0
+    assert np.all(np.isfinite(info["ref"]["spectrum"])) and info["ref"]["spectrum"].shape == (24,)
+    gs = np.where(shell, np.abs(g), 0)
+    h = 1e-6
+    for flat in np.argsort(-gs.reshape(-1))[:4]:
+        idx = tuple(int(v) for v in np.unravel_index(flat, g.shape))
+        vals = []
+        for sgn in (1, -1):
+            x = base.clone()
+            if x.dim() == 4:
+                x[(slice(None),) + idx] += sgn * h
+            else:
+                x[idx] += sgn * h
+            run.set_inv_eps_box(x)
+            vals.append(run.forward(n_steps, keep=False)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
+    run.close()
