@@ -1,9 +1,10 @@
 """Gradients of an FDTD objective by the discrete adjoint, behind ``torch.autograd``.
 
 lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
-the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase) and pure (staircase)
-dispersive groups at most (a slab waveguide device, a metal nanoparticle cluster, a 2D device with its
-periodic invariant axis), a real objective J of one DFT monitor's accumulators (or several monitors'),
+the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase) and dispersive groups,
+pure (staircase) or mixed (subpixel interface cells) (a slab waveguide device, a metal nanoparticle cluster, a
+2D device with its periodic invariant axis), a real objective J of one DFT monitor's accumulators (or several
+monitors'),
 and its gradient with respect to 1/eps over a design box of non-dispersive nodes. J is either
 |sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2 at one frequency f, or any torch function of the
 accumulators (a flux spectrum, say): its adjoint source G = 2 dJ/d(acc) comes from torch autograd on J.
@@ -17,8 +18,9 @@ while recording H of the box at every step (``lsfdtd_adjoint_record``), then app
 dJ/dcbE over the box. Sources only add field-independent terms, so they have no adjoint; the ones allowed
 here (point dipoles, port modes, table-fed TF/SF) keep no state of their own, and their nodes must lie
 outside the box (their coefficients are fixed, not functions of the design). A dispersive group's step (D, E
-of the previous step and the poles' P) is linear too: its transpose (``k_adj_ade``) runs before the E
-update's, and its state is part of each checkpoint.
+of the previous step and the poles' P; for a mixed group also each medium's harmonic-path E and the
+arithmetic path's E) is linear too: its transpose (``k_adj_ade``) runs before the E update's, and its state
+is part of each checkpoint.
 
 ``FDTDObjective.apply(inv_eps_box, run)`` is the ``torch.autograd.Function``: forward returns J, backward
 dJ/d(1/eps) of the box (isotropic: the three E components of a node share its 1/eps, so the gradient is
@@ -58,8 +60,6 @@ class AdjointRun:
         torch = _torch()
         if plan["complex"]:
             raise ValueError("the adjoint serves real fields (no Bloch phase)")
-        if any(g["w"] is not None for g in plan["groups"]):
-            raise ValueError("the adjoint serves pure (staircase) dispersive groups, not mixed (subpixel) ones")
         for s in plan["sources"]:
             if not isinstance(s, (DipoleSource, ModeSource, TableSource)):
                 raise ValueError(f"{type(s).__name__} keeps state of its own; the adjoint does not restore it")

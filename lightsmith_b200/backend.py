@@ -191,9 +191,9 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     coordinates and the step count.
 
     The set-up is lightsmith's own (plan, voxelisation, mode tables, pulse band, CPML), with two choices the
-    adjoint needs: the mesh is staircase where a dispersive medium is present (its D-form groups must be pure)
-    and subpixel or staircase otherwise as the options ask (conformal asks for subpixel: the adjoint has no
-    off-diagonal terms); the step count is fixed: the options' ``run_time_fs`` (the driver's ``max_steps``),
+    adjoint needs: the mesh is subpixel or staircase as the options ask (conformal asks for subpixel: the
+    adjoint has no off-diagonal terms or vertex tensor; subpixel interface cells of a dispersive medium are mixed
+    D-form groups, which it serves); the step count is fixed: the options' ``run_time_fs`` (the driver's ``max_steps``),
     ``n_steps``, or else the count lightsmith's run loop reaches on the base structure's first run (on
     ``engine``: the CUDA engine on ``device`` by default). ``keep_tables`` adds lightsmith's mode tables (not
     plain data) under ``"tables"``."""
@@ -226,7 +226,7 @@ def device_runs(problem, device=None, n_steps: int | None = None, keep_tables: b
     two_d = bool(grid.two_d)
     slot_fn = D._slot_fn(problem, slots, problem.domain_center_nm[2] if two_d else None)
     asked = opts.mesh_refinement or ("subpixel" if opts.subpixel else "staircase")
-    mode = "staircase" if asked == "staircase" or any(m.dispersive for m in media) else "subpixel"
+    mode = "staircase" if asked == "staircase" else "subpixel"
     inv_eps, groups, _, _ = voxelise(slot_fn, media, grid.shape, grid.origin, dx, np.array([1, 1, 1]),
                                      np.array(grid.shape) - 1, mode=mode, samples=opts.subpixel_samples,
                                      periodic=grid.periodic, grid=grid.graded)

@@ -394,10 +394,84 @@ __global__ void k_adj_inject(R* Eb, R* Hb, const long long* e_idx, const double*
 // node, and the adjoint state Dbar, Epbar, Pbar_k, Ppbar_k of the step after): g = Ebar + Epbar; Dbar +=
 // g / eps_inf; Phat_k = Pbar_k - g / eps_inf; Epbar = -Dbar + sum_k c3 Phat_k; Pbar_k = c1 Phat_k + Ppbar_k;
 // Ppbar_k = c2 Phat_k; and the adjoint of e (the new Ebar at the node) is Dbar. The state's layout is k_ade's.
+//
+// A mixed group's step (k_ade's mixed branch, lightsmith's engine.py:776-791) is linear too. With g = Ebar +
+// Epbar the adjoint of e': the harmonic path's hbar = w g, each medium's e_s adjoint esbar_s = f_s hbar +
+// Ehbar_s, Dbar += h0 hbar + sum_s esbar_s / eps_inf_s, and per pole Phat = Phbar - esbar_s / eps_inf_s, the
+// drive's adjoint (the new Ehbar_s) sum_k c3 Phat; the arithmetic path's abar = ((1 - w) g + Eabar) inv_a,
+// Dbar += abar, per pole Phat = Pabar - f_s abar, the new Eabar = sum_{s,k} c3 Phat; then as for a pure node
+// Pbar = c1 Phat + Ppbar, Ppbar = c2 Phat, and the adjoints of e and of the old D and E_prev are Dbar, Dbar,
+// -Dbar. A path the group does not run leaves its state, and so its adjoint, as it was.
+template <typename R>
+__device__ void adj_ade_mixed(const AdeArgs<R>& g, R* Eb, R* bar, long long t) {
+  const long long n = g.n;
+  const int S = g.n_media;
+  R* Db = bar;
+  R* Epb = bar + n;
+  R* Eab = bar + 2 * n;
+  R* Ehb = bar + 3 * n;  // [S][n]
+  int n_tot = 0;
+  for (int s = 0; s < S; ++s) n_tot += g.n_poles[s];
+  R* Phb = bar + (3 + S) * n;      // [sum poles][2][n]
+  R* Pab = Phb + 2 * n_tot * n;    // same layout
+  const long long node = g.idx[t];
+  const R w = g.w[t];
+  const R gs = Eb[node] + Epb[t];
+  R dbar = Db[t];
+  if (g.has_h) {
+    const R hbar = w * gs;
+    dbar += g.h0[t] * hbar;
+    int off = 0;
+    for (int s = 0; s < S; ++s) {
+      const R esb = g.frac[s * n + t] * hbar + Ehb[s * n + t];
+      dbar += g.inv_inf[s] * esb;
+      R drive = R(0);
+      for (int k = 0; k < g.n_poles[s]; ++k) {
+        R* pk = Phb + (2 * (off + k)) * n;
+        R* pp = Phb + (2 * (off + k) + 1) * n;
+        const R ph = pk[t] - g.inv_inf[s] * esb;
+        drive += g.c3[s][k] * ph;
+        const R npk = g.c1[s][k] * ph + pp[t];
+        pp[t] = g.c2[s][k] * ph;
+        pk[t] = npk;
+      }
+      Ehb[s * n + t] = drive;
+      off += g.n_poles[s];
+    }
+  }
+  if (g.has_a) {
+    const R abar = ((R(1) - w) * gs + Eab[t]) * g.inv_a[t];
+    dbar += abar;
+    R drive = R(0);
+    int off = 0;
+    for (int s = 0; s < S; ++s) {
+      const R fb = g.frac[s * n + t] * abar;
+      for (int k = 0; k < g.n_poles[s]; ++k) {
+        R* pk = Pab + (2 * (off + k)) * n;
+        R* pp = Pab + (2 * (off + k) + 1) * n;
+        const R ph = pk[t] - fb;
+        drive += g.c3[s][k] * ph;
+        const R npk = g.c1[s][k] * ph + pp[t];
+        pp[t] = g.c2[s][k] * ph;
+        pk[t] = npk;
+      }
+      off += g.n_poles[s];
+    }
+    Eab[t] = drive;
+  }
+  Db[t] = dbar;
+  Epb[t] = -dbar;
+  Eb[node] = dbar;
+}
+
 template <typename R>
 __global__ void k_adj_ade(const AdeArgs<R> g, R* Eb, R* bar) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.n) return;
+  if (g.mixed) {
+    adj_ade_mixed(g, Eb, bar, t);
+    return;
+  }
   const long long n = g.n;
   R* Db = bar;
   R* Epb = bar + n;

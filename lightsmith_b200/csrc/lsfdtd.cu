@@ -737,8 +737,6 @@ struct Engine final : lsfdtd_engine {
       return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
     if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no conformal off-diagonal terms");
     if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no vertex-tensor mesh");
-    for (auto& gr : groups)
-      if (gr.mixed) return fail(LSFDTD_EUNSUPPORTED, "adjoint: mixed (subpixel) dispersive groups have no adjoint");
     if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
     const YeeArgs<F> a = current_args();
     std::memcpy(yee, &a, sizeof a);

@@ -2,8 +2,9 @@
 
 The checker of ``lightsmith_b200.adjoint``: the same update equations as ``oracle/engine.py`` (lightsmith's
 ``engine.py:613-663`` curl updates over the stepped regions, ``engine.py:344-418`` CPML terms in their order,
-``emission.py:130-140`` point-current corrections after the E update, ``engine.py:769-775`` pure D-form ADE
-groups after the sources), for real fields, no periodic axes and point-dipole sources, written out of place so
+``emission.py:130-140`` point-current corrections after the E update, ``engine.py:769-793`` D-form ADE groups,
+pure and mixed, after the sources), for real fields, no periodic axes and point-dipole sources, written out of
+place so
 that autograd can differentiate a DFT objective (|sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2, or any
 function of the accumulators) with respect to 1/eps over a box of nodes.
 """
@@ -118,17 +119,42 @@ def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_s
     acc_h = None if h1 is None else torch.zeros((len(omegas), len(h1)), dtype=torch.complex128)
     cells = int(np.prod(shape))
 
-    # pure dispersive groups (oracle/engine.py:_Group): D, E_prev and (P, P') per pole, out of place
+    # dispersive groups (lightsmith's engine.py:722-793, _Group): D, E_prev and (P, P') per pole; a mixed group
+    # (interface cells) also a harmonic path per dispersive medium (its E_s driving its poles, weight w) and an
+    # arithmetic path (one E_a driving every medium's poles, weight 1 - w); out of place
     groups = []
     for g in plan["groups"]:
-        if g["w"] is not None:
-            raise ValueError("pure dispersive groups only")
-        (m,) = g["media"]
         idx = torch.as_tensor(np.asarray(g["idx"], np.int64))
         z = torch.zeros(len(idx), dtype=dt)
-        coef = [pole_coefficients(_Pole(*p), step_dt) for p in m["poles"]]
-        groups.append({"idx": idx, "D": z, "Ep": z, "P": [(z, z) for _ in coef], "coef": coef,
-                       "inv_inf": 1.0 / m["eps_inf"]})
+        coef = [[pole_coefficients(_Pole(*p), step_dt) for p in m["poles"]] for m in g["media"]]
+        if g["w"] is None:
+            (m,) = g["media"]
+            groups.append({"idx": idx, "pure": True, "D": z, "Ep": z, "P": [(z, z) for _ in coef[0]],
+                           "coef": coef[0], "inv_inf": 1.0 / m["eps_inf"]})
+            continue
+        f = np.asarray(g["frac"], float)
+        media = g["media"]
+        disp = [s for s, m in enumerate(media) if m["poles"]]
+        w = np.asarray(g["w"], float)
+        groups.append({"idx": idx, "pure": False, "D": z, "Ep": z, "disp": disp, "coef": coef,
+                       "h0": torch.as_tensor(sum(f[s] / m["eps_inf"] for s, m in enumerate(media)
+                                                 if not m["poles"]) + 0 * f[0], dtype=dt),
+                       "f": {s: torch.as_tensor(f[s], dtype=dt) for s in disp},
+                       "inv_inf": {s: 1.0 / media[s]["eps_inf"] for s in disp},
+                       "inv_a": torch.as_tensor(1.0 / sum(f[s] * m["eps_inf"] for s, m in enumerate(media)), dtype=dt),
+                       "w": torch.as_tensor(w, dtype=dt), "has_h": bool(np.any(w > 0)), "has_a": bool(np.any(w < 1)),
+                       "Eh": {s: z for s in disp}, "Ea": z,
+                       "Ph": {s: [(z, z) for _ in coef[s]] for s in disp},
+                       "Pa": {s: [(z, z) for _ in coef[s]] for s in disp}})
+
+    def advance(pairs, coefs, drive):
+        """The poles' new (P, P') and their sum (lightsmith's _Group._advance)."""
+        tot, new = None, []
+        for (P, Pp), (c1, c2, c3) in zip(pairs, coefs):
+            nw = c1 * P + c2 * Pp + c3 * drive
+            new.append((nw, P))
+            tot = nw if tot is None else tot + nw
+        return new, tot
     for n in range(n_steps):
         H = [_put(H[c], sl(RH[c]), -curl(E, c, sl(RH[c]), True) * cH) for c in range(3)]
         H = pml(H, E, "H")
@@ -140,18 +166,31 @@ def objective(plan: dict, inv_eps_box, box, monitor: int, freq: int, wE, wH, n_s
                                                    torch.as_tensor(s.coef * s.wave[n], dtype=dt))
             flat = flat - upd
             E = [flat[c * cells:(c + 1) * cells].reshape(shape) for c in range(3)]
-        if groups:  # D += E - E_prev; P <- c1 P + c2 P' + c3 E_prev; E = (D - sum P) / eps_inf; E_prev = E
+        if groups:  # D += E - E_prev; P <- c1 P + c2 P' + c3 drive; E from D and P; E_prev = E
             flat = torch.cat([e.reshape(-1) for e in E])
             for g in groups:
                 e_now = flat[g["idx"]]
                 g["D"] = g["D"] + (e_now - g["Ep"])
-                tot, newP = None, []
-                for (P, Pp), (c1, c2, c3) in zip(g["P"], g["coef"]):
-                    nw = c1 * P + c2 * Pp + c3 * g["Ep"]
-                    newP.append((nw, P))
-                    tot = nw if tot is None else tot + nw
-                g["P"] = newP
-                e_new = (g["D"] - tot) * g["inv_inf"]
+                if g["pure"]:
+                    g["P"], tot = advance(g["P"], g["coef"], g["Ep"])
+                    e_new = (g["D"] - tot) * g["inv_inf"]
+                else:
+                    parts = []
+                    if g["has_h"]:
+                        harm = g["D"] * g["h0"]
+                        for s in g["disp"]:
+                            g["Ph"][s], tot = advance(g["Ph"][s], g["coef"][s], g["Eh"][s])
+                            g["Eh"][s] = (g["D"] - tot) * g["inv_inf"][s]
+                            harm = harm + g["f"][s] * g["Eh"][s]
+                        parts.append(g["w"] * harm)
+                    if g["has_a"]:
+                        acc = g["D"]
+                        for s in g["disp"]:
+                            g["Pa"][s], tot = advance(g["Pa"][s], g["coef"][s], g["Ea"])
+                            acc = acc - g["f"][s] * tot
+                        g["Ea"] = acc * g["inv_a"]
+                        parts.append((1 - g["w"]) * g["Ea"])
+                    e_new = parts[0] if len(parts) == 1 else parts[0] + parts[1]
                 g["Ep"] = e_new
                 flat = flat.index_put((g["idx"],), e_new)
             E = [flat[c * cells:(c + 1) * cells].reshape(shape) for c in range(3)]

@@ -120,3 +120,46 @@ def dispersive_case(seed: int = 7, n_chunks: int = 4, pml_cells: int = 4):
     plan = make_plan(shape=SHAPE, dx=DX, dt=dt, single=False, inv_eps=inv_eps, groups=[group], pml=pml,
                      sources=[dip], monitors=[mon], dft_stride=stride)
     return plan, n_steps, flux_objective
+
+
+def mixed_case(seed: int = 9, n_chunks: int = 4, pml_cells: int = 4):
+    """dispersive_case's grid, dipole, monitor and flux objective with its block of interface cells instead: a
+    mixed D-form group (lightsmith's subpixel interface cells) of the Drude-Lorentz metal and a dielectric of
+    index 1.8, each node's metal fraction drawn from U(0.2, 0.8) and its harmonic weight w from U(0, 1) (a few
+    nodes at exactly 0 and 1), so that both paths run. Returns (plan, n_steps, objective)."""
+    from lightsmith_b200.plan import DispersiveGroup, Medium, Pole
+
+    dt = 0.99 * DX / math.sqrt(3)
+    rng = np.random.default_rng(seed)
+    inv_eps = 1.0 / rng.uniform(1.0, 4.0, size=SHAPE)
+    block = (slice(8, 10), slice(5, 9), slice(4, 8))
+    inv_eps[block] = 1.0
+    omega = 2 * np.pi / 300.0
+    stride = 7
+    n_steps = n_chunks * stride
+    ii, jj, kk = (a.ravel() for a in np.meshgrid(*(np.arange(s.start, s.stop) for s in block), indexing="ij"))
+    cells = int(np.prod(SHAPE))
+    node = np.ravel_multi_index((ii, jj, kk), SHAPE)
+    idx = np.concatenate([c * cells + node for c in range(3)])
+    metal = Medium(3.7, (Pole(0.002, 0.0, 0.002), Pole(0.0005, 0.02, 0.004)))
+    glass = Medium(1.8 ** 2, ())
+    fm = rng.uniform(0.2, 0.8, len(idx))
+    w = rng.uniform(0.0, 1.0, len(idx))
+    w[:3], w[3:6] = 0.0, 1.0
+    group = DispersiveGroup(idx=idx, media=[metal, glass], frac=np.stack([fm, 1.0 - fm]), w=w)
+
+    def at(flat):
+        rest = np.asarray(flat) % cells
+        return inv_eps[np.unravel_index(rest, SHAPE)]
+
+    dip = point_dipole(SHAPE, np.zeros(3), DX, dt, np.array([6.37, 9.37, 8.37]) * DX, (0.3, 1.0, 0.2), at,
+                       omega, 0.4 * omega, n_steps + 400)
+    wv = dip.wave
+    first = int(np.nonzero(np.abs(wv) > 1e-3 * np.abs(wv).max())[0][0])
+    dip.wave = np.concatenate([wv[first:], np.zeros(first)])
+    mon = plane_monitor(SHAPE, 12, [0.8 * omega, omega, 1.2 * omega], energy=1)
+    pml = PMLSpec(cells=((pml_cells, pml_cells),) * 3, alpha_max=0.02, eps_ref=1.5)
+    plan = make_plan(shape=SHAPE, dx=DX, dt=dt, single=False, inv_eps=inv_eps, groups=[group], pml=pml,
+                     sources=[dip], monitors=[mon], dft_stride=stride)
+    return plan, n_steps, flux_objective
+

@@ -65,3 +65,23 @@ def test_autograd_restatement_with_a_dispersive_group_matches_oracle():
     J0 = float(J_of(torch.as_tensor(m["acc_e"]), torch.as_tensor(m["acc_h"])))
     assert abs(J0) > 0
     assert abs(J - J0) / abs(J0) < 1e-12
+
+
+def test_autograd_restatement_with_a_mixed_group_matches_oracle():
+    """The restatement's mixed D-form group (harmonic and arithmetic paths, lightsmith's subpixel interface
+    cells) against the oracle's run of the same plan."""
+    from adjoint_cases import mixed_case
+    from oracle.autograd import objective
+    from oracle.engine import OracleEngine
+
+    plan, n_steps, J_of = mixed_case()
+    box_vals = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in BOX)])
+    J = float(objective(plan, box_vals, BOX, 0, 0, None, None, n_steps, J=J_of))
+    eng = OracleEngine(plan)
+    for _ in range(n_steps // plan["stride"]):
+        eng.chunk()
+    m = eng.monitors[0]
+    J0 = float(J_of(torch.as_tensor(m["acc_e"]), torch.as_tensor(m["acc_h"])))
+    assert abs(J0) > 0
+    assert abs(J - J0) / abs(J0) < 1e-12
+

@@ -323,3 +323,44 @@ def test_cluster_scattering_gradient_matches_finite_differences():
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
     run.close()
+
+
+def test_mixed_dispersive_group_gradient():
+    """A mixed D-form group (lightsmith's subpixel interface cells of a Drude-Lorentz metal and a dielectric,
+    both paths running) between the dipole and the design box, the flux spectrum as the objective: the float64
+    gradient against torch autograd through the restatement, against central differences of the CUDA forward,
+    and bitwise across two checkpoint intervals."""
+    from adjoint_cases import mixed_case
+    from lightsmith_b200.adjoint import AdjointRun
+    from oracle.autograd import objective
+
+    plan, n_steps, J_of = mixed_case()
+    base = torch.as_tensor(np.asarray(plan["inv_eps"])[tuple(slice(a, b) for a, b in BOX)])
+    x = base.clone().requires_grad_(True)
+    J_ref = objective(plan, x, BOX, 0, 0, None, None, n_steps, J=J_of)
+    (g_ref,) = torch.autograd.grad(J_ref, x)
+    J_ref = float(J_ref.detach())
+    grads = []
+    for K in (plan["stride"], n_steps):
+        run = AdjointRun(plan, BOX, objective=J_of, checkpoint=K, precision="double")
+        run.set_inv_eps_box(base)
+        J, _ = run.forward(n_steps)
+        grads.append(run.backward().cpu().numpy())
+        assert abs(J - J_ref) / abs(J_ref) < 1e-11
+        if K == n_steps:
+            g = grads[-1]
+            h = 1e-6
+            for flat in np.argsort(-np.abs(g).reshape(-1))[:3]:
+                idx = tuple(int(v) for v in np.unravel_index(flat, g.shape))
+                vals = []
+                for sgn in (1, -1):
+                    xp = base.clone()
+                    xp[idx] += sgn * h
+                    run.set_inv_eps_box(xp)
+                    vals.append(run.forward(n_steps)[0])
+                fd = (vals[0] - vals[1]) / (2 * h)
+                assert abs(fd - g[idx]) <= 1e-5 * abs(fd), (idx, fd, g[idx])
+        run.close()
+    assert np.abs(g_ref.numpy()).max() > 0
+    assert _rel(grads[0], g_ref.numpy()) < 1e-9
+    assert np.array_equal(grads[0], grads[1])
