@@ -112,6 +112,40 @@ def tune_batch(engines, last, shapes=BATCH_SHAPES, steps: int = 30, launches: in
     return best, res
 
 
+# steps a run advances per visit of its CTAs (one launch): while in flight a run's fields stay in L2 from one
+# step to the next, and the steps of a visit reuse them; fewer steps switch runs (and reload them) more often
+BATCH_DEPTHS = (8, 32, 128, 512)
+
+
+def tune_batch_depth(engines, last, shape=(0, 0), depths=BATCH_DEPTHS, launches: int = 2):
+    """Time the batched kernel's steps per visit (the depth of its L2-resident blocking in time) under launch
+    shape ``shape`` on ``engines`` (which advance) and return (best depth, {depth: Gcell-updates/s})."""
+    import numpy as np
+    import torch
+
+    from .batch import BlochBatch
+
+    cells = [int(np.prod(e.shape)) for e in engines]
+    res = {}
+    b = BlochBatch(engines, last, cluster_ctas=shape[0], max_clusters=shape[1])
+    try:
+        for depth in depths:
+            b.run(depth, 1)  # capture the graph of this step count
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            before = [e.n_host for e in engines]
+            t0.record(b.stream)
+            b.run(depth, launches)
+            t1.record(b.stream)
+            torch.cuda.synchronize()
+            moved = sum(c * (e.n_host - n) for c, e, n in zip(cells, engines, before))
+            if moved:
+                res[int(depth)] = moved / max(t0.elapsed_time(t1), 1e-9) / 1e6
+    finally:
+        b.close()
+    best = max(res, key=res.get) if res else int(depths[-1])
+    return best, res
+
+
 def _main():
     import torch
 

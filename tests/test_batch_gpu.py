@@ -162,3 +162,20 @@ def test_a_run_turning_non_finite_retires_alone():
         x.close()
     for e in engs + ref:
         e.close()
+
+
+def test_batch_depth_tuner():
+    """tune.tune_batch_depth times the batched kernel at each steps-per-visit depth on the runs it is given
+    (which advance by the steps it runs: two timed launches and a capture per depth) and returns the fastest."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.tune import tune_batch_depth
+
+    plans = _small_runs("single")
+    lasts = [(200 // p["stride"]) * p["stride"] for p in plans]  # the runs' waveforms cover 240 steps
+    engines = [Engine.from_plan(p) for p in plans]
+    depths = (7, 21)
+    best, res = tune_batch_depth(engines, lasts, depths=depths, launches=2)
+    assert best in depths and sorted(res) == sorted(depths) and all(v > 0 for v in res.values())
+    for e, last in zip(engines, lasts):
+        assert e.n_host == min(last, 3 * sum(depths))
+        e.close()
