@@ -441,6 +441,15 @@ typedef struct lsfdtd_adjoint_desc {
   int32_t n_freq;
   int32_t n_groups;                  /* the engine's dispersive groups, in the order they were added */
   void* group_bar[LSFDTD_ADJ_MAX_GROUPS]; /* adjoint state per group, shaped as its forward state, zeroed */
+  /* the engine's conformal off-diagonal terms (lsfdtd_engine_add_offdiag), transposed: row r < od_rows adds
+   * sum_{j in [od_ptr[r], od_ptr[r + 1])} od_w[j] Ebar[od_e[j]] to Hbar[od_h[r]], the od_h distinct (device
+   * arrays; od_w in the engine's precision). Required, with od_rows > 0, when the engine has such terms. The
+   * gradient holds them fixed: it is the derivative with respect to the diagonal coefficients. */
+  const int64_t* od_h;
+  const int64_t* od_ptr;             /* (od_rows + 1) */
+  const int64_t* od_e;
+  const void* od_w;
+  int64_t od_rows;
 } lsfdtd_adjoint_desc;
 
 /* sets the engine's host step count (after the caller rewinds its device counter and fields to a saved step,

@@ -97,7 +97,8 @@ class AdjointDesc(C.Structure):
     _fields_ = [("Eb", vp), ("Hb", vp), ("psi_bar", vp * 72), ("box_lo", i32 * 3), ("box_hi", i32 * 3),
                 ("hist", vp), ("hist_slots", i32), ("grad", vp), ("e_idx", vp), ("ge", vp), ("n_e", i64),
                 ("h_idx1", vp), ("h_idx2", vp), ("gh", vp), ("n_h", i64), ("omega", vp), ("n_freq", i32),
-                ("n_groups", i32), ("group_bar", vp * 8)]
+                ("n_groups", i32), ("group_bar", vp * 8), ("od_h", vp), ("od_ptr", vp), ("od_e", vp), ("od_w", vp),
+                ("od_rows", i64)]
 
 
 # the GPU voxeliser's descriptors (lsfdtd_vox_* in include/lsfdtd.h)

@@ -1,10 +1,11 @@
 """Gradients of an FDTD objective by the discrete adjoint, behind ``torch.autograd``.
 
 lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
-the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase) and dispersive groups,
-pure (staircase) or mixed (subpixel interface cells) (a slab waveguide device, a metal nanoparticle cluster, a
-2D device with its periodic invariant axis), a real objective J of one DFT monitor's accumulators (or several
-monitors'),
+the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase; mirror planes, as
+lightsmith's scattering driver picks them by default) with dispersive groups, pure (staircase) or mixed
+(subpixel interface cells), and the conformal off-diagonal terms of its default dielectric meshing (a slab
+waveguide device, a metal nanoparticle cluster, a 2D device with its periodic invariant axis, a dielectric
+particle in a mirrored run), a real objective J of one DFT monitor's accumulators (or several monitors'),
 and its gradient with respect to 1/eps over a design box of non-dispersive nodes. J is either
 |sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2 at one frequency f, or any torch function of the
 accumulators (a flux spectrum, say): its adjoint source G = 2 dJ/d(acc) comes from torch autograd on J.
@@ -20,7 +21,9 @@ here (point dipoles, port modes, table-fed TF/SF) keep no state of their own, an
 outside the box (their coefficients are fixed, not functions of the design). A dispersive group's step (D, E
 of the previous step and the poles' P; for a mixed group also each medium's harmonic-path E and the
 arithmetic path's E) is linear too: its transpose (``k_adj_ade``) runs before the E update's, and its state
-is part of each checkpoint.
+is part of each checkpoint. The off-diagonal terms (E += W H after the E update) are transposed by a gather
+over the rows of W^T (``transposed_offdiag``); the gradient holds W fixed (it is the derivative with respect to
+the diagonal 1/eps of the box, W's entries being separate coefficients).
 
 ``FDTDObjective.apply(inv_eps_box, run)`` is the ``torch.autograd.Function``: forward returns J, backward
 dJ/d(1/eps) of the box (isotropic: the three E components of a node share its 1/eps, so the gradient is
@@ -43,6 +46,23 @@ def _torch():
     import torch
 
     return torch
+
+
+def transposed_offdiag(od: dict):
+    """The conformal off-diagonal gather tables (``plan["offdiag"]``: row t adds sum_k w[t, k] H[h[t, k]] to
+    E[e[t]]) transposed for the adjoint: (rows, ptr, e, w) with row r adding sum_{j in [ptr[r], ptr[r + 1])}
+    w[j] Ebar[e[j]] to Hbar[rows[r]]. The rows are the distinct H nodes read with a nonzero weight, ascending;
+    each row's entries run in ascending E index."""
+    e = np.asarray(od["e"], np.int64)
+    h = np.asarray(od["h"], np.int64)
+    w = np.asarray(od["w"])
+    ee, hh, ww = np.repeat(e, h.shape[1]), h.reshape(-1), w.reshape(-1)
+    keep = ww != 0
+    ee, hh, ww = ee[keep], hh[keep], ww[keep]
+    order = np.lexsort((ee, hh))
+    ee, hh, ww = ee[order], hh[order], ww[order]
+    rows, start = np.unique(hh, return_index=True)
+    return rows, np.append(start, len(hh)).astype(np.int64), ee, ww
 
 
 class AdjointRun:
@@ -148,6 +168,13 @@ class AdjointRun:
         d.n_groups = len(self.group_bar)
         for gi, t in enumerate(self.group_bar):
             d.group_bar[gi] = t.data_ptr()
+        od = plan.get("offdiag")
+        if od is not None and len(od["e"]):  # the conformal off-diagonal terms, transposed
+            rows, ptr, e, w = transposed_offdiag(od)
+            self._od = [torch.as_tensor(rows, device=self.dev), torch.as_tensor(ptr, device=self.dev),
+                        torch.as_tensor(e, device=self.dev), torch.as_tensor(w, dtype=eng.fdt, device=self.dev)]
+            d.od_h, d.od_ptr, d.od_e, d.od_w = (t.data_ptr() for t in self._od)
+            d.od_rows = len(rows)
         self._desc = d
         h = C.c_void_p()
         _abi.check(_abi.lib().lsfdtd_adjoint_create(eng._h, C.byref(d), C.byref(h)), "lsfdtd_adjoint_create")

@@ -18,7 +18,10 @@
 // A periodic axis steps nodes 1 .. n-2 of both fields between two ghost planes, which the forward step fills
 // by copies (E's high ghost n-1 from plane 1 before the H update, H's low ghost 0 from plane n-2 before the
 // E update); their transposes (k_adj_ghost) move a ghost plane's adjoint onto its source plane and clear it,
-// after the transposed E update for H and after the transposed H update for E.
+// after the transposed E update for H and after the transposed H update for E. A mirror plane at node 1
+// narrows the stepped regions (the masks follow in_e_region and in_h_region); a symmetric one also fills
+// tangential H's plane 0 with minus plane 1 before the E update, transposed by k_adj_mirror. The conformal
+// off-diagonal terms, added to E after its update from the same H, are transposed (k_adj_offdiag) before it.
 //
 // The objective's adjoint source (the DFT samples' weights times e^{i omega t}) is added to Ebar and Hbar at
 // the steps the monitor sampled, before that step's reverse. The gradient with respect to the E curl
@@ -63,13 +66,16 @@ template <bool UNI, typename R>
 __device__ __forceinline__ void adj_e_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
-  // E_c's stepped range along each axis: [1, n - 1), or [0, n - 1) along c itself on a non-periodic axis
+  // E_c's stepped range along each axis (in_e_region): [1, n - 1), or [0, n - 1) along c itself on a
+  // non-periodic axis; along a mirror axis from node 1, or from 2 for the tangential components of an
+  // antisymmetric plane. okc: x in range along the component's own axis, oko: along another, nb: x + e_a
   bool okc[3], oko[3], nb[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    oko[a] = x[a] >= 1 && x[a] < g.n[a] - 1;
-    okc[a] = g.periodic[a] ? oko[a] : x[a] < g.n[a] - 1;  // along the component's own axis
-    nb[a] = x[a] + 1 < g.n[a] - 1;
+    const int lo_oth = g.mirror[a] < 0 ? 2 : 1, lo_own = (g.periodic[a] || g.mirror[a]) ? 1 : 0;
+    oko[a] = x[a] >= lo_oth && x[a] < g.n[a] - 1;
+    okc[a] = x[a] >= lo_own && x[a] < g.n[a] - 1;
+    nb[a] = x[a] + 1 >= lo_oth && x[a] + 1 < g.n[a] - 1;
   }
   R eb0[3], cb0[3], eb1[3][3], cb1[3][3];
   bool m0[3], m1[3][3];
@@ -209,25 +215,28 @@ template <bool UNI, typename R>
 __device__ __forceinline__ void adj_h_lean(const AdjArgs<R>& A, const int* x, long long p, const long long* st,
                                            R* acc) {
   const YeeArgs<R>& g = A.y;
-  // H_c's stepped range: [0, n - 1), or [0, n) along c itself; [1, n - 1) along a periodic axis. own[a]: x
-  // in range along axis a != c (and along c on a periodic axis), back[a]: x - e_a in range along a
-  bool own[3], back[3];
+  // H_c's stepped range (in_h_region): [0, n - 1), or [0, n) along c itself; [1, n - 1) along a periodic
+  // axis; along a mirror axis from node 1, or from 2 for the normal component of an antisymmetric plane.
+  // own[a]: x in range along axis a != c, alc[a]: along a == c, back[a]: x - e_a in range along a != c
+  bool own[3], back[3], alc[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    own[a] = x[a] < g.n[a] - 1 && (!g.periodic[a] || x[a] >= 1);
-    back[a] = g.periodic[a] ? x[a] >= 2 : x[a] >= 1;
+    const int lo_oth = (g.periodic[a] || g.mirror[a]) ? 1 : 0;
+    const int lo_own = g.mirror[a] < 0 ? 2 : lo_oth, hi_own = g.periodic[a] ? g.n[a] - 1 : g.n[a];
+    own[a] = x[a] >= lo_oth && x[a] < g.n[a] - 1;
+    alc[a] = x[a] >= lo_own && x[a] < hi_own;
+    back[a] = x[a] - 1 >= lo_oth;
   }
   R hb0[3], hb1[3][3];
   bool m0[3], m1[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const bool alc = !g.periodic[c] || own[c];  // along c itself
-    m0[c] = own[(c + 1) % 3] && own[(c + 2) % 3] && alc;
+    m0[c] = own[(c + 1) % 3] && own[(c + 2) % 3] && alc[c];
     hb0[c] = m0[c] ? A.Hb[c][p] : R(0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (d == c) continue;
-      m1[c][d] = back[d] && own[3 - c - d] && alc;
+      m1[c][d] = back[d] && own[3 - c - d] && alc[c];
       hb1[c][d] = m1[c][d] ? A.Hb[c][p - st[d]] : R(0);
     }
   }
@@ -345,6 +354,47 @@ __global__ void k_adj_ghost(R* f0, R* f1, R* f2, int n0, int n1, int n2, int axi
   const long long ps = ((long long)xs[0] * n1 + xs[1]) * n2 + xs[2];
   f[ps] += f[pd];
   f[pd] = R(0);
+}
+
+// Transpose of a symmetric mirror plane's ghost fill (k_mirror_ghost: the tangential H components' plane 0
+// set to minus plane 1): plane 1's adjoint loses plane 0's, and plane 0's is cleared.
+template <typename R>
+__global__ void k_adj_mirror(R* h0, R* h1, R* h2, int n0, int n1, int n2, int axis) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = axis == 0 ? n1 : n0, nb = axis == 2 ? n1 : n2;
+  const long long per = (long long)na * nb;
+  if (t >= 2 * per) return;
+  const int comp = (axis + 1 + (int)(t / per)) % 3;
+  const long long r = t % per;
+  const int u = (int)(r / nb), v = (int)(r % nb);
+  long long pg, ps;
+  if (axis == 0) {
+    pg = (long long)u * n2 + v;
+    ps = (long long)n1 * n2 + pg;
+  } else if (axis == 1) {
+    pg = (long long)u * n1 * n2 + v;
+    ps = pg + n2;
+  } else {
+    pg = ((long long)u * n1 + v) * n2;
+    ps = pg + 1;
+  }
+  R* f = comp == 0 ? h0 : (comp == 1 ? h1 : h2);
+  f[ps] -= f[pg];
+  f[pg] = R(0);
+}
+
+// Transpose of the conformal off-diagonal terms (k_offdiag: E[e[t]] += sum_k w[t][k] H[h[t][k]] after the E
+// update). The caller gives the rows transposed, one per H node that any term reads: row r adds
+// sum_{j in [ptr[r], ptr[r + 1])} w[j] Ebar[e[j]] to Hbar[h[r]]. The rows' H nodes are distinct, so one thread
+// per row needs no atomics, and each sum runs in the caller's order (the result does not depend on the launch).
+template <typename R>
+__global__ void k_adj_offdiag(const long long* h, const long long* ptr, const long long* e, const R* w,
+                              long long rows, const R* Eb, R* Hb) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  R acc = R(0);
+  for (long long j = ptr[r]; j < ptr[r + 1]; ++j) acc += w[j] * Eb[e[j]];
+  Hb[h[r]] += acc;
 }
 
 constexpr int kAdjMaxFreq = 128;

@@ -160,6 +160,8 @@ struct lsfdtd_engine {
   virtual int adjoint_args(void* yee, size_t bytes, void** H) = 0;
   // the dispersive groups (AdeArgs of a real engine), for the adjoint
   virtual int adjoint_n_groups() const = 0;
+  // the conformal off-diagonal terms (rows, entries per row), for the adjoint
+  virtual void adjoint_offdiag(long long* rows, int* width) const = 0;
   virtual int adjoint_group(int gi, void* out, size_t bytes) = 0;
 };
 
@@ -733,15 +735,17 @@ struct Engine final : lsfdtd_engine {
 
   int adjoint_args(void* yee, size_t bytes, void** H) override {
     if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
-    if (desc.mirror[0] || desc.mirror[1] || desc.mirror[2])
-      return fail(LSFDTD_EUNSUPPORTED, "adjoint: no mirror plane");
-    if (od_n > 0) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no conformal off-diagonal terms");
     if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no vertex-tensor mesh");
     if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
     const YeeArgs<F> a = current_args();
     std::memcpy(yee, &a, sizeof a);
     *H = Hflat();
     return LSFDTD_OK;
+  }
+
+  void adjoint_offdiag(long long* rows, int* width) const override {
+    *rows = od_n;
+    *width = od_width;
   }
 
   int bloch_desc(void* out, size_t bytes, int64_t last) override {
@@ -1711,8 +1715,8 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
   A.grad = a->d.grad;
   // inner node ranges per axis: in every component's stepped region and past every slab of the field
   for (int ax = 0; ax < 3; ++ax) {
-    const int n = A.y.n[ax];
-    int elo = 1, ehi = n - 1, hlo = A.y.periodic[ax] ? 1 : 0, hhi = n - 1;
+    const int n = A.y.n[ax], mir = A.y.mirror[ax];
+    int elo = mir < 0 ? 2 : 1, ehi = n - 1, hlo = mir < 0 ? 2 : ((A.y.periodic[ax] || mir) ? 1 : 0), hhi = n - 1;
     const PmlAxis<R>& pm = A.y.pml[ax];
     if (pm.on) {
       const int c = (ax + 1) % 3;  // a component with slabs along ax (both share their extent)
@@ -1756,9 +1760,25 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
     }
     return LSFDTD_OK;
   };
+  // the off-diagonal terms were added to E from the H the E update read
+  if (a->d.od_rows > 0) {
+    k_adj_offdiag<R><<<cdiv(a->d.od_rows, 256), 256, 0, s>>>(
+        reinterpret_cast<const long long*>(a->d.od_h), reinterpret_cast<const long long*>(a->d.od_ptr),
+        reinterpret_cast<const long long*>(a->d.od_e), static_cast<const R*>(a->d.od_w), a->d.od_rows, A.Eb[0],
+        A.Hb[0]);
+    LS_LAUNCHED();
+  }
   if (A.y.uniform) k_adj_e<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
   else k_adj_e<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
   LS_LAUNCHED();
+  // the symmetric mirror planes' ghosts were filled after the periodic ones, before the E update
+  for (int ax = 2; ax >= 0; --ax) {
+    if (A.y.mirror[ax] <= 0) continue;
+    const long long plane = cells / A.y.n[ax];
+    k_adj_mirror<R><<<cdiv(2 * plane, 256), 256, 0, s>>>(A.Hb[0], A.Hb[1], A.Hb[2], A.y.n[0], A.y.n[1], A.y.n[2],
+                                                        ax);
+    LS_LAUNCHED();
+  }
   LS_TRY(ghosts_t(A.Hb, true));  // H's low ghosts were filled before the E update
   if (A.y.uniform) k_adj_h<R, true><<<grid, dim3(32, 8), 0, s>>>(A);
   else k_adj_h<R, false><<<grid, dim3(32, 8), 0, s>>>(A);
@@ -2250,9 +2270,35 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
     a->groups.push_back(std::move(ga));
   }
   const int32_t* n = eng->desc.shape;
+  // inside every E component's stepped region: from node 2 along an antisymmetric mirror plane's axis
   for (int ax = 0; ax < 3; ++ax)
-    if (d->box_lo[ax] < 1 || d->box_hi[ax] > n[ax] - 1 || d->box_hi[ax] <= d->box_lo[ax])
+    if (d->box_lo[ax] < (eng->desc.mirror[ax] < 0 ? 2 : 1) || d->box_hi[ax] > n[ax] - 1 ||
+        d->box_hi[ax] <= d->box_lo[ax])
       return fail(LSFDTD_EINVAL, "adjoint: gradient box out of range");
+  long long od_rows = 0;
+  int od_width = 0;
+  eng->adjoint_offdiag(&od_rows, &od_width);
+  if (od_rows > 0) {
+    if (d->od_rows <= 0 || !d->od_h || !d->od_ptr || !d->od_e || !d->od_w)
+      return fail(LSFDTD_EINVAL, "adjoint: the engine has conformal off-diagonal terms; give them transposed");
+    // index ranges checked here, once (the kernel trusts them)
+    const long long flat = 3LL * n[0] * n[1] * n[2];
+    std::vector<long long> ptr(d->od_rows + 1), hh(d->od_rows);
+    LS_CUDA(cudaMemcpy(ptr.data(), d->od_ptr, ptr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    LS_CUDA(cudaMemcpy(hh.data(), d->od_h, hh.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    if (ptr[0] != 0 || ptr.back() > od_rows * (long long)od_width)
+      return fail(LSFDTD_EINVAL, "adjoint: off-diagonal row pointers out of range");
+    for (long long r = 0; r < d->od_rows; ++r)
+      if (ptr[r + 1] < ptr[r] || hh[r] < 0 || hh[r] >= flat)
+        return fail(LSFDTD_ERANGE, "adjoint: an off-diagonal row out of range");
+    std::vector<long long> ee(ptr.back());
+    if (!ee.empty())
+      LS_CUDA(cudaMemcpy(ee.data(), d->od_e, ee.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    for (long long v : ee)
+      if (v < 0 || v >= flat) return fail(LSFDTD_ERANGE, "adjoint: an off-diagonal E index out of range");
+  } else if (d->od_rows != 0) {
+    return fail(LSFDTD_EINVAL, "adjoint: off-diagonal rows given for an engine without such terms");
+  }
   // every E node of the box outside every E slab (there the E update's coefficient enters only through the
   // curl term; the H values of the box and its halo are recorded, wherever they lie)
   auto slabs_ok = [&](const auto& y) {

@@ -23,7 +23,8 @@ def scattering_setup(sim):
     """(plan, post, layout) for lightsmith ``Simulation`` ``sim``: ``plan`` as ``plan.make_plan`` makes it from the
     driver's ``Engine(...)`` arguments; ``post`` with ``wavelengths_nm``, ``omega``, ``n_inc``, ``n_sym``,
     ``sca_coeff`` and ``tot_coeff`` (the flux weights of the scattered- and total-field boxes, in their points'
-    order); ``layout`` lightsmith's grid layout (origin, TF/SF box, spacing)."""
+    order); ``layout`` lightsmith's grid layout of the run (origin, TF/SF box, spacing; with mirror planes the
+    part the run steps, symmetry.py:116-127)."""
     from lightsmith.backends._fdtd import scattering as S
     from lightsmith.backends._fdtd import symmetry as Y
     from lightsmith.backends._fdtd.setup import scattering_layout
@@ -61,7 +62,7 @@ def scattering_setup(sim):
     post = {"wavelengths_nm": wl, "omega": 2 * np.pi / wl, "n_inc": float(getattr(src, "n_inc", sim.medium_index)),
             "n_sym": float(Y.factor(kw.get("mirror", (0, 0, 0)))),
             "sca_coeff": np.asarray(boxes[0][3], dtype=float), "tot_coeff": np.asarray(boxes[1][3], dtype=float)}
-    lay = scattering_layout(sim, opts, float(opts.spacing_nm))
+    lay = Y.halve(scattering_layout(sim, opts, float(opts.spacing_nm)), tuple(kw.get("mirror", (0, 0, 0))))
     return got["plan"], post, lay
 
 

@@ -85,3 +85,27 @@ def test_autograd_restatement_with_a_mixed_group_matches_oracle():
     assert abs(J0) > 0
     assert abs(J - J0) / abs(J0) < 1e-12
 
+
+
+def test_transposed_offdiag_rows_are_the_gather_transposed():
+    """``transposed_offdiag`` against the forward gather it transposes, on a random table shaped as the plan's
+    (distinct targets, padded rows with zero weights, H nodes shared between rows): <Ebar, W H> = <W^T Ebar, H>
+    to rounding, distinct ascending rows, and no zero weight kept."""
+    from lightsmith_b200.adjoint import transposed_offdiag
+
+    rng = np.random.default_rng(7)
+    n_flat, n_rows, width = 600, 80, 6
+    e = rng.choice(n_flat, n_rows, replace=False)
+    h = np.stack([rng.choice(n_flat // 4, width, replace=False) for _ in range(n_rows)])
+    w = rng.normal(size=(n_rows, width))
+    w[rng.random(size=w.shape) < 0.3] = 0.0
+    H, Eb = rng.normal(size=n_flat), rng.normal(size=n_flat)
+    WH = np.zeros(n_flat)
+    WH[e] = (w * H[h]).sum(axis=1)
+    rows, ptr, ee, ww = transposed_offdiag({"e": e, "h": h, "w": w})
+    assert np.all(np.diff(rows) > 0) and ptr[0] == 0 and ptr[-1] == len(ee) == np.count_nonzero(w)
+    assert np.all(ww != 0)
+    WtE = np.zeros(n_flat)
+    for r, q in enumerate(rows):
+        WtE[q] = sum(ww[j] * Eb[ee[j]] for j in range(ptr[r], ptr[r + 1]))
+    assert abs(Eb @ WH - WtE @ H) <= 1e-12 * np.abs(Eb).sum() * np.abs(WH).max()

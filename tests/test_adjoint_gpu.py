@@ -325,6 +325,88 @@ def test_cluster_scattering_gradient_matches_finite_differences():
     run.close()
 
 
+def _fd_check(run, base, g, n_steps, flats, h=1e-6, tol=1e-5):
+    """Central differences of the CUDA forward at the box nodes ``flats`` (the three E components of a node
+    together when ``base`` holds one value per component) against the adjoint's gradient ``g``."""
+    for flat in flats:
+        idx = tuple(int(v) for v in np.unravel_index(int(flat), g.shape))
+        vals = []
+        for sgn in (1, -1):
+            x = base.clone()
+            if x.dim() == 4:
+                x[(slice(None),) + idx] += sgn * h
+            else:
+                x[idx] += sgn * h
+            run.set_inv_eps_box(x)
+            vals.append(run.forward(n_steps, keep=False)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[idx]) <= tol * abs(fd), (idx, fd, g[idx])
+    run.set_inv_eps_box(base)
+
+
+def test_default_scattering_pose_gradient_matches_finite_differences(monkeypatch):
+    """A dielectric sphere posed to lightsmith with its defaults: mirror planes through the centre (symmetry
+    "auto": an antisymmetric plane normal to x and a symmetric one normal to y for the x-polarised plane wave)
+    and conformal meshing (the off-diagonal terms of its tensor smoothing), float64. J = sum_f C_sca(f) of the
+    scattered-field box; dJ/d(1/eps) over a box around the sphere, its interface cells with off-diagonal rows
+    among its nodes, against central differences of the CUDA forward at its largest entries and at the largest
+    on the planes next to each mirror plane. Without the transposed off-diagonal rows the C-ABI refuses."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from refsrc import add_to_path
+
+    if not add_to_path():
+        pytest.skip("lightsmith (the reference install, baseline/_ref) not available")
+    import lightsmith as ls
+
+    from lightsmith_b200 import adjoint as A
+    from lightsmith_b200.scattering import cross_section_objective, scattering_setup
+
+    r = 14.0
+    sim = ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=r), material=ls.ConstantIndex(n_real=2.0),
+                                               position_nm=(0.0, 0.0, 0.0))],
+                        medium_index=1.33, wavelengths={"start_nm": 450.0, "stop_nm": 650.0, "num": 4},
+                        options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, padding_nm=16.0, pml_gap_nm=8.0,
+                                              run_time_fs=6.0, precision="double")})
+    plan, post, lay = scattering_setup(sim)
+    assert tuple(plan["mirror"]) == (-1, 1, 0) and len(plan["offdiag"]["e"]) > 0
+    shape = tuple(int(v) for v in plan["shape"])
+    pos = [np.asarray(lay.origin, float)[a] + 4.0 * np.arange(shape[a]) for a in range(3)]
+    lo_node = [2, 1, 0]  # the first node every E component steps: 2 next to the antisymmetric plane
+    box = tuple((max(lo_node[a], int(np.searchsorted(pos[a], -r - 6.0))),
+                 int(np.searchsorted(pos[a], r + 6.0, side="right"))) for a in range(3))
+    rest = np.asarray(plan["offdiag"]["e"]) % int(np.prod(shape))
+    ijk = np.stack(np.unravel_index(rest, shape), axis=1)
+    assert np.any(np.all((ijk >= [a for a, _ in box]) & (ijk < [b for _, b in box]), axis=1))
+    stride = int(plan["stride"])
+    n_steps = 10 * stride
+    ref: dict = {}
+    J_of = cross_section_objective(post, ref)
+    with monkeypatch.context() as m:  # no transposed rows: refused
+        m.setattr(A, "transposed_offdiag", lambda od: tuple(np.zeros(k, dt) for k, dt in
+                                                             ((0, np.int64), (1, np.int64), (0, np.int64),
+                                                              (0, np.float64))))
+        with pytest.raises(RuntimeError, match="off-diagonal"):
+            A.AdjointRun(plan, box, objective=J_of, checkpoint=2 * stride, precision="double")
+    run = A.AdjointRun(plan, box, objective=J_of, checkpoint=2 * stride, precision="double")
+    ref["acc_ref"] = run.eng.monitors[2]["acc_e"]
+    inv = np.asarray(plan["inv_eps"]).reshape((-1,) + shape)
+    base = torch.as_tensor(inv[(slice(None),) + tuple(slice(a, b) for a, b in box)]).clone()
+    run.set_inv_eps_box(base)
+    J0, _ = run.forward(n_steps)
+    g = run.backward().cpu().numpy()
+    assert J0 > 0 and np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    flats = list(np.argsort(-np.abs(g).reshape(-1))[:3])
+    for a in (0, 1):  # the largest entry on the box's face next to each mirror plane
+        face = np.zeros(g.shape, bool)
+        face[(slice(None),) * a + (0,)] = True
+        flats.append(int(np.argmax(np.where(face, np.abs(g), -1).reshape(-1))))
+    _fd_check(run, base, g, n_steps, flats)
+    run.close()
+
+
 def test_mixed_dispersive_group_gradient():
     """A mixed D-form group (lightsmith's subpixel interface cells of a Drude-Lorentz metal and a dielectric,
     both paths running) between the dipole and the design box, the flux spectrum as the objective: the float64
