@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const unsigned nx = n0 - 2, ny = n1 - 2, un2 = n2;
     const long long s1 = n2, s0 = (long long)n1 * n2;
+    const unsigned us1 = n2, us0 = (unsigned)n1 * n2;  // 32-bit node offsets within a component
     const unsigned n_main = nx * ny * un2;  // fewer than 2^32 nodes (checked on the host)
     const unsigned n_work = n_main + un2;   // the cell's interior nodes, then the column's (1, 1, z)
     const long long cs1 = n2, cs0 = 3LL * n2;
@@ -223,7 +224,9 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     long long n = *r.nstep;
     // a run that turned non-finite in an earlier launch is skipped (the word was written before this launch)
     long long n_end = *reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite ? n : min(n + (long long)steps, r.last);
-    bool bad = false;  // this thread's E values of the run: any non-finite
+    // this thread's E values of the run times zero, summed: zero while every value is finite, NaN after one
+    // is not (cheaper than testing each value)
+    R nonfinite = R(0);
     if (!sync()) return;  // every thread has read the counter
     if (n < n_end) {
       // E's high ghosts as lightsmith refreshes them before each H update (x = n0 - 1 from x = 1, then
@@ -269,10 +272,10 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           const int z = (int)(w - t * un2);
           const unsigned xm = udiv(t, r.div_ny);
           const int x = 1 + (int)xm, y = 1 + (int)(t - xm * ny);
-          const long long p = x * s0 + y * s1 + z;
+          const unsigned p = (unsigned)x * us0 + (unsigned)y * us1 + (unsigned)z;
           const bool zin = z <= n2 - 2;
           const F e0 = g.E[0][p], e1 = g.E[1][p], e2 = g.E[2][p];
-          const F e2y = g.E[2][p + s1], e2x = g.E[2][p + s0], e1x = g.E[1][p + s0], e0y = g.E[0][p + s1];
+          const F e2y = g.E[2][p + us1], e2x = g.E[2][p + us0], e1x = g.E[1][p + us0], e0y = g.E[0][p + us1];
           const F e1z = zin ? g.E[1][p + 1] : e1, e0z = zin ? g.E[0][p + 1] : e0;
           // (a, b) per component: H_c -= cH (dE_{d2}/dd1 - dE_{d1}/dd2)
           const F av[3] = {e2y - e2, e0z - e0, e1x - e1};
@@ -352,11 +355,11 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           const int z = (int)(w - t * un2);
           const unsigned xm = udiv(t, r.div_ny);
           const int x = 1 + (int)xm, y = 1 + (int)(t - xm * ny);
-          const long long p = x * s0 + y * s1 + z;
+          const unsigned p = (unsigned)x * us0 + (unsigned)y * us1 + (unsigned)z;
           if (z > n2 - 2) continue;
           const bool zlo = z >= 1;
           const F h0 = g.H[0][p], h1 = g.H[1][p], h2 = g.H[2][p];
-          const F h2y = g.H[2][p - s1], h2x = g.H[2][p - s0], h1x = g.H[1][p - s0], h0y = g.H[0][p - s1];
+          const F h2y = g.H[2][p - us1], h2x = g.H[2][p - us0], h1x = g.H[1][p - us0], h0y = g.H[0][p - us1];
           const F h1z = zlo ? g.H[1][p - 1] : h1, h0z = zlo ? g.H[0][p - 1] : h0;
           // (a, b) per component: E_c += cbE_c (dH_{d2}/dd1 - dH_{d1}/dd2)
           const F av[3] = {h2 - h2y, h0 - h0z, h1 - h1x};
@@ -403,7 +406,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
               e += psi;
             }
             if (plane && c < 2) e = c == 0 ? e + r.cE * inc[0] : e - r.cE * inc[1];  // correct_E
-            bad |= !(isfinite(e.re) && isfinite(e.im));
+            nonfinite += e.re * R(0) + e.im * R(0);
             g.E[c][p] = e;
             // high ghosts (x = n0 - 1 from x = 1, then y = n1 - 1 from y = 1, and the corner)
             if (!through) continue;
@@ -433,7 +436,7 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
           }
         }
       }
-      if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(r.status, kBatchNonFinite);
+      if (__any_sync(0xffffffffu, nonfinite != R(0)) && (threadIdx.x & 31) == 0) atomicExch(r.status, kBatchNonFinite);
       if (!sync()) return;
       if (*reinterpret_cast<volatile int*>(r.status) == kBatchNonFinite) {  // every CTA reads it after the barrier
         n_end = n + 1;

@@ -2135,7 +2135,8 @@ int32_t lsfdtd_batch_create_shaped(lsfdtd_engine* const* engines, int32_t n, con
   b->ctas = clusters * cluster_ctas;
   for (int32_t i = 0; i < n; ++i) {
     const auto& d = b->engines[i]->desc;
-    if ((double)(d.shape[0] - 2) * (d.shape[1] - 2) * d.shape[2] + d.shape[2] >= 4294967296.0)
+    // the kernel's node offsets within a component are 32-bit
+    if ((double)d.shape[0] * d.shape[1] * d.shape[2] >= 4294967296.0)
       return fail(LSFDTD_EUNSUPPORTED, "batch: a run of 2^32 nodes or more");
   }
   std::vector<double> cost(n);
