@@ -450,6 +450,33 @@ typedef struct lsfdtd_adjoint_desc {
   const int64_t* od_e;
   const void* od_w;
   int64_t od_rows;
+  /* the engine's vertex-tensor mesh (lsfdtd_engine_add_tensor), required when it has one: tm_bar its adjoint
+   * state, lsfdtd_tensor_state_len scalars laid out as the forward state, zeroed; tm_work 6 n_vert + 2 n_tslots
+   * + n_pslots scalars of scratch; the slots by vertex (tm_vs_ptr (n_vert + 1), tm_vs_idx (n_tslots): the
+   * tensor slots of vertex v, ascending) and the contributions by node (tm_nd_ptr (n_nodes + 1), tm_nd_src:
+   * for node i the positions, ascending, among the 6 n_vert vertex entries (v * 6 + 2 d + side, the node
+   * vn[v * 6 + 2 d + side]), then the n_tslots tensor slots (the node vn[t_g[t]]), then the n_pslots plain
+   * slots (the node p_node[p]) that read its D). Device arrays, the engine's precision. */
+  void* tm_bar;
+  void* tm_work;
+  const int64_t* tm_vs_ptr;
+  const int64_t* tm_vs_idx;
+  const int64_t* tm_nd_ptr;
+  const int64_t* tm_nd_src;
+  /* the objective's adjoint source by target node, in a fixed order (optional; without it each point adds its
+   * value with an atomic add, whose order can change the last bit of a node that several points share): the
+   * distinct E targets inj_e_tgt (inj_n_e) with, per target r, the E points inj_e_src[inj_e_ptr[r] ..
+   * inj_e_ptr[r + 1]] that sample it, ascending; the distinct H targets inj_h_tgt (inj_n_h) with their H points
+   * (a point listed once for each of its two samples at the target); inj_work n_e + n_h doubles of scratch */
+  const int64_t* inj_e_tgt;
+  const int64_t* inj_e_ptr;
+  const int64_t* inj_e_src;
+  int64_t inj_n_e;
+  const int64_t* inj_h_tgt;
+  const int64_t* inj_h_ptr;
+  const int64_t* inj_h_src;
+  int64_t inj_n_h;
+  double* inj_work;
 } lsfdtd_adjoint_desc;
 
 /* sets the engine's host step count (after the caller rewinds its device counter and fields to a saved step,

@@ -98,7 +98,10 @@ class AdjointDesc(C.Structure):
                 ("hist", vp), ("hist_slots", i32), ("grad", vp), ("e_idx", vp), ("ge", vp), ("n_e", i64),
                 ("h_idx1", vp), ("h_idx2", vp), ("gh", vp), ("n_h", i64), ("omega", vp), ("n_freq", i32),
                 ("n_groups", i32), ("group_bar", vp * 8), ("od_h", vp), ("od_ptr", vp), ("od_e", vp), ("od_w", vp),
-                ("od_rows", i64)]
+                ("od_rows", i64), ("tm_bar", vp), ("tm_work", vp), ("tm_vs_ptr", vp), ("tm_vs_idx", vp),
+                ("tm_nd_ptr", vp), ("tm_nd_src", vp), ("inj_e_tgt", vp), ("inj_e_ptr", vp), ("inj_e_src", vp),
+                ("inj_n_e", i64), ("inj_h_tgt", vp), ("inj_h_ptr", vp), ("inj_h_src", vp), ("inj_n_h", i64),
+                ("inj_work", vp)]
 
 
 # the GPU voxeliser's descriptors (lsfdtd_vox_* in include/lsfdtd.h)

@@ -3,9 +3,10 @@
 lightsmith's FDTD has no gradient (its inverse design runs through other solvers). This module adds one for
 the FDTD path: for a run with real fields (periodic axes allowed, without a Bloch phase; mirror planes, as
 lightsmith's scattering driver picks them by default) with dispersive groups, pure (staircase) or mixed
-(subpixel interface cells), and the conformal off-diagonal terms of its default dielectric meshing (a slab
-waveguide device, a metal nanoparticle cluster, a 2D device with its periodic invariant axis, a dielectric
-particle in a mirrored run), a real objective J of one DFT monitor's accumulators (or several monitors'),
+(subpixel interface cells), the conformal off-diagonal terms of its default dielectric meshing and the
+vertex-tensor mesh of its default meshing next to a dispersive medium (a slab waveguide device, a metal
+nanoparticle cluster, a 2D device with its periodic invariant axis, a dielectric or metal particle in a
+mirrored run), a real objective J of one DFT monitor's accumulators (or several monitors'),
 and its gradient with respect to 1/eps over a design box of non-dispersive nodes. J is either
 |sum_p wE_p acc_e[f, p] + sum_q wH_q acc_h[f, q]|^2 at one frequency f, or any torch function of the
 accumulators (a flux spectrum, say): its adjoint source G = 2 dJ/d(acc) comes from torch autograd on J.
@@ -23,7 +24,10 @@ of the previous step and the poles' P; for a mixed group also each medium's harm
 arithmetic path's E) is linear too: its transpose (``k_adj_ade``) runs before the E update's, and its state
 is part of each checkpoint. The off-diagonal terms (E += W H after the E update) are transposed by a gather
 over the rows of W^T (``transposed_offdiag``); the gradient holds W fixed (it is the derivative with respect to
-the diagonal 1/eps of the box, W's entries being separate coefficients).
+the diagonal 1/eps of the box, W's entries being separate coefficients). The vertex-tensor mesh's step runs
+last in a forward step and is linear with fixed coefficients; its transpose (``k_adj_tm_*``) runs first in a
+reverse step, on an adjoint state laid out as its forward state, with gathers over the inverse maps of
+``tensor_adjoint_maps``; its forward state is part of each checkpoint.
 
 ``FDTDObjective.apply(inv_eps_box, run)`` is the ``torch.autograd.Function``: forward returns J, backward
 dJ/d(1/eps) of the box (isotropic: the three E components of a node share its 1/eps, so the gradient is
@@ -63,6 +67,37 @@ def transposed_offdiag(od: dict):
     ee, hh, ww = ee[order], hh[order], ww[order]
     rows, start = np.unique(hh, return_index=True)
     return rows, np.append(start, len(hh)).astype(np.int64), ee, ww
+
+
+def injection_map(targets, points):
+    """(tgt, ptr, src): the distinct target nodes ``targets`` holds, ascending, and for target r the points
+    src[ptr[r]:ptr[r + 1]] (from ``points``, in the same order as ``targets``) that sample it, ascending."""
+    t, p = np.asarray(targets, np.int64), np.asarray(points, np.int64)
+    order = np.lexsort((p, t))
+    t, p = t[order], p[order]
+    tgt, start = np.unique(t, return_index=True)
+    return tgt.astype(np.int64), np.append(start, len(t)).astype(np.int64), p
+
+
+def tensor_adjoint_maps(tm: dict):
+    """The inverse maps of a vertex-tensor mesh (``plan["tensor"]``) for its transposed step: (vs_ptr, vs_idx)
+    the tensor slots of each vertex, ascending; (nd_ptr, nd_src) for each node the entries that read its D,
+    ascending among the 6 n_vert (vertex, axis, side) entries (node ``vn[e]``), the n_tslots tensor slots (node
+    ``vn[t_g[t]]``) and the n_pslots plain slots (node ``p_node[p]``), in that order; and the scratch length,
+    6 n_vert + 2 n_tslots + n_pslots."""
+    def ints(key):
+        a = tm.get(key)
+        return np.zeros(0, np.int64) if a is None else np.asarray(a, np.int64)
+    n_nodes, n_vert = int(tm["n_nodes"]), len(np.asarray(tm["normal"])) // 3
+    vn, t_v, t_vc, t_g, p_node = ints("vn"), ints("t_v"), ints("t_vc"), ints("t_g"), ints("p_node")
+    if len(vn) != 6 * n_vert or np.any(t_vc // 3 != t_v):
+        raise ValueError("vertex-tensor tables: each slot's component must be one of its vertex's")
+    vs_idx = np.argsort(t_v, kind="stable").astype(np.int64)
+    vs_ptr = np.concatenate([[0], np.cumsum(np.bincount(t_v, minlength=n_vert))]).astype(np.int64)
+    node_of = np.concatenate([vn, vn[t_g], p_node])
+    nd_src = np.argsort(node_of, kind="stable").astype(np.int64)
+    nd_ptr = np.concatenate([[0], np.cumsum(np.bincount(node_of, minlength=n_nodes))]).astype(np.int64)
+    return vs_ptr, vs_idx, nd_ptr, nd_src, 6 * n_vert + 2 * len(t_v) + len(p_node)
 
 
 class AdjointRun:
@@ -160,6 +195,21 @@ class AdjointRun:
             self.gh = torch.zeros((nf, len(mon["h_idx1"]), 2), dtype=torch.float64, device=self.dev)
             d.h_idx1, d.h_idx2, d.gh, d.n_h = self.h1.data_ptr(), self.h2.data_ptr(), self.gh.data_ptr(), len(
                 mon["h_idx1"])
+        # the adjoint source gathered per target node in a fixed order (flux boxes share nodes between points)
+        e_t, e_p, e_s = injection_map(mon["e_idx"], np.arange(len(mon["e_idx"])))
+        self._inj = [torch.as_tensor(a, dtype=i64, device=self.dev) for a in (e_t, e_p, e_s)]
+        d.inj_e_tgt, d.inj_e_ptr, d.inj_e_src = (t.data_ptr() for t in self._inj)
+        d.inj_n_e = len(e_t)
+        if self.has_h:
+            nh = len(mon["h_idx1"])
+            h_t, h_p, h_s = injection_map(np.concatenate([mon["h_idx1"], mon["h_idx2"]]),
+                                          np.concatenate([np.arange(nh), np.arange(nh)]))
+            self._inj += [torch.as_tensor(a, dtype=i64, device=self.dev) for a in (h_t, h_p, h_s)]
+            d.inj_h_tgt, d.inj_h_ptr, d.inj_h_src = (t.data_ptr() for t in self._inj[3:])
+            d.inj_n_h = len(h_t)
+        self._inj.append(torch.zeros(max(len(mon["e_idx"]) + (len(mon["h_idx1"]) if self.has_h else 0), 1),
+                                     dtype=torch.float64, device=self.dev))
+        d.inj_work = self._inj[-1].data_ptr()
         om = (C.c_double * nf)(*self.omegas.tolist())
         d.omega = C.cast(om, C.c_void_p)
         d.n_freq = nf
@@ -175,6 +225,15 @@ class AdjointRun:
                         torch.as_tensor(e, device=self.dev), torch.as_tensor(w, dtype=eng.fdt, device=self.dev)]
             d.od_h, d.od_ptr, d.od_e, d.od_w = (t.data_ptr() for t in self._od)
             d.od_rows = len(rows)
+        self._tm_bar = []
+        tm = plan.get("tensor")
+        if tm is not None and int(tm["n_nodes"]) > 0:  # the vertex-tensor mesh: adjoint state, scratch and maps
+            vs_ptr, vs_idx, nd_ptr, nd_src, n_work = tensor_adjoint_maps(tm)
+            self._tm_bar = [torch.zeros_like(eng.tensor["state"])]
+            self._tm = [torch.zeros(max(n_work, 1), dtype=eng.fdt, device=self.dev)] + [
+                torch.as_tensor(a, device=self.dev) for a in (vs_ptr, vs_idx, nd_ptr, nd_src)]
+            d.tm_bar = self._tm_bar[0].data_ptr()
+            d.tm_work, d.tm_vs_ptr, d.tm_vs_idx, d.tm_nd_ptr, d.tm_nd_src = (t.data_ptr() for t in self._tm)
         self._desc = d
         h = C.c_void_p()
         _abi.check(_abi.lib().lsfdtd_adjoint_create(eng._h, C.byref(d), C.byref(h)), "lsfdtd_adjoint_create")
@@ -272,7 +331,7 @@ class AdjointRun:
             self.gh.copy_(torch.view_as_real(g_h.conj().resolve_conj()))
         self.Eb.zero_()
         self.Hb.zero_()
-        for t in self.group_bar:
+        for t in self.group_bar + self._tm_bar:
             t.zero_()
         for b in range(2):
             for f in range(2):

@@ -31,6 +31,7 @@
 
 #include "ade.cuh"
 #include "common.cuh"
+#include "tensor.cuh"
 #include "yee.cuh"
 
 namespace lsfdtd {
@@ -397,6 +398,135 @@ __global__ void k_adj_offdiag(const long long* h, const long long* ptr, const lo
   Hb[h[r]] += acc;
 }
 
+// ---- the vertex-tensor ADE, transposed ----
+// Forward, after the groups (tensor.cuh): D' = D + E[idx] - E_prev per node; per vertex the means D~_d of its
+// d-nodes and s = n . D~; per tensor slot sigma = s + n_c (D_p - D~_c) into its harmonic (a) and arithmetic (b)
+// operators, out = (b + n_c a) / 2; per plain slot out = m[D] / 2; then E[idx] = E_prev = out[i] + out[nN + i].
+// Every map is linear with fixed coefficients, so the reverse step needs no forward values: it applies the
+// transposes in the opposite order to an adjoint state laid out as the forward's (the bars of D, E_prev and of
+// the path and pole states; `out`'s place holds each output's adjoint). Fan-ins are gathers over maps the caller
+// builds (the slots of each vertex, the contributions to each node), so every sum runs in a fixed order. The
+// work array: contrib, per (vertex, axis, side) [6 nV], tensor slot [nT] and plain slot [nP] the adjoint that
+// entry sends to one node's D'; then sig [nT], each tensor slot's sigma adjoint.
+
+// the poles of medium s at slot t of n, transposed: from the adjoint tbar of their sum (added to each new P_k's
+// adjoint), the adjoints of the old P_k and P'_k (in place) and the returned adjoint of the drive
+template <typename R>
+__device__ __forceinline__ R adj_tm_poles(const TensorArgs<R>& b, int s, R* P, long long t, long long n, R tbar) {
+  R drive = R(0);
+  for (int k = 0; k < b.n_poles[s]; ++k) {
+    R* pk = P + (2 * k) * n;
+    R* pp = P + (2 * k + 1) * n;
+    const R hat = pk[t] + tbar;
+    pk[t] = b.c1[s][k] * hat + pp[t];
+    pp[t] = b.c2[s][k] * hat;
+    drive += b.c3[s][k] * hat;
+  }
+  return drive;
+}
+
+// E[idx] = E_prev = out[i] + out[nN + i]: both slots' adjoint is that of the node's new E and E_prev; E's own
+// adjoint there restarts (the curl update's value was overwritten) and D's path adds to it (k_adj_tm_nodes_d)
+template <typename R>
+__global__ void k_adj_tm_out(TensorArgs<R> b, R* Eb) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.nN) return;
+  const long long q = b.idx[i];
+  const R e = Eb[q] + b.Ep[i];
+  Eb[q] = R(0);
+  b.Ep[i] = R(0);
+  b.out[i] = e;
+  b.out[b.nN + i] = e;
+}
+
+template <typename R>
+__global__ void k_adj_tm_plain(TensorArgs<R> b, R* work) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= b.nP) return;
+  const int m = (int)b.p_medium[p];
+  R ybar = R(0.5) * b.out[b.p_pos[p]];
+  R ubar;
+  if (!b.n_poles[m]) {
+    ubar = ybar * (R(1) / b.eps_inf[m]);
+  } else {  // y = (u - sum of the poles) / eps_inf, kept as the next step's drive
+    ybar += b.pl_E[m][p];
+    ubar = ybar * b.inv_inf[m];
+    b.pl_E[m][p] = adj_tm_poles(b, m, b.pl_P[m], p, b.nP, -ubar);
+  }
+  work[6 * b.nV + b.nT + p] = ubar;
+}
+
+template <typename R>
+__global__ void k_adj_tm_slots(TensorArgs<R> b, R* work) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.nT) return;
+  const R nc = b.t_nc[t];
+  const R cbar = b.out[b.t_pos[t]];
+  // b[u_b] = (u_b - sum_s f_s poles_s(y_prev)) / <eps>, kept as y
+  R den = R(0);
+  for (int s = 0; s < b.n_media; ++s) den += b.frac[s * b.nT + t] * b.eps_inf[s];
+  const R accbar = (R(0.5) * cbar + b.ar_y[t]) * (R(1) / den);
+  R drive = R(0);
+  for (int s = 0; s < b.n_media; ++s)
+    if (b.n_poles[s]) drive += adj_tm_poles(b, s, b.ar_P[s], t, b.nT, -(b.frac[s * b.nT + t] * accbar));
+  b.ar_y[t] = drive;
+  // a[u_a] = u_a h0 + sum_s f_s E_s, E_s = (u_a - poles_s(E_s prev)) / eps_inf_s
+  const R yabar = R(0.5) * nc * cbar;
+  R h0 = R(0);
+  for (int s = 0; s < b.n_media; ++s)
+    if (!b.n_poles[s]) h0 += b.frac[s * b.nT + t] / b.eps_inf[s];
+  R uabar = yabar * h0;
+  for (int s = 0; s < b.n_media; ++s) {
+    if (!b.n_poles[s]) continue;
+    const R g = (b.frac[s * b.nT + t] * yabar + b.ha_E[s][t]) * b.inv_inf[s];
+    uabar += g;
+    b.ha_E[s][t] = adj_tm_poles(b, s, b.ha_P[s], t, b.nT, -g);
+  }
+  // u_a = sigma, u_b = D_p - n_c sigma, sigma = s_v + n_c (D_p - D~_c)
+  const R sg = uabar - nc * accbar;
+  const R dpbar = accbar + nc * sg;
+  work[6 * b.nV + b.nT + b.nP + t] = sg;
+  work[6 * b.nV + t] = (b.scale ? b.scale[b.t_g[t]] : R(1)) * dpbar;
+}
+
+// per vertex: s's adjoint (its slots' sigma adjoints) and D~_d's (n_d times it, less n_c sigma adjoint of the
+// slots on component d), each mean's half to its two d-nodes with their parity
+template <typename R>
+__global__ void k_adj_tm_vertices(TensorArgs<R> b, R* work, const long long* vs_ptr, const long long* vs_idx) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= b.nV) return;
+  const R* sig = work + 6 * b.nV + b.nT + b.nP;
+  R sv = R(0), ex[3] = {R(0), R(0), R(0)};
+  for (long long j = vs_ptr[v]; j < vs_ptr[v + 1]; ++j) {
+    const long long t = vs_idx[j];
+    const R sgt = sig[t];
+    sv += sgt;
+    const int c = (int)(b.t_vc[t] - 3 * v);
+    ex[c] -= b.t_nc[t] * sgt;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const R h = R(0.5) * (b.normal[v * 3 + d] * sv + ex[d]);
+    const long long e = v * 6 + 2 * d;
+    work[e] = (b.scale ? b.scale[e] : R(1)) * h;
+    work[e + 1] = (b.scale ? b.scale[e + 1] : R(1)) * h;
+  }
+}
+
+// D' = D + E[idx] - E_prev: D' gathers its adjoint (the step after's, plus every entry that read it); it is
+// D's, E's at the node, and minus E_prev's
+template <typename R>
+__global__ void k_adj_tm_nodes_d(TensorArgs<R> b, R* Eb, const R* work, const long long* nd_ptr,
+                                 const long long* nd_src) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.nN) return;
+  R dd = b.D[i];
+  for (long long j = nd_ptr[i]; j < nd_ptr[i + 1]; ++j) dd += work[nd_src[j]];
+  b.D[i] = dd;
+  b.Ep[i] = -dd;
+  Eb[b.idx[i]] += dd;
+}
+
 constexpr int kAdjMaxFreq = 128;
 
 // the objective's frequencies, passed by value
@@ -404,6 +534,46 @@ struct AdjFreqs {
   double omega[kAdjMaxFreq];
   int nf;
 };
+
+// each point's adjoint source value at one sample (after n steps), in double: E point p sum_f Re(G_e[f][p]
+// e^{i w_f t_e}) at v[p], H point q half of sum_f Re(G_h[f][q] e^{i w_f t_h}) at v[ne + q]
+__global__ void k_adj_inject_values(const double* ge, long long ne, const double* gh, long long nh,
+                                    const __grid_constant__ AdjFreqs fr, double dt, long long n, double* v) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ne + nh) return;
+  const bool is_h = t >= ne;
+  const long long p = is_h ? t - ne : t;
+  const double tt = (double)n * dt - (is_h ? 0.5 * dt : 0.0);
+  const double* g = is_h ? gh : ge;
+  const long long np = is_h ? nh : ne;
+  double s = 0.0;
+  for (int f = 0; f < fr.nf; ++f) {
+    double sn, cs;
+    sincos(fr.omega[f] * tt, &sn, &cs);
+    const double* gp = g + 2 * ((long long)f * np + p);
+    s += gp[0] * cs - gp[1] * sn;
+  }
+  v[t] = is_h ? 0.5 * s : s;
+}
+
+// the values gathered per distinct target node, in the maps' order, and added once: E targets first, then H
+template <typename R>
+__global__ void k_adj_inject_gather(R* Eb, R* Hb, const double* v, long long ne, const long long* e_tgt,
+                                    const long long* e_ptr, const long long* e_src, long long n_e,
+                                    const long long* h_tgt, const long long* h_ptr, const long long* h_src,
+                                    long long n_h) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n_e) {
+    double s = 0.0;
+    for (long long j = e_ptr[r]; j < e_ptr[r + 1]; ++j) s += v[e_src[j]];
+    Eb[e_tgt[r]] += (R)s;
+  } else if (r < n_e + n_h) {
+    const long long q = r - n_e;
+    double s = 0.0;
+    for (long long j = h_ptr[q]; j < h_ptr[q + 1]; ++j) s += v[ne + h_src[j]];
+    Hb[h_tgt[q]] += (R)s;
+  }
+}
 
 // the objective's adjoint source at one sample (after n steps): Ebar[e_idx[p]] += sum_f Re(G_e[f][p]
 // e^{i w_f t_e}); Hbar[h1[q]], Hbar[h2[q]] += sum_f Re(G_h[f][q] e^{i w_f t_h}) / 2 each (the monitor's H

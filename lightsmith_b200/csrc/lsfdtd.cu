@@ -162,6 +162,8 @@ struct lsfdtd_engine {
   virtual int adjoint_n_groups() const = 0;
   // the conformal off-diagonal terms (rows, entries per row), for the adjoint
   virtual void adjoint_offdiag(long long* rows, int* width) const = 0;
+  // the vertex-tensor mesh (TensorArgs of a real engine; nN = 0 without one), for the adjoint
+  virtual int adjoint_tensor(void* out, size_t bytes) const = 0;
   virtual int adjoint_group(int gi, void* out, size_t bytes) = 0;
 };
 
@@ -735,7 +737,6 @@ struct Engine final : lsfdtd_engine {
 
   int adjoint_args(void* yee, size_t bytes, void** H) override {
     if (kComplex) return fail(LSFDTD_EUNSUPPORTED, "adjoint: real fields only");
-    if (has_tensor) return fail(LSFDTD_EUNSUPPORTED, "adjoint: no vertex-tensor mesh");
     if (bytes != sizeof(YeeArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: argument size");
     const YeeArgs<F> a = current_args();
     std::memcpy(yee, &a, sizeof a);
@@ -746,6 +747,12 @@ struct Engine final : lsfdtd_engine {
   void adjoint_offdiag(long long* rows, int* width) const override {
     *rows = od_n;
     *width = od_width;
+  }
+  int adjoint_tensor(void* out, size_t bytes) const override {
+    if (kComplex || bytes != sizeof(TensorArgs<F>)) return fail(LSFDTD_EINVAL, "adjoint: tensor argument size");
+    TensorArgs<F> a = has_tensor ? tm : TensorArgs<F>{};
+    std::memcpy(out, &a, sizeof a);
+    return LSFDTD_OK;
   }
 
   int bloch_desc(void* out, size_t bytes, int64_t last) override {
@@ -953,36 +960,7 @@ struct Engine final : lsfdtd_engine {
         a.c3[s][k] = R(d->c3[s][k]);
       }
     }
-    // the state buffer, in lsfdtd_tensor_state_len's order
-    F* st = static_cast<F*>(d->state);
-    a.D = st;
-    st += a.nN;
-    a.Ep = st;
-    st += a.nN;
-    a.out = st;
-    st += 2 * a.nN;
-    a.dbar = st;
-    st += 3 * a.nV;
-    a.sv = st;
-    st += a.nV;
-    for (int s = 0; s < a.n_media; ++s) {
-      a.ha_E[s] = st;
-      st += a.nT;
-      a.ha_P[s] = st;
-      st += 2LL * a.n_poles[s] * a.nT;
-    }
-    a.ar_y = st;
-    st += a.nT;
-    for (int s = 0; s < a.n_media; ++s) {
-      a.ar_P[s] = st;
-      st += 2LL * a.n_poles[s] * a.nT;
-    }
-    for (int s = 0; s < a.n_media; ++s) {
-      a.pl_E[s] = st;
-      st += a.nP;
-      a.pl_P[s] = st;
-      st += 2LL * a.n_poles[s] * a.nP;
-    }
+    tm_bind_state(a, static_cast<F*>(d->state));  // the state buffer, in lsfdtd_tensor_state_len's order
     tm = a;
     has_tensor = a.nN > 0;
     return LSFDTD_OK;
@@ -1667,6 +1645,7 @@ struct lsfdtd_adjoint {
   size_t slot_elems = 0;
   AdjFreqs freqs{};                // the objective's frequencies
   std::vector<std::vector<unsigned char>> groups;  // AdeArgs of the engine's dispersive groups
+  std::vector<unsigned char> tm;  // TensorArgs of the vertex-tensor mesh, state in tm_bar (nN = 0: none)
 };
 
 namespace {
@@ -1734,13 +1713,50 @@ int adjoint_step(lsfdtd_adjoint* a, long long n, int slot, cudaStream_t s) {
   }
   const auto& desc = a->eng->desc;
   if ((n + 1) % desc.dft_stride == 0 && a->d.n_e + a->d.n_h > 0) {
-    k_adj_inject<R><<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(
-        A.Eb[0], A.Hb[0], reinterpret_cast<const long long*>(a->d.e_idx), a->d.ge, a->d.n_e,
-        reinterpret_cast<const long long*>(a->d.h_idx1), reinterpret_cast<const long long*>(a->d.h_idx2), a->d.gh,
-        a->d.n_h, a->freqs, desc.dt, n + 1);
+    if (a->d.inj_work) {  // per point, then per target node in the maps' order
+      k_adj_inject_values<<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(a->d.ge, a->d.n_e, a->d.gh, a->d.n_h,
+                                                                         a->freqs, desc.dt, n + 1, a->d.inj_work);
+      LS_LAUNCHED();
+      using LL = const long long*;
+      k_adj_inject_gather<R><<<cdiv(a->d.inj_n_e + a->d.inj_n_h, 256), 256, 0, s>>>(
+          A.Eb[0], A.Hb[0], a->d.inj_work, a->d.n_e, reinterpret_cast<LL>(a->d.inj_e_tgt),
+          reinterpret_cast<LL>(a->d.inj_e_ptr), reinterpret_cast<LL>(a->d.inj_e_src), a->d.inj_n_e,
+          reinterpret_cast<LL>(a->d.inj_h_tgt), reinterpret_cast<LL>(a->d.inj_h_ptr),
+          reinterpret_cast<LL>(a->d.inj_h_src), a->d.inj_n_h);
+      LS_LAUNCHED();
+    } else {
+      k_adj_inject<R><<<cdiv(a->d.n_e + a->d.n_h, 256), 256, 0, s>>>(
+          A.Eb[0], A.Hb[0], reinterpret_cast<const long long*>(a->d.e_idx), a->d.ge, a->d.n_e,
+          reinterpret_cast<const long long*>(a->d.h_idx1), reinterpret_cast<const long long*>(a->d.h_idx2),
+          a->d.gh, a->d.n_h, a->freqs, desc.dt, n + 1);
+      LS_LAUNCHED();
+    }
+  }
+  // the vertex-tensor mesh ran last in the step (after the groups): its transpose comes first
+  const auto& tb = *reinterpret_cast<const TensorArgs<R>*>(a->tm.data());
+  if (tb.nN > 0) {
+    R* work = static_cast<R*>(a->d.tm_work);
+    k_adj_tm_out<R><<<cdiv(tb.nN, 256), 256, 0, s>>>(tb, A.Eb[0]);
+    LS_LAUNCHED();
+    if (tb.nP > 0) {
+      k_adj_tm_plain<R><<<cdiv(tb.nP, 256), 256, 0, s>>>(tb, work);
+      LS_LAUNCHED();
+    }
+    if (tb.nT > 0) {
+      k_adj_tm_slots<R><<<cdiv(tb.nT, 256), 256, 0, s>>>(tb, work);
+      LS_LAUNCHED();
+    }
+    if (tb.nV > 0) {
+      k_adj_tm_vertices<R><<<cdiv(tb.nV, 256), 256, 0, s>>>(tb, work, reinterpret_cast<const long long*>(a->d.tm_vs_ptr),
+                                                            reinterpret_cast<const long long*>(a->d.tm_vs_idx));
+      LS_LAUNCHED();
+    }
+    k_adj_tm_nodes_d<R><<<cdiv(tb.nN, 256), 256, 0, s>>>(tb, A.Eb[0], work,
+                                                         reinterpret_cast<const long long*>(a->d.tm_nd_ptr),
+                                                         reinterpret_cast<const long long*>(a->d.tm_nd_src));
     LS_LAUNCHED();
   }
-  // the dispersive groups ran after the E curl update: their transposes come first
+  // the dispersive groups ran after the E curl update: their transposes come next
   for (size_t gi = 0; gi < a->groups.size(); ++gi) {
     const auto& ga = *reinterpret_cast<const AdeArgs<R>*>(a->groups[gi].data());
     if (ga.n <= 0) continue;
@@ -2260,6 +2276,27 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
     a->freqs.nf = d->n_freq;
   }
   a->d.omega = nullptr;  // copied: the caller's array need not outlive this call
+  if (d->inj_work) {  // the injection maps: every target in the field, every listed point one of the objective's
+    const long long flat = 3LL * eng->desc.shape[0] * eng->desc.shape[1] * eng->desc.shape[2];
+    auto check_map = [&](const int64_t* tgt, const int64_t* ptr, const int64_t* src, long long n_t,
+                         long long n_pts) -> int {
+      if (n_t < 0 || (n_t > 0 && (!tgt || !ptr || !src))) return fail(LSFDTD_EINVAL, "adjoint: injection map missing");
+      if (n_t == 0) return LSFDTD_OK;
+      std::vector<long long> t(n_t), p(n_t + 1);
+      LS_CUDA(cudaMemcpy(t.data(), tgt, n_t * sizeof(long long), cudaMemcpyDeviceToHost));
+      LS_CUDA(cudaMemcpy(p.data(), ptr, (n_t + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+      if (p[0] != 0 || p.back() > 2 * n_pts) return fail(LSFDTD_EINVAL, "adjoint: injection map out of range");
+      std::vector<long long> sr(p.back());
+      if (!sr.empty()) LS_CUDA(cudaMemcpy(sr.data(), src, sr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+      for (long long r = 0; r < n_t; ++r)
+        if (p[r + 1] < p[r] || t[r] < 0 || t[r] >= flat) return fail(LSFDTD_ERANGE, "adjoint: injection map out of range");
+      for (long long v : sr)
+        if (v < 0 || v >= n_pts) return fail(LSFDTD_ERANGE, "adjoint: injection map out of range");
+      return LSFDTD_OK;
+    };
+    LS_TRY(check_map(d->inj_e_tgt, d->inj_e_ptr, d->inj_e_src, d->inj_n_e, d->n_e));
+    LS_TRY(check_map(d->inj_h_tgt, d->inj_h_ptr, d->inj_h_src, d->inj_n_h, d->n_h));
+  }
   if (d->n_groups != eng->adjoint_n_groups() || d->n_groups > LSFDTD_ADJ_MAX_GROUPS)
     return fail(LSFDTD_EINVAL, "adjoint: n_groups must equal the engine's dispersive groups");
   for (int gi = 0; gi < d->n_groups; ++gi) {
@@ -2300,6 +2337,47 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
   } else if (d->od_rows != 0) {
     return fail(LSFDTD_EINVAL, "adjoint: off-diagonal rows given for an engine without such terms");
   }
+  // the vertex-tensor mesh: its arguments with the state pointed into tm_bar, and the caller's maps checked
+  a->tm.resize(a->precision == LSFDTD_F32 ? sizeof(TensorArgs<float>) : sizeof(TensorArgs<double>));
+  LS_TRY(eng->adjoint_tensor(a->tm.data(), a->tm.size()));
+  auto bind = [&](auto* ta) -> int {
+    if (ta->nN <= 0) {
+      if (d->tm_bar) return fail(LSFDTD_EINVAL, "adjoint: tensor adjoint given for an engine without a vertex-tensor mesh");
+      return LSFDTD_OK;
+    }
+    if (!d->tm_bar || !d->tm_work || !d->tm_vs_ptr || !d->tm_nd_ptr || (ta->nT > 0 && !d->tm_vs_idx))
+      return fail(LSFDTD_EINVAL, "adjoint: the engine has a vertex-tensor mesh; give its adjoint state and maps");
+    auto host = [&](const int64_t* src, long long n, std::vector<long long>& out) -> int {
+      out.resize(n);
+      if (n > 0) LS_CUDA(cudaMemcpy(out.data(), src, n * sizeof(long long), cudaMemcpyDeviceToHost));
+      return LSFDTD_OK;
+    };
+    std::vector<long long> vp, vi, np_, ns, tv, tvc;
+    LS_TRY(host(d->tm_vs_ptr, ta->nV + 1, vp));
+    LS_TRY(host(d->tm_nd_ptr, ta->nN + 1, np_));
+    LS_TRY(host(reinterpret_cast<const int64_t*>(ta->t_v), ta->nT, tv));
+    LS_TRY(host(reinterpret_cast<const int64_t*>(ta->t_vc), ta->nT, tvc));
+    if (vp[0] != 0 || vp.back() != ta->nT) return fail(LSFDTD_EINVAL, "adjoint: tensor slot map out of range");
+    LS_TRY(host(d->tm_vs_idx, ta->nT, vi));
+    for (long long v = 0; v < ta->nV; ++v) {
+      if (vp[v + 1] < vp[v]) return fail(LSFDTD_EINVAL, "adjoint: tensor slot map out of range");
+      for (long long j = vp[v]; j < vp[v + 1]; ++j)  // the slots listed for v are v's, on one of its components
+        if (vi[j] < 0 || vi[j] >= ta->nT || tv[vi[j]] != v || tvc[vi[j]] / 3 != v)
+          return fail(LSFDTD_ERANGE, "adjoint: tensor slot map does not match the mesh");
+    }
+    const long long entries = 6 * ta->nV + ta->nT + ta->nP;
+    if (np_[0] != 0 || np_.back() > entries) return fail(LSFDTD_EINVAL, "adjoint: tensor node map out of range");
+    LS_TRY(host(d->tm_nd_src, np_.back(), ns));
+    for (long long i = 0; i < ta->nN; ++i)
+      if (np_[i + 1] < np_[i]) return fail(LSFDTD_EINVAL, "adjoint: tensor node map out of range");
+    for (long long v : ns)
+      if (v < 0 || v >= entries) return fail(LSFDTD_ERANGE, "adjoint: tensor node map out of range");
+    using Fld = std::remove_pointer_t<decltype(ta->D)>;
+    tm_bind_state(*ta, static_cast<Fld*>(d->tm_bar));
+    return LSFDTD_OK;
+  };
+  LS_TRY(a->precision == LSFDTD_F32 ? bind(reinterpret_cast<TensorArgs<float>*>(a->tm.data()))
+                                    : bind(reinterpret_cast<TensorArgs<double>*>(a->tm.data())));
   // every E node of the box outside every E slab (there the E update's coefficient enters only through the
   // curl term; the H values of the box and its halo are recorded, wherever they lie)
   auto slabs_ok = [&](const auto& y) {

@@ -48,6 +48,41 @@ struct TensorArgs {
   F* pl_P[kMaxMedia];  // [pole][2][nP]
 };
 
+// points the state arrays of `a` into one buffer of lsfdtd_tensor_state_len field scalars (sizes and media
+// set): D, E_prev, out (2 nN), D~ (3 nV), s (nV); per medium the harmonic E_s and its poles; the arithmetic y;
+// per medium its poles; per medium the plain slots' E_s and poles
+template <typename F>
+inline void tm_bind_state(TensorArgs<F>& a, F* st) {
+  a.D = st;
+  st += a.nN;
+  a.Ep = st;
+  st += a.nN;
+  a.out = st;
+  st += 2 * a.nN;
+  a.dbar = st;
+  st += 3 * a.nV;
+  a.sv = st;
+  st += a.nV;
+  for (int s = 0; s < a.n_media; ++s) {
+    a.ha_E[s] = st;
+    st += a.nT;
+    a.ha_P[s] = st;
+    st += 2LL * a.n_poles[s] * a.nT;
+  }
+  a.ar_y = st;
+  st += a.nT;
+  for (int s = 0; s < a.n_media; ++s) {
+    a.ar_P[s] = st;
+    st += 2LL * a.n_poles[s] * a.nT;
+  }
+  for (int s = 0; s < a.n_media; ++s) {
+    a.pl_E[s] = st;
+    st += a.nP;
+    a.pl_P[s] = st;
+    st += 2LL * a.n_poles[s] * a.nP;
+  }
+}
+
 // P_k <- c1 P_k + c2 P'_k + c3 drive, P'_k <- old P_k, for every pole of medium s at slot t of n; the sum of
 // the new P_k (_Group._advance, engine.py:759-767)
 template <typename F>

@@ -555,16 +555,22 @@ class Engine:
         return self._H[int(_abi.lib().lsfdtd_engine_buffer(self._h))]
 
     def state(self) -> list:
-        """The fields, CPML psi and dispersive-group state of the current step, in a fixed order (E, H, psi in
-        ``self.psi``'s order, the groups' state): on the fused path, the buffers of the current parity."""
+        """The fields, CPML psi and dispersive state of the current step, in a fixed order (E, H, psi in
+        ``self.psi``'s order, the groups' state, the vertex-tensor mesh's state): on the fused path, the buffers
+        of the current parity."""
         b = int(_abi.lib().lsfdtd_engine_buffer(self._h))
         return [self._E[b], self._H[b]] + [self.psi_alt[k] if b and k in self.psi_alt else t
-                                           for k, t in self.psi.items()] + [g["state"] for g in self.groups]
+                                           for k, t in self.psi.items()] + [g["state"] for g in self.groups] + \
+            self._tensor_state()
+
+    def _tensor_state(self) -> list:
+        t = getattr(self, "tensor", None)
+        return [] if t is None else [t["state"]]
 
     def all_state(self) -> list:
         """Every state buffer of both parities (for clearing the state)."""
         return (self._E + self._H + list(self.psi.values()) + list(self.psi_alt.values()) +
-                [g["state"] for g in self.groups])
+                [g["state"] for g in self.groups] + self._tensor_state())
 
     @property
     def E_flat(self):

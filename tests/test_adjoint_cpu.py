@@ -2,6 +2,7 @@
 the same objective from the same run, and gradients that agree with central finite differences of itself."""
 
 import numpy as np
+import pytest
 import torch
 
 from adjoint_cases import BOX, small_case
@@ -109,3 +110,50 @@ def test_transposed_offdiag_rows_are_the_gather_transposed():
     for r, q in enumerate(rows):
         WtE[q] = sum(ww[j] * Eb[ee[j]] for j in range(ptr[r], ptr[r + 1]))
     assert abs(Eb @ WH - WtE @ H) <= 1e-12 * np.abs(Eb).sum() * np.abs(WH).max()
+
+
+def test_tensor_adjoint_maps_list_every_entry_once_under_its_node():
+    """``tensor_adjoint_maps`` on a random table shaped as a vertex-tensor mesh's: every (vertex, axis, side)
+    entry, tensor slot and plain slot appears once, under the node whose D it reads, in ascending order; every
+    tensor slot once under its vertex; the scratch length is 6 n_vert + 2 n_tslots + n_pslots."""
+    from lightsmith_b200.adjoint import tensor_adjoint_maps
+
+    rng = np.random.default_rng(3)
+    n_nodes, n_vert, n_t, n_p = 40, 9, 25, 12
+    vn = rng.integers(0, n_nodes, 6 * n_vert)
+    t_v = rng.integers(0, n_vert, n_t)
+    t_vc = 3 * t_v + rng.integers(0, 3, n_t)
+    t_g = rng.integers(0, 6 * n_vert, n_t)
+    p_node = rng.integers(0, n_nodes, n_p)
+    tm = {"n_nodes": n_nodes, "normal": np.zeros(3 * n_vert), "vn": vn, "t_v": t_v, "t_vc": t_vc, "t_g": t_g,
+          "p_node": p_node}
+    vs_ptr, vs_idx, nd_ptr, nd_src, n_work = tensor_adjoint_maps(tm)
+    assert n_work == 6 * n_vert + 2 * n_t + n_p
+    node_of = np.concatenate([vn, vn[t_g], p_node])
+    assert sorted(nd_src.tolist()) == list(range(len(node_of)))
+    for i in range(n_nodes):
+        src = nd_src[nd_ptr[i]:nd_ptr[i + 1]]
+        assert np.all(node_of[src] == i) and np.all(np.diff(src) > 0)
+    assert sorted(vs_idx.tolist()) == list(range(n_t))
+    for v in range(n_vert):
+        sl = vs_idx[vs_ptr[v]:vs_ptr[v + 1]]
+        assert np.all(t_v[sl] == v) and np.all(np.diff(sl) > 0)
+    tm["t_vc"] = t_vc + 3  # a slot on another vertex's component: refused
+    with pytest.raises(ValueError):
+        tensor_adjoint_maps(tm)
+
+
+def test_injection_map_groups_points_by_target_in_order():
+    """``injection_map``: each distinct target once, ascending, with the points that sample it in ascending
+    order; every point listed as often as it appears."""
+    from lightsmith_b200.adjoint import injection_map
+
+    targets = np.array([7, 3, 7, 9, 3, 7, 1])
+    points = np.array([0, 1, 2, 3, 4, 5, 6])
+    tgt, ptr, src = injection_map(targets, points)
+    assert tgt.tolist() == [1, 3, 7, 9] and ptr.tolist() == [0, 1, 3, 6, 7]
+    assert src.tolist() == [6, 1, 4, 0, 2, 5, 3]
+    nh = 4  # H points: both samples of a point may share a target
+    h1, h2 = np.array([5, 6, 5, 8]), np.array([6, 6, 9, 5])
+    tgt, ptr, src = injection_map(np.concatenate([h1, h2]), np.concatenate([np.arange(nh), np.arange(nh)]))
+    assert tgt.tolist() == [5, 6, 8, 9] and src[ptr[1]:ptr[2]].tolist() == [0, 1, 1]

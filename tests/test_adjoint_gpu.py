@@ -344,6 +344,89 @@ def _fd_check(run, base, g, n_steps, flats, h=1e-6, tol=1e-5):
     run.set_inv_eps_box(base)
 
 
+def _default_pose(material, r=14.0):
+    """A sphere of ``material`` (radius r nm, in water) posed to lightsmith with its default options (mirror
+    planes, conformal meshing), 4 nm cells, float64: (plan, post, box, r), the box the nodes within r + 6 nm of
+    the centre that every E component steps."""
+    import lightsmith as ls
+
+    from lightsmith_b200.scattering import scattering_setup
+
+    sim = ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=r), material=material,
+                                               position_nm=(0.0, 0.0, 0.0))],
+                        medium_index=1.33, wavelengths={"start_nm": 450.0, "stop_nm": 650.0, "num": 4},
+                        options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, padding_nm=16.0, pml_gap_nm=8.0,
+                                              run_time_fs=6.0, precision="double")})
+    plan, post, lay = scattering_setup(sim)
+    assert tuple(plan["mirror"]) == (-1, 1, 0)
+    shape = tuple(int(v) for v in plan["shape"])
+    pos = [np.asarray(lay.origin, float)[a] + 4.0 * np.arange(shape[a]) for a in range(3)]
+    lo_node = [2, 1, 0]  # the first node every E component steps: 2 next to the antisymmetric plane
+    box = tuple((max(lo_node[a], int(np.searchsorted(pos[a], -r - 6.0))),
+                 int(np.searchsorted(pos[a], r + 6.0, side="right"))) for a in range(3))
+    return plan, post, box, r
+
+
+def _lightsmith():
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from refsrc import add_to_path
+
+    if not add_to_path():
+        pytest.skip("lightsmith (the reference install, baseline/_ref) not available")
+    import lightsmith as ls
+
+    return ls
+
+
+def test_default_pose_of_a_metal_sphere_gradient_matches_finite_differences():
+    """A Drude-Lorentz sphere posed to lightsmith with its defaults: mirror planes and conformal meshing, which
+    next to a dispersive medium is the vertex-tensor mesh (its nodes' E from tensor slots with their own pole
+    states and plain slots), beside the metal's D-form groups; float64, J = sum_f C_sca(f). The gradient over a
+    box around the sphere, which holds tensor nodes, against central differences of the CUDA forward at its
+    largest entries overall and on tensor nodes, and bitwise the same for two checkpoint intervals."""
+    ls = _lightsmith()
+    from problems import DRUDE_LORENTZ
+
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.scattering import cross_section_objective
+
+    plan, post, box, r = _default_pose(ls.DrudeLorentz(**DRUDE_LORENTZ))
+    tm = plan["tensor"]
+    assert tm is not None and int(tm["n_nodes"]) > 0 and len(tm["t_pos"]) > 0 and len(tm["p_pos"]) > 0
+    shape = tuple(int(v) for v in plan["shape"])
+    node = np.asarray(tm["idx"]) % int(np.prod(shape))
+    ijk = np.stack(np.unravel_index(node, shape), axis=1)
+    inside = np.all((ijk >= [a for a, _ in box]) & (ijk < [b for _, b in box]), axis=1)
+    assert inside.any()
+    on_tensor = np.zeros(tuple(b - a for a, b in box), bool)
+    on_tensor[tuple((ijk[inside] - [a for a, _ in box]).T)] = True
+    stride = int(plan["stride"])
+    n_steps = 10 * stride
+    inv = np.asarray(plan["inv_eps"]).reshape((-1,) + shape)
+    base = torch.as_tensor(inv[(slice(None),) + tuple(slice(a, b) for a, b in box)]).clone()
+    if base.shape[0] == 1:
+        base = base[0]
+    grads = []
+    for K in (stride, 5 * stride):
+        ref: dict = {}
+        run = AdjointRun(plan, box, objective=cross_section_objective(post, ref), checkpoint=K, precision="double")
+        ref["acc_ref"] = run.eng.monitors[2]["acc_e"]
+        run.set_inv_eps_box(base)
+        J0, _ = run.forward(n_steps)
+        g = run.backward().cpu().numpy()
+        grads.append(g)
+        if K == stride:
+            assert J0 > 0 and np.all(np.isfinite(g)) and np.abs(g).max() > 0
+            flats = list(np.argsort(-np.abs(g).reshape(-1))[:2])
+            flats += list(np.argsort(-np.where(on_tensor, np.abs(g), -1).reshape(-1))[:3])
+            _fd_check(run, base, g, n_steps, flats)
+        run.close()
+    assert np.array_equal(grads[0], grads[1])
+
+
 def test_default_scattering_pose_gradient_matches_finite_differences(monkeypatch):
     """A dielectric sphere posed to lightsmith with its defaults: mirror planes through the centre (symmetry
     "auto": an antisymmetric plane normal to x and a symmetric one normal to y for the x-polarised plane wave)
@@ -362,21 +445,11 @@ def test_default_scattering_pose_gradient_matches_finite_differences(monkeypatch
     import lightsmith as ls
 
     from lightsmith_b200 import adjoint as A
-    from lightsmith_b200.scattering import cross_section_objective, scattering_setup
+    from lightsmith_b200.scattering import cross_section_objective
 
-    r = 14.0
-    sim = ls.Simulation(particles=[ls.Particle(shape=ls.Sphere(radius_nm=r), material=ls.ConstantIndex(n_real=2.0),
-                                               position_nm=(0.0, 0.0, 0.0))],
-                        medium_index=1.33, wavelengths={"start_nm": 450.0, "stop_nm": 650.0, "num": 4},
-                        options={"fdtd": dict(spacing_nm=4.0, pml_cells=8, padding_nm=16.0, pml_gap_nm=8.0,
-                                              run_time_fs=6.0, precision="double")})
-    plan, post, lay = scattering_setup(sim)
-    assert tuple(plan["mirror"]) == (-1, 1, 0) and len(plan["offdiag"]["e"]) > 0
+    plan, post, box, r = _default_pose(ls.ConstantIndex(n_real=2.0))
+    assert len(plan["offdiag"]["e"]) > 0
     shape = tuple(int(v) for v in plan["shape"])
-    pos = [np.asarray(lay.origin, float)[a] + 4.0 * np.arange(shape[a]) for a in range(3)]
-    lo_node = [2, 1, 0]  # the first node every E component steps: 2 next to the antisymmetric plane
-    box = tuple((max(lo_node[a], int(np.searchsorted(pos[a], -r - 6.0))),
-                 int(np.searchsorted(pos[a], r + 6.0, side="right"))) for a in range(3))
     rest = np.asarray(plan["offdiag"]["e"]) % int(np.prod(shape))
     ijk = np.stack(np.unravel_index(rest, shape), axis=1)
     assert np.any(np.all((ijk >= [a for a, _ in box]) & (ijk < [b for _, b in box]), axis=1))
