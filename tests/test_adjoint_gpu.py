@@ -427,6 +427,39 @@ def test_default_pose_of_a_metal_sphere_gradient_matches_finite_differences():
     assert np.array_equal(grads[0], grads[1])
 
 
+def test_default_pose_of_a_metal_sphere_float32_gradient_against_float64():
+    """The metal sphere's default pose (mirror planes, vertex-tensor mesh, D-form groups) on the float32
+    kernels: C_sca within 1e-4 and the gradient within 1e-3 of the largest float64 entry (the agreement the
+    adjoint is held to), both runs from the same plan."""
+    ls = _lightsmith()
+    from problems import DRUDE_LORENTZ
+
+    from lightsmith_b200.adjoint import AdjointRun
+    from lightsmith_b200.scattering import cross_section_objective
+
+    plan, post, box, r = _default_pose(ls.DrudeLorentz(**DRUDE_LORENTZ))
+    shape = tuple(int(v) for v in plan["shape"])
+    stride = int(plan["stride"])
+    n_steps = 10 * stride
+    inv = np.asarray(plan["inv_eps"]).reshape((-1,) + shape)
+    base = torch.as_tensor(inv[(slice(None),) + tuple(slice(a, b) for a, b in box)]).clone()
+    if base.shape[0] == 1:
+        base = base[0]
+    out = {}
+    for prec in ("double", "single"):
+        ref: dict = {}
+        run = AdjointRun(plan, box, objective=cross_section_objective(post, ref), checkpoint=2 * stride,
+                         precision=prec)
+        ref["acc_ref"] = run.eng.monitors[2]["acc_e"]
+        run.set_inv_eps_box(base)
+        J, _ = run.forward(n_steps)
+        out[prec] = (J, run.backward().cpu().numpy())
+        run.close()
+    (J64, g64), (J32, g32) = out["double"], out["single"]
+    assert abs(J32 - J64) <= 1e-4 * abs(J64)
+    assert np.abs(g32 - g64).max() <= 1e-3 * np.abs(g64).max()
+
+
 def test_default_scattering_pose_gradient_matches_finite_differences(monkeypatch):
     """A dielectric sphere posed to lightsmith with its defaults: mirror planes through the centre (symmetry
     "auto": an antisymmetric plane normal to x and a symmetric one normal to y for the x-polarised plane wave)
