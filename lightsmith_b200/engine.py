@@ -180,7 +180,15 @@ class Engine:
 
     def _build_pml(self, plan, L):
         spec = _Spec(plan["pml"])
-        prof = cpml_profiles(spec, self.shape, self.spacing, self.dt)
+        pad = int(plan.get("pad_z") or 0)  # rows padded along z (plan.pad_rows): the profiles of the original grid
+        orig = (self.shape[0], self.shape[1], self.shape[2] - pad)
+        prof = cpml_profiles(spec, orig, self.spacing, self.dt)
+        if pad and 2 in prof:  # the high z slab widened over the frozen planes, where psi stays zero
+            lo_n, hi_n, pr = prof[2]
+            one, zero = np.ones(pad), np.zeros(pad)
+            prof[2] = (lo_n, hi_n + pad if hi_n else 0,
+                       {k: (np.concatenate([b, zero]), np.concatenate([c, zero]), np.concatenate([kap, one]))
+                        for k, (b, c, kap) in pr.items()})
         shp = (C.c_int32 * 3)(*self.shape)
         per = (C.c_int32 * 3)(*[int(p) for p in self.periodic])
         self.psi = {}

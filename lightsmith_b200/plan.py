@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import io
 import json
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 
 import numpy as np
 
@@ -719,6 +719,79 @@ def make_plan(*, shape, dx, dt, single, inv_eps, groups, pml, sources, monitors,
                      "energy": int(m.energy), "space": space})
     plan["monitors"] = mons
     return plan
+
+
+# --- rows padded for the tensor-memory copies -----------------------------------------------------------
+# The fused pass moves planes with tensor-memory (TMA) copies, whose row stride must be a multiple of 16 bytes;
+# lightsmith's scattering layouts are odd along every axis (setup.py:640). pad_rows appends planes along z so
+# that a row of nodes is a multiple of `multiple` values, and freezes them: every E component from z = n2 - 1
+# on (where lightsmith steps none: e_range) gets a zero curl coefficient, so it keeps its zero start value, and
+# H there, whose every difference then reads zeros, stays zero too. The high z CPML slab keeps its start (the
+# engine widens it over the new planes, where its profile is b = 0, c = 0, kappa = 1, so psi stays zero), and
+# every flat index of the plan is moved to the wider rows. The run's values on the original nodes are then
+# the original run's.
+
+
+def _remap_flat(idx, shape, n2p):
+    """Flat indices (component-stacked, c * N + (x * n1 + y) * n2 + z) of a grid of `shape` on rows of n2p."""
+    a = np.asarray(idx, np.int64)
+    n0, n1, n2 = shape
+    N = n0 * n1 * n2
+    c, rest = np.divmod(a, N)
+    xy, z = np.divmod(rest, n2)
+    return c * (n0 * n1 * n2p) + xy * n2p + z
+
+
+def pad_rows(plan: dict, multiple: int = 4) -> dict:
+    """The plan on rows padded to a multiple of `multiple` nodes along z (the plan itself when its rows are
+    already, or when it has complex fields, periodic axes or a z mirror plane, or already padded)."""
+    n0, n1, n2 = (int(v) for v in plan["shape"])
+    n2p = -(-n2 // multiple) * multiple
+    if (n2p == n2 or plan["complex"] or any(plan["periodic"]) or plan.get("mirror", (0, 0, 0))[2]
+            or plan.get("pad_z")):
+        return plan
+    shape = (n0, n1, n2)
+
+    def rm(a):
+        return None if a is None else _remap_flat(a, shape, n2p)
+
+    out = dict(plan)
+    out["shape"] = (n0, n1, n2p)
+    out["pad_z"] = n2p - n2
+    inv = np.asarray(plan["inv_eps"])
+    pad = [(0, 0)] * (inv.ndim - 1) + [(0, n2p - n2)]
+    inv = np.pad(inv, pad).astype(inv.dtype, copy=False)
+    inv[..., n2 - 1:] = 0
+    out["inv_eps"] = inv
+    out["groups"] = [{**g, "idx": rm(g["idx"])} for g in plan["groups"]]
+    srcs = []
+    for src in plan["sources"]:
+        if isinstance(src, DipoleSource):
+            src = replace(src, idx=rm(src.idx))
+        elif isinstance(src, TableSource):
+            src = replace(src, E=None if src.E is None else replace(src.E, node=rm(src.E.node)),
+                          H=None if src.H is None else replace(src.H, node=rm(src.H.node)))
+        elif isinstance(src, LineSource):
+            src = replace(src, E=None if src.E is None else replace(src.E, node=rm(src.E.node)),
+                          H=None if src.H is None else replace(src.H, node=rm(src.H.node)))
+        elif isinstance(src, ModeSource):
+            src = replace(src, h_idx=rm(src.h_idx), e_idx=rm(src.e_idx))
+        else:
+            raise NotImplementedError(f"pad_rows: no row padding for the source {type(src).__name__}")
+        srcs.append(src)
+    out["sources"] = srcs
+    if plan.get("tensor") is not None:
+        out["tensor"] = {**plan["tensor"], "idx": rm(plan["tensor"]["idx"])}
+    if plan.get("offdiag") is not None:
+        od = plan["offdiag"]
+        out["offdiag"] = {**od, "e": rm(od["e"]), "h": rm(od["h"])}
+    mons = []
+    for m in plan["monitors"]:
+        if m["space"][0] == "grid":
+            m = {**m, "e_idx": rm(m["e_idx"]), "h_idx1": rm(m["h_idx1"]), "h_idx2": rm(m["h_idx2"])}
+        mons.append(m)
+    out["monitors"] = mons
+    return out
 
 
 def _monitor_space(obj, sources, plans):

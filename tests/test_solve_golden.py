@@ -146,3 +146,33 @@ def test_full_size_sphere_on_the_fused_pass_gives_the_in_place_kernels_values(go
         assert np.abs(ea - eb).max() <= 1e-12 * np.abs(eb).max()
         if hb is not None:
             assert np.abs(ha - hb).max() <= 1e-12 * np.abs(hb).max()
+
+
+@pytest.mark.gpu
+def test_full_size_sphere_on_padded_rows_takes_the_tensor_copies_and_gives_the_same_values(golden):
+    """The 129^3 sphere on rows padded to 132 nodes (``plan.pad_rows``: frozen planes beyond the last node
+    lightsmith steps, the high z CPML slab kept in place): the engine takes the fused pass with tensor-memory
+    copies (the odd rows cannot), and after 3 chunks in FP64 its fields on the original nodes and every
+    monitor's accumulators are the in-place run's on the original rows; the added planes hold zeros."""
+    from lightsmith_b200.engine import Engine
+    from lightsmith_b200.plan import pad_rows
+
+    plan = golden("solve_c0")["plan"]
+    padded = pad_rows(plan)
+    n2 = plan["shape"][2]
+    assert padded["shape"][2] == 132 and padded["pad_z"] == 3
+    out = {}
+    for name, p in (("orig", plan), ("padded", padded)):
+        eng = Engine.from_plan(p, precision="double")
+        eng.chunk(3, use_graph=True)
+        out[name] = (eng.fused, eng.uses_tma, eng.E.cpu().numpy(), eng.H.cpu().numpy(),
+                     [eng.results(k) for k in range(len(p["monitors"]))])
+        eng.close()
+    assert out["padded"][:2] == (True, True) and out["orig"][0] is False
+    for a, b in ((out["padded"][2], out["orig"][2]), (out["padded"][3], out["orig"][3])):
+        assert np.abs(a[..., :n2] - b).max() <= 1e-12 * np.abs(b).max()
+        assert not np.any(a[..., n2:])
+    for (ea, ha), (eb, hb) in zip(out["padded"][4], out["orig"][4]):
+        assert np.abs(ea - eb).max() <= 1e-12 * np.abs(eb).max()
+        if hb is not None:
+            assert np.abs(ha - hb).max() <= 1e-12 * np.abs(hb).max()
