@@ -123,7 +123,7 @@ struct lsfdtd_engine {
   // the lean pass steps the clean interior of the grid with a kernel that has no region or CPML code, beside
   // the lean kernel on the CTAs around it (where the grid has such an interior and no source corrects H)
   int split_clean = 1;
-  virtual int init_side() = 0;  // the second stream of that split and its fork and join events
+  virtual int init_side() = 0;  // the side streams of that split and their fork and join events
   // when set, event pairs around every bulk (Yee) kernel launch are appended here (diagnostic timing)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timing = nullptr;
   virtual ~lsfdtd_engine() {
@@ -271,22 +271,27 @@ struct Engine final : lsfdtd_engine {
   int maps_tile_y = 0;  // tile rows the tensor-map boxes were made for
   CUtensorMap mapE[2][3], mapH[2][3], mapC;  // per buffer and component; the coefficient of component 0
   static constexpr int kStages = 4;  // x planes in the fused pass's copy ring
-  // the lean pass's boundary CTAs run on this second stream, beside the clean interior's (fork and join
-  // events on the caller's stream; made when the engine settles on the lean pass)
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // the lean pass's boundary classes run on streams of their own, one per class, beside the clean
+  // interior's and each other (fork and join events on the caller's stream; made with the engine)
+  static constexpr int kSides = 4;
+  cudaStream_t side[kSides] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kSides] = {};
   int init_side() override {
     if constexpr (!kComplex) {
-      LS_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      for (int i = 0; i < kSides; ++i) {
+        LS_CUDA(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+        LS_CUDA(cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming));
+      }
       LS_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-      LS_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     }
     return LSFDTD_OK;
   }
   ~Engine() override {
-    if (side) cudaStreamDestroy(side);
+    for (int i = 0; i < kSides; ++i) {
+      if (side[i]) cudaStreamDestroy(side[i]);
+      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    }
     if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   F* Eflat() const { return Ebuf[cur]; }
@@ -434,7 +439,8 @@ struct Engine final : lsfdtd_engine {
   }
   // whether the lean pass runs as two kernels (clean interior and the rest)
   bool lean_split() const {
-    if (kComplex || !tma_ok || !split_clean || !side || !lean_ok() || tile_y != 8 || stages != 4) return false;
+    if (kComplex || !tma_ok || !split_clean || !side[kSides - 1] || !lean_ok() || tile_y != 8 || stages != 4)
+      return false;
     for (auto& tb : tables)
       if (tb.has[1] && tb.hc.n > 0) return false;
     int zc0, zc1, yc0, yc1, xc0, xc1;
@@ -665,8 +671,8 @@ struct Engine final : lsfdtd_engine {
       }
       if (kind == 2) {
         // the lean pass: where the grid has a clean interior, one kernel per class of CTA box (launch_class),
-        // the interior's on the caller's stream and the others one after another on the second stream; else
-        // every CTA by the lean kernel
+        // the interior's on the caller's stream and each other class on a side stream of its own, all at once;
+        // else every CTA by the lean kernel
         CtaMap maps[kClasses];
         long long n[kClasses];
         const bool two = lean_plan(rows, fa.seg, lean_split(), maps, n);
@@ -678,18 +684,19 @@ struct Engine final : lsfdtd_engine {
           if (r != LSFDTD_OK) return r;
         } else {
           LS_CUDA(cudaEventRecord(ev_fork, s));
-          LS_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
-          for (int c = kClasses - 1; c >= 1; --c) {
+          for (int c = kClasses - 1; c >= 1; --c) {  // class c on side stream c - 1
             if (n[c] == 0) continue;
+            LS_CUDA(cudaStreamWaitEvent(side[c - 1], ev_fork, 0));
             ta.map = maps[c];
-            LS_TRY(launch_class(c, dim3((unsigned)n[c]), ta, side));
+            LS_TRY(launch_class(c, dim3((unsigned)n[c]), ta, side[c - 1]));
             LS_LAUNCHED();
+            LS_CUDA(cudaEventRecord(ev_join[c - 1], side[c - 1]));
           }
           ta.map = maps[0];
           LS_TRY(launch_class(0, dim3((unsigned)n[0]), ta, s));
           LS_LAUNCHED();
-          LS_CUDA(cudaEventRecord(ev_join, side));
-          LS_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
+          for (int c = 1; c < kClasses; ++c)
+            if (n[c] > 0) LS_CUDA(cudaStreamWaitEvent(s, ev_join[c - 1], 0));
         }
       } else if (tma_ok) {
         LS_TRY(launch_ring(ta, grid, s));
