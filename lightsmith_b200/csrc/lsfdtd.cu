@@ -2287,16 +2287,17 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
     const long long flat = 3LL * eng->desc.shape[0] * eng->desc.shape[1] * eng->desc.shape[2];
     auto check_map = [&](const int64_t* tgt, const int64_t* ptr, const int64_t* src, long long n_t,
                          long long n_pts) -> int {
-      if (n_t < 0 || (n_t > 0 && (!tgt || !ptr || !src))) return fail(LSFDTD_EINVAL, "adjoint: injection map missing");
+      if (n_t < 0 || n_t > flat || (n_t > 0 && (!tgt || !ptr || !src)))
+        return fail(LSFDTD_EINVAL, "adjoint: injection map missing or larger than the field");
       if (n_t == 0) return LSFDTD_OK;
       std::vector<long long> t(n_t), p(n_t + 1);
       LS_CUDA(cudaMemcpy(t.data(), tgt, n_t * sizeof(long long), cudaMemcpyDeviceToHost));
       LS_CUDA(cudaMemcpy(p.data(), ptr, (n_t + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
       if (p[0] != 0 || p.back() > 2 * n_pts) return fail(LSFDTD_EINVAL, "adjoint: injection map out of range");
+      for (long long r = 0; r < n_t; ++r)  // non-decreasing from 0: every pointer in [0, 2 n_pts]
+        if (p[r + 1] < p[r] || t[r] < 0 || t[r] >= flat) return fail(LSFDTD_ERANGE, "adjoint: injection map out of range");
       std::vector<long long> sr(p.back());
       if (!sr.empty()) LS_CUDA(cudaMemcpy(sr.data(), src, sr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
-      for (long long r = 0; r < n_t; ++r)
-        if (p[r + 1] < p[r] || t[r] < 0 || t[r] >= flat) return fail(LSFDTD_ERANGE, "adjoint: injection map out of range");
       for (long long v : sr)
         if (v < 0 || v >= n_pts) return fail(LSFDTD_ERANGE, "adjoint: injection map out of range");
       return LSFDTD_OK;
@@ -2328,6 +2329,7 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
       return fail(LSFDTD_EINVAL, "adjoint: the engine has conformal off-diagonal terms; give them transposed");
     // index ranges checked here, once (the kernel trusts them)
     const long long flat = 3LL * n[0] * n[1] * n[2];
+    if (d->od_rows > flat) return fail(LSFDTD_EINVAL, "adjoint: more off-diagonal rows than H values");
     std::vector<long long> ptr(d->od_rows + 1), hh(d->od_rows);
     LS_CUDA(cudaMemcpy(ptr.data(), d->od_ptr, ptr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
     LS_CUDA(cudaMemcpy(hh.data(), d->od_h, hh.size() * sizeof(long long), cudaMemcpyDeviceToHost));
@@ -2374,9 +2376,9 @@ int32_t lsfdtd_adjoint_create(lsfdtd_engine* eng, const lsfdtd_adjoint_desc* d, 
     }
     const long long entries = 6 * ta->nV + ta->nT + ta->nP;
     if (np_[0] != 0 || np_.back() > entries) return fail(LSFDTD_EINVAL, "adjoint: tensor node map out of range");
-    LS_TRY(host(d->tm_nd_src, np_.back(), ns));
-    for (long long i = 0; i < ta->nN; ++i)
+    for (long long i = 0; i < ta->nN; ++i)  // non-decreasing from 0: every pointer in [0, entries]
       if (np_[i + 1] < np_[i]) return fail(LSFDTD_EINVAL, "adjoint: tensor node map out of range");
+    LS_TRY(host(d->tm_nd_src, np_.back(), ns));
     for (long long v : ns)
       if (v < 0 || v >= entries) return fail(LSFDTD_ERANGE, "adjoint: tensor node map out of range");
     using Fld = std::remove_pointer_t<decltype(ta->D)>;
