@@ -219,6 +219,11 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     const unsigned us1 = n2, us0 = (unsigned)n1 * n2;  // 32-bit node offsets within a component
     const unsigned n_main = nx * ny * un2;  // fewer than 2^32 nodes (checked on the host)
     const unsigned n_work = n_main + un2;   // the cell's interior nodes, then the column's (1, 1, z)
+    // a thread's nodes advance by tstride: (z, y, x) carried forward with two carries, not divided anew
+    const unsigned dq = udiv(tstride, r.div_n2), dz = tstride - dq * un2;
+    const unsigned dxm = udiv(dq, r.div_ny), dym = dq - dxm * ny;
+    const unsigned q0 = udiv(t0, r.div_n2), z00 = t0 - q0 * un2;
+    const unsigned xm00 = udiv(q0, r.div_ny), ym00 = q0 - xm00 * ny;
     const long long cs1 = n2, cs0 = 3LL * n2;
     const long long ccol = 4LL * n2;  // flat index of the column node (1, 1, 0)
     long long n = *r.nstep;
@@ -264,14 +269,14 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
     for (; n < n_end; ++n) {
       const bool through = n + 1 < n_end;  // E ghosts written through, except after the launch's last step
       // ---- H phase ----
-      for (unsigned w = t0; w < n_work; w += tstride) {
+      unsigned zc = z00, ymc = ym00, xmc = xm00;
+      for (unsigned w = t0; w < n_work; w += tstride, zc += dz, ymc += dym + (zc >= un2 ? 1u : 0u),
+                    zc -= zc >= un2 ? un2 : 0u, xmc += dxm + (ymc >= ny ? 1u : 0u), ymc -= ymc >= ny ? ny : 0u) {
         if (w < n_main) {
           // periodic x and y: every component is stepped at every interior (x, y); along z, H_x and H_y
           // stop one node short of the last plane (in_h_region), and only z carries CPML
-          const unsigned t = udiv(w, r.div_n2);
-          const int z = (int)(w - t * un2);
-          const unsigned xm = udiv(t, r.div_ny);
-          const int x = 1 + (int)xm, y = 1 + (int)(t - xm * ny);
+          const int z = (int)zc;
+          const int x = 1 + (int)xmc, y = 1 + (int)ymc;
           const unsigned p = (unsigned)x * us0 + (unsigned)y * us1 + (unsigned)z;
           const bool zin = z <= n2 - 2;
           const F e0 = g.E[0][p], e1 = g.E[1][p], e2 = g.E[2][p];
@@ -348,13 +353,13 @@ __global__ void __launch_bounds__(kBatchThreads, sizeof(F) == 8 ? 2 : 1)
       if (!sync()) return;
       // ---- E phase ----
       const R w_src = r.wave[n];
-      for (unsigned w = t0; w < n_work; w += tstride) {
+      zc = z00, ymc = ym00, xmc = xm00;
+      for (unsigned w = t0; w < n_work; w += tstride, zc += dz, ymc += dym + (zc >= un2 ? 1u : 0u),
+                    zc -= zc >= un2 ? un2 : 0u, xmc += dxm + (ymc >= ny ? 1u : 0u), ymc -= ymc >= ny ? ny : 0u) {
         if (w < n_main) {
           // along z, E_x and E_y are stepped on [1, n2 - 2], E_z on [0, n2 - 2] (in_e_region)
-          const unsigned t = udiv(w, r.div_n2);
-          const int z = (int)(w - t * un2);
-          const unsigned xm = udiv(t, r.div_ny);
-          const int x = 1 + (int)xm, y = 1 + (int)(t - xm * ny);
+          const int z = (int)zc;
+          const int x = 1 + (int)xmc, y = 1 + (int)ymc;
           const unsigned p = (unsigned)x * us0 + (unsigned)y * us1 + (unsigned)z;
           if (z > n2 - 2) continue;
           const bool zlo = z >= 1;
